@@ -1,0 +1,188 @@
+// icb_internal.hpp -- shared declarations of the B200 SIMP library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/icarat_b200.h"
+
+namespace icb
+{
+
+// ---------------------------------------------------------------- errors --
+void set_error(const std::string &msg);
+/// add to the process-wide count of kernel launches (icb_launch_count)
+void count_launch(long long n = 1);
+struct Error
+{
+  int code;
+  std::string msg;
+};
+#define ICB_CUDA(call)                                                          \
+  do                                                                            \
+  {                                                                             \
+    cudaError_t e__ = (call);                                                   \
+    if(e__ != cudaSuccess)                                                      \
+      throw ::icb::Error{e__ == cudaErrorMemoryAllocation ? ICB_ERR_OOM          \
+                                                          : ICB_ERR_CUDA,       \
+                         std::string(#call) + ": " + cudaGetErrorString(e__)};  \
+  } while(0)
+#define ICB_REQUIRE(cond, msg)                                                  \
+  do                                                                            \
+  {                                                                             \
+    if(!(cond))                                                                 \
+      throw ::icb::Error{ICB_ERR_BAD_ARG, msg};                                 \
+  } while(0)
+
+// ---------------------------------------------------------- device memory --
+template <typename T> struct DevBuf
+{
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t cnt) { alloc(cnt); }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr, o.n = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept
+  {
+    release();
+    p = o.p;
+    n = o.n;
+    o.p = nullptr;
+    o.n = 0;
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t cnt)
+  {
+    release();
+    if(cnt)
+      ICB_CUDA(cudaMalloc(&p, cnt * sizeof(T)));
+    n = cnt;
+  }
+  void release()
+  {
+    if(p)
+      cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------- geometry --
+/// one structured grid (a multigrid level): elements nx*ny(*nz), nodes sx*sy(*sz)
+struct Dims
+{
+  int dim = 3;
+  int nx = 0, ny = 0, nz = 1;
+  int sx = 0, sy = 0, sz = 1;
+  long long nnode = 0, nel = 0;
+  long long ld = 0; ///< SoA stride of one displacement component (padded nnode)
+};
+Dims make_dims(int dim, int nx, int ny, int nz);
+
+/// unit element matrix passed by value to kernels (lives in the constant bank)
+template <typename T, int N> struct KMat
+{
+  T k[N * N];
+};
+
+/// reduction scratch: per-block partials + a completion counter.  The block
+/// that finishes last sums the partials in block order (deterministic).
+struct RedScratch
+{
+  double *partials = nullptr; ///< [maxBlocks * nvals]
+  unsigned *counter = nullptr;
+  int maxBlocks = 0;
+};
+
+/// device-resident Krylov state (all scalars stay on the GPU between launches)
+struct KState
+{
+  double bb;     ///< ||b||^2
+  double thr;    ///< max(tol^2 ||b||^2, DBL_MIN)
+  double rz;     ///< r.z of the current iterate
+  double rr;     ///< r.r
+  double pq;     ///< p.Ap
+  double alpha, beta;
+  double rzo; ///< r_{k+1}.z_k (flexible CG: Polak-Ribiere beta)
+  double tol;
+  int iter;      ///< completed iterations (Eigen's count)
+  int matvecs;
+  int maxit;
+  int conv;      ///< converged in the current iteration (x still to update)
+  int stop;      ///< no further work: converged, maxit or breakdown
+  int status;    ///< ICB_OK, ICB_ERR_MAXITER, ICB_ERR_BREAKDOWN, ICB_ERR_NAN
+  int pad;
+};
+
+// -------------------------------------------------------------- kernels --
+int num_sms();
+
+/// output stage of the element operator
+enum OpMode
+{
+  OP_APPLY = 0,    ///< y = K u
+  OP_RESIDUAL = 1, ///< y = b - K u
+  OP_JACOBI = 2,   ///< y = u + omega D^-1 (b - K u)
+  OP_CHEB = 3      ///< d = c1 d + c2 D^-1 (b - K u); y = u + d (Chebyshev step)
+};
+template <typename T> struct Epi
+{
+  const T *b;
+  const T *dinv;
+  T omega;
+  T *d;
+  T c1, c2;
+};
+template <typename T> struct OpExtras
+{
+  int mode = OP_APPLY;
+  const T *b = nullptr;
+  const T *dinv = nullptr;
+  double omega = 0.0;
+  T *d = nullptr; ///< OP_CHEB direction vector (read and written at each node)
+  double c1 = 0.0, c2 = 0.0;
+  RedScratch *dotRed = nullptr; ///< fused u.y reduction (OP_APPLY) into *dotOut
+  double *dotOut = nullptr;
+  const KState *gate = nullptr; ///< skip when gate->stop (or gate->conv if gateConv)
+  int gateConv = 0;
+};
+/// K: HOST pointer to the unit element matrix ((d*ne)^2 entries); it is
+/// passed by value, so the kernel's FMAs take it from the constant bank.
+template <typename T>
+void launch_op(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,
+               cudaStream_t s, const OpExtras<T> &x);
+
+// operators (operator.cu): every launcher takes the element matrix as a HOST
+// pointer and passes it by value.
+template <typename T>
+void launch_matvec(const Dims &d, const T *K, const T *E, const T *u, T *y,
+                   const uint8_t *fix, cudaStream_t s, RedScratch *dotRed = nullptr,
+                   double *dotOut = nullptr, const KState *gate = nullptr);
+template <typename T>
+void launch_diag(const Dims &d, const T *K, const T *E, const uint8_t *fix, T *invdiag,
+                 T *diag, cudaStream_t s);
+void launch_gather_free(const Dims &d, const long long *freeIdx, long long numeq,
+                        const double *soa, double *numeqv, cudaStream_t s);
+void launch_scatter_free(const Dims &d, const long long *freeIdx, long long numeq,
+                         const double *numeqv, double *soa, cudaStream_t s);
+void launch_simp(long long n, double y1, double y2, double p, const double *rho,
+                 double *E, float *Ef, cudaStream_t s);
+void launch_sensitivity(const Dims &d, const double *K, double y1, double y2, double p,
+                        const double *rho, const double *u, double *dc, cudaStream_t s);
+
+// reductions / vector kernels (krylov.cu)
+void red_alloc(RedScratch &r, int maxBlocks, int nvals, std::vector<void *> &owned);
+void launch_dot(long long n, const double *a, const double *b, RedScratch &red,
+                double *out, cudaStream_t s);
+void launch_axpby(long long n, double a, const double *x, double b, double *y,
+                  cudaStream_t s);
+
+} // namespace icb

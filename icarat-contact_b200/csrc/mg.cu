@@ -1,0 +1,973 @@
+// mg.cu -- geometric multigrid preconditioner on the structured grid
+// hierarchy and the multigrid-preconditioned flexible CG, in FP64 throughout
+// (ICB_FP64) or with an FP32 V-cycle under the FP64 Krylov iteration
+// (ICB_MIXED: FP64 iterate, residual, operator and reductions; FP32
+// smoother, transfers and coarse apply; FP64 coarse factorisation).
+//
+// FP32 inner solves inside FP64 defect correction were tried first: with
+// SIMP contrast (E from 1e-6 to 1 and Emin = 1e-9) the FP32 operator loses
+// p.Kp to cancellation once the search directions are smooth, and the inner
+// CG breaks down; keeping the Krylov recurrence in FP64 and only the
+// preconditioner in FP32 converges like the FP64 solve.
+//
+// ICARAT has no multigrid (its iterative path is Eigen's Jacobi CG,
+// src/analysis/solver/solvers.cpp:64-92); this is the B200 replacement of
+// that solve for large grids.  Design:
+//  * levels by 2:1 coarsening of the element grid (ceil for odd counts: the
+//    last coarse element then sticks out of the domain and only averages the
+//    children that exist), coarse moduli = mean of the children's E, coarse
+//    element matrix = K0 of the 2h element (rediscretisation; equal to the
+//    Galerkin product for constant coefficients);
+//  * transfer: (bi/tri)linear prolongation P, restriction R = P^T;
+//    constrained DOFs are masked on every level (a coarse DOF is constrained
+//    when the fine DOF at the same point is);
+//  * smoother: damped Jacobi with the fused operator epilogue (one kernel per
+//    sweep), nu sweeps before and after the coarse correction;
+//  * coarsest level: dense FP64 inverse built on the device (one CTA,
+//    Gauss-Jordan), applied as a dense product.
+// The whole V-cycle is a fixed kernel sequence, so a batch of PCG
+// iterations including their V-cycles is captured as one CUDA graph.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+
+#include "mg.hpp"
+#include "reduce.cuh"
+
+namespace icb
+{
+namespace
+{
+constexpr int VB = 256;
+inline int vblocks(long long n)
+{
+  return int(std::max<long long>(1, std::min<long long>((n + VB - 1) / VB, num_sms() * 8LL)));
+}
+inline unsigned nblocks(long long n, int bs) { return unsigned((n + bs - 1) / bs); }
+__device__ __forceinline__ bool gated(const KState *g)
+{
+  return g && (g->stop || g->conv);
+}
+
+// ------------------------------------------------------- grid transfer ----
+template <typename T>
+__global__ void k_coarsen_E(Dims df, Dims dc, const T *__restrict__ Ef, T *__restrict__ Ec)
+{
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(e >= dc.nel)
+    return;
+  int ci = int(e % dc.nx), cj = int((e / dc.nx) % dc.ny), ck = int(e / ((long long)dc.nx * dc.ny));
+  double s = 0.0;
+  int nk = df.dim == 3 ? 2 : 1;
+  for(int c = 0; c < nk; c++)
+    for(int b = 0; b < 2; b++)
+      for(int a = 0; a < 2; a++)
+      {
+        int i = 2 * ci + a, j = 2 * cj + b, k = 2 * ck + c;
+        if(i < df.nx && j < df.ny && (df.dim == 2 || k < df.nz))
+          s += double(Ef[i + (long long)j * df.nx + (long long)k * df.nx * df.ny]);
+      }
+  Ec[e] = T(s / (df.dim == 3 ? 8.0 : 4.0));
+}
+
+/// b_c = R r_f (R = P^T), constrained coarse DOFs zeroed
+template <typename T>
+__global__ void k_restrict(Dims df, Dims dc, const T *__restrict__ rf, T *__restrict__ bc,
+                           const uint8_t *__restrict__ fixc, const KState *gate)
+{
+  if(gated(gate))
+    return;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(n >= dc.nnode)
+    return;
+  long long sxy = (long long)dc.sx * dc.sy;
+  int I = int(n % dc.sx), J = int((n / dc.sx) % dc.sy), K = int(n / sxy);
+  long long fsxy = (long long)df.sx * df.sy;
+  double s[3] = {0, 0, 0};
+  int kr = df.dim == 3 ? 1 : 0;
+  for(int dk = -kr; dk <= kr; dk++)
+  {
+    int k = 2 * K + dk;
+    if(k < 0 || k >= df.sz)
+      continue;
+    double wk = dk ? 0.5 : 1.0;
+    for(int dj = -1; dj <= 1; dj++)
+    {
+      int j = 2 * J + dj;
+      if(j < 0 || j >= df.sy)
+        continue;
+      double wj = wk * (dj ? 0.5 : 1.0);
+      for(int di = -1; di <= 1; di++)
+      {
+        int i = 2 * I + di;
+        if(i < 0 || i >= df.sx)
+          continue;
+        double w = wj * (di ? 0.5 : 1.0);
+        long long f = i + (long long)j * df.sx + (long long)k * fsxy;
+        for(int c = 0; c < df.dim; c++)
+          s[c] += w * double(rf[c * df.ld + f]);
+      }
+    }
+  }
+  unsigned fx = fixc[n];
+  for(int c = 0; c < dc.dim; c++)
+    bc[c * dc.ld + n] = ((fx >> c) & 1u) ? T(0) : T(s[c]);
+}
+
+/// x_f += P x_c, constrained fine DOFs untouched (they stay 0)
+template <typename T>
+__global__ void k_prolong_add(Dims df, Dims dc, const T *__restrict__ xc, T *__restrict__ xf,
+                              const uint8_t *__restrict__ fixf, const KState *gate)
+{
+  if(gated(gate))
+    return;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(n >= df.nnode)
+    return;
+  long long sxy = (long long)df.sx * df.sy;
+  int i = int(n % df.sx), j = int((n / df.sx) % df.sy), k = int(n / sxy);
+  int I[2], J[2], K[2], ni, nj, nk;
+  double wi[2], wj[2], wk[2];
+  auto split = [](int v, int *C, double *w, int &cnt) {
+    if(v & 1)
+    {
+      C[0] = (v - 1) / 2;
+      C[1] = (v + 1) / 2;
+      w[0] = w[1] = 0.5;
+      cnt = 2;
+    }
+    else
+    {
+      C[0] = v / 2;
+      w[0] = 1.0;
+      cnt = 1;
+    }
+  };
+  split(i, I, wi, ni);
+  split(j, J, wj, nj);
+  if(df.dim == 3)
+    split(k, K, wk, nk);
+  else
+  {
+    K[0] = 0;
+    wk[0] = 1.0;
+    nk = 1;
+  }
+  long long csxy = (long long)dc.sx * dc.sy;
+  double s[3] = {0, 0, 0};
+  for(int c3 = 0; c3 < nk; c3++)
+    for(int b = 0; b < nj; b++)
+      for(int a = 0; a < ni; a++)
+      {
+        double w = wi[a] * wj[b] * wk[c3];
+        long long cn = I[a] + (long long)J[b] * dc.sx + (long long)K[c3] * csxy;
+        for(int c = 0; c < df.dim; c++)
+          s[c] += w * double(xc[c * dc.ld + cn]);
+      }
+  unsigned fx = fixf[n];
+  for(int c = 0; c < df.dim; c++)
+    if(!((fx >> c) & 1u))
+      xf[c * df.ld + n] += T(s[c]);
+}
+
+/// first smoothing step from a zero guess: x = d = c D^-1 b
+template <typename T>
+__global__ void k_jacobi0(long long n, T c, const T *__restrict__ dinv,
+                          const T *__restrict__ b, T *__restrict__ x, T *__restrict__ d,
+                          const KState *gate)
+{
+  if(gated(gate))
+    return;
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    T v = c * dinv[i] * b[i];
+    x[i] = v;
+    d[i] = v;
+  }
+}
+
+// --------------------------------------------------------- coarse level ----
+template <typename T>
+__global__ void k_dense_assemble(Dims d, KMat<double, 24> K, const T *__restrict__ E,
+                                 const int *__restrict__ dense, int n, double *A)
+{
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(e >= d.nel)
+    return;
+  const int ne = d.dim == 2 ? 4 : 8, nd = ne * d.dim;
+  int ei = int(e % d.nx), ej = int((e / d.nx) % d.ny), ek = int(e / ((long long)d.nx * d.ny));
+  long long sxy = (long long)d.sx * d.sy;
+  int idx[24];
+  for(int l = 0; l < ne; l++)
+  {
+    int q = l & 3, top = l >> 2;
+    long long node = ei + ((q == 1 || q == 2) ? 1 : 0) + (long long)(ej + (q >= 2 ? 1 : 0)) * d.sx +
+                     (long long)(ek + top) * sxy;
+    for(int c = 0; c < d.dim; c++)
+      idx[l * d.dim + c] = dense[c * d.ld + node];
+  }
+  double Ee = double(E[e]);
+  for(int a = 0; a < nd; a++)
+  {
+    if(idx[a] < 0)
+      continue;
+    for(int b = 0; b < nd; b++)
+      if(idx[b] >= 0)
+        atomicAdd(A + (long long)idx[a] * n + idx[b], Ee * K.k[a * nd + b]);
+  }
+}
+
+/// In-place Gauss-Jordan inversion of the SPD coarse matrix (no pivoting is
+/// needed for SPD).  One CTA; a non-positive pivot is recorded in *status
+/// and replaced by a tiny positive value so the preconditioner stays usable.
+__global__ void __launch_bounds__(1024) k_invert_spd(int n, double *A, int *status)
+{
+  __shared__ double rowk[1024];
+  __shared__ double colk[1024];
+  __shared__ double piv;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  double dmax = 0.0;
+  for(int i = 0; i < n; i++)
+    dmax = fmax(dmax, A[(long long)i * n + i]);
+  for(int k = 0; k < n; k++)
+  {
+    if(tid == 0)
+    {
+      double p = A[(long long)k * n + k];
+      if(!(p > 1e-14 * dmax))
+      {
+        status[0] = k + 1;
+        p = fmax(1e-14 * dmax, DBL_MIN);
+      }
+      piv = p;
+    }
+    __syncthreads();
+    const double p = piv;
+    for(int j = tid; j < n; j += nth)
+    {
+      rowk[j] = (j == k ? 1.0 : A[(long long)k * n + j]) / p;
+      colk[j] = A[(long long)j * n + k];
+    }
+    __syncthreads();
+    for(long long t = tid; t < (long long)n * n; t += nth)
+    {
+      int i = int(t / n), j = int(t % n);
+      if(i == k)
+        A[t] = rowk[j];
+      else
+      {
+        double f = colk[i];
+        A[t] = (j == k ? 0.0 : A[t]) - f * rowk[j];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+/// x_c = A^-1 b_c over the free coarse DOFs (warp per row)
+template <typename T>
+__global__ void k_dense_apply(int n, const double *__restrict__ Ainv,
+                              const long long *__restrict__ soa, const T *__restrict__ b,
+                              T *__restrict__ x, const KState *gate)
+{
+  if(gated(gate))
+    return;
+  extern __shared__ double sb[];
+  for(int j = threadIdx.x; j < n; j += blockDim.x)
+    sb[j] = double(b[soa[j]]);
+  __syncthreads();
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  int nw = (gridDim.x * blockDim.x) >> 5;
+  for(int i = warp; i < n; i += nw)
+  {
+    double s = 0.0;
+    for(int j = lane; j < n; j += 32)
+      s += Ainv[(long long)i * n + j] * sb[j];
+    s = warp_sum_d(s);
+    if(lane == 0)
+      x[soa[i]] = T(s);
+  }
+}
+
+template <typename T>
+__global__ void k_fill(long long n, T v, T *__restrict__ x)
+{
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+// ------------------------------------------------------------- MG-PCG ------
+// Flexible (Polak-Ribiere) CG in precision TK preconditioned by a V-cycle in
+// precision TP.  TK = TP = double is the FP64 GMG path; TK = double,
+// TP = float is the mixed path: FP64 iterate, residual, operator and
+// reductions, FP32 multigrid.  The precision casts are fused into the Krylov
+// kernels (rP = TP(r) written by the residual update, z read as TP).
+struct FinInitMg
+{
+  KState *st;
+  double tol;
+  int maxit;
+  __device__ void operator()(const double *t) const
+  {
+    st->bb = t[0];
+    st->rr = t[0];
+    st->tol = tol;
+    st->thr = fmax(tol * tol * t[0], DBL_MIN);
+    st->iter = 0;
+    st->matvecs = 0;
+    st->maxit = maxit;
+    st->conv = 0;
+    st->alpha = st->beta = 0.0;
+    st->status = ICB_OK;
+    st->stop = 0;
+    if(!isfinite(t[0]))
+    {
+      st->status = ICB_ERR_NAN;
+      st->stop = 1;
+    }
+    else if(t[0] == 0.0 || t[0] < st->thr)
+      st->stop = 1;
+  }
+};
+
+template <typename TK, typename TP>
+__global__ void k_mg_init(long long n, const TK *__restrict__ b, TK *__restrict__ x,
+                          TK *__restrict__ r, TP *__restrict__ rP, RedScratch red, KState *st,
+                          double tol, int maxit)
+{
+  double v[1] = {0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    TK bi = b[i];
+    r[i] = bi;
+    if(rP)
+      rP[i] = TP(bi);
+    x[i] = TK(0);
+    v[0] += double(bi) * double(bi);
+  }
+  block_reduce<1>(v, red, FinInitMg{st, tol, maxit});
+}
+
+struct FinRz0
+{
+  KState *st;
+  __device__ void operator()(const double *t) const
+  {
+    st->rz = t[0];
+    if(!isfinite(t[0]) || !(t[0] > 0.0))
+    {
+      st->status = isfinite(t[0]) ? ICB_ERR_BREAKDOWN : ICB_ERR_NAN;
+      st->stop = 1;
+    }
+  }
+};
+
+/// p = z; rz = r.z
+template <typename TK, typename TP>
+__global__ void k_mg_init2(long long n, const TK *__restrict__ r, const TP *__restrict__ z,
+                           TK *__restrict__ p, RedScratch red, KState *st)
+{
+  if(st->stop)
+    return;
+  double v[1] = {0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    TK zi = TK(z[i]);
+    p[i] = zi;
+    v[0] += double(r[i]) * double(zi);
+  }
+  block_reduce<1>(v, red, FinRz0{st});
+}
+
+struct FinRmg
+{
+  KState *st;
+  double pq, alpha;
+  bool bad;
+  __device__ void operator()(const double *t) const
+  {
+    st->matvecs++;
+    if(bad)
+    {
+      st->status = ICB_ERR_BREAKDOWN;
+      st->stop = 1;
+      return;
+    }
+    st->pq = pq;
+    st->alpha = alpha;
+    st->rr = t[0];
+    st->rzo = t[1];
+    if(!isfinite(t[0]))
+    {
+      st->status = ICB_ERR_NAN;
+      st->stop = 1;
+    }
+    else if(t[0] < st->thr)
+      st->conv = 1;
+  }
+};
+
+/// r -= alpha q (and rP = TP(r)); sums r.r and r.z_old (z still holds the
+/// previous preconditioned residual) for the flexible beta
+template <typename TK, typename TP>
+__global__ void k_mg_r(long long n, TK *__restrict__ r, TP *__restrict__ rP,
+                       const TK *__restrict__ q, const TP *__restrict__ zold,
+                       const double *__restrict__ pq, RedScratch red, KState *st)
+{
+  if(st->stop)
+    return;
+  const double pqv = *pq;
+  const double alpha = st->rz / pqv;
+  const bool bad = !(pqv > 0.0) || !isfinite(alpha);
+  double v[2] = {0.0, 0.0};
+  if(!bad)
+  {
+    const TK a = TK(alpha);
+    for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+        i += (long long)gridDim.x * blockDim.x)
+    {
+      TK ri = r[i] - a * q[i];
+      r[i] = ri;
+      if(rP)
+        rP[i] = TP(ri);
+      v[0] += double(ri) * double(ri);
+      v[1] += double(ri) * double(zold[i]);
+    }
+  }
+  block_reduce<2>(v, red, FinRmg{st, pqv, alpha, bad});
+}
+
+struct FinRz
+{
+  KState *st;
+  __device__ void operator()(const double *t) const
+  {
+    if(!isfinite(t[0]))
+    {
+      st->status = ICB_ERR_NAN;
+      st->stop = 1;
+      return;
+    }
+    // Polak-Ribiere (flexible CG): tolerates a V-cycle that is only
+    // symmetric up to rounding, and a preconditioner in lower precision
+    st->beta = (t[0] - st->rzo) / st->rz;
+    st->rz = t[0];
+  }
+};
+
+template <typename TK, typename TP>
+__global__ void k_mg_rz(long long n, const TK *__restrict__ r, const TP *__restrict__ z,
+                        RedScratch red, KState *st)
+{
+  if(st->stop || st->conv)
+    return;
+  double v[1] = {0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+    v[0] += double(r[i]) * double(z[i]);
+  block_reduce<1>(v, red, FinRz{st});
+}
+
+struct FinXPmg
+{
+  KState *st;
+  __device__ void operator()(const double *) const
+  {
+    if(st->conv)
+    {
+      st->stop = 1;
+      return;
+    }
+    st->iter++;
+    if(st->iter >= st->maxit)
+    {
+      st->status = ICB_ERR_MAXITER;
+      st->stop = 1;
+    }
+  }
+};
+
+template <typename TK, typename TP>
+__global__ void k_mg_xp(long long n, TK *__restrict__ x, TK *__restrict__ p,
+                        const TP *__restrict__ z, RedScratch red, KState *st)
+{
+  if(st->stop)
+    return;
+  const TK a = TK(st->alpha), bt = TK(st->beta);
+  const bool conv = st->conv;
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    TK pi = p[i];
+    x[i] += a * pi;
+    if(!conv)
+      p[i] = TK(z[i]) + bt * pi;
+  }
+  double v[1] = {0.0};
+  block_reduce<1>(v, red, FinXPmg{st});
+}
+} // namespace
+
+// ============================================================ hierarchy ====
+/// lambda_max(diag(K0)^-1 K0) by power iteration on D^-1/2 K0 D^-1/2 (host)
+template <typename T> double element_lmax(int dim, const T *K)
+{
+  const int nd = dim == 2 ? 8 : 24;
+  std::vector<double> M(nd * nd), v(nd, 1.0), w(nd);
+  for(int i = 0; i < nd; i++)
+    for(int j = 0; j < nd; j++)
+      M[i * nd + j] = double(K[i * nd + j]) / std::sqrt(double(K[i * nd + i]) * double(K[j * nd + j]));
+  for(int i = 0; i < nd; i++)
+    v[i] = 1.0 + 0.1 * i;
+  double lam = 0.0;
+  for(int it = 0; it < 2000; it++)
+  {
+    double nn = 0.0;
+    for(int i = 0; i < nd; i++)
+    {
+      double s = 0.0;
+      for(int j = 0; j < nd; j++)
+        s += M[i * nd + j] * v[j];
+      w[i] = s;
+      nn += s * s;
+    }
+    nn = std::sqrt(nn);
+    lam = nn;
+    for(int i = 0; i < nd; i++)
+      v[i] = w[i] / nn;
+  }
+  return lam * 1.02;
+}
+
+template <typename T> struct Level
+{
+  Dims d;
+  double h[3];
+  T K[576]; ///< unit element matrix of this level (passed by value)
+  DevBuf<T> Eown;
+  const T *E = nullptr;
+  DevBuf<uint8_t> fixOwn;
+  const uint8_t *fix = nullptr;
+  DevBuf<T> dinv, x, b, r, t, dv;
+};
+
+/// Flexible CG in TK with a TP V-cycle (see the kernels above).
+template <typename TK, typename TP> struct MgPcg
+{
+  std::vector<Level<TP>> lv;
+  int nu = 2;
+  /// Chebyshev interval [lmax/10, lmax] for D^-1 K; lmax is the element
+  /// bound lambda_max(diag(K0)^-1 K0), which holds for any moduli E because
+  /// x^T K x / x^T D x is a weighted mean of the element quotients.
+  double lmax = 4.0;
+  std::vector<double> cc1, cc2; ///< per-step Chebyshev coefficients
+  // Krylov operator (fine level in TK)
+  TK Kk[576];
+  const TK *Ek = nullptr;
+  // coarsest dense system
+  int nc = 0;
+  DevBuf<long long> cSoa;
+  DevBuf<int> cDense;
+  DevBuf<double> cA;
+  DevBuf<int> cStatus;
+  // Krylov vectors (fine level)
+  long long n = 0;
+  DevBuf<TK> r, p, q;
+  DevBuf<TP> rP, z;
+  DevBuf<KState> st;
+  DevBuf<double> partials, dots;
+  DevBuf<unsigned> counter;
+  RedScratch red;
+  KState *hst = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void *key[4] = {};
+  int batch = 8;
+  long long graphNodes = 0;
+
+  ~MgPcg()
+  {
+    if(exec)
+      cudaGraphExecDestroy(exec);
+    if(hst)
+      cudaFreeHost(hst);
+  }
+
+  static constexpr bool same() { return sizeof(TK) == sizeof(TP); }
+  TP *rin() { return same() ? (TP *)r.p : rP.p; }
+
+  /// level dims, element matrices and Dirichlet masks (host), device buffers
+  void build(const HostSetup &hs, const TK *Kkrylov, const TK *Ekrylov, const TP *Kfine,
+             const TP *Efine, const uint8_t *fixFine, int coarseDofs, int smooth)
+  {
+    nu = smooth > 0 ? smooth : 2;
+    lmax = element_lmax(hs.desc.dim, Kfine);
+    // Chebyshev coefficients of steps 0..nu-1 (Saad, Iterative Methods for
+    // Sparse Linear Systems, 2nd ed., Alg. 12.1) on [lmax/10, lmax]
+    {
+      double a = lmax / 10.0, b = lmax, theta = 0.5 * (b + a), delta = 0.5 * (b - a);
+      double sigma = theta / delta, rho0 = 1.0 / sigma;
+      cc1.assign(nu, 0.0);
+      cc2.assign(nu, 0.0);
+      cc2[0] = 1.0 / theta;
+      for(int k = 1; k < nu; k++)
+      {
+        double rho1 = 1.0 / (2.0 * sigma - rho0);
+        cc1[k] = rho1 * rho0;
+        cc2[k] = 2.0 * rho1 / delta;
+        rho0 = rho1;
+      }
+    }
+    std::copy(Kkrylov, Kkrylov + 576, Kk);
+    Ek = Ekrylov;
+    Level<TP> L0;
+    L0.d = hs.dims;
+    std::memcpy(L0.h, hs.h, sizeof(L0.h));
+    std::copy(Kfine, Kfine + 576, L0.K);
+    L0.E = Efine;
+    L0.fix = fixFine;
+    lv.clear();
+    lv.push_back(std::move(L0));
+    std::vector<uint8_t> fm(hs.dims.nnode, 0);
+    for(long long nd = 0; nd < hs.dims.nnode; nd++)
+      for(int c = 0; c < hs.desc.dim; c++)
+        if(hs.fixed[nd * hs.desc.dim + c])
+          fm[nd] |= uint8_t(1u << c);
+    const int dim = hs.desc.dim;
+    const int cd = coarseDofs > 0 ? coarseDofs : 600;
+    while(true)
+    {
+      const Dims &f = lv.back().d;
+      long long dofs = f.nnode * dim;
+      bool can = f.nx >= 2 && f.ny >= 2 && (dim == 2 || f.nz >= 2);
+      if(dofs <= cd || !can)
+        break;
+      Level<TP> c;
+      c.d = make_dims(dim, (f.nx + 1) / 2, (f.ny + 1) / 2, dim == 3 ? (f.nz + 1) / 2 : 1);
+      for(int k = 0; k < 3; k++)
+        c.h[k] = 2.0 * lv.back().h[k];
+      double Kd[576];
+      unit_stiffness(dim, hs.desc.state, hs.desc.poisson, c.h, Kd);
+      for(int i = 0; i < 576; i++)
+        c.K[i] = TP(Kd[i]);
+      // coarse mask: a coarse DOF is constrained when a constrained fine DOF
+      // interpolates from it (P(i, I) != 0); for constraints on even grid
+      // lines this is the fine DOF at the same point, a constraint at an odd
+      // index (a point support between coarse nodes) constrains the coarse
+      // neighbours so the coarse operator never loses it.
+      std::vector<uint8_t> cm(c.d.nnode, 0);
+      for(long long nd = 0; nd < f.nnode; nd++)
+      {
+        if(!fm[nd])
+          continue;
+        long long i = nd % f.sx, j = (nd / f.sx) % f.sy, k = nd / ((long long)f.sx * f.sy);
+        long long I0 = i / 2, I1 = (i + 1) / 2, J0 = j / 2, J1 = (j + 1) / 2, K0 = k / 2,
+                  K1 = dim == 3 ? (k + 1) / 2 : 0;
+        for(long long K = K0; K <= K1; K++)
+          for(long long J = J0; J <= J1; J++)
+            for(long long I = I0; I <= I1; I++)
+              cm[I + J * c.d.sx + K * (long long)c.d.sx * c.d.sy] |= fm[nd];
+      }
+      c.fixOwn.alloc(c.d.nnode);
+      ICB_CUDA(cudaMemcpy(c.fixOwn.p, cm.data(), cm.size(), cudaMemcpyHostToDevice));
+      c.fix = c.fixOwn.p;
+      c.Eown.alloc(c.d.nel);
+      c.E = c.Eown.p;
+      fm.swap(cm);
+      lv.push_back(std::move(c));
+    }
+    for(size_t l = 0; l < lv.size(); l++)
+    {
+      long long m = (long long)dim * lv[l].d.ld;
+      lv[l].dinv.alloc(m);
+      lv[l].r.alloc(m);
+      lv[l].t.alloc(m);
+      lv[l].dv.alloc(m);
+      if(l > 0)
+      {
+        lv[l].x.alloc(m);
+        lv[l].b.alloc(m);
+      }
+      for(DevBuf<TP> *v : {&lv[l].dinv, &lv[l].r, &lv[l].t, &lv[l].x, &lv[l].b, &lv[l].dv})
+        if(v->p)
+          ICB_CUDA(cudaMemset(v->p, 0, v->bytes()));
+    }
+    // coarsest dense index map
+    const Level<TP> &C = lv.back();
+    std::vector<uint8_t> cmask(C.d.nnode);
+    ICB_CUDA(cudaMemcpy(cmask.data(), C.fix, C.d.nnode, cudaMemcpyDeviceToHost));
+    std::vector<int> dense((size_t)dim * C.d.ld, -1);
+    std::vector<long long> soa;
+    for(long long nd = 0; nd < C.d.nnode; nd++)
+      for(int c = 0; c < dim; c++)
+        if(!((cmask[nd] >> c) & 1u))
+        {
+          dense[c * C.d.ld + nd] = int(soa.size());
+          soa.push_back(c * C.d.ld + nd);
+        }
+    nc = int(soa.size());
+    if(nc > 1024)
+      throw Error{ICB_ERR_BAD_ARG, "coarsest grid too large for the dense solve (>1024 DOFs)"};
+    cSoa.alloc(std::max(nc, 1));
+    cDense.alloc(dense.size());
+    if(nc)
+      ICB_CUDA(cudaMemcpy(cSoa.p, soa.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice));
+    ICB_CUDA(cudaMemcpy(cDense.p, dense.data(), sizeof(int) * dense.size(), cudaMemcpyHostToDevice));
+    cA.alloc((size_t)std::max(nc, 1) * std::max(nc, 1));
+    cStatus.alloc(1);
+    n = (long long)dim * lv[0].d.ld;
+    for(DevBuf<TK> *v : {&r, &p, &q})
+    {
+      v->alloc(n);
+      ICB_CUDA(cudaMemset(v->p, 0, v->bytes()));
+    }
+    z.alloc(n);
+    ICB_CUDA(cudaMemset(z.p, 0, z.bytes()));
+    if(!same())
+    {
+      rP.alloc(n);
+      ICB_CUDA(cudaMemset(rP.p, 0, rP.bytes()));
+    }
+    st.alloc(1);
+    int mb = reduction_blocks(lv[0].d);
+    partials.alloc((size_t)mb * 2);
+    dots.alloc(4);
+    counter.alloc(1);
+    ICB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned)));
+    red = RedScratch{partials.p, counter.p, mb};
+    ICB_CUDA(cudaMallocHost(&hst, sizeof(KState)));
+  }
+
+  /// per density: coarse moduli, diagonals, coarse inverse
+  void refresh(cudaStream_t s)
+  {
+    for(size_t l = 1; l < lv.size(); l++)
+    {
+      k_coarsen_E<TP><<<nblocks(lv[l].d.nel, 256), 256, 0, s>>>(lv[l - 1].d, lv[l].d,
+                                                                lv[l - 1].E, lv[l].Eown.p);
+      count_launch();
+    }
+    for(auto &L : lv)
+      launch_diag<TP>(L.d, L.K, L.E, L.fix, L.dinv.p, nullptr, s);
+    const Level<TP> &C = lv.back();
+    if(nc)
+    {
+      ICB_CUDA(cudaMemsetAsync(cA.p, 0, sizeof(double) * (size_t)nc * nc, s));
+      ICB_CUDA(cudaMemsetAsync(cStatus.p, 0, sizeof(int), s));
+      KMat<double, 24> kd;
+      for(int i = 0; i < 576; i++)
+        kd.k[i] = double(C.K[i]);
+      k_dense_assemble<TP><<<nblocks(C.d.nel, 128), 128, 0, s>>>(C.d, kd, C.E, cDense.p, nc, cA.p);
+      k_invert_spd<<<1, 1024, 0, s>>>(nc, cA.p, cStatus.p);
+      count_launch(2);
+    }
+    ICB_CUDA(cudaGetLastError());
+  }
+
+  void coarseSolve(const TP *b, TP *x, cudaStream_t s, const KState *gate)
+  {
+    const Level<TP> &C = lv.back();
+    long long m = (long long)C.d.dim * C.d.ld;
+    k_fill<TP><<<vblocks(m), VB, 0, s>>>(m, TP(0), x);
+    if(nc)
+      k_dense_apply<TP><<<8, 256, sizeof(double) * nc, s>>>(nc, cA.p, cSoa.p, b, x, gate);
+    count_launch(2);
+  }
+
+  /// out = V-cycle(b) on level l
+  void level(size_t l, const TP *b, TP *out, cudaStream_t s, const KState *gate)
+  {
+    Level<TP> &L = lv[l];
+    if(l + 1 == lv.size())
+    {
+      coarseSolve(b, out, s, gate);
+      return;
+    }
+    long long m = (long long)L.d.dim * L.d.ld;
+    // step 0 from zero, then 2nu-1 operator steps: an odd number of
+    // ping-pongs ends in out
+    TP *cur = L.t.p, *oth = out;
+    k_jacobi0<TP><<<vblocks(m), VB, 0, s>>>(m, TP(cc2[0]), L.dinv.p, b, cur, L.dv.p, gate);
+    count_launch();
+    OpExtras<TP> ch;
+    ch.mode = OP_CHEB;
+    ch.b = b;
+    ch.dinv = L.dinv.p;
+    ch.d = L.dv.p;
+    ch.gate = gate;
+    ch.gateConv = 1;
+    for(int k = 1; k < nu; k++)
+    {
+      ch.c1 = cc1[k];
+      ch.c2 = cc2[k];
+      launch_op<TP>(L.d, L.K, L.E, cur, oth, L.fix, s, ch);
+      std::swap(cur, oth);
+    }
+    OpExtras<TP> res;
+    res.mode = OP_RESIDUAL;
+    res.b = b;
+    res.gate = gate;
+    res.gateConv = 1;
+    launch_op<TP>(L.d, L.K, L.E, cur, L.r.p, L.fix, s, res);
+    Level<TP> &Cn = lv[l + 1];
+    k_restrict<TP><<<nblocks(Cn.d.nnode, 256), 256, 0, s>>>(L.d, Cn.d, L.r.p, Cn.b.p, Cn.fix, gate);
+    count_launch();
+    level(l + 1, Cn.b.p, Cn.x.p, s, gate);
+    k_prolong_add<TP><<<nblocks(L.d.nnode, 256), 256, 0, s>>>(L.d, Cn.d, Cn.x.p, cur, L.fix, gate);
+    count_launch();
+    for(int k = 0; k < nu; k++)
+    {
+      ch.c1 = cc1[k];
+      ch.c2 = cc2[k];
+      launch_op<TP>(L.d, L.K, L.E, cur, oth, L.fix, s, ch);
+      std::swap(cur, oth);
+    }
+    if(cur != out)
+      ICB_CUDA(cudaMemcpyAsync(out, cur, sizeof(TP) * m, cudaMemcpyDeviceToDevice, s));
+  }
+
+  void iteration(TK *x, cudaStream_t s)
+  {
+    const Dims &d = lv[0].d;
+    int nb = vblocks(n);
+    OpExtras<TK> a;
+    a.dotRed = &red;
+    a.dotOut = dots.p;
+    a.gate = st.p;
+    launch_op<TK>(d, Kk, Ek, p.p, q.p, lv[0].fix, s, a);
+    k_mg_r<TK, TP><<<nb, VB, 0, s>>>(n, r.p, same() ? nullptr : rP.p, q.p, z.p, dots.p, red, st.p);
+    level(0, rin(), z.p, s, st.p);
+    k_mg_rz<TK, TP><<<nb, VB, 0, s>>>(n, r.p, z.p, red, st.p);
+    k_mg_xp<TK, TP><<<nb, VB, 0, s>>>(n, x, p.p, z.p, red, st.p);
+    count_launch(3);
+  }
+
+  int solve(const TK *b, TK *x, double tol, int maxit, cudaStream_t s, icb_solve_info *info)
+  {
+    int nb = vblocks(n);
+    k_mg_init<TK, TP><<<nb, VB, 0, s>>>(n, b, x, r.p, same() ? nullptr : rP.p, red, st.p, tol,
+                                         maxit);
+    count_launch();
+    level(0, rin(), z.p, s, nullptr);
+    k_mg_init2<TK, TP><<<nb, VB, 0, s>>>(n, r.p, z.p, p.p, red, st.p);
+    count_launch();
+    ICB_CUDA(cudaGetLastError());
+    const void *k[4] = {x, Ek, lv[0].E, (const void *)s};
+    bool same_ = exec != nullptr;
+    for(int i = 0; i < 4 && same_; i++)
+      same_ = k[i] == key[i];
+    if(!same_)
+    {
+      if(exec)
+        cudaGraphExecDestroy(exec);
+      exec = nullptr;
+      cudaStream_t cs;
+      ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      long long before = 0;
+      cudaGraph_t g;
+      ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      for(int it = 0; it < batch; it++)
+        iteration(x, cs);
+      ICB_CUDA(cudaStreamEndCapture(cs, &g));
+      ICB_CUDA(cudaGraphInstantiate(&exec, g, 0));
+      size_t nn = 0;
+      cudaGraphGetNodes(g, nullptr, &nn);
+      cudaGraphDestroy(g);
+      cudaStreamDestroy(cs);
+      (void)before;
+      graphNodes = (long long)nn;
+      for(int i = 0; i < 4; i++)
+        key[i] = k[i];
+    }
+    long long launched = 0;
+    for(;;)
+    {
+      ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+      ICB_CUDA(cudaStreamSynchronize(s));
+      if(hst->stop || launched > (long long)maxit + batch)
+        break;
+      ICB_CUDA(cudaGraphLaunch(exec, s));
+      launched += batch;
+      count_launch(graphNodes);
+    }
+    if(info)
+    {
+      info->iters = hst->iter;
+      info->matvecs = hst->matvecs;
+      info->relres = hst->bb > 0 ? std::sqrt(hst->rr / hst->bb) : 0.0;
+      info->status = hst->status;
+    }
+    return hst->status;
+  }
+};
+
+// ============================================================== Mixed ======
+struct Mixed
+{
+  int coarseDofs = -1, smooth = -1;
+  std::unique_ptr<MgPcg<double, double>> mg64;
+  std::unique_ptr<MgPcg<double, float>> mgmx;
+};
+
+int solve_multigrid(icb_problem p, const icb_solve_opts &o, const double *b, icb_solve_info *info)
+{
+  cudaStream_t s = p->stream();
+  const HostSetup &hs = *p->hs;
+  if(!p->mixed)
+    p->mixed = std::make_unique<Mixed>();
+  Mixed &M = *p->mixed;
+  if(M.coarseDofs != o.mg_coarse_dofs || M.smooth != o.mg_smooth)
+  {
+    M.mg64.reset();
+    M.mgmx.reset();
+    M.coarseDofs = o.mg_coarse_dofs;
+    M.smooth = o.mg_smooth;
+  }
+  cudaEvent_t e0, e1;
+  ICB_CUDA(cudaEventCreate(&e0));
+  ICB_CUDA(cudaEventCreate(&e1));
+  ICB_CUDA(cudaEventRecord(e0, s));
+  int status;
+  icb_solve_info inf{};
+  if(o.precision == ICB_FP64)
+  {
+    if(!M.mg64)
+    {
+      M.mg64 = std::make_unique<MgPcg<double, double>>();
+      M.mg64->build(hs, p->K0, p->E.p, p->K0, p->E.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth);
+    }
+    M.mg64->refresh(s);
+    status = M.mg64->solve(b, p->x.p, o.tol, o.maxit, s, &inf);
+  }
+  else
+  {
+    if(!M.mgmx)
+    {
+      M.mgmx = std::make_unique<MgPcg<double, float>>();
+      M.mgmx->build(hs, p->K0, p->E.p, p->K0f, p->Ef.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth);
+    }
+    M.mgmx->refresh(s);
+    status = M.mgmx->solve(b, p->x.p, o.tol, o.maxit, s, &inf);
+  }
+  inf.outer = 1;
+  ICB_CUDA(cudaEventRecord(e1, s));
+  ICB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  inf.seconds = ms * 1e-3;
+  inf.status = status;
+  if(info)
+    *info = inf;
+  return status;
+}
+
+} // namespace icb
+
+icb_problem_s::icb_problem_s() = default;
+icb_problem_s::~icb_problem_s() = default;

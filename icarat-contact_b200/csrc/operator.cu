@@ -1,0 +1,653 @@
+// operator.cu -- matrix-free element-by-element stiffness operator on the
+// structured Q4 / Hex8 grids, its diagonal, SIMP moduli and sensitivities.
+//
+// Replaces the assembled path of ICARAT: LinearElastic::makeKeFint
+// (src/problem/elasticity.cpp:210-254) + assembling()
+// (src/misc/assembling.hpp:17-38) + SparseMatrix::setFromTriplets
+// (src/analysis/linear.hpp:155-161) + Eigen's SpMV inside ConjugateGradient.
+// On a uniform grid Ke = E(rho_e) K0, so K(rho) u = sum_e E_e K0 u_e; nothing
+// is assembled.
+//
+// Layout in HBM: displacement-like vectors are SoA, one plane per component,
+// node index n = i + j*sx + k*sx*sy (MeshIcarat numbering), component c at
+// c*ld + n.  Constrained DOFs are masked by a per-node bit mask (bit c set:
+// component c fixed), so the operator acts on the free space exactly as the
+// eliminated numeq system of assembling() does.
+//
+// Hex8 kernel: a CTA owns a 31x7 tile of output nodes in x-y and marches up a
+// chunk of z planes.  Each thread owns one element column (the tile's
+// elements plus a one-element halo on the low side), keeps the 4 bottom
+// corner displacements of its current element in registers (they are the top
+// corners of the element below) and carries the element's top-corner
+// contributions up to the next plane in registers, so the vertical sharing
+// needs no memory at all.  The four columns around a node are summed with one
+// warp shuffle (x) and one shared-memory exchange (y).  No atomics, no
+// colouring, deterministic results.
+#include "icb_internal.hpp"
+#include "reduce.cuh"
+
+#include <algorithm>
+
+namespace icb
+{
+namespace
+{
+constexpr int TX = 32; // threads along x (one warp)
+constexpr int TY3 = 8; // warps along y (3D)
+constexpr int TY2 = 4; // warps per CTA (2D: independent x strips)
+
+/// local node index of the corner with offsets (a,b) in a plane (meshBox order)
+__host__ __device__ constexpr int lnode(int a, int b) { return (a ^ b) + 2 * b; }
+
+/// fused output stage: y = Au (OP_APPLY), b - Au (OP_RESIDUAL), a damped
+/// Jacobi sweep u + w D^-1 (b - Au) (OP_JACOBI) or a Chebyshev step
+/// (OP_CHEB); Au is already 0 on constrained DOFs and so are b and D^-1.
+template <typename T, int MODE>
+__device__ __forceinline__ T epilogue(T Au, T uself, long long i, const Epi<T> &ep)
+{
+  if(MODE == OP_APPLY)
+    return Au;
+  T r = __ldg(ep.b + i) - Au;
+  if(MODE == OP_RESIDUAL)
+    return r;
+  if(MODE == OP_JACOBI)
+    return uself + ep.omega * __ldg(ep.dinv + i) * r;
+  // OP_CHEB: the direction is read and written only at this node
+  T dn = ep.c2 * __ldg(ep.dinv + i) * r;
+  if(ep.c1 != T(0))
+    dn += ep.c1 * ep.d[i];
+  ep.d[i] = dn;
+  return uself + dn;
+}
+
+// ----------------------------------------------------------------- Hex8 ----
+template <typename T, bool DOT, int MODE>
+__global__ void __launch_bounds__(TX *TY3)
+    k_matvec_h8(const KMat<T, 24> K, const Dims d, const int zchunk,
+                const T *__restrict__ E, const T *__restrict__ u, T *__restrict__ y,
+                const uint8_t *__restrict__ fix, RedScratch red, double *dotOut,
+                const KState *gate, const int gateConv, const Epi<T> ep)
+{
+  if(gate && (gate->stop || (gateConv && gate->conv)))
+    return;
+  __shared__ T sB[2][3][TY3][TX];
+  const int lx = threadIdx.x, ly = threadIdx.y;
+  const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TY3 - 1);
+  const int ei = X0 - 1 + lx, ej = Y0 - 1 + ly;
+  const int Z0 = blockIdx.z * zchunk;
+  const int Z1 = min(Z0 + zchunk, d.sz) - 1;
+  const bool col = ei >= 0 && ei < d.nx && ej >= 0 && ej < d.ny;
+  const long long sxy = (long long)d.sx * d.sy;
+  const long long ld = d.ld;
+  const long long nb = col ? (long long)ei + (long long)ej * d.sx : 0;
+  // corner q (lnode order) -> node offset within a plane
+  const long long qoff[4] = {0, 1, 1 + (long long)d.sx, (long long)d.sx};
+
+  T ub[3][4], ut[3][4], carry[3][4];
+#pragma unroll
+  for(int c = 0; c < 3; c++)
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+    {
+      carry[c][q] = T(0);
+      ub[c][q] = T(0);
+    }
+  if(col && Z0 - 1 >= 0)
+  {
+    long long base = nb + (long long)(Z0 - 1) * sxy;
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+        ub[c][q] = __ldg(u + c * ld + base + qoff[q]);
+  }
+  double dot = 0.0;
+  for(int ek = Z0 - 1; ek <= Z1; ++ek)
+  {
+    const bool lay = col && ek >= 0 && ek < d.nz;
+    const bool topok = col && ek + 1 >= 0 && ek + 1 <= d.nz;
+    if(topok)
+    {
+      long long base = nb + (long long)(ek + 1) * sxy;
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+#pragma unroll
+        for(int q = 0; q < 4; q++)
+          ut[c][q] = __ldg(u + c * ld + base + qoff[q]);
+    }
+    else
+    {
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+#pragma unroll
+        for(int q = 0; q < 4; q++)
+          ut[c][q] = T(0);
+    }
+    const T Ee = lay ? __ldg(E + (long long)ei + (long long)ej * d.nx +
+                             (long long)ek * d.nx * d.ny)
+                     : T(0);
+    // rows of the bottom corners: complete the column contribution to plane ek
+    T acc[3][4];
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const int row = q * 3 + c;
+        T s = T(0);
+#pragma unroll
+        for(int q2 = 0; q2 < 4; q2++)
+#pragma unroll
+          for(int c2 = 0; c2 < 3; c2++)
+            s = fma(K.k[row * 24 + q2 * 3 + c2], ub[c2][q2], s);
+#pragma unroll
+        for(int q2 = 0; q2 < 4; q2++)
+#pragma unroll
+          for(int c2 = 0; c2 < 3; c2++)
+            s = fma(K.k[row * 24 + 12 + q2 * 3 + c2], ut[c2][q2], s);
+        acc[c][q] = fma(Ee, s, carry[c][q]);
+      }
+    if(ek >= Z0)
+    {
+      T A[3];
+      const int buf = ek & 1;
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        A[c] = acc[c][lnode(1, 1)] + __shfl_down_sync(0xffffffffu, acc[c][lnode(0, 1)], 1);
+        sB[buf][c][ly][lx] =
+            acc[c][lnode(1, 0)] + __shfl_down_sync(0xffffffffu, acc[c][lnode(0, 0)], 1);
+      }
+      __syncthreads();
+      const int ni = ei + 1, nj = ej + 1;
+      if(lx < TX - 1 && ly < TY3 - 1 && ni < d.sx && nj < d.sy)
+      {
+        const long long node = (long long)ni + (long long)nj * d.sx + (long long)ek * sxy;
+        const unsigned f = __ldg(fix + node);
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          T o = A[c] + sB[buf][c][ly + 1][lx];
+          if((f >> c) & 1u)
+            o = T(0);
+          // the node's own input value: read it here, the thread owning this
+          // node may be a halo column (i = 0 or j = 0) with no element
+          T us = T(0);
+          if(DOT || MODE >= OP_JACOBI)
+            us = __ldg(u + c * ld + node);
+          if(DOT)
+            dot += double(us) * double(o);
+          y[c * ld + node] = epilogue<T, MODE>(o, us, c * ld + node, ep);
+        }
+      }
+    }
+    // rows of the top corners: carried to plane ek+1
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const int row = 12 + q * 3 + c;
+        T s = T(0);
+#pragma unroll
+        for(int q2 = 0; q2 < 4; q2++)
+#pragma unroll
+          for(int c2 = 0; c2 < 3; c2++)
+            s = fma(K.k[row * 24 + q2 * 3 + c2], ub[c2][q2], s);
+#pragma unroll
+        for(int q2 = 0; q2 < 4; q2++)
+#pragma unroll
+          for(int c2 = 0; c2 < 3; c2++)
+            s = fma(K.k[row * 24 + 12 + q2 * 3 + c2], ut[c2][q2], s);
+        carry[c][q] = Ee * s;
+      }
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+        ub[c][q] = ut[c][q];
+  }
+  if(DOT)
+  {
+    double v[1] = {dot};
+    block_reduce<1>(v, red, FinStore{dotOut});
+  }
+}
+
+// ------------------------------------------------------------------- Q4 ----
+template <typename T, bool DOT, int MODE>
+__global__ void __launch_bounds__(TX *TY2)
+    k_matvec_q4(const KMat<T, 8> K, const Dims d, const int ychunk,
+                const T *__restrict__ E, const T *__restrict__ u, T *__restrict__ y,
+                const uint8_t *__restrict__ fix, RedScratch red, double *dotOut,
+                const KState *gate, const int gateConv, const Epi<T> ep)
+{
+  if(gate && (gate->stop || (gateConv && gate->conv)))
+    return;
+  const int lx = threadIdx.x, w = threadIdx.y;
+  const int X0 = (blockIdx.x * TY2 + w) * (TX - 1);
+  const int ei = X0 - 1 + lx;
+  const int Y0 = blockIdx.y * ychunk;
+  const int Y1 = min(Y0 + ychunk, d.sy) - 1;
+  const bool col = ei >= 0 && ei < d.nx;
+  const long long ld = d.ld;
+  T ub[2][2], ut[2][2], carry[2][2];
+#pragma unroll
+  for(int c = 0; c < 2; c++)
+#pragma unroll
+    for(int a = 0; a < 2; a++)
+    {
+      carry[c][a] = T(0);
+      ub[c][a] = T(0);
+    }
+  if(col && Y0 - 1 >= 0)
+  {
+    long long base = ei + (long long)(Y0 - 1) * d.sx;
+#pragma unroll
+    for(int c = 0; c < 2; c++)
+#pragma unroll
+      for(int a = 0; a < 2; a++)
+        ub[c][a] = __ldg(u + c * ld + base + a);
+  }
+  double dot = 0.0;
+  for(int ej = Y0 - 1; ej <= Y1; ++ej)
+  {
+    const bool lay = col && ej >= 0 && ej < d.ny;
+    const bool topok = col && ej + 1 >= 0 && ej + 1 <= d.ny;
+#pragma unroll
+    for(int c = 0; c < 2; c++)
+#pragma unroll
+      for(int a = 0; a < 2; a++)
+        ut[c][a] = topok ? __ldg(u + c * ld + ei + (long long)(ej + 1) * d.sx + a) : T(0);
+    const T Ee = lay ? __ldg(E + (long long)ei + (long long)ej * d.nx) : T(0);
+    // element vector in local order: n0=(0,0) n1=(1,0) n2=(1,1) n3=(0,1)
+    T ue[8];
+#pragma unroll
+    for(int c = 0; c < 2; c++)
+    {
+      ue[0 * 2 + c] = ub[c][0];
+      ue[1 * 2 + c] = ub[c][1];
+      ue[2 * 2 + c] = ut[c][1];
+      ue[3 * 2 + c] = ut[c][0];
+    }
+    T acc[2][2];
+#pragma unroll
+    for(int a = 0; a < 2; a++)
+#pragma unroll
+      for(int c = 0; c < 2; c++)
+      {
+        const int row = lnode(a, 0) * 2 + c;
+        T s = T(0);
+#pragma unroll
+        for(int j = 0; j < 8; j++)
+          s = fma(K.k[row * 8 + j], ue[j], s);
+        acc[c][a] = fma(Ee, s, carry[c][a]);
+      }
+    if(ej >= Y0)
+    {
+      const int ni = ei + 1;
+      T o[2];
+#pragma unroll
+      for(int c = 0; c < 2; c++)
+        o[c] = acc[c][1] + __shfl_down_sync(0xffffffffu, acc[c][0], 1);
+      if(lx < TX - 1 && ni < d.sx && X0 < d.sx)
+      {
+        const long long node = (long long)ni + (long long)ej * d.sx;
+        const unsigned f = __ldg(fix + node);
+#pragma unroll
+        for(int c = 0; c < 2; c++)
+        {
+          T v = ((f >> c) & 1u) ? T(0) : o[c];
+          T us = T(0);
+          if(DOT || MODE >= OP_JACOBI)
+            us = __ldg(u + c * ld + node); // node i = 0 belongs to a halo column
+          if(DOT)
+            dot += double(us) * double(v);
+          y[c * ld + node] = epilogue<T, MODE>(v, us, c * ld + node, ep);
+        }
+      }
+    }
+#pragma unroll
+    for(int a = 0; a < 2; a++)
+#pragma unroll
+      for(int c = 0; c < 2; c++)
+      {
+        const int row = lnode(a, 1) * 2 + c;
+        T s = T(0);
+#pragma unroll
+        for(int j = 0; j < 8; j++)
+          s = fma(K.k[row * 8 + j], ue[j], s);
+        carry[c][a] = Ee * s;
+      }
+#pragma unroll
+    for(int c = 0; c < 2; c++)
+#pragma unroll
+      for(int a = 0; a < 2; a++)
+        ub[c][a] = ut[c][a];
+  }
+  if(DOT)
+  {
+    double v[1] = {dot};
+    block_reduce<1>(v, red, FinStore{dotOut});
+  }
+}
+
+// ------------------------------------------------------------ diagonal ----
+template <typename T, int DIM>
+__global__ void k_diag(const KMat<T, 24> K, const Dims d, const T *__restrict__ E,
+                       const uint8_t *__restrict__ fix, T *__restrict__ invdiag,
+                       T *__restrict__ diag)
+{
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(n >= d.nnode)
+    return;
+  const int nd = DIM == 2 ? 8 : 24;
+  long long sxy = (long long)d.sx * d.sy;
+  int i = int(n % d.sx), j = int((n / d.sx) % d.sy), k = DIM == 3 ? int(n / sxy) : 0;
+  double s[3] = {0, 0, 0};
+  for(int dk = (DIM == 3 ? -1 : 0); dk <= 0; dk++)
+    for(int dj = -1; dj <= 0; dj++)
+      for(int di = -1; di <= 0; di++)
+      {
+        int ei = i + di, ej = j + dj, ek = k + dk;
+        if(ei < 0 || ej < 0 || ek < 0 || ei >= d.nx || ej >= d.ny || (DIM == 3 && ek >= d.nz))
+          continue;
+        long long e = ei + (long long)ej * d.nx + (long long)ek * d.nx * d.ny;
+        int l = lnode(-di, -dj) + (DIM == 3 ? 4 * (-dk) : 0);
+        double Ee = E[e];
+        for(int c = 0; c < DIM; c++)
+          s[c] += Ee * double(K.k[(l * DIM + c) * nd + l * DIM + c]);
+      }
+  unsigned f = fix[n];
+  for(int c = 0; c < DIM; c++)
+  {
+    bool fx = (f >> c) & 1u;
+    if(diag)
+      diag[c * d.ld + n] = fx ? T(0) : T(s[c]);
+    // Eigen's DiagonalPreconditioner: 1 where the diagonal is 0
+    invdiag[c * d.ld + n] = fx ? T(0) : (s[c] != 0.0 ? T(1.0 / s[c]) : T(1));
+  }
+}
+
+__global__ void k_gather_free(long long numeq, const long long *__restrict__ idx,
+                              const double *__restrict__ soa, double *__restrict__ out)
+{
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(i < numeq)
+    out[i] = soa[idx[i]];
+}
+__global__ void k_scatter_free(long long numeq, const long long *__restrict__ idx,
+                               const double *__restrict__ in, double *__restrict__ soa)
+{
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(i < numeq)
+    soa[idx[i]] = in[i];
+}
+
+/// SIMP of src/problem/elasticity.hpp:15-22
+__global__ void k_simp(long long n, double y1, double y2, double p,
+                       const double *__restrict__ rho, double *__restrict__ E,
+                       float *__restrict__ Ef)
+{
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(i >= n)
+    return;
+  double s = rho[i], v;
+  if(y2 - y1 >= 0.0)
+    v = (1.0 - pow(s, p)) * y1 + pow(s, p) * y2;
+  else
+    v = pow(1.0 - s, p) * y1 + (1.0 - pow(1.0 - s, p)) * y2;
+  E[i] = v;
+  if(Ef)
+    Ef[i] = float(v);
+}
+
+/// sensitivity() of opt_macro_oc.cpp:182-207 / opt_mma_Helmholtz.cpp:173-205:
+/// dc_e = -(E'/E) u_e^T (E K0) u_e, u from the node values with |u| < 1e-15
+/// zeroed as divideValIntoNode does.
+template <int DIM>
+__global__ void k_sensitivity(const KMat<double, 24> K, const Dims d, double y1, double y2,
+                              double p, const double *__restrict__ rho,
+                              const double *__restrict__ u, double *__restrict__ dc)
+{
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(e >= d.nel)
+    return;
+  constexpr int NE = DIM == 2 ? 4 : 8, ND = NE * DIM;
+  int ei = int(e % d.nx), ej = int((e / d.nx) % d.ny);
+  int ek = DIM == 3 ? int(e / ((long long)d.nx * d.ny)) : 0;
+  long long base = ei + (long long)ej * d.sx + (long long)ek * d.sx * d.sy;
+  long long sxy = (long long)d.sx * d.sy;
+  double ue[ND];
+#pragma unroll
+  for(int l = 0; l < NE; l++)
+  {
+    int q = l & 3, top = l >> 2;
+    long long off = (q == 1 || q == 2 ? 1 : 0) + (q >= 2 ? (long long)d.sx : 0) + top * sxy;
+#pragma unroll
+    for(int c = 0; c < DIM; c++)
+    {
+      double v = u[c * d.ld + base + off];
+      ue[l * DIM + c] = fabs(v) < 1.0e-15 ? 0.0 : v;
+    }
+  }
+  double s = rho[e], young, dyoung;
+  if(y2 >= y1)
+  {
+    young = (1.0 - pow(s, p)) * y1 + pow(s, p) * y2;
+    dyoung = p * pow(s, p - 1.0) * (y2 - y1);
+  }
+  else
+  {
+    young = pow(1.0 - s, p) * y1 + (1.0 - pow(1.0 - s, p)) * y2;
+    dyoung = (y2 - y1) * p * pow(1.0 - s, p - 1.0);
+  }
+  double q = 0.0;
+#pragma unroll
+  for(int i = 0; i < ND; i++)
+  {
+    double t = 0.0;
+#pragma unroll
+    for(int j = 0; j < ND; j++)
+      t = fma(young * K.k[i * ND + j], ue[j], t);
+    q = fma(ue[i], t, q);
+  }
+  dc[e] = -(dyoung / young) * q;
+}
+
+inline unsigned blocks_for(long long n, int bs) { return unsigned((n + bs - 1) / bs); }
+} // namespace
+
+Dims make_dims(int dim, int nx, int ny, int nz)
+{
+  Dims d;
+  d.dim = dim;
+  d.nx = nx;
+  d.ny = ny;
+  d.nz = dim == 3 ? nz : 1;
+  d.sx = nx + 1;
+  d.sy = ny + 1;
+  d.sz = dim == 3 ? nz + 1 : 1;
+  d.nnode = (long long)d.sx * d.sy * d.sz;
+  d.nel = (long long)d.nx * d.ny * d.nz;
+  d.ld = (d.nnode + 63) / 64 * 64;
+  return d;
+}
+
+int num_sms()
+{
+  static int n = 0;
+  if(!n)
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if(n <= 0)
+      n = 148;
+  }
+  return n;
+}
+
+int matvec_blocks(const Dims &d)
+{
+  const int target = num_sms() * 4;
+  if(d.dim == 3)
+  {
+    int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TY3 - 2) / (TY3 - 1);
+    int bz = std::max(1, std::min(d.sz, (target + bx * by - 1) / (bx * by)));
+    int zchunk = (d.sz + bz - 1) / bz;
+    return bx * by * ((d.sz + zchunk - 1) / zchunk);
+  }
+  int strips = (d.sx + TX - 2) / (TX - 1);
+  int bx = (strips + TY2 - 1) / TY2;
+  int by = std::max(1, std::min(d.sy, (target + bx - 1) / bx));
+  int ychunk = (d.sy + by - 1) / by;
+  return bx * ((d.sy + ychunk - 1) / ychunk);
+}
+
+template <typename T, int MODE>
+static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T *y,
+                           const uint8_t *fix, cudaStream_t s, const OpExtras<T> &x)
+{
+  RedScratch red = x.dotRed ? *x.dotRed : RedScratch{};
+  const int target = num_sms() * 4;
+  Epi<T> ep{x.b, x.dinv, T(x.omega), x.d, T(x.c1), T(x.c2)};
+  if(d.dim == 3)
+  {
+    KMat<T, 24> km;
+    std::copy(K, K + 576, km.k);
+    int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TY3 - 2) / (TY3 - 1);
+    int bz = std::max(1, std::min(d.sz, (target + bx * by - 1) / (bx * by)));
+    int zchunk = (d.sz + bz - 1) / bz;
+    bz = (d.sz + zchunk - 1) / zchunk;
+    dim3 grid(bx, by, bz), block(TX, TY3);
+    if(x.dotRed)
+    {
+      ICB_REQUIRE(bx * by * bz <= red.maxBlocks, "reduction scratch too small");
+      k_matvec_h8<T, true, MODE><<<grid, block, 0, s>>>(km, d, zchunk, E, u, y, fix, red,
+                                                        x.dotOut, x.gate, x.gateConv, ep);
+    }
+    else
+      k_matvec_h8<T, false, MODE><<<grid, block, 0, s>>>(km, d, zchunk, E, u, y, fix, red,
+                                                         x.dotOut, x.gate, x.gateConv, ep);
+  }
+  else
+  {
+    KMat<T, 8> km;
+    std::copy(K, K + 64, km.k);
+    int strips = (d.sx + TX - 2) / (TX - 1);
+    int bx = (strips + TY2 - 1) / TY2;
+    int by = std::max(1, std::min(d.sy, (target + bx - 1) / bx));
+    int ychunk = (d.sy + by - 1) / by;
+    by = (d.sy + ychunk - 1) / ychunk;
+    dim3 grid(bx, by), block(TX, TY2);
+    if(x.dotRed)
+    {
+      ICB_REQUIRE(bx * by <= red.maxBlocks, "reduction scratch too small");
+      k_matvec_q4<T, true, MODE><<<grid, block, 0, s>>>(km, d, ychunk, E, u, y, fix, red,
+                                                        x.dotOut, x.gate, x.gateConv, ep);
+    }
+    else
+      k_matvec_q4<T, false, MODE><<<grid, block, 0, s>>>(km, d, ychunk, E, u, y, fix, red,
+                                                         x.dotOut, x.gate, x.gateConv, ep);
+  }
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+template <typename T>
+void launch_op(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,
+               cudaStream_t s, const OpExtras<T> &x)
+{
+  if(x.mode == OP_APPLY)
+    launch_op_mode<T, OP_APPLY>(d, K, E, u, y, fix, s, x);
+  else if(x.mode == OP_RESIDUAL)
+    launch_op_mode<T, OP_RESIDUAL>(d, K, E, u, y, fix, s, x);
+  else if(x.mode == OP_JACOBI)
+    launch_op_mode<T, OP_JACOBI>(d, K, E, u, y, fix, s, x);
+  else
+    launch_op_mode<T, OP_CHEB>(d, K, E, u, y, fix, s, x);
+}
+template void launch_op<double>(const Dims &, const double *, const double *, const double *,
+                                double *, const uint8_t *, cudaStream_t,
+                                const OpExtras<double> &);
+template void launch_op<float>(const Dims &, const float *, const float *, const float *,
+                               float *, const uint8_t *, cudaStream_t, const OpExtras<float> &);
+
+template <typename T>
+void launch_matvec(const Dims &d, const T *K, const T *E, const T *u, T *y,
+                   const uint8_t *fix, cudaStream_t s, RedScratch *dotRed, double *dotOut,
+                   const KState *gate)
+{
+  OpExtras<T> x;
+  x.dotRed = dotRed;
+  x.dotOut = dotOut;
+  x.gate = gate;
+  launch_op<T>(d, K, E, u, y, fix, s, x);
+}
+template void launch_matvec<double>(const Dims &, const double *, const double *,
+                                    const double *, double *, const uint8_t *, cudaStream_t,
+                                    RedScratch *, double *, const KState *);
+template void launch_matvec<float>(const Dims &, const float *, const float *, const float *,
+                                   float *, const uint8_t *, cudaStream_t, RedScratch *,
+                                   double *, const KState *);
+
+template <typename T>
+void launch_diag(const Dims &d, const T *K, const T *E, const uint8_t *fix, T *invdiag,
+                 T *diag, cudaStream_t s)
+{
+  KMat<T, 24> km;
+  int nd = d.dim == 2 ? 8 : 24;
+  std::copy(K, K + nd * nd, km.k);
+  if(d.dim == 3)
+    k_diag<T, 3><<<blocks_for(d.nnode, 256), 256, 0, s>>>(km, d, E, fix, invdiag, diag);
+  else
+    k_diag<T, 2><<<blocks_for(d.nnode, 256), 256, 0, s>>>(km, d, E, fix, invdiag, diag);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+template void launch_diag<double>(const Dims &, const double *, const double *,
+                                  const uint8_t *, double *, double *, cudaStream_t);
+template void launch_diag<float>(const Dims &, const float *, const float *, const uint8_t *,
+                                 float *, float *, cudaStream_t);
+
+void launch_gather_free(const Dims &d, const long long *freeIdx, long long numeq,
+                        const double *soa, double *numeqv, cudaStream_t s)
+{
+  (void)d;
+  if(numeq)
+    k_gather_free<<<blocks_for(numeq, 256), 256, 0, s>>>(numeq, freeIdx, soa, numeqv);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+void launch_scatter_free(const Dims &d, const long long *freeIdx, long long numeq,
+                         const double *numeqv, double *soa, cudaStream_t s)
+{
+  (void)d;
+  if(numeq)
+    k_scatter_free<<<blocks_for(numeq, 256), 256, 0, s>>>(numeq, freeIdx, numeqv, soa);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+void launch_simp(long long n, double y1, double y2, double p, const double *rho, double *E,
+                 float *Ef, cudaStream_t s)
+{
+  k_simp<<<blocks_for(n, 256), 256, 0, s>>>(n, y1, y2, p, rho, E, Ef);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+void launch_sensitivity(const Dims &d, const double *K, double y1, double y2, double p,
+                        const double *rho, const double *u, double *dc, cudaStream_t s)
+{
+  KMat<double, 24> km;
+  int nd = d.dim == 2 ? 8 : 24;
+  std::copy(K, K + nd * nd, km.k);
+  if(d.dim == 3)
+    k_sensitivity<3><<<blocks_for(d.nel, 128), 128, 0, s>>>(km, d, y1, y2, p, rho, u, dc);
+  else
+    k_sensitivity<2><<<blocks_for(d.nel, 128), 128, 0, s>>>(km, d, y1, y2, p, rho, u, dc);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+} // namespace icb

@@ -1,0 +1,97 @@
+// reduce.cuh -- deterministic grid-wide reductions without a second launch.
+//
+// Every block reduces its values (warp shuffles, then shared memory) and
+// writes them to red.partials[block]; the block that finishes last (atomic
+// ticket) sums all partials in block order and hands the totals to a
+// finisher functor run by its thread 0.  The summation order depends only on
+// the launch shape, so results are bitwise reproducible run to run.
+#pragma once
+#include "icb_internal.hpp"
+
+namespace icb
+{
+
+__device__ __forceinline__ double warp_sum_d(double v)
+{
+#pragma unroll
+  for(int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int NV, class Fin>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], const RedScratch &red,
+                                             Fin fin)
+{
+  __shared__ double sw[32][NV];
+  __shared__ int last;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nth = blockDim.x * blockDim.y * blockDim.z;
+  const int nw = (nth + 31) >> 5;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  const int nb = gridDim.x * gridDim.y * gridDim.z;
+#pragma unroll
+  for(int k = 0; k < NV; k++)
+    v[k] = warp_sum_d(v[k]);
+  if((tid & 31) == 0)
+#pragma unroll
+    for(int k = 0; k < NV; k++)
+      sw[tid >> 5][k] = v[k];
+  __syncthreads();
+  if(tid == 0)
+  {
+#pragma unroll
+    for(int k = 0; k < NV; k++)
+    {
+      double s = 0.0;
+      for(int w = 0; w < nw; w++)
+        s += sw[w][k];
+      red.partials[(long long)bid * NV + k] = s;
+    }
+    __threadfence();
+    unsigned t = atomicAdd(red.counter, 1u);
+    last = (t == unsigned(nb - 1));
+  }
+  __syncthreads();
+  if(!last)
+    return;
+  __threadfence();
+  double s[NV];
+#pragma unroll
+  for(int k = 0; k < NV; k++)
+    s[k] = 0.0;
+  for(int b = tid; b < nb; b += nth)
+#pragma unroll
+    for(int k = 0; k < NV; k++)
+      s[k] += __ldcg(red.partials + (long long)b * NV + k);
+#pragma unroll
+  for(int k = 0; k < NV; k++)
+    s[k] = warp_sum_d(s[k]);
+  __syncthreads();
+  if((tid & 31) == 0)
+#pragma unroll
+    for(int k = 0; k < NV; k++)
+      sw[tid >> 5][k] = s[k];
+  __syncthreads();
+  if(tid == 0)
+  {
+    double tot[NV];
+#pragma unroll
+    for(int k = 0; k < NV; k++)
+    {
+      tot[k] = 0.0;
+      for(int w = 0; w < nw; w++)
+        tot[k] += sw[w][k];
+    }
+    *red.counter = 0u;
+    fin(tot);
+  }
+}
+
+struct FinStore
+{
+  double *out;
+  __device__ void operator()(const double *t) const { *out = t[0]; }
+};
+
+} // namespace icb

@@ -1,0 +1,290 @@
+"""ctypes binding of libicarat_b200.so (the C ABI in include/icarat_b200.h).
+
+This is the thin layer the tests, the smoke check and bench.py drive the
+library through; every call goes through the exported C entry points.  There
+is no fallback: if the shared library is missing or no CUDA device is present
+the calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.dirname(os.path.dirname(_HERE))  # icarat-contact_b200/
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libicarat_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "icarat_b200.h")
+
+FP64, MIXED = 0, 1
+JACOBI, GMG = 0, 1
+PLANE_STRESS, PLANE_STRAIN, THREE_D = 0, 1, 2
+STATUS = {0: "OK", -1: "BAD_ARG", -2: "OOM", -3: "BREAKDOWN", -4: "MAXITER", -5: "TIMEOUT",
+          -6: "NAN", -7: "CUDA", -8: "STATE", -9: "REJECTED"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u8p = C.POINTER(C.c_uint8)
+_llp = C.POINTER(C.c_longlong)
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("state", C.c_int), ("young1", C.c_double), ("young2", C.c_double),
+                ("poisson", C.c_double), ("penalty", C.c_double)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("precond", C.c_int), ("tol", C.c_double),
+                ("maxit", C.c_int), ("inner_tol", C.c_double), ("mg_smooth", C.c_int),
+                ("mg_coarse_dofs", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iters", C.c_int), ("matvecs", C.c_int), ("outer", C.c_int),
+                ("relres", C.c_double), ("true_relres", C.c_double), ("seconds", C.c_double),
+                ("status", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class IcbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+# exported symbol -> (restype, argtypes); every name declared in the header
+_SIGS = {
+    "icb_last_error": (C.c_char_p, []),
+    "icb_version": (C.c_char_p, []),
+    "icb_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "icb_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "icb_ctx_stream": (C.c_void_p, [C.c_void_p]),
+    "icb_ctx_synchronize": (C.c_int, [C.c_void_p]),
+    "icb_problem_create": (C.c_int, [C.c_void_p, C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
+    "icb_problem_destroy": (C.c_int, [C.c_void_p]),
+    "icb_dirichlet_box": (C.c_int, [C.c_void_p, _ip, _dp, _dp]),
+    "icb_dirichlet_mask": (C.c_int, [C.c_void_p, _u8p, _dp]),
+    "icb_traction_box": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "icb_nodal_load": (C.c_int, [C.c_void_p, C.c_longlong, _dp]),
+    "icb_finalize": (C.c_int, [C.c_void_p, _llp]),
+    "icb_get_dof_map": (C.c_int, [C.c_void_p, _ip]),
+    "icb_get_load": (C.c_int, [C.c_void_p, _dp]),
+    "icb_problem_sizes": (C.c_int, [C.c_void_p, _llp, _llp, _llp, _llp]),
+    "icb_get_K0": (C.c_int, [C.c_void_p, _dp]),
+    "icb_element_volume": (C.c_int, [C.c_void_p, _dp]),
+    "icb_set_density": (C.c_int, [C.c_void_p, _dp]),
+    "icb_set_density_device": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "icb_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+    "icb_get_displacement": (C.c_int, [C.c_void_p, _dp]),
+    "icb_get_node_values": (C.c_int, [C.c_void_p, _dp]),
+    "icb_compliance": (C.c_int, [C.c_void_p, _dp]),
+    "icb_sensitivity": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "icb_sensitivity_device": (C.c_void_p, [C.c_void_p]),
+    "icb_matvec": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "icb_diagonal": (C.c_int, [C.c_void_p, _dp]),
+    "icb_soa_length": (C.c_longlong, [C.c_void_p]),
+    "icb_operator_apply_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "icb_launch_count": (C.c_longlong, []),
+}
+
+
+def lib():
+    """Load the shared library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} not built: run python icarat-contact_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def launch_count():
+    return lib().icb_launch_count()
+
+
+def header_symbols():
+    """Function names declared in include/icarat_b200.h."""
+    import re
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(icb_[a-z0-9_]+)\s*\(", txt)))
+
+
+def check(rc):
+    if rc != 0:
+        raise IcbError(rc, lib().icb_last_error().decode())
+    return rc
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class Context:
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        check(lib().icb_ctx_create(device, C.byref(h)))
+        self.h = h
+
+    def stream(self):
+        return lib().icb_ctx_stream(self.h)
+
+    def synchronize(self):
+        check(lib().icb_ctx_synchronize(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().icb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Problem:
+    """A structured SIMP problem on the device (the LinearAnalysis equivalent)."""
+
+    def __init__(self, ctx, dim, nx, ny, nz=1, lx=None, ly=None, lz=None, state=None,
+                 young=(1e-9, 1.0), nu=0.3, penal=3.0):
+        self.ctx = ctx
+        self.dim = dim
+        self.desc = GridDesc(dim, nx, ny, nz if dim == 3 else 1,
+                             float(nx if lx is None else lx), float(ny if ly is None else ly),
+                             float((nz if dim == 3 else 1) if lz is None else lz),
+                             (THREE_D if dim == 3 else PLANE_STRESS) if state is None else state,
+                             float(young[0]), float(young[1]), float(nu), float(penal))
+        h = C.c_void_p()
+        check(lib().icb_problem_create(ctx.h, C.byref(self.desc), C.byref(h)))
+        self.h = h
+        nel, nn, neq, ne = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_longlong()
+        check(lib().icb_problem_sizes(self.h, C.byref(nel), C.byref(nn), C.byref(neq), C.byref(ne)))
+        self.nel, self.nnode, self.neq = nel.value, nn.value, neq.value
+        self.numeq = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().icb_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # set-up -------------------------------------------------------------
+    def dirichlet_box(self, flag, val, rng):
+        f = np.asarray(list(flag) + [0] * (6 - len(flag)), np.int32)
+        v = np.asarray(list(val) + [0.0] * (6 - len(val)), np.float64)
+        r = np.asarray(rng, np.float64).reshape(6)
+        check(lib().icb_dirichlet_box(self.h, _p(f, _ip), _p(v), _p(r)))
+
+    def dirichlet_mask(self, fixed, val=None):
+        f = np.ascontiguousarray(fixed, np.uint8)
+        v = None if val is None else _p(np.ascontiguousarray(val, np.float64))
+        check(lib().icb_dirichlet_mask(self.h, _p(f, _u8p), v))
+
+    def traction_box(self, val, rng):
+        v = np.zeros(3)
+        v[:len(val)] = val
+        r = np.asarray(rng, np.float64).reshape(6)
+        check(lib().icb_traction_box(self.h, _p(v), _p(r)))
+
+    def nodal_load(self, node, f):
+        v = np.zeros(3)
+        v[:len(f)] = f
+        check(lib().icb_nodal_load(self.h, int(node), _p(v)))
+
+    def finalize(self):
+        ne = C.c_longlong()
+        check(lib().icb_finalize(self.h, C.byref(ne)))
+        self.numeq = ne.value
+        return self.numeq
+
+    def dof_map(self):
+        d = np.zeros(self.neq, np.int32)
+        check(lib().icb_get_dof_map(self.h, _p(d, _ip)))
+        return d
+
+    def load(self):
+        f = np.zeros(self.numeq)
+        check(lib().icb_get_load(self.h, _p(f)))
+        return f
+
+    def K0(self):
+        nd = self.dim * (4 if self.dim == 2 else 8)
+        K = np.zeros((nd, nd))
+        check(lib().icb_get_K0(self.h, _p(K)))
+        return K
+
+    def element_volume(self):
+        v = C.c_double()
+        check(lib().icb_element_volume(self.h, C.byref(v)))
+        return v.value
+
+    # analysis -----------------------------------------------------------
+    def set_density(self, rho):
+        r = np.ascontiguousarray(rho, np.float64)
+        assert r.size == self.nel
+        check(lib().icb_set_density(self.h, _p(r)))
+
+    def set_density_device(self, ptr):
+        check(lib().icb_set_density_device(self.h, C.c_void_p(ptr)))
+
+    def solve(self, precision=FP64, precond=JACOBI, tol=1e-10, maxit=10000, inner_tol=0.0,
+              mg_smooth=0, mg_coarse_dofs=0, raise_on_error=True):
+        o = SolveOpts(precision, precond, tol, maxit, inner_tol, mg_smooth, mg_coarse_dofs)
+        info = SolveInfo()
+        rc = lib().icb_solve(self.h, C.byref(o), C.byref(info))
+        if raise_on_error:
+            check(rc)
+        d = info.as_dict()
+        d["rc"] = rc
+        return d
+
+    def displacement(self):
+        u = np.zeros(self.numeq)
+        check(lib().icb_get_displacement(self.h, _p(u)))
+        return u
+
+    def node_values(self):
+        v = np.zeros(self.neq)
+        check(lib().icb_get_node_values(self.h, _p(v)))
+        return v
+
+    def compliance(self):
+        c = C.c_double()
+        check(lib().icb_compliance(self.h, C.byref(c)))
+        return c.value
+
+    def sensitivity(self, with_dv=False):
+        dc = np.zeros(self.nel)
+        dv = np.zeros(self.nel) if with_dv else None
+        check(lib().icb_sensitivity(self.h, _p(dc), None if dv is None else _p(dv)))
+        return (dc, dv) if with_dv else dc
+
+    def matvec(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.numeq)
+        check(lib().icb_matvec(self.h, _p(x), _p(y)))
+        return y
+
+    def soa_length(self):
+        return lib().icb_soa_length(self.h)
+
+    def operator_apply_device(self, x_ptr, y_ptr, precision=FP64):
+        check(lib().icb_operator_apply_device(self.h, precision, C.c_void_p(x_ptr), C.c_void_p(y_ptr)))
+
+    def diagonal(self):
+        d = np.zeros(self.numeq)
+        check(lib().icb_diagonal(self.h, _p(d)))
+        return d

@@ -1,0 +1,176 @@
+/*
+ * icarat_b200.h -- C ABI of the B200-native SIMP analysis-and-sensitivity
+ * library (libicarat_b200.so).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes
+ * (0 = ok, negative = error; icb_last_error() gives the message).  Every
+ * entry point names the ICARAT interface it replaces (path inside the ICARAT
+ * project, file:line).  Arrays follow ICARAT's layouts:
+ *   - element arrays: element index of MeshIcarat::meshBox
+ *     (src/io/mesh_icarat.hpp:340-354 quad4, 459-493 hexa8);
+ *   - "neq" arrays: node-major, components interleaved (node*dim + c);
+ *   - "numeq" arrays: free DOFs in countDOF order
+ *     (src/io/boundary_condition_base.hpp:35-88), i.e. Value::val / Force.
+ * Host-pointer entry points copy through pinned staging; *_device entry points
+ * take device pointers on the context's device and stream.
+ */
+#ifndef ICARAT_B200_H
+#define ICARAT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define ICB_OK 0
+#define ICB_ERR_BAD_ARG (-1)
+#define ICB_ERR_OOM (-2)
+#define ICB_ERR_BREAKDOWN (-3)
+#define ICB_ERR_MAXITER (-4)
+#define ICB_ERR_TIMEOUT (-5)
+#define ICB_ERR_NAN (-6)
+#define ICB_ERR_CUDA (-7)
+#define ICB_ERR_STATE (-8)
+#define ICB_ERR_REJECTED (-9)
+
+/* ---- enums ------------------------------------------------------------- */
+#define ICB_PLANE_STRESS 0
+#define ICB_PLANE_STRAIN 1
+#define ICB_3D 2
+
+#define ICB_FP64 0  /* plain FP64 path: the drop-in for Solvers "Eigen_CG"   */
+#define ICB_MIXED 1 /* FP64 Krylov + operator, FP32 multigrid preconditioner */
+
+#define ICB_PRECOND_JACOBI 0 /* DiagonalPreconditioner (solvers.cpp:64-92)  */
+#define ICB_PRECOND_GMG 1    /* geometric multigrid V-cycle                 */
+
+typedef struct icb_ctx_s *icb_ctx;
+typedef struct icb_problem_s *icb_problem;
+typedef struct icb_cone_s *icb_cone;
+typedef struct icb_helm_s *icb_helm;
+typedef struct icb_mma_s *icb_mma;
+
+/* Structured box problem: the `[mesh]` keys of MeshIcarat::setParameter
+ * (src/io/mesh_icarat.hpp:69-128) and the `[material]` keys of
+ * Elastic::setParameter (src/problem/elasticity.cpp:19-32). */
+typedef struct
+{
+  int dim;           /* 2 (quad4) or 3 (hexa8)                             */
+  int nx, ny, nz;    /* division                                           */
+  double lx, ly, lz; /* length                                             */
+  int state;         /* ICB_PLANE_STRESS | ICB_PLANE_STRAIN | ICB_3D       */
+  double young1;     /* young[0]  (E of rho = 0 when young[1] >= young[0]) */
+  double young2;     /* young[1]                                           */
+  double poisson;
+  double penalty;
+} icb_grid_desc;
+
+typedef struct
+{
+  int precision;  /* ICB_FP64 | ICB_MIXED                                   */
+  int precond;    /* ICB_PRECOND_JACOBI | ICB_PRECOND_GMG                   */
+  double tol;     /* relative residual ||r||/||f|| (Solvers tol_, 1e-10)    */
+  int maxit;      /* Solvers maxIter_ (10000)                               */
+  double inner_tol; /* reserved (0)                                       */
+  int mg_smooth;  /* GMG: Jacobi sweeps before and after (0 = default)      */
+  int mg_coarse_dofs; /* GMG: coarsen while the grid has more DOFs (0 = default) */
+} icb_solve_opts;
+
+typedef struct
+{
+  int iters;          /* Krylov iterations (Eigen's count: the converging one excluded) */
+  int matvecs;        /* fine-level operator applications in the Krylov loop(s) */
+  int outer;          /* Krylov cycles (1)                                  */
+  double relres;      /* ||r||/||f|| as the solver tracked it               */
+  double true_relres; /* ||f - K u|| / ||f|| recomputed in FP64             */
+  double seconds;     /* device time of the solve                           */
+  int status;         /* ICB_OK, ICB_ERR_MAXITER, ICB_ERR_BREAKDOWN, ...    */
+} icb_solve_info;
+
+const char *icb_last_error(void);
+const char *icb_version(void);
+
+/* ---- context ----------------------------------------------------------- */
+int icb_ctx_create(int device, icb_ctx *out);
+int icb_ctx_destroy(icb_ctx ctx);
+/* cudaStream_t the library launches on (for events / interop) */
+void *icb_ctx_stream(icb_ctx ctx);
+int icb_ctx_synchronize(icb_ctx ctx);
+
+/* ---- problem set-up ---------------------------------------------------- */
+/* MeshIcarat(fem, config).setParameter + generate + LinearElastic
+ * setParameter for every element (opt_mma_Helmholtz.cpp:31-50). */
+int icb_problem_create(icb_ctx ctx, const icb_grid_desc *desc, icb_problem *out);
+int icb_problem_destroy(icb_problem p);
+/* BCIcarat::input_dirich (src/io/boundary_condition_icarat.hpp:68-127):
+ * flag[6], val[6], range[6] = {xmin,xmax,ymin,ymax,zmin,zmax}, tol 1e-7. */
+int icb_dirichlet_box(icb_problem p, const int *flag, const double *val,
+                      const double *range);
+/* per-DOF Dirichlet flags (neq bytes) and values (neq, or NULL for 0) */
+int icb_dirichlet_mask(icb_problem p, const unsigned char *fixed, const double *val);
+/* BCIcarat::input_neumann / generateLoadMain / SurfaceLoad::generate
+ * (boundary_condition_icarat.hpp:253-396, boundary_condition_base.cpp:143-180):
+ * constant traction val[3] on element sides selected by the box range[6]. */
+int icb_traction_box(icb_problem p, const double *val, const double *range);
+/* nodal point load (extension: ICARAT's TOML cannot express point/line loads) */
+int icb_nodal_load(icb_problem p, long long node, const double *f);
+/* BCIcarat::makeDOF -> countDOF (boundary_condition_base.hpp:35-88), load
+ * assembly into Force::fext_org, upload to the device.  Returns numeq. */
+int icb_finalize(icb_problem p, long long *numeq);
+/* node[i].dof[j] of countDOF, neq ints */
+int icb_get_dof_map(icb_problem p, int *dof);
+/* Force::fext_org (numeq) */
+int icb_get_load(icb_problem p, double *fext);
+/* sizes: nelx, numnp, neq, numeq */
+int icb_problem_sizes(icb_problem p, long long *nel, long long *nnode, long long *neq,
+                      long long *numeq);
+/* unit-modulus element matrix K0 (Ke of LinearElastic::makeKeFint,
+ * elasticity.cpp:210-254, with E = 1), (d*ne)^2 row-major */
+int icb_get_K0(icb_problem p, double *K0);
+/* element volume: sum of Gauss jac (elasticity.cpp:249) */
+int icb_element_volume(icb_problem p, double *v);
+
+/* ---- analysis ---------------------------------------------------------- */
+/* Elastic::setDesignS for every element (elasticity.hpp:55): the physical
+ * (filtered, thresholded) density the stiffness uses. */
+int icb_set_density(icb_problem p, const double *rho);
+int icb_set_density_device(icb_problem p, const double *rho_dev);
+/* LinearAnalysis::solve(solvName, log) (src/analysis/linear.hpp:54-104)
+ * with Solvers::solve (src/analysis/solver/solvers.cpp:28-92): Dirichlet
+ * values, fres = fext - fint, K(rho) u = fres from u0 = 0 to
+ * ||r|| < tol ||fres||.  opts may be NULL (FP64, Jacobi, tol 1e-10). */
+int icb_solve(icb_problem p, const icb_solve_opts *opts, icb_solve_info *info);
+/* Value::val (numeq) */
+int icb_get_displacement(icb_problem p, double *u);
+/* node[].val after divideValIntoNode (analysis_utility.hpp:8-31), neq */
+int icb_get_node_values(icb_problem p, double *nodeval);
+/* value.val . force.fext (opt_macro_oc.cpp:110) */
+int icb_compliance(icb_problem p, double *c);
+/* sensitivity() of the apps (opt_macro_oc.cpp:182-207,
+ * opt_mma_Helmholtz.cpp:173-205): dc_e = -(E'/E) u_e^T Ke u_e; dv_e = v_e
+ * (dv may be NULL). */
+int icb_sensitivity(icb_problem p, double *dc, double *dv);
+/* device pointers (valid until the problem is destroyed) */
+const double *icb_sensitivity_device(icb_problem p);
+/* K(rho) x over free DOFs (numeq in, numeq out): the product globalK * x of
+ * the assembled LinearAnalysis::K() (linear.hpp:31), matrix-free. */
+int icb_matvec(icb_problem p, const double *x, double *y);
+/* the diagonal of K(rho) over free DOFs (numeq) */
+int icb_diagonal(icb_problem p, double *d);
+
+/* ---- device-level access (benchmarks, interop) --------------------------- */
+/* length of one SoA field vector on the device (dim * padded node count):
+ * component c of node n sits at c*ld + n, n in MeshIcarat numbering */
+long long icb_soa_length(icb_problem p);
+/* y = K(rho) x on device SoA vectors of icb_soa_length() entries; precision
+ * ICB_FP64 (double*) or ICB_MIXED (float*); one operator launch on the
+ * context's stream, no synchronisation.  Constrained rows of y are 0. */
+int icb_operator_apply_device(icb_problem p, int precision, const void *x, void *y);
+/* number of kernels this library has launched in the process (graph nodes
+ * counted one by one) */
+long long icb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

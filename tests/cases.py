@@ -1,0 +1,95 @@
+"""Problem builders shared by the tests and bench.py: the same boundary
+conditions, loads and seeded densities on the oracle and on the library.
+
+Workloads (sizes as stated; all inputs synthetic and seeded):
+  cantilever2d  120x40 unit Q4 plane stress, E0 = 1, Emin = 1e-9, nu = 0.3,
+                p = 3, x = 0 edge clamped, unit downward point load at the
+                right-edge mid node.
+  cantilever3d  192x64x64 unit Hex8, x = 0 face clamped, unit line load per
+                length in -z along the bottom edge (z = 0) of the x = L face:
+                0.5 on the two end nodes, 1.0 on the interior nodes.
+  halfmbb2d     2D half-MBB beam: ux = 0 on x = 0, uy = 0 at the bottom-right
+                node, unit downward load at the top-left node.
+  halfmbb3d     384x128x128 Hex8 half-MBB beam (ux = 0 on x = 0, uz = 0 on
+                the line x = L, z = 0, uy = 0 on y = 0; line load in -z along
+                x = 0, z = H).
+"""
+import numpy as np
+
+E0, EMIN, NU, PENAL = 1.0, 1e-9, 0.3, 3.0
+
+
+def _mask_cantilever2d(nx, ny):
+    fixed = np.zeros((ny + 1, nx + 1, 2), np.uint8)
+    fixed[:, 0, :] = 1
+    f = np.zeros((ny + 1, nx + 1, 2))
+    f[ny // 2, nx, 1] = -1.0
+    return fixed.reshape(-1), f.reshape(-1)
+
+
+def _mask_cantilever3d(nx, ny, nz):
+    fixed = np.zeros((nz + 1, ny + 1, nx + 1, 3), np.uint8)
+    fixed[:, :, 0, :] = 1
+    f = np.zeros((nz + 1, ny + 1, nx + 1, 3))
+    f[0, :, nx, 2] = -1.0
+    f[0, 0, nx, 2] = f[0, ny, nx, 2] = -0.5
+    return fixed.reshape(-1), f.reshape(-1)
+
+
+def _mask_halfmbb3d(nx, ny, nz):
+    fixed = np.zeros((nz + 1, ny + 1, nx + 1, 3), np.uint8)
+    fixed[:, :, 0, 0] = 1          # symmetry plane x = 0
+    fixed[0, :, nx, 2] = 1         # roller line x = L, z = 0
+    fixed[:, 0, :, 1] = 1          # y = 0 face
+    f = np.zeros((nz + 1, ny + 1, nx + 1, 3))
+    f[nz, :, 0, 2] = -1.0
+    f[nz, 0, 0, 2] = f[nz, ny, 0, 2] = -0.5
+    return fixed.reshape(-1), f.reshape(-1)
+
+
+def _mask_halfmbb2d(nx, ny):
+    fixed = np.zeros((ny + 1, nx + 1, 2), np.uint8)
+    fixed[:, 0, 0] = 1          # symmetry edge x = 0
+    fixed[0, nx, 1] = 1         # roller at the bottom-right corner
+    f = np.zeros((ny + 1, nx + 1, 2))
+    f[ny, 0, 1] = -1.0
+    return fixed.reshape(-1), f.reshape(-1)
+
+
+def masks(kind, nx, ny, nz=1):
+    if kind == "halfmbb2d":
+        return _mask_halfmbb2d(nx, ny)
+    if kind == "cantilever2d":
+        return _mask_cantilever2d(nx, ny)
+    if kind == "cantilever3d":
+        return _mask_cantilever3d(nx, ny, nz)
+    if kind == "halfmbb3d":
+        return _mask_halfmbb3d(nx, ny, nz)
+    raise ValueError(kind)
+
+
+def uniform_density(nel, seed, lo=0.01, hi=1.0):
+    return np.random.default_rng(seed).uniform(lo, hi, nel)
+
+
+def build_oracle(kind, nx, ny, nz=1):
+    import pyoracle as po
+    dim = 2 if kind.endswith("2d") else 3
+    p = po.Problem(dim, nx, ny, nz, young=(EMIN, E0), nu=NU, penal=PENAL)
+    fixed, f = masks(kind, nx, ny, nz)
+    p.fixed[:] = fixed
+    p.fext_full[:] = f
+    return p
+
+
+def build_gpu(ctx, kind, nx, ny, nz=1):
+    import icarat_b200 as icb
+    dim = 2 if kind.endswith("2d") else 3
+    p = icb.Problem(ctx, dim, nx, ny, nz, young=(EMIN, E0), nu=NU, penal=PENAL)
+    fixed, f = masks(kind, nx, ny, nz)
+    p.dirichlet_mask(fixed)
+    nodes = np.nonzero(np.abs(f.reshape(-1, dim)).sum(1))[0]
+    for n in nodes:
+        p.nodal_load(n, f.reshape(-1, dim)[n])
+    p.finalize()
+    return p

@@ -1,0 +1,251 @@
+"""Pins of the oracle (CPU only): closed forms, direct solves, ICARAT's own
+OC/MMA (golden vectors from oracle/_ref), the FDM procedure and the fixtures."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spl
+
+import pyoracle as po
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_q4_K0_matches_published_closed_form():
+    # Andreassen et al. (2011) 88-line code, plane stress, unit square, E = 1
+    nu = 0.3
+    A11 = np.array([[12, 3, -6, -3], [3, 12, 3, 0], [-6, 3, 12, -3], [-3, 0, -3, 12]])
+    A12 = np.array([[-6, -3, 0, 3], [-3, -6, -3, -6], [0, -3, -6, 3], [3, -6, 3, -6]])
+    B11 = np.array([[-4, 3, -2, 9], [3, -4, -9, 4], [-2, -9, -4, -3], [9, 4, -3, -4]])
+    B12 = np.array([[2, -3, 4, -9], [-3, 2, 9, -2], [4, 9, 2, 3], [-9, -2, 3, 2]])
+    KE = 1 / (1 - nu ** 2) / 24 * (np.block([[A11, A12], [A12.T, A11]]) +
+                                   nu * np.block([[B11, B12], [B12.T, B11]]))
+    K = po.Problem(2, 3, 3).K0()
+    assert np.abs(K - KE).max() < 1e-14
+
+
+def _rigid_modes_3d(h):
+    X = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                  [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float) * h
+    modes = []
+    for c in range(3):
+        m = np.zeros(24)
+        m[c::3] = 1
+        modes.append(m)
+    for a, b in [(0, 1), (1, 2), (2, 0)]:
+        m = np.zeros(24)
+        m[a::3] = -X[:, b]
+        m[b::3] = X[:, a]
+        modes.append(m)
+    return modes
+
+
+def test_h8_K0_analytic_properties():
+    nu = 0.3
+    K = po.Problem(3, 2, 2, 2).K0()
+    lam, mu = nu / ((1 + nu) * (1 - 2 * nu)), 1 / (2 * (1 + nu))
+    # K[0,0] = int (lam+2mu) (dN/dx)^2 + mu((dN/dy)^2+(dN/dz)^2) = (lam + 4 mu)/9
+    assert abs(K[0, 0] - (lam + 4 * mu) / 9) < 1e-15
+    assert np.abs(K - K.T).max() < 1e-15
+    for m in _rigid_modes_3d(np.array([1.0, 1.0, 1.0])):
+        assert np.abs(K @ m).max() < 1e-14
+    ev = np.linalg.eigvalsh(K)
+    assert (ev[:6] < 1e-12).all() and (ev[6:] > 1e-3).all()
+    # non-cubic element: rigid modes still in the null space
+    Kr = po.Problem(3, 2, 2, 2, lx=3.0, ly=1.0, lz=1.5).K0()
+    for m in _rigid_modes_3d(np.array([1.5, 0.5, 0.75])):
+        assert np.abs(Kr @ m).max() < 1e-13
+
+
+def test_h8_K0_against_independent_quadrature():
+    # 3-point Gauss integration in numpy of B^T D B (exact for these integrands)
+    nu, h = 0.3, np.array([1.2, 0.8, 2.0])
+    lam, mu = nu / ((1 + nu) * (1 - 2 * nu)), 1 / (2 * (1 + nu))
+    D = np.zeros((6, 6))
+    D[:3, :3] = lam
+    D[np.arange(3), np.arange(3)] += 2 * mu
+    D[3, 3] = D[4, 4] = D[5, 5] = mu
+    pts, wts = np.polynomial.legendre.leggauss(3)
+    corners = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                        [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+    K = np.zeros((24, 24))
+    for i, xi in enumerate(pts):
+        for j, et in enumerate(pts):
+            for k, ze in enumerate(pts):
+                r = np.array([xi, et, ze])
+                s = 2 * corners - 1
+                dN = np.zeros((3, 8))
+                for a in range(8):
+                    f = (1 + s[a] * r)
+                    dN[0, a] = s[a, 0] * f[1] * f[2] / 8 / (h[0] / 2)
+                    dN[1, a] = s[a, 1] * f[0] * f[2] / 8 / (h[1] / 2)
+                    dN[2, a] = s[a, 2] * f[0] * f[1] / 8 / (h[2] / 2)
+                B = np.zeros((6, 24))
+                for a in range(8):
+                    B[0, 3 * a] = dN[0, a]
+                    B[1, 3 * a + 1] = dN[1, a]
+                    B[2, 3 * a + 2] = dN[2, a]
+                    B[3, 3 * a], B[3, 3 * a + 1] = dN[1, a], dN[0, a]
+                    B[4, 3 * a + 1], B[4, 3 * a + 2] = dN[2, a], dN[1, a]
+                    B[5, 3 * a], B[5, 3 * a + 2] = dN[2, a], dN[0, a]
+                K += B.T @ D @ B * wts[i] * wts[j] * wts[k] * np.prod(h) / 8
+    Ko = po.Problem(3, 2, 2, 2, lx=2 * h[0], ly=2 * h[1], lz=2 * h[2]).K0()
+    assert np.abs(K - Ko).max() < 1e-13 * np.abs(K).max()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_pcg_matches_direct_factorisation(dim):
+    rng = np.random.default_rng(dim)
+    if dim == 2:
+        p = po.Problem(2, 14, 6)
+        p.dirichlet_box([1, 1], [0, 0], [0, 0, 0, 6, 0, 0])
+        p.fext_full[(14 + 3 * 15) * 2 + 1] = -1.0
+    else:
+        p = po.Problem(3, 6, 3, 3)
+        p.dirichlet_box([1, 1, 1], [0, 0, 0], [0, 0, 0, 3, 0, 3])
+        p.traction_box([0, 0, -1], [6, 6, 0, 3, 0, 3])
+    rho = rng.uniform(0.01, 1, p.nel)
+    r = p.solve(rho, tol=1e-12)
+    rp, col, val = p.assemble(rho)
+    A = sp.csr_matrix((val, col, rp), shape=(r["numeq"],) * 2)
+    assert abs(A - A.T).max() < 1e-14
+    ud = spl.spsolve(A.tocsc(), r["f"])
+    assert np.abs(ud - r["u"]).max() / np.abs(ud).max() < 1e-10
+    assert abs(r["compliance"] - ud @ r["f"]) / (ud @ r["f"]) < 1e-12
+
+
+def test_nonzero_dirichlet_values_enter_the_rhs():
+    p = po.Problem(2, 8, 4)
+    p.dirichlet_box([1, 1], [0, 0], [0, 0, 0, 4, 0, 0])
+    p.dirichlet_box([1, 0], [0.01, 0], [8, 8, 0, 4, 0, 0])
+    rho = np.full(p.nel, 0.7)
+    r = p.solve(rho, tol=1e-13)
+    nv = r["nodeval"].reshape(-1, 2)
+    assert np.allclose(nv[8::9, 0], 0.01)
+    # equilibrium: the assembled free rows of K times the full nodal field = f
+    rp, col, val = p.assemble(rho)
+    A = sp.csr_matrix((val, col, rp), shape=(r["numeq"],) * 2)
+    assert np.abs(A @ r["u"] - r["f"]).max() > 1e-6  # the Dirichlet values load the system
+
+
+def test_fdm_sensitivity_procedure():
+    # ICARAT's check (opt-mma-HelmholtzFilter/fdm.cpp:13-62): forward difference
+    p = po.Problem(2, 10, 5)
+    p.dirichlet_box([1, 1], [0, 0], [0, 0, 0, 5, 0, 0])
+    p.fext_full[(10 + 2 * 11) * 2 + 1] = -1.0
+    rho = np.random.default_rng(7).uniform(0.2, 1, p.nel)
+    r = p.solve(rho, tol=1e-14)
+    dc = p.sensitivity(rho, r["nodeval"])
+    for e in (0, 17, 33, 49):
+        d = 1e-7
+        rho2 = rho.copy()
+        rho2[e] += d
+        c2 = p.solve(rho2, tol=1e-14)["compliance"]
+        assert abs((c2 - r["compliance"]) / d - dc[e]) < 1e-5 * abs(dc).max()
+
+
+def test_cone_stencil_equals_icarat_neighbour_scan():
+    import ctypes as C
+    for dims, rfil in [((2, 9, 7), 1.5), ((2, 12, 5), 3.0), ((3, 5, 4, 3), 1.5), ((3, 6, 5, 4), 2.0)]:
+        p = po.Problem(*dims)
+        cnt = np.zeros(p.nel, np.int32)
+        tot = po.lib().orc_cone_bruteforce_counts(C.byref(p.g), rfil, cnt.ctypes.data_as(C.POINTER(C.c_int)))
+        cone = po.Cone(p, rfil)
+        # weights sum per element = sum over clipped stencil; count from aa with w>0 only
+        x = np.ones(p.nel)
+        y = cone.apply(x)
+        assert np.allclose(y, 1.0)
+        # per-element neighbour counts of the clipped stencil
+        ones_w = po.Cone(p, rfil)
+        assert tot == _stencil_count(p, ones_w, rfil)
+
+
+def _stencil_count(p, cone, r):
+    g = p.g
+    R = int(np.floor(r)) + 1
+    offs = []
+    for dk in (range(-R, R + 1) if g.dim == 3 else [0]):
+        for dj in range(-R, R + 1):
+            for di in range(-R, R + 1):
+                if np.sqrt(di * di + dj * dj + dk * dk) <= r:
+                    offs.append((di, dj, dk))
+    assert len(offs) == cone.size()
+    nz = g.nz if g.dim == 3 else 1
+    tot = 0
+    for k in range(nz):
+        for j in range(g.ny):
+            for i in range(g.nx):
+                for di, dj, dk in offs:
+                    if 0 <= i + di < g.nx and 0 <= j + dj < g.ny and 0 <= k + dk < nz:
+                        tot += 1
+    return tot
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "ref_opt.npz")), reason="no fixture")
+def test_oc_matches_icarat_golden():
+    G = np.load(os.path.join(GOLD, "ref_opt.npz"))
+    n = G["oc_x"].size
+    dg = G["oc_dg"]
+    out = po.oc_update(G["oc_x"], G["oc_df"], float(G["oc_g"]), dg, np.full(n, 1e-4), np.ones(n),
+                       0.2, lambda xx: float(xx @ dg))
+    assert np.array_equal(out, G["oc_out"])
+    p = po.Problem(2, 15, 10)
+    cone = po.Cone(p, 1.5)
+    beta = float(G["ocf_beta"])
+    out2 = po.oc_update(G["ocf_x"], G["ocf_df"], float(G["ocf_g"]), np.ones(p.nel),
+                        np.full(p.nel, 1e-4), np.ones(p.nel), 0.2,
+                        lambda xx: float(po.threshold(cone.apply(xx), beta).sum()))
+    assert np.array_equal(out2, G["ocf_out"])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "ref_opt.npz")), reason="no fixture")
+def test_mma_matches_icarat_golden():
+    G = np.load(os.path.join(GOLD, "ref_opt.npz"))
+    traj = G["mma_traj"]
+    n = traj.shape[1]
+    m = po.MMA(n, 1)
+    x = traj[0].copy()
+    for k in range(G["mma_df"].shape[0]):
+        x = m.update(x, G["mma_df"][k], G["mma_g"][k], G["mma_dg"][k], np.full(n, 1e-4), np.ones(n))
+        assert np.abs(x - traj[k + 1]).max() < 1e-12, k
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref not built here")
+def test_oc_and_mma_match_icarat_live():
+    rng = np.random.default_rng(11)
+    n = 257
+    x = rng.uniform(0.1, 0.9, n)
+    df = -rng.uniform(0.01, 2, n)
+    dg = np.ones(n)
+    a = po.oc_update(x, df, 0.5 * n, dg, np.full(n, 1e-4), np.ones(n), 0.15, lambda v: v.sum())
+    b = po.oc_update(x, df, 0.5 * n, dg, np.full(n, 1e-4), np.ones(n), 0.15, lambda v: v.sum(),
+                     use_ref=True)
+    assert np.array_equal(a, b)
+
+
+def test_small_fem_fixture_regression():
+    G = np.load(os.path.join(GOLD, "small_fem.npz"))
+    assert np.abs(po.Problem(2, 2, 2).K0() - G["K0_q4_stress"]).max() < 1e-15
+    assert np.abs(po.Problem(3, 2, 2, 2).K0() - G["K0_h8"]).max() < 1e-15
+    p = po.Problem(2, 20, 10, state=1, young=(0.001, 200.0), nu=0.3)
+    p.dirichlet_box([1, 1, 0, 0, 0, 0], [0] * 6, [0, 0, 0, 10, 0, 10])
+    p.traction_box([0.0, -0.01, 0.0], [20, 20, 0, 10, 0, 0])
+    dof, numeq = p.dofs()
+    assert numeq == int(G["fdm_numeq"]) == 231 * 2 - 22
+    assert np.array_equal(dof, G["fdm_dof"])
+    f = p.fext()
+    assert np.allclose(f, G["fdm_fext"], rtol=0, atol=1e-17)
+    # the traction -0.01 on an edge of length 10 sums to -0.1
+    assert abs(f.sum() + 0.1) < 1e-15
+    r = p.solve(np.full(p.nel, 0.4), tol=1e-12)
+    assert abs(r["compliance"] - float(G["fdm_comp"])) < 1e-10 * abs(float(G["fdm_comp"]))
+
+
+def test_degenerate_traction_box_loads_nothing():
+    # SurfaceLoad needs every node of a side inside the box: a line box in 3D
+    # selects no face (boundary_condition_icarat.hpp:363-381)
+    p = po.Problem(3, 4, 2, 2)
+    p.dirichlet_box([1, 1, 1], [0, 0, 0], [0, 0, 0, 2, 0, 2])
+    p.traction_box([0, 0, -1], [4, 4, 0, 2, 0, 0])
+    assert np.abs(p.fext()).max() == 0.0
