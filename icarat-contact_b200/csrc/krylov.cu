@@ -340,6 +340,40 @@ int JacobiPcg<T>::solve(const T *K, const T *E, const uint8_t *fix, const T *inv
 template struct JacobiPcg<double>;
 template struct JacobiPcg<float>;
 
+/// Jacobi-PCG with every buffer supplied by the caller and no CUDA graph:
+/// the same three kernels per iteration as JacobiPcg, launched directly, the
+/// stop flag polled every 16 iterations into a caller-owned host KState.
+int pcg_run_external(const Dims &d, const double *K, const double *E, const uint8_t *fix,
+                     const double *invdiag, const double *b, double *x, double *r, double *p,
+                     double *q, double *dotOut, KState *st, RedScratch red, double tol,
+                     int maxit, cudaStream_t s, KState *hostState)
+{
+  const long long n = (long long)d.dim * d.ld;
+  const int nb = vec_blocks(n);
+  ICB_REQUIRE(reduction_blocks(d) <= red.maxBlocks, "reduction scratch too small");
+  k_pcg_init<double><<<nb, VB, 0, s>>>(n, b, x, r, p, invdiag, red, st, tol, maxit);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+  long long launched = 0;
+  for(;;)
+  {
+    ICB_CUDA(cudaMemcpyAsync(hostState, st, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    if(hostState->stop || launched > (long long)maxit + 16)
+      break;
+    for(int it = 0; it < 16; it++)
+    {
+      launch_matvec<double>(d, K, E, p, q, fix, s, &red, dotOut, st);
+      k_pcg_r<double><<<nb, VB, 0, s>>>(n, r, q, invdiag, dotOut, red, st);
+      k_pcg_xp<double><<<nb, VB, 0, s>>>(n, x, p, r, invdiag, red, st);
+      count_launch(2);
+    }
+    ICB_CUDA(cudaGetLastError());
+    launched += 16;
+  }
+  return hostState->status;
+}
+
 void red_alloc(RedScratch &r, int maxBlocks, int nvals, std::vector<void *> &owned)
 {
   double *p = nullptr;

@@ -34,6 +34,14 @@ template <typename T> struct JacobiPcg
             double tol, int maxit, cudaStream_t s, icb_solve_info *info);
 };
 
+/// Jacobi-PCG (FP64) on caller-supplied buffers, no graph, no allocation:
+/// r, p, q are SoA vectors of dim*ld entries, dotOut one double, st one
+/// device KState, red a reduction scratch with >= reduction_blocks(d) slots.
+int pcg_run_external(const Dims &d, const double *K, const double *E, const uint8_t *fix,
+                     const double *invdiag, const double *b, double *x, double *r, double *p,
+                     double *q, double *dotOut, KState *st, RedScratch red, double tol,
+                     int maxit, cudaStream_t s, KState *hostState);
+
 /// partial-sum slots a reduction over this grid's vectors or operator needs
 int reduction_blocks(const Dims &d);
 

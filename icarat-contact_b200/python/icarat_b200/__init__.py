@@ -90,6 +90,9 @@ _SIGS = {
     "icb_soa_length": (C.c_longlong, [C.c_void_p]),
     "icb_operator_apply_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "icb_launch_count": (C.c_longlong, []),
+    "icb_solve_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                                    C.POINTER(SolveInfo)]),
+    "icb_noalloc_max_soa": (C.c_longlong, []),
 }
 
 

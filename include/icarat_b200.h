@@ -170,6 +170,28 @@ int icb_operator_apply_device(icb_problem p, int precision, const void *x, void 
  * counted one by one) */
 long long icb_launch_count(void);
 
+/* ---- solve without device allocation ------------------------------------ */
+/* No counterpart in ICARAT.  For callers that cannot allocate device memory
+ * when they solve: code running under CUDA stream capture (cudaMalloc cannot
+ * be captured), hosts that give all GPU memory to their own pool and treat
+ * outside allocations as failures, and real-time or serving loops that must
+ * not stall on the allocator or hit out-of-memory mid-request.
+ * The same FP64 Jacobi-PCG as icb_solve with ICB_FP64 / ICB_PRECOND_JACOBI
+ * (Eigen_CG semantics), on caller-provided device SoA vectors: b_dev holds
+ * the right-hand side (0 on constrained DOFs), x_dev receives the solution;
+ * both have icb_soa_length(p) doubles.  Scratch comes from a 32 MiB static
+ * device array that every GPU loading this library holds until exit; problems
+ * with icb_soa_length(p) > icb_noalloc_max_soa() are rejected with
+ * ICB_ERR_BAD_ARG.  The call itself allocates nothing.  Its first call on a
+ * device looks up that array's device address, so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race, so serialise them.  info->true_relres is -1 (not
+ * recomputed). */
+int icb_solve_noalloc(icb_problem p, const double *b_dev, double *x_dev, double tol, int maxit,
+                      icb_solve_info *info);
+/* largest icb_soa_length() icb_solve_noalloc accepts */
+long long icb_noalloc_max_soa(void);
+
 #ifdef __cplusplus
 }
 #endif
