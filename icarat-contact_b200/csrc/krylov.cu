@@ -11,6 +11,8 @@
 #include <cfloat>
 #include <cmath>
 
+#include <functional>
+
 #include "krylov.hpp"
 #include "reduce.cuh"
 
@@ -266,6 +268,22 @@ int JacobiPcg<T>::solve(const T *K, const T *E, const uint8_t *fix, const T *inv
                         const T *b, T *x, double tol, int maxit, cudaStream_t s,
                         icb_solve_info *info)
 {
+  const Dims dd = d;
+  RedScratch *rp = &red;
+  double *dp = dots.p;
+  KState *sp = st.p;
+  T *pp = p.p, *qp = q.p;
+  auto op = [=](cudaStream_t cs) {
+    launch_matvec<T>(dd, K, E, pp, qp, fix, cs, rp, dp, sp);
+  };
+  return solveOp(op, K, E, fix, invdiag, b, x, tol, maxit, s, info);
+}
+
+template <typename T>
+int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const void *opKey0,
+                          const void *opKey1, const void *opKey2, const T *invdiag, const T *b,
+                          T *x, double tol, int maxit, cudaStream_t s, icb_solve_info *info)
+{
   cudaEvent_t e0, e1;
   ICB_CUDA(cudaEventCreate(&e0));
   ICB_CUDA(cudaEventCreate(&e1));
@@ -276,12 +294,10 @@ int JacobiPcg<T>::solve(const T *K, const T *E, const uint8_t *fix, const T *inv
   count_launch();
 
   // (re)capture the batch graph when the operands changed
-  const void *key[6] = {K, E, fix, invdiag, x, (const void *)s};
+  const void *key[6] = {opKey0, opKey1, opKey2, invdiag, x, (const void *)s};
   bool same = exec != nullptr;
   for(int i = 0; i < 6 && same; i++)
     same = key[i] == graphKey[i];
-  // the element matrix is passed by value: a graph keyed on its pointer would
-  // miss a change of values, so the caller owns a stable K per level.
   if(!same)
   {
     if(exec)
@@ -294,12 +310,12 @@ int JacobiPcg<T>::solve(const T *K, const T *E, const uint8_t *fix, const T *inv
     ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     for(int it = 0; it < batch; it++)
     {
-      launch_matvec<T>(d, K, E, p.p, q.p, fix, cs, &red, dots.p, st.p);
+      op(cs); // q = K p with the fused p.q reduction into dots[0]
       k_pcg_r<T><<<nb, VB, 0, cs>>>(n, r.p, q.p, invdiag, dots.p, red, st.p);
       k_pcg_xp<T><<<nb, VB, 0, cs>>>(n, x, p.p, r.p, invdiag, red, st.p);
     }
     ICB_CUDA(cudaStreamEndCapture(cs, &g));
-    count_launch(-(long long)batch); // matvec launches recorded during capture
+    count_launch(-(long long)batch); // operator launches recorded during capture
     ICB_CUDA(cudaGraphInstantiate(&exec, g, 0));
     cudaGraphDestroy(g);
     cudaStreamDestroy(cs);

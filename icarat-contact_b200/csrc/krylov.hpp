@@ -1,5 +1,7 @@
 // krylov.hpp -- preconditioned conjugate gradients on the device.
 #pragma once
+#include <functional>
+
 #include "icb_internal.hpp"
 
 namespace icb
@@ -32,6 +34,12 @@ template <typename T> struct JacobiPcg
   /// level (captured by value into the batch graph: keep it stable).
   int solve(const T *K, const T *E, const uint8_t *fix, const T *invdiag, const T *b, T *x,
             double tol, int maxit, cudaStream_t s, icb_solve_info *info);
+  /// the same iteration with any operator: `op(stream)` must compute q = A p
+  /// on this object's p/q buffers and store p.q in dots[0] through `red`;
+  /// opKey* identify the operator's operands for the graph cache.
+  int solveOp(const std::function<void(cudaStream_t)> &op, const void *opKey0,
+              const void *opKey1, const void *opKey2, const T *invdiag, const T *b, T *x,
+              double tol, int maxit, cudaStream_t s, icb_solve_info *info);
 };
 
 /// Jacobi-PCG (FP64) on caller-supplied buffers, no graph, no allocation:

@@ -1,0 +1,656 @@
+// opt.cu -- density filter, threshold projection, OC and MMA updates on the
+// device.
+//
+// * Cone filter: Filter<E,N>::densityFilter (src/optimization/filter.hpp:
+//   102-151).  The neighbour set of ICARAT's O(N^2) preNeighbour scan
+//   (filter.hpp:191-234) is, on a uniform grid, the set of integer element
+//   offsets with |offset * h| <= r; it is built once on the host, in
+//   increasing element-index order (the order preNeighbour lists them, so the
+//   sums are taken in ICARAT's order), and the per-element weight sums aa
+//   (dfilters_ds) are computed once on the device.
+// * Threshold: Filter::threshold / thresholdDerivative (filter.hpp:153-185),
+//   fused into the forward filter.
+// * OC: OC::UpdateVariables (src/optimization/opt-solver/OCSolver.hpp:20-68)
+//   with the volume callback of opt_macro_oc.cpp:155-164 (re-filter and
+//   re-threshold the candidate).  One kernel per bisection step evaluates the
+//   candidate on the fly inside the filter stencil and reduces its volume;
+//   the last block runs the bisection logic, so a whole update is one CUDA
+//   graph with early exit.
+// * MMA: Svanberg's MMA with ICARAT's MMASolver parameters
+//   (MMASolver.cpp:41-55), m = 1: GenSub as one element pass, the dual
+//   interior-point iteration as one fused pass per Newton step (x(lambda),
+//   the dual gradient and Hessian sums) whose last block runs SolveDIP's
+//   scalar logic (MMASolver.cpp:88-154, 214-344) as a state machine.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+#include "opt.hpp"
+#include "reduce.cuh"
+
+namespace icb
+{
+namespace
+{
+constexpr int VB = 256;
+inline int vblocks(long long n)
+{
+  return int(std::max<long long>(1, std::min<long long>((n + VB - 1) / VB, num_sms() * 8LL)));
+}
+
+__device__ __forceinline__ void elemIJK(const Dims &d, long long e, int &i, int &j, int &k)
+{
+  i = int(e % d.nx);
+  j = int((e / d.nx) % d.ny);
+  k = int(e / ((long long)d.nx * d.ny));
+}
+
+__device__ __forceinline__ double thresh(double x, double beta, double T)
+{
+  return 0.5 * (tanh(T * beta) + tanh(beta * (x - T))) / tanh(T * beta);
+}
+__device__ __forceinline__ double thresh_d(double x, double beta, double T)
+{
+  double t = tanh(beta * (x - T));
+  return (0.5 * (beta * (1.0 - pow(t, 2.0))) / tanh(T * beta));
+}
+
+// ---------------------------------------------------------------- cone ----
+__global__ void k_cone_aa(Dims d, const int *__restrict__ off, const double *__restrict__ w,
+                          int nnb, double *__restrict__ aa)
+{
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(e >= d.nel)
+    return;
+  int i, j, k;
+  elemIJK(d, e, i, j, k);
+  double s = 0.0;
+  for(int t = 0; t < nnb; t++)
+  {
+    int ii = i + off[3 * t], jj = j + off[3 * t + 1], kk = k + off[3 * t + 2];
+    if(ii < 0 || jj < 0 || kk < 0 || ii >= d.nx || jj >= d.ny || kk >= d.nz)
+      continue;
+    s += w[t];
+  }
+  aa[e] = s;
+}
+
+/// forward: out = sum w x / aa (+ threshold and its derivative when beta > 0)
+/// adjoint: out = sum w g / aa_j
+template <bool SENS>
+__global__ void k_cone(Dims d, const int *__restrict__ off, const double *__restrict__ w,
+                       int nnb, const double *__restrict__ aa, const double *__restrict__ in,
+                       double *__restrict__ out, double beta, double T,
+                       double *__restrict__ xhat, double *__restrict__ dxhat)
+{
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(e >= d.nel)
+    return;
+  int i, j, k;
+  elemIJK(d, e, i, j, k);
+  double s = 0.0;
+  for(int t = 0; t < nnb; t++)
+  {
+    int ii = i + off[3 * t], jj = j + off[3 * t + 1], kk = k + off[3 * t + 2];
+    if(ii < 0 || jj < 0 || kk < 0 || ii >= d.nx || jj >= d.ny || kk >= d.nz)
+      continue;
+    long long f = ii + (long long)jj * d.nx + (long long)kk * d.nx * d.ny;
+    if(SENS)
+      s += w[t] * in[f] / aa[f];
+    else
+      s += w[t] * in[f];
+  }
+  double v = SENS ? s : s / aa[e];
+  out[e] = v;
+  if(!SENS && xhat)
+  {
+    xhat[e] = beta > 0.0 ? thresh(v, beta, T) : v;
+    dxhat[e] = beta > 0.0 ? thresh_d(v, beta, T) : 1.0;
+  }
+}
+
+__global__ void k_threshold(long long n, const double *__restrict__ x, double beta, double T,
+                            double *__restrict__ xh, double *__restrict__ dxh)
+{
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(i >= n)
+    return;
+  if(xh)
+    xh[i] = thresh(x[i], beta, T);
+  if(dxh)
+    dxh[i] = thresh_d(x[i], beta, T);
+}
+
+// ------------------------------------------------------------------ OC ----
+__device__ __forceinline__ double oc_candidate(double x, double df, double dg, double lam,
+                                               double eta, double move, double xmin,
+                                               double xmax)
+{
+  double v = pow(fmax(0.0, -df / (dg * lam)), eta) * x;
+  double lo = fmax(xmin, (1.0 - move) * x), hi = fmin(xmax, (1.0 + move) * x);
+  if(v < lo)
+    v = lo;
+  else if(v > hi)
+    v = hi;
+  return v;
+}
+
+struct FinOc
+{
+  OcState *st;
+  __device__ void operator()(const double *t) const
+  {
+    // OCSolver.hpp:52-60: lambda goes up while the candidate's volume exceeds g
+    if(t[0] - st->g > 0.0)
+      st->l0 = st->lam;
+    else
+      st->l1 = st->lam;
+    st->counter++;
+    st->vol = t[0];
+    if(!((st->l1 - st->l0) / (st->l1 + st->l0) > st->lambdaeps && st->maxiter > st->counter))
+      st->done = 1;
+    else
+      st->lam = 0.5 * (st->l1 + st->l0);
+  }
+};
+
+/// one bisection step: volume of threshold(filter(x+(lambda))) at st->lam
+__global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__restrict__ w,
+                          int nnb, const double *__restrict__ aa, const double *__restrict__ x,
+                          const double *__restrict__ df, const double *__restrict__ dg,
+                          const double *__restrict__ xmin, const double *__restrict__ xmax,
+                          const double *__restrict__ vol, OcParams P, RedScratch red,
+                          OcState *st)
+{
+  if(st->done)
+    return;
+  const double lam = st->lam;
+  double v[1] = {0.0};
+  for(long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < d.nel;
+      e += (long long)gridDim.x * blockDim.x)
+  {
+    double xf;
+    if(P.useFilter)
+    {
+      int i, j, k;
+      elemIJK(d, e, i, j, k);
+      double s = 0.0;
+      for(int t = 0; t < nnb; t++)
+      {
+        int ii = i + off[3 * t], jj = j + off[3 * t + 1], kk = k + off[3 * t + 2];
+        if(ii < 0 || jj < 0 || kk < 0 || ii >= d.nx || jj >= d.ny || kk >= d.nz)
+          continue;
+        long long f = ii + (long long)jj * d.nx + (long long)kk * d.nx * d.ny;
+        s += w[t] * oc_candidate(x[f], df[f], dg[f], lam, P.eta, P.move, xmin[f], xmax[f]);
+      }
+      xf = s / aa[e];
+    }
+    else
+      xf = oc_candidate(x[e], df[e], dg[e], lam, P.eta, P.move, xmin[e], xmax[e]);
+    double xh = P.beta > 0.0 ? thresh(xf, P.beta, P.T) : xf;
+    v[0] += xh * vol[e];
+  }
+  block_reduce<1>(v, red, FinOc{st});
+}
+
+__global__ void k_oc_init(OcState *st, double g, OcParams P)
+{
+  st->l0 = 0.0;
+  st->l1 = 1.0e4;
+  st->lambdaeps = 1.0e-5;
+  st->maxiter = 100;
+  st->counter = 0;
+  st->g = g;
+  st->done = 0;
+  st->vol = 0.0;
+  // the first lambda of the bisection (OCSolver.hpp:33)
+  st->lam = 0.5 * (st->l1 + st->l0);
+  if(!((st->l1 - st->l0) / (st->l1 + st->l0) > st->lambdaeps && st->maxiter > st->counter))
+    st->done = 1;
+  (void)P;
+}
+
+/// x = x+(lambda of the last bisection step): OCSolver.hpp keeps the last
+/// evaluated candidate, not the midpoint of the final bracket
+__global__ void k_oc_final(long long n, double *__restrict__ x, const double *__restrict__ df,
+                           const double *__restrict__ dg, const double *__restrict__ xmin,
+                           const double *__restrict__ xmax, OcParams P, const OcState *st)
+{
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(e >= n)
+    return;
+  // the last evaluated lambda is the one whose result set l0 or l1 last
+  double lam = st->lastLam;
+  x[e] = oc_candidate(x[e], df[e], dg[e], lam, P.eta, P.move, xmin[e], xmax[e]);
+}
+
+__global__ void k_oc_latch(OcState *st)
+{
+  // record the lambda just evaluated before the bisection moves it
+  if(!st->done)
+    st->lastLam = st->lam;
+}
+
+// ----------------------------------------------------------------- MMA ----
+struct FinSum2
+{
+  double *out;
+  __device__ void operator()(const double *t) const
+  {
+    out[0] = t[0];
+    out[1] = t[1];
+  }
+};
+
+/// GenSub (MMASolver.cpp:400-512) for m = 1: asymptotes, move bounds, p0,
+/// q0, p, q; the constraint constant b = -g + sum(p/(U-x) + q/(x-L)) is
+/// reduced into st->b by the finisher.
+struct FinGenSub
+{
+  MmaState *st;
+  __device__ void operator()(const double *t) const { st->b = -st->g + t[0]; }
+};
+
+__global__ void k_mma_gensub(long long n, MmaVec V, const double *__restrict__ x,
+                             const double *__restrict__ dfdx, const double *__restrict__ dgdx,
+                             const double *__restrict__ xmin, const double *__restrict__ xmax,
+                             MmaParams P, int iter, RedScratch red, MmaState *st)
+{
+  double v[1] = {0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    double xv = x[i], range = xmax[i] - xmin[i];
+    double lo, up;
+    if(iter < 3)
+    {
+      lo = xv - P.asyminit * range;
+      up = xv + P.asyminit * range;
+    }
+    else
+    {
+      double o1 = V.xold1[i], o2 = V.xold2[i];
+      double zzz = (xv - o1) * (o1 - o2);
+      double gam = zzz < 0.0 ? P.asymdec : (zzz > 0.0 ? P.asyminc : 1.0);
+      lo = xv - gam * (o1 - V.low[i]);
+      up = xv + gam * (V.upp[i] - o1);
+      double xmami = fmax(P.xmamieps, range);
+      lo = fmax(lo, xv - 100.0 * xmami);
+      lo = fmin(lo, xv - 1.0e-5 * xmami);
+      up = fmax(up, xv + 1.0e-5 * xmami);
+      up = fmin(up, xv + 100.0 * xmami);
+      double xmi = xmin[i] - 1.0e-6, xma = xmax[i] + 1.0e-6;
+      if(xv < xmi)
+      {
+        lo = xv - (xma - xv) / 0.9;
+        up = xv + (xma - xv) / 0.9;
+      }
+      if(xv > xma)
+      {
+        lo = xv - (xv - xmi) / 0.9;
+        up = xv + (xv - xmi) / 0.9;
+      }
+    }
+    V.low[i] = lo;
+    V.upp[i] = up;
+    double al = fmax(xmin[i], lo + P.albefa * (xv - lo));
+    al = fmax(al, xv - P.move * range);
+    al = fmin(al, xmax[i]);
+    double be = fmin(xmax[i], up - P.albefa * (up - xv));
+    be = fmin(be, xv + P.move * range);
+    be = fmax(be, xmin[i]);
+    V.alpha[i] = al;
+    V.beta[i] = be;
+    double inv = 1.0 / fmax(P.xmamieps, range);
+    double u2 = pow(up - xv, 2.0), l2 = pow(xv - lo, 2.0);
+    double df = dfdx[i], dg = dgdx[i];
+    double pq = 0.001 * fabs(df) + P.raa0 * inv;
+    V.p0[i] = u2 * (fmax(0.0, df) + pq);
+    V.q0[i] = l2 * (fmax(0.0, -df) + pq);
+    double pqg = 0.001 * fabs(dg) + P.raa0 * inv;
+    double pij = u2 * (fmax(0.0, dg) + pqg), qij = l2 * (fmax(0.0, -dg) + pqg);
+    V.pij[i] = pij;
+    V.qij[i] = qij;
+    v[0] += pij / (up - xv) + qij / (xv - lo);
+    // xold2 = xold1; xold1 = x (Update, MMASolver.cpp:74-75)
+    V.xold2[i] = V.xold1[i];
+    V.xold1[i] = xv;
+  }
+  block_reduce<1>(v, red, FinGenSub{st});
+}
+
+/// SolveDIP's scalar logic for m = 1, run by the last block of each pass
+/// with the sums S_g = sum(p/(U-x)+q/(x-L)) and S_h = sum(PQ^2 df2) taken at
+/// the current lambda.
+struct FinDip
+{
+  MmaState *st;
+  MmaParams P;
+  __device__ void newton(double Sg, double Sh) const
+  {
+    // XYZofLAMBDA clamps lambda (MMASolver.cpp:365-368); y = max(0, lam - c)
+    double lam = fmax(st->lam, 0.0), mu = st->mu, epsi = st->epsi;
+    double y = fmax(0.0, lam - P.c);
+    st->loop++;
+    double grad = -st->b - P.a * st->z - y + Sg;
+    grad = -1.0 * grad - epsi / lam;
+    // DualHess (MMASolver.cpp:238-344)
+    double hess = Sh;
+    if(lam > P.c)
+      hess += -1.0;
+    hess += -mu / lam;
+    double corr = 1e-4 * hess;
+    if(-1.0 * corr < 1.0e-7)
+      corr = -1.0e-7;
+    hess += corr;
+    double s0 = grad / hess;
+    double s1 = -mu + epsi / lam - s0 * mu / lam;
+    // DualLineSearch (MMASolver.cpp:214-236)
+    double theta = 1.005;
+    if(theta < -1.01 * s0 / lam)
+      theta = -1.01 * s0 / lam;
+    if(theta < -1.01 * s1 / mu)
+      theta = -1.01 * s1 / mu;
+    theta = 1.0 / theta;
+    st->lam = lam + theta * s0;
+    st->mu = mu + theta * s1;
+  }
+  __device__ void operator()(const double *t) const
+  {
+    const double Sg = t[0], Sh = t[1];
+    st->passes++;
+    if(st->phase == 0)
+    {
+      // first pass of an update: outer loop 1, inner loop 1 at lambda = c/2
+      st->outloop = 1;
+      st->loop = 0;
+      newton(Sg, Sh);
+      st->phase = 1;
+      return;
+    }
+    // phase 1: sums at the lambda after a Newton step: KKT residual
+    double lam = fmax(st->lam, 0.0);
+    st->lam = lam;
+    double y = fmax(0.0, lam - P.c);
+    double r0 = -st->b - P.a * st->z - y + st->mu + Sg;
+    double r1 = st->mu * lam - st->epsi;
+    st->err = fmax(fabs(r0), fabs(r1));
+    // inner loop continues with the sums already at this lambda
+    if(st->err > 0.9 * st->epsi && st->loop < 100)
+    {
+      newton(Sg, Sh);
+      return;
+    }
+    // inner loop over: next outer loops until one runs an inner iteration
+    for(;;)
+    {
+      st->epsi *= 0.1;
+      if(!(st->epsi > P.epsimin && st->outloop < 100))
+      {
+        st->done = 1;
+        return;
+      }
+      st->outloop++;
+      st->loop = 0;
+      if(st->err > 0.9 * st->epsi)
+      {
+        newton(Sg, Sh);
+        return;
+      }
+    }
+  }
+};
+
+/// one pass at the current lambda: x(lambda) (XYZofLAMBDA), S_g (DualGrad)
+/// and S_h (DualHess) with ICARAT's expressions
+__global__ void k_mma_pass(long long n, MmaVec V, double *__restrict__ x, MmaParams P,
+                           RedScratch red, MmaState *st)
+{
+  if(st->done)
+    return;
+  const double lam = fmax(st->lam, 0.0);
+  double v[2] = {0.0, 0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    double low = V.low[i], upp = V.upp[i];
+    double pl = V.p0[i] + V.pij[i] * lam, ql = V.q0[i] + V.qij[i] * lam;
+    double sp = sqrt(pl), sq = sqrt(ql);
+    double xp = (sp * low + sq * upp) / (sp + sq);
+    double xi = xp;
+    if(xi < V.alpha[i])
+      xi = V.alpha[i];
+    if(xi > V.beta[i])
+      xi = V.beta[i];
+    x[i] = xi;
+    v[0] += V.pij[i] / (upp - xi) + V.qij[i] / (xi - low);
+    double PQ = V.pij[i] / pow(upp - xi, 2.0) - V.qij[i] / pow(xi - low, 2.0);
+    double df2 = -1.0 / (2.0 * pl / pow(upp - xi, 3.0) + 2.0 * ql / pow(xi - low, 3.0));
+    if(xp < V.alpha[i] || xp > V.beta[i])
+      df2 = 0.0;
+    v[1] += PQ * df2 * PQ;
+  }
+  block_reduce<2>(v, red, FinDip{st, P});
+}
+
+__global__ void k_mma_dip_init(MmaState *st, MmaParams P)
+{
+  st->lam = P.c / 2.0;
+  st->mu = 1.0;
+  st->epsi = 1.0;
+  st->err = 1.0;
+  st->outloop = 0;
+  st->loop = 0;
+  st->phase = 0;
+  st->done = !(st->epsi > P.epsimin);
+  st->passes = 0;
+  st->z = 0.0; // z = max(0, 10 (lam a - 1)) with a = 0
+}
+} // namespace
+
+// =============================================================== Cone =====
+ConeFilter::ConeFilter(const Dims &dims, const double *h, double radius, cudaStream_t s)
+    : d(dims), r(radius)
+{
+  if(!(radius > 0.0))
+    throw Error{ICB_ERR_BAD_ARG, "filter radius must be > 0"};
+  int R[3];
+  for(int a = 0; a < 3; a++)
+    R[a] = int(std::floor(radius / h[a])) + 1;
+  if(d.dim == 2)
+    R[2] = 0;
+  std::vector<int> off;
+  std::vector<double> w;
+  for(int dk = -R[2]; dk <= R[2]; dk++)
+    for(int dj = -R[1]; dj <= R[1]; dj++)
+      for(int di = -R[0]; di <= R[0]; di++)
+      {
+        double dx = di * h[0], dy = dj * h[1], dz = dk * h[2];
+        double dist = std::sqrt(dx * dx + dy * dy + (d.dim == 3 ? dz * dz : 0.0));
+        if(dist <= radius)
+        {
+          off.push_back(di);
+          off.push_back(dj);
+          off.push_back(dk);
+          w.push_back(radius - dist);
+        }
+      }
+  nnb = int(w.size());
+  offs.alloc(off.size());
+  wts.alloc(w.size());
+  ICB_CUDA(cudaMemcpy(offs.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+  ICB_CUDA(cudaMemcpy(wts.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
+  aa.alloc(d.nel);
+  k_cone_aa<<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d, offs.p, wts.p, nnb, aa.p);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+void ConeFilter::forward(const double *in, double *out, double beta, double T, double *xhat,
+                         double *dxhat, cudaStream_t s) const
+{
+  k_cone<false><<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d, offs.p, wts.p, nnb, aa.p, in, out,
+                                                             beta, T, xhat, dxhat);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+void ConeFilter::adjoint(const double *in, double *out, cudaStream_t s) const
+{
+  k_cone<true><<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d, offs.p, wts.p, nnb, aa.p, in, out,
+                                                            0.0, 0.5, nullptr, nullptr);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+void launch_threshold(long long n, const double *x, double beta, double T, double *xh,
+                      double *dxh, cudaStream_t s)
+{
+  k_threshold<<<unsigned((n + 255) / 256), 256, 0, s>>>(n, x, beta, T, xh, dxh);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ================================================================= OC =====
+OcUpdater::OcUpdater(const Dims &dims) : d(dims)
+{
+  st.alloc(1);
+  int nb = vblocks(d.nel);
+  partials.alloc(nb);
+  counter.alloc(1);
+  ICB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned)));
+  red = RedScratch{partials.p, counter.p, nb};
+  ICB_CUDA(cudaMallocHost(&hst, sizeof(OcState)));
+}
+OcUpdater::~OcUpdater()
+{
+  if(exec)
+    cudaGraphExecDestroy(exec);
+  if(hst)
+    cudaFreeHost(hst);
+}
+
+int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const double *dg,
+                      double g, const double *xmin, const double *xmax, const double *vol,
+                      const OcParams &P, cudaStream_t s)
+{
+  const int nb = vblocks(d.nel);
+  k_oc_init<<<1, 1, 0, s>>>(st.p, g, P);
+  count_launch();
+  const int *off = cone ? cone->offs.p : nullptr;
+  const double *w = cone ? cone->wts.p : nullptr;
+  const double *aa = cone ? cone->aa.p : nullptr;
+  int nnb = cone ? cone->nnb : 0;
+  OcParams Pp = P;
+  Pp.useFilter = cone != nullptr;
+  // graph of the 100 bisection steps (each gated on done), rebuilt when the
+  // operands or parameters change
+  const void *k[9] = {cone, x, df, dg, xmin, xmax, vol, (const void *)s, nullptr};
+  bool same = exec != nullptr && std::memcmp(&Pp, &keyP, sizeof(OcParams)) == 0;
+  for(int i = 0; i < 9 && same; i++)
+    same = k[i] == key[i];
+  if(!same)
+  {
+    if(exec)
+      cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    cudaStream_t cs;
+    ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t gr;
+    ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    for(int it = 0; it < 100; it++)
+    {
+      k_oc_latch<<<1, 1, 0, cs>>>(st.p);
+      k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, Pp, red, st.p);
+    }
+    k_oc_final<<<unsigned((d.nel + 255) / 256), 256, 0, cs>>>(d.nel, x, df, dg, xmin, xmax, Pp,
+                                                             st.p);
+    ICB_CUDA(cudaStreamEndCapture(cs, &gr));
+    ICB_CUDA(cudaGraphInstantiate(&exec, gr, 0));
+    cudaGraphDestroy(gr);
+    cudaStreamDestroy(cs);
+    for(int i = 0; i < 9; i++)
+      key[i] = k[i];
+    keyP = Pp;
+  }
+  ICB_CUDA(cudaGraphLaunch(exec, s));
+  count_launch(201);
+  ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(OcState), cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  return hst->counter;
+}
+
+// ================================================================ MMA =====
+MmaUpdater::MmaUpdater(long long nvar) : n(nvar)
+{
+  for(DevBuf<double> *b : {&low, &upp, &alpha, &beta, &p0, &q0, &pij, &qij, &xold1, &xold2})
+  {
+    b->alloc(n);
+    ICB_CUDA(cudaMemset(b->p, 0, b->bytes()));
+  }
+  st.alloc(1);
+  int nb = vblocks(n);
+  partials.alloc((size_t)nb * 2);
+  counter.alloc(1);
+  ICB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned)));
+  red = RedScratch{partials.p, counter.p, nb};
+  ICB_CUDA(cudaMallocHost(&hst, sizeof(MmaState)));
+  P.epsimin = std::sqrt(double(n + 1)) * 1e-9;
+}
+MmaUpdater::~MmaUpdater()
+{
+  if(exec)
+    cudaGraphExecDestroy(exec);
+  if(hst)
+    cudaFreeHost(hst);
+}
+
+int MmaUpdater::update(double *x, const double *dfdx, double g, const double *dgdx,
+                       const double *xmin, const double *xmax, cudaStream_t s)
+{
+  iter++;
+  MmaVec V{low.p, upp.p, alpha.p, beta.p, p0.p, q0.p, pij.p, qij.p, xold1.p, xold2.p};
+  const int nb = vblocks(n);
+  // the constraint value for GenSub's b
+  ICB_CUDA(cudaMemcpyAsync(&st.p->g, &g, sizeof(double), cudaMemcpyHostToDevice, s));
+  k_mma_gensub<<<nb, VB, 0, s>>>(n, V, x, dfdx, dgdx, xmin, xmax, P, iter, red, st.p);
+  k_mma_dip_init<<<1, 1, 0, s>>>(st.p, P);
+  count_launch(2);
+  const void *k[3] = {x, (const void *)s, nullptr};
+  bool same = exec != nullptr;
+  for(int i = 0; i < 3 && same; i++)
+    same = k[i] == key[i];
+  const int batch = 32;
+  if(!same)
+  {
+    if(exec)
+      cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    cudaStream_t cs;
+    ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t gr;
+    ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    for(int it = 0; it < batch; it++)
+      k_mma_pass<<<nb, VB, 0, cs>>>(n, V, x, P, red, st.p);
+    ICB_CUDA(cudaStreamEndCapture(cs, &gr));
+    ICB_CUDA(cudaGraphInstantiate(&exec, gr, 0));
+    cudaGraphDestroy(gr);
+    cudaStreamDestroy(cs);
+    for(int i = 0; i < 3; i++)
+      key[i] = k[i];
+  }
+  // SolveDIP needs at most 100 x 100 Newton steps; each pass is one step
+  for(int launches = 0; launches < 10000 / batch + 1; launches++)
+  {
+    ICB_CUDA(cudaGraphLaunch(exec, s));
+    count_launch(batch);
+    ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(MmaState), cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    if(hst->done)
+      break;
+  }
+  return hst->passes;
+}
+
+} // namespace icb

@@ -1,0 +1,430 @@
+// toapi.cu -- C entry points of the optimisation side: cone and Helmholtz
+// filters, threshold, OC and MMA updates, and the two ICARAT app loops run
+// end to end on the device (opt_macro_oc.cpp:84-172,
+// opt_mma_Helmholtz.cpp:81-163).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "helm.hpp"
+#include "mg.hpp"
+#include "opt.hpp"
+#include "problem.hpp"
+#include "reduce.cuh"
+
+using namespace icb;
+
+struct icb_cone_s
+{
+  icb_problem p;
+  std::unique_ptr<ConeFilter> f;
+  DevBuf<double> a, b; ///< staging for the host-pointer entry points
+};
+struct icb_helm_s
+{
+  icb_problem p;
+  std::unique_ptr<HelmFilter> f;
+  DevBuf<double> a, b;
+  double tol = 1e-10;
+};
+struct icb_mma_s
+{
+  icb_ctx ctx;
+  std::unique_ptr<MmaUpdater> m;
+  DevBuf<double> x, df, dg, lo, hi;
+};
+
+namespace
+{
+#define API_TRY try {
+#define API_CATCH                                                                          \
+  }                                                                                        \
+  catch(const Error &e)                                                                    \
+  {                                                                                        \
+    set_error(e.msg);                                                                      \
+    return e.code;                                                                         \
+  }                                                                                        \
+  catch(const std::bad_alloc &)                                                            \
+  {                                                                                        \
+    set_error("host allocation failed");                                                   \
+    return ICB_ERR_OOM;                                                                    \
+  }                                                                                        \
+  catch(const std::exception &e)                                                           \
+  {                                                                                        \
+    set_error(e.what());                                                                   \
+    return ICB_ERR_STATE;                                                                  \
+  }                                                                                        \
+  return ICB_OK;
+
+void need(bool c, const char *m)
+{
+  if(!c)
+    throw Error{ICB_ERR_BAD_ARG, m};
+}
+void needFinal(icb_problem p)
+{
+  if(!p || !p->hs->finalized)
+    throw Error{ICB_ERR_STATE, "problem not finalized"};
+}
+
+__global__ void k_scale_mul(long long n, double *__restrict__ a, const double *__restrict__ m,
+                            double s)
+{
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(i < n)
+    a[i] = s * a[i] * m[i];
+}
+__global__ void k_fill_d(long long n, double v, double *__restrict__ a)
+{
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(i < n)
+    a[i] = v;
+}
+__global__ void k_sum(long long n, const double *__restrict__ a, RedScratch red, double *out)
+{
+  double v[1] = {0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+    v[0] += a[i];
+  block_reduce<1>(v, red, FinStore{out});
+}
+unsigned nb256(long long n) { return unsigned((n + 255) / 256); }
+
+double deviceSum(icb_problem p, const double *a, long long n)
+{
+  int nb = int(std::min<long long>(nb256(n), (long long)p->red.maxBlocks));
+  k_sum<<<nb, 256, 0, p->stream()>>>(n, a, p->red, p->scal.p + 8);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+  double h;
+  ICB_CUDA(cudaMemcpyAsync(&h, p->scal.p + 8, sizeof(double), cudaMemcpyDeviceToHost, p->stream()));
+  ICB_CUDA(cudaStreamSynchronize(p->stream()));
+  return h;
+}
+
+void toDev(DevBuf<double> &b, const double *h, long long n, cudaStream_t s)
+{
+  if((long long)b.n < n)
+    b.alloc(n);
+  ICB_CUDA(cudaMemcpyAsync(b.p, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+}
+} // namespace
+
+extern "C" {
+
+// ----------------------------------------------------------------- cone ----
+int icb_cone_create(icb_problem p, double radius, icb_cone *out)
+{
+  API_TRY
+  need(out != nullptr, "out is NULL");
+  needFinal(p);
+  ICB_CUDA(cudaSetDevice(p->ctx->device));
+  auto c = std::make_unique<icb_cone_s>();
+  c->p = p;
+  c->f = std::make_unique<ConeFilter>(p->d, p->hs->h, radius, p->stream());
+  ICB_CUDA(cudaStreamSynchronize(p->stream()));
+  *out = c.release();
+  API_CATCH
+}
+
+int icb_cone_destroy(icb_cone c)
+{
+  API_TRY
+  delete c;
+  API_CATCH
+}
+
+int icb_cone_filter_device(icb_cone c, const double *in, double *out, int isSens)
+{
+  API_TRY
+  need(c && in && out, "NULL argument");
+  ICB_CUDA(cudaSetDevice(c->p->ctx->device));
+  if(isSens)
+    c->f->adjoint(in, out, c->p->stream());
+  else
+    c->f->forward(in, out, 0.0, 0.5, nullptr, nullptr, c->p->stream());
+  API_CATCH
+}
+
+int icb_cone_filter(icb_cone c, const double *in, double *out, int isSens)
+{
+  API_TRY
+  need(c && in && out, "NULL argument");
+  long long n = c->p->d.nel;
+  cudaStream_t s = c->p->stream();
+  ICB_CUDA(cudaSetDevice(c->p->ctx->device));
+  toDev(c->a, in, n, s);
+  if((long long)c->b.n < n)
+    c->b.alloc(n);
+  if(isSens)
+    c->f->adjoint(c->a.p, c->b.p, s);
+  else
+    c->f->forward(c->a.p, c->b.p, 0.0, 0.5, nullptr, nullptr, s);
+  ICB_CUDA(cudaMemcpyAsync(out, c->b.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+int icb_threshold(icb_ctx ctx, long long n, const double *x, double beta, double T, double *xhat,
+                  double *dxhat)
+{
+  API_TRY
+  need(ctx && x && n >= 0, "bad argument");
+  need(beta > 0.0, "beta must be > 0");
+  ICB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  DevBuf<double> a(n), b(n), c(n);
+  ICB_CUDA(cudaMemcpyAsync(a.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  launch_threshold(n, a.p, beta, T, b.p, c.p, s);
+  if(xhat)
+    ICB_CUDA(cudaMemcpyAsync(xhat, b.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  if(dxhat)
+    ICB_CUDA(cudaMemcpyAsync(dxhat, c.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+// ------------------------------------------------------------ Helmholtz ----
+int icb_helm_create(icb_problem p, double radius, icb_helm *out)
+{
+  API_TRY
+  need(out != nullptr, "out is NULL");
+  needFinal(p);
+  ICB_CUDA(cudaSetDevice(p->ctx->device));
+  auto h = std::make_unique<icb_helm_s>();
+  h->p = p;
+  h->f = std::make_unique<HelmFilter>(p->d, p->hs->h, radius, p->stream());
+  ICB_CUDA(cudaStreamSynchronize(p->stream()));
+  *out = h.release();
+  API_CATCH
+}
+
+int icb_helm_destroy(icb_helm h)
+{
+  API_TRY
+  delete h;
+  API_CATCH
+}
+
+int icb_helm_filter(icb_helm h, const double *in, double *out, int sensFlag)
+{
+  API_TRY
+  need(h && in && out, "NULL argument");
+  long long n = h->p->d.nel;
+  cudaStream_t s = h->p->stream();
+  ICB_CUDA(cudaSetDevice(h->p->ctx->device));
+  toDev(h->a, in, n, s);
+  if((long long)h->b.n < n)
+    h->b.alloc(n);
+  icb_solve_info inf{};
+  int st = h->f->apply(h->a.p, h->b.p, sensFlag != 0, h->tol, s, &inf);
+  ICB_CUDA(cudaMemcpyAsync(out, h->b.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  if(st != ICB_OK)
+    throw Error{st, "Helmholtz filter solve did not converge"};
+  API_CATCH
+}
+
+// ------------------------------------------------------------------- OC ----
+int icb_oc_update(icb_problem p, icb_cone cone, double *x, const double *dfdx, double g,
+                  const double *dgdx, const double *xmin, const double *xmax, double movelimit,
+                  double beta, double T, int *steps)
+{
+  API_TRY
+  needFinal(p);
+  need(x && dfdx && dgdx && xmin && xmax, "NULL argument");
+  ICB_CUDA(cudaSetDevice(p->ctx->device));
+  cudaStream_t s = p->stream();
+  long long n = p->d.nel;
+  DevBuf<double> X(n), DF(n), DG(n), LO(n), HI(n), V(n);
+  ICB_CUDA(cudaMemcpyAsync(X.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(DF.p, dfdx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(DG.p, dgdx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(LO.p, xmin, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(HI.p, xmax, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, p->hs->volume, V.p);
+  count_launch();
+  OcUpdater oc(p->d);
+  OcParams P;
+  P.move = movelimit;
+  P.beta = beta;
+  P.T = T;
+  int k = oc.update(cone ? cone->f.get() : nullptr, X.p, DF.p, DG.p, g, LO.p, HI.p, V.p, P, s);
+  ICB_CUDA(cudaMemcpyAsync(x, X.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  if(steps)
+    *steps = k;
+  API_CATCH
+}
+
+// ------------------------------------------------------------------ MMA ----
+int icb_mma_create(icb_ctx ctx, long long n, int m, icb_mma *out)
+{
+  API_TRY
+  need(ctx && out && n > 0, "bad argument");
+  need(m == 1, "the device MMA supports one constraint (m = 1)");
+  ICB_CUDA(cudaSetDevice(ctx->device));
+  auto h = std::make_unique<icb_mma_s>();
+  h->ctx = ctx;
+  h->m = std::make_unique<MmaUpdater>(n);
+  for(DevBuf<double> *b : {&h->x, &h->df, &h->dg, &h->lo, &h->hi})
+    b->alloc(n);
+  *out = h.release();
+  API_CATCH
+}
+
+int icb_mma_destroy(icb_mma h)
+{
+  API_TRY
+  delete h;
+  API_CATCH
+}
+
+int icb_mma_update(icb_mma h, double *x, const double *dfdx, const double *gx,
+                   const double *dgdx, const double *xmin, const double *xmax)
+{
+  API_TRY
+  need(h && x && dfdx && gx && dgdx && xmin && xmax, "NULL argument");
+  ICB_CUDA(cudaSetDevice(h->ctx->device));
+  cudaStream_t s = h->ctx->stream;
+  long long n = h->m->n;
+  ICB_CUDA(cudaMemcpyAsync(h->x.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->df.p, dfdx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->dg.p, dgdx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->lo.p, xmin, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->hi.p, xmax, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  h->m->update(h->x.p, h->df.p, gx[0], h->dg.p, h->lo.p, h->hi.p, s);
+  ICB_CUDA(cudaMemcpyAsync(x, h->x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+// ---------------------------------------------------------------- loops ----
+/// The opt-macro-oc loop (opt_macro_oc.cpp:84-172) on the device, without
+/// I/O and with a fixed number of steps.  hist[step] = compliance.
+int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
+               double *xout)
+{
+  API_TRY
+  needFinal(p);
+  need(o && rho0 && hist, "NULL argument");
+  need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
+  ICB_CUDA(cudaSetDevice(p->ctx->device));
+  cudaStream_t s = p->stream();
+  const long long n = p->d.nel;
+  const double vol = p->hs->volume;
+  ConeFilter cone(p->d, p->hs->h, o->filter_radius, s);
+  OcUpdater oc(p->d);
+  DevBuf<double> x(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n), V(n);
+  ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, vol, V.p);
+  count_launch(3);
+  icb_solve_opts so = o->solve;
+  double V0 = 0.0;
+  OcParams P;
+  P.move = o->move_limit;
+  for(int step = 1; step <= o->nsteps; step++)
+  {
+    const double beta = o->use_threshold ? std::min(std::pow(2.0, (int)(step / 40)), 16.0) : 0.0;
+    cone.forward(x.p, xf.p, beta, 0.5, xh.p, dxh.p, s); // beta 0: xh = xf, dxh = 1
+    int rc = icb_set_density_device(p, xh.p);
+    if(rc)
+      return rc;
+    rc = icb_solve(p, &so, nullptr);
+    if(rc)
+      return rc;
+    rc = icb_compliance(p, &hist[step - 1]);
+    if(rc)
+      return rc;
+    if(step == 1)
+      V0 = deviceSum(p, xh.p, n) * vol;
+    const double *dcd = icb_sensitivity_device(p);
+    if(!dcd)
+      throw Error{ICB_ERR_STATE, "sensitivity failed"};
+    ICB_CUDA(cudaMemcpyAsync(dc.p, dcd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    k_scale_mul<<<nb256(n), 256, 0, s>>>(n, dc.p, dxh.p, 1.0);
+    ICB_CUDA(cudaMemcpyAsync(dv.p, V.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    k_scale_mul<<<nb256(n), 256, 0, s>>>(n, dv.p, dxh.p, 1.0);
+    count_launch(2);
+    cone.adjoint(dc.p, dcf.p, s);
+    cone.adjoint(dv.p, dvf.p, s);
+    P.beta = beta;
+    oc.update(&cone, x.p, dcf.p, dvf.p, V0, lo.p, hi.p, V.p, P, s);
+  }
+  if(xout)
+    ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+/// The opt-mma-HelmholtzFilter loop (opt_mma_Helmholtz.cpp:81-163) on the
+/// device: Helmholtz filter, threshold, solve, constraint sum x v / V0 - 1
+/// (0 at step 1 unless o->volume_ref > 0, then V0 = volume_ref), MMA.
+int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
+                double *xout)
+{
+  API_TRY
+  needFinal(p);
+  need(o && rho0 && hist, "NULL argument");
+  need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
+  ICB_CUDA(cudaSetDevice(p->ctx->device));
+  cudaStream_t s = p->stream();
+  const long long n = p->d.nel;
+  const double vol = p->hs->volume;
+  HelmFilter helm(p->d, p->hs->h, o->filter_radius, s);
+  MmaUpdater mma(n);
+  DevBuf<double> x(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n);
+  ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);
+  count_launch(2);
+  icb_solve_opts so = o->solve;
+  double V0 = o->volume_ref;
+  for(int step = 1; step <= o->nsteps; step++)
+  {
+    icb_solve_info hi_{};
+    int rc = helm.apply(x.p, xf.p, false, 1e-10, s, &hi_);
+    if(rc)
+      throw Error{rc, "Helmholtz filter solve did not converge"};
+    const double beta = std::min(std::pow(2.0, (int)(step / 40)), 16.0);
+    launch_threshold(n, xf.p, beta, 0.5, xh.p, dxh.p, s);
+    rc = icb_set_density_device(p, xh.p);
+    if(rc)
+      return rc;
+    rc = icb_solve(p, &so, nullptr);
+    if(rc)
+      return rc;
+    double g = 0.0;
+    if(step == 1 && o->volume_ref <= 0.0)
+      V0 = deviceSum(p, xh.p, n) * vol;
+    else
+      g = deviceSum(p, xh.p, n) * vol / V0 - 1.0;
+    rc = icb_compliance(p, &hist[step - 1]);
+    if(rc)
+      return rc;
+    const double *dcd = icb_sensitivity_device(p);
+    if(!dcd)
+      throw Error{ICB_ERR_STATE, "sensitivity failed"};
+    ICB_CUDA(cudaMemcpyAsync(dc.p, dcd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    k_scale_mul<<<nb256(n), 256, 0, s>>>(n, dc.p, dxh.p, 1.0);
+    k_fill_d<<<nb256(n), 256, 0, s>>>(n, vol / V0, dv.p);
+    k_scale_mul<<<nb256(n), 256, 0, s>>>(n, dv.p, dxh.p, 1.0);
+    count_launch(3);
+    rc = helm.apply(dc.p, dcf.p, true, 1e-10, s, &hi_);
+    if(rc == ICB_OK)
+      rc = helm.apply(dv.p, dvf.p, true, 1e-10, s, &hi_);
+    if(rc)
+      throw Error{rc, "Helmholtz filter solve did not converge"};
+    mma.update(x.p, dcf.p, g, dvf.p, lo.p, hi.p, s);
+  }
+  if(xout)
+    ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+} // extern "C"

@@ -49,6 +49,11 @@ class SolveInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class LoopOpts(C.Structure):
+    _fields_ = [("nsteps", C.c_int), ("filter_radius", C.c_double), ("move_limit", C.c_double),
+                ("use_threshold", C.c_int), ("volume_ref", C.c_double), ("solve", SolveOpts)]
+
+
 class IcbError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{STATUS.get(code, code)}: {msg}")
@@ -93,6 +98,21 @@ _SIGS = {
     "icb_solve_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                     C.POINTER(SolveInfo)]),
     "icb_noalloc_max_soa": (C.c_longlong, []),
+    "icb_cone_create": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_void_p)]),
+    "icb_cone_destroy": (C.c_int, [C.c_void_p]),
+    "icb_cone_filter": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    "icb_cone_filter_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "icb_threshold": (C.c_int, [C.c_void_p, C.c_longlong, _dp, C.c_double, C.c_double, _dp, _dp]),
+    "icb_helm_create": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_void_p)]),
+    "icb_helm_destroy": (C.c_int, [C.c_void_p]),
+    "icb_helm_filter": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    "icb_oc_update": (C.c_int, [C.c_void_p, C.c_void_p, _dp, _dp, C.c_double, _dp, _dp, _dp,
+                                C.c_double, C.c_double, C.c_double, _ip]),
+    "icb_mma_create": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_void_p)]),
+    "icb_mma_destroy": (C.c_int, [C.c_void_p]),
+    "icb_mma_update": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "icb_run_oc": (C.c_int, [C.c_void_p, C.POINTER(LoopOpts), _dp, _dp, _dp]),
+    "icb_run_mma": (C.c_int, [C.c_void_p, C.POINTER(LoopOpts), _dp, _dp, _dp]),
 }
 
 
@@ -291,3 +311,103 @@ class Problem:
         d = np.zeros(self.numeq)
         check(lib().icb_diagonal(self.h, _p(d)))
         return d
+
+
+# ------------------------------------------------------ optimisation side --
+class Cone:
+    """Filter<E,N> density filter on the device."""
+
+    def __init__(self, prob, radius):
+        self.p = prob
+        h = C.c_void_p()
+        check(lib().icb_cone_create(prob.h, radius, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().icb_cone_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def apply(self, x, sens=False):
+        x = np.ascontiguousarray(x, np.float64)
+        out = np.zeros(self.p.nel)
+        check(lib().icb_cone_filter(self.h, _p(x), _p(out), int(sens)))
+        return out
+
+
+class Helmholtz:
+    """FilterHelmholtz on the device."""
+
+    def __init__(self, prob, radius):
+        self.p = prob
+        h = C.c_void_p()
+        check(lib().icb_helm_create(prob.h, radius, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().icb_helm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def apply(self, x, sens=False):
+        x = np.ascontiguousarray(x, np.float64)
+        out = np.zeros(self.p.nel)
+        check(lib().icb_helm_filter(self.h, _p(x), _p(out), int(sens)))
+        return out
+
+
+def threshold(ctx, x, beta, T=0.5):
+    x = np.ascontiguousarray(x, np.float64)
+    a, b = np.zeros_like(x), np.zeros_like(x)
+    check(lib().icb_threshold(ctx.h, x.size, _p(x), beta, T, _p(a), _p(b)))
+    return a, b
+
+
+def oc_update(prob, cone, x, dfdx, g, dgdx, xmin, xmax, move, beta=0.0, T=0.5):
+    x = np.array(x, np.float64)
+    steps = C.c_int()
+    args = [np.ascontiguousarray(v, np.float64) for v in (dfdx, dgdx, xmin, xmax)]
+    check(lib().icb_oc_update(prob.h, None if cone is None else cone.h, _p(x), _p(args[0]),
+                              float(g), _p(args[1]), _p(args[2]), _p(args[3]), move, beta, T,
+                              C.byref(steps)))
+    return x, steps.value
+
+
+class MMA:
+    def __init__(self, ctx, n, m=1):
+        h = C.c_void_p()
+        check(lib().icb_mma_create(ctx.h, n, m, C.byref(h)))
+        self.h, self.n = h, n
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().icb_mma_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def update(self, x, dfdx, gx, dgdx, xmin, xmax):
+        x = np.array(x, np.float64)
+        a = [np.ascontiguousarray(v, np.float64) for v in (dfdx, np.atleast_1d(gx), dgdx, xmin, xmax)]
+        check(lib().icb_mma_update(self.h, _p(x), *[_p(v) for v in a]))
+        return x
+
+
+def run_loop(prob, kind, rho0, nsteps, radius, move=0.15, use_threshold=True, volume_ref=0.0,
+             precision=FP64, precond=GMG, tol=1e-8, maxit=20000):
+    """icb_run_oc (kind "oc") or icb_run_mma (kind "mma"): compliance history, design."""
+    o = LoopOpts(nsteps, radius, move, int(use_threshold), volume_ref,
+                 SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0))
+    hist = np.zeros(nsteps)
+    x = np.zeros(prob.nel)
+    rho0 = np.ascontiguousarray(rho0, np.float64)
+    f = lib().icb_run_oc if kind == "oc" else lib().icb_run_mma
+    check(f(prob.h, C.byref(o), _p(rho0), _p(hist), _p(x)))
+    return hist, x

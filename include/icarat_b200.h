@@ -158,6 +158,57 @@ int icb_matvec(icb_problem p, const double *x, double *y);
 /* the diagonal of K(rho) over free DOFs (numeq) */
 int icb_diagonal(icb_problem p, double *d);
 
+/* ---- filters, projection and design updates ----------------------------- */
+/* Filter<E,N>(fem, element, node, radius) (src/optimization/filter.hpp:17-66):
+ * neighbour stencil |offset * h| <= radius and the weight sums, on the device */
+int icb_cone_create(icb_problem p, double radius, icb_cone *out);
+int icb_cone_destroy(icb_cone c);
+/* Filter::densityFilter(in, isSens) (filter.hpp:102-151): element arrays */
+int icb_cone_filter(icb_cone c, const double *in, double *out, int isSens);
+int icb_cone_filter_device(icb_cone c, const double *in, double *out, int isSens);
+/* Filter::threshold / thresholdDerivative (filter.hpp:153-185); either output
+ * may be NULL */
+int icb_threshold(icb_ctx ctx, long long n, const double *x, double beta, double T,
+                  double *xhat, double *dxhat);
+/* FilterHelmholtz<E,N>(fem, element, node, R) and densityFilter(in,
+ * "Eigen_CG", 0, sensFlag) (src/optimization/filter_helm.hpp:28-137) */
+int icb_helm_create(icb_problem p, double radius, icb_helm *out);
+int icb_helm_destroy(icb_helm h);
+int icb_helm_filter(icb_helm h, const double *in, double *out, int sensFlag);
+/* OC::UpdateVariables(x, dfdx, g, dgdx, xmin, xmax, gkp1) with setMoveLimit
+ * (src/optimization/opt-solver/OCSolver.hpp:20-70); gkp1 is the volume callback
+ * of opt_macro_oc.cpp:155-164: sum of threshold(filter(x+)) * v over elements
+ * (cone may be NULL: no filter; beta <= 0: no threshold).  steps: bisections. */
+int icb_oc_update(icb_problem p, icb_cone cone, double *x, const double *dfdx, double g,
+                  const double *dgdx, const double *xmin, const double *xmax,
+                  double movelimit, double beta, double T, int *steps);
+/* MMASolver(n, m) and Update(x, dfdx, gx, dgdx, xmin, xmax)
+ * (src/optimization/opt-solver/MMASolver.hpp:67-78); m must be 1 */
+int icb_mma_create(icb_ctx ctx, long long n, int m, icb_mma *out);
+int icb_mma_destroy(icb_mma h);
+int icb_mma_update(icb_mma h, double *x, const double *dfdx, const double *gx,
+                   const double *dgdx, const double *xmin, const double *xmax);
+
+/* ---- the ICARAT app loops on the device ----------------------------------- */
+typedef struct
+{
+  int nsteps;           /* optimisation steps (fixed count, no I/O)          */
+  double filter_radius; /* cone radius (icb_run_oc) or Helmholtz R (icb_run_mma) */
+  double move_limit;    /* OC move limit (0.15 in OCSolver.hpp:78)           */
+  int use_threshold;    /* beta = min(2^(step/40), 16) projection (icb_run_oc) */
+  double volume_ref;    /* icb_run_mma: V0 of the constraint (<= 0: step-1 volume) */
+  icb_solve_opts solve; /* the structural solve of every step                */
+} icb_loop_opts;
+/* opt-macro-oc/opt_macro_oc.cpp:84-172: cone filter, threshold, solve,
+ * compliance, V0 at step 1, sensitivities, adjoint filter, OC; hist[nsteps]
+ * receives the compliance of every step, xout (nel, may be NULL) the design. */
+int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
+               double *xout);
+/* opt-mma-HelmholtzFilter/opt_mma_Helmholtz.cpp:81-163: Helmholtz filter,
+ * threshold, solve, volume constraint, sensitivities, adjoint filters, MMA. */
+int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
+                double *xout);
+
 /* ---- device-level access (benchmarks, interop) --------------------------- */
 /* length of one SoA field vector on the device (dim * padded node count):
  * component c of node n sits at c*ld + n, n in MeshIcarat numbering */

@@ -1,0 +1,110 @@
+"""Filters, threshold, OC, MMA and the ICARAT app loops on the GPU, through
+the C ABI, against the oracle and against ICARAT's own OC/MMA (golden
+vectors from oracle/_ref).
+
+Bars: filters and threshold 1e-13 relative (same sums, same order);
+Helmholtz filter 1e-7 (both sides solve to 1e-10); OC 1e-4 on x (the
+bisection stops at a relative lambda width of 1e-5); MMA 1e-9; loop
+histories 1e-4 per step (relative compliance).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import icarat_b200 as icb
+import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("dims,kw,r", [((2, 23, 11), {}, 1.5), ((2, 30, 12), {}, 3.0),
+                                       ((2, 16, 9), {"lx": 8.0, "ly": 9.0}, 1.2),
+                                       ((3, 9, 7, 5), {}, 1.5), ((3, 8, 6, 6), {}, 2.0)])
+def test_cone_filter_matches_oracle(ctx, dims, kw, r):
+    o = po.Problem(*dims, **kw)
+    g = icb.Problem(ctx, *dims, **kw)
+    g.finalize()
+    x = np.random.default_rng(1).uniform(0.01, 1.0, o.nel)
+    oc, gc = po.Cone(o, r), icb.Cone(g, r)
+    a, b = oc.apply(x), gc.apply(x)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
+    s = np.random.default_rng(2).standard_normal(o.nel)
+    a, b = oc.apply(s, sens=True), gc.apply(s, sens=True)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
+
+
+def test_threshold_matches_oracle(ctx):
+    x = np.random.default_rng(3).uniform(0, 1, 1000)
+    for beta in (1.0, 2.0, 16.0):
+        a, b = icb.threshold(ctx, x, beta)
+        assert np.abs(a - po.threshold(x, beta)).max() <= 1e-14
+        assert np.abs(b - po.threshold_deriv(x, beta)).max() <= 1e-12 * beta
+
+
+@pytest.mark.parametrize("dims,R", [((2, 40, 20), 2.0), ((2, 25, 10), 3.0), ((3, 12, 8, 6), 3.0)])
+def test_helmholtz_filter_matches_oracle(ctx, dims, R):
+    o = po.Problem(*dims)
+    g = icb.Problem(ctx, *dims)
+    g.finalize()
+    x = np.random.default_rng(4).uniform(0.01, 1.0, o.nel)
+    h = icb.Helmholtz(g, R)
+    for sens in (False, True):
+        a, b = o.helmholtz(R, x, sens=sens), h.apply(x, sens=sens)
+        assert np.abs(a - b).max() <= 1e-7 * np.abs(a).max()
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "ref_opt.npz")), reason="no fixture")
+def test_oc_update_matches_icarat(ctx):
+    G = np.load(os.path.join(GOLD, "ref_opt.npz"))
+    # filtered + thresholded volume callback on a 15x10 grid (golden from ICARAT's OC)
+    g = icb.Problem(ctx, 2, 15, 10)
+    g.finalize()
+    cone = icb.Cone(g, 1.5)
+    n = g.nel
+    x, steps = icb.oc_update(g, cone, G["ocf_x"], G["ocf_df"], float(G["ocf_g"]), np.ones(n),
+                             np.full(n, 1e-4), np.ones(n), 0.2, beta=float(G["ocf_beta"]))
+    assert np.abs(x - G["ocf_out"]).max() <= 1e-4
+    assert 10 <= steps <= 100
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "ref_opt.npz")), reason="no fixture")
+def test_mma_matches_icarat(ctx):
+    G = np.load(os.path.join(GOLD, "ref_opt.npz"))
+    traj = G["mma_traj"]
+    n = traj.shape[1]
+    m = icb.MMA(ctx, n)
+    for k in range(G["mma_df"].shape[0]):
+        # ICARAT's own iterate in, so both sides see the same history
+        x = m.update(traj[k], G["mma_df"][k], G["mma_g"][k], G["mma_dg"][k], np.full(n, 1e-4),
+                     np.ones(n))
+        assert np.abs(x - traj[k + 1]).max() <= 1e-9, k
+
+
+def test_oc_loop_c1_history(ctx):
+    """The opt-macro-oc loop on the 120x40 cantilever (cone r = 1.5, move 0.2,
+    threshold schedule, 50 steps): per-step compliance within 1e-4 of the
+    oracle's loop."""
+    kind, n = "cantilever2d", (120, 40)
+    o = cases.build_oracle(kind, *n)
+    g = cases.build_gpu(ctx, kind, *n)
+    rho0 = np.full(o.nel, 0.5)
+    ho, xo, _ = o.oc_loop(rho0, 50, 1.5, 0.2, use_beta=True, tol=1e-10)
+    hg, xg = icb.run_loop(g, "oc", rho0, 50, 1.5, move=0.2, use_threshold=True, tol=1e-10)
+    rel = np.abs(hg - ho) / np.abs(ho)
+    assert rel.max() <= 1e-4, rel
+    assert hg[-1] < 0.5 * hg[0]  # the design improves
+
+
+def test_mma_helmholtz_loop_history(ctx):
+    kind, n = "halfmbb2d", (40, 16)
+    o = cases.build_oracle(kind, *n)
+    g = cases.build_gpu(ctx, kind, *n)
+    rho0 = np.full(o.nel, 0.4)
+    ho, xo = o.mma_loop(rho0, 15, 2.0, tol=1e-10)
+    hg, xg = icb.run_loop(g, "mma", rho0, 15, 2.0, tol=1e-10)
+    rel = np.abs(hg - ho) / np.abs(ho)
+    assert rel.max() <= 1e-4, rel
+    assert np.abs(xg - xo).max() <= 1e-3
