@@ -338,6 +338,27 @@ def ours_arm(args):
     return 0
 
 
+def profile_operator(args):
+    """Set up the bench problem and launch each operator variant 3 times (for
+    an ncu capture of k_matvec_h8 on the full workload; no timing printed)."""
+    import torch
+    import cases
+    import icarat_b200 as icb
+    ctx = icb.Context(0)
+    kind, n = WORKLOAD
+    prob = cases.build_gpu(ctx, kind, *n)
+    prob.set_density(cases.uniform_density(prob.nel, SEED))
+    nsoa = prob.soa_length()
+    for prec, dt in ((icb.FP64, torch.float64), (icb.MIXED, torch.float32)):
+        x = torch.randn(nsoa, dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(3):
+            prob.operator_apply_device(x.data_ptr(), y.data_ptr(), prec)
+    ctx.synchronize()
+    print("profile-operator done")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,7 +366,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--profile-operator", action="store_true",
+                    help="only launch the operator kernels on the bench problem (for ncu)")
     args = ap.parse_args()
+    if args.profile_operator:
+        return profile_operator(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

@@ -532,6 +532,30 @@ long long icb_soa_length(icb_problem p) { return p ? p->nsoa : -1; }
 
 long long icb_launch_count(void) { return icb::g_launches.load(); }
 
+int icb_set_option(const char *name, long long value)
+{
+  ICB_API_BEGIN
+  need(name != nullptr, "NULL name");
+  std::string n(name);
+  if(n == "tc_operator")
+    set_tc_operator(value != 0);
+  else
+    need(false, "unknown option");
+  ICB_API_END
+}
+
+long long icb_get_option(const char *name)
+{
+  if(!name)
+    return -1;
+  std::string n(name);
+  if(n == "tc_operator")
+    return tc_operator_enabled() ? 1 : 0;
+  if(n == "tc_timeouts")
+    return (long long)tc_timeouts();
+  return -1;
+}
+
 int icb_operator_apply_device(icb_problem p, int precision, const void *x, void *y)
 {
   ICB_API_BEGIN
@@ -542,8 +566,19 @@ int icb_operator_apply_device(icb_problem p, int precision, const void *x, void 
     launch_matvec<double>(p->d, p->K0, p->E.p, (const double *)x, (double *)y, p->fix.p,
                           p->stream());
   else if(precision == ICB_MIXED)
+  {
+    // the FP32 CUDA-core kernel, whatever the tensor-core switch says
+    bool tc = tc_operator_enabled();
+    set_tc_operator(false);
     launch_matvec<float>(p->d, p->K0f, p->Ef.p, (const float *)x, (float *)y, p->fix.p,
                          p->stream());
+    set_tc_operator(tc);
+  }
+  else if(precision == ICB_TF32)
+  {
+    OpExtras<float> ex;
+    launch_op_tc(p->d, p->K0f, p->Ef.p, (const float *)x, (float *)y, p->fix.p, p->stream(), ex);
+  }
   else
     need(false, "unknown precision");
   ICB_API_END

@@ -154,6 +154,14 @@ template <typename T> struct OpExtras
   const KState *gate = nullptr; ///< skip when gate->stop (or gate->conv if gateConv)
   int gateConv = 0;
 };
+/// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)
+void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u, float *y,
+                  const uint8_t *fix, cudaStream_t s, const OpExtras<float> &x);
+unsigned tc_timeouts();
+/// whether FP32 Hex8 operator launches use the tensor-core kernel
+bool tc_operator_enabled();
+void set_tc_operator(bool on);
+
 /// K: HOST pointer to the unit element matrix ((d*ne)^2 entries); it is
 /// passed by value, so the kernel's FMAs take it from the constant bank.
 template <typename T>

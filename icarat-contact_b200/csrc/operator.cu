@@ -555,10 +555,22 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   count_launch();
 }
 
+static bool g_tc_operator = false;
+bool tc_operator_enabled() { return g_tc_operator; }
+void set_tc_operator(bool on) { g_tc_operator = on; }
+
 template <typename T>
 void launch_op(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,
                cudaStream_t s, const OpExtras<T> &x)
 {
+  if constexpr(sizeof(T) == 4)
+  {
+    if(d.dim == 3 && g_tc_operator)
+    {
+      launch_op_tc(d, K, E, u, y, fix, s, x);
+      return;
+    }
+  }
   if(x.mode == OP_APPLY)
     launch_op_mode<T, OP_APPLY>(d, K, E, u, y, fix, s, x);
   else if(x.mode == OP_RESIDUAL)

@@ -15,7 +15,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(_HERE))  # icarat-contact_b200/
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libicarat_b200.so")
 HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "icarat_b200.h")
 
-FP64, MIXED = 0, 1
+FP64, MIXED, TF32 = 0, 1, 2
 JACOBI, GMG = 0, 1
 PLANE_STRESS, PLANE_STRAIN, THREE_D = 0, 1, 2
 STATUS = {0: "OK", -1: "BAD_ARG", -2: "OOM", -3: "BREAKDOWN", -4: "MAXITER", -5: "TIMEOUT",
@@ -98,6 +98,8 @@ _SIGS = {
     "icb_solve_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                     C.POINTER(SolveInfo)]),
     "icb_noalloc_max_soa": (C.c_longlong, []),
+    "icb_set_option": (C.c_int, [C.c_char_p, C.c_longlong]),
+    "icb_get_option": (C.c_longlong, [C.c_char_p]),
     "icb_cone_create": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_void_p)]),
     "icb_cone_destroy": (C.c_int, [C.c_void_p]),
     "icb_cone_filter": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
@@ -131,6 +133,14 @@ def lib():
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def set_option(name, value):
+    check(lib().icb_set_option(name.encode(), int(value)))
+
+
+def get_option(name):
+    return lib().icb_get_option(name.encode())
 
 
 def launch_count():
@@ -168,9 +178,9 @@ class Context:
         check(lib().icb_ctx_synchronize(self.h))
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().icb_ctx_destroy(self.h)
-            self.h = None
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.icb_ctx_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -197,9 +207,9 @@ class Problem:
         self.numeq = None
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().icb_problem_destroy(self.h)
-            self.h = None
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.icb_problem_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         self.close()

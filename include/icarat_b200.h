@@ -40,6 +40,7 @@ extern "C" {
 
 #define ICB_FP64 0  /* plain FP64 path: the drop-in for Solvers "Eigen_CG"   */
 #define ICB_MIXED 1 /* FP64 Krylov + operator, FP32 multigrid preconditioner */
+#define ICB_TF32 2  /* icb_operator_apply_device only: tensor-core FP32 operator */
 
 #define ICB_PRECOND_JACOBI 0 /* DiagonalPreconditioner (solvers.cpp:64-92)  */
 #define ICB_PRECOND_GMG 1    /* geometric multigrid V-cycle                 */
@@ -214,12 +215,19 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
  * component c of node n sits at c*ld + n, n in MeshIcarat numbering */
 long long icb_soa_length(icb_problem p);
 /* y = K(rho) x on device SoA vectors of icb_soa_length() entries; precision
- * ICB_FP64 (double*) or ICB_MIXED (float*); one operator launch on the
- * context's stream, no synchronisation.  Constrained rows of y are 0. */
+ * ICB_FP64 (double*), ICB_MIXED (float*, CUDA cores) or ICB_TF32 (float*,
+ * tensor cores, Hex8 only); one operator launch on the context's stream, no
+ * synchronisation.  Constrained rows of y are 0. */
 int icb_operator_apply_device(icb_problem p, int precision, const void *x, void *y);
 /* number of kernels this library has launched in the process (graph nodes
  * counted one by one) */
 long long icb_launch_count(void);
+/* process-wide switches: "tc_operator" (1: the FP32 Hex8 operator inside the
+ * ICB_MIXED V-cycle runs on the tcgen05 tensor cores in TF32; 0: CUDA
+ * cores).  icb_get_option also reports "tc_timeouts" (tensor-core waits that
+ * gave up; 0 in a healthy run).  Unknown names: ICB_ERR_BAD_ARG / -1. */
+int icb_set_option(const char *name, long long value);
+long long icb_get_option(const char *name);
 
 /* ---- solve without device allocation ------------------------------------ */
 /* No counterpart in ICARAT.  For callers that cannot allocate device memory
