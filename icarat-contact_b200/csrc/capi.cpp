@@ -263,7 +263,7 @@ int icb_finalize(icb_problem p, long long *numeq)
   p->redCnt.alloc(1);
   ICB_CUDA(cudaMemsetAsync(p->redCnt.p, 0, sizeof(unsigned), s));
   p->red = RedScratch{p->redPart.p, p->redCnt.p, mb};
-  p->pcg = std::make_unique<JacobiPcg<double>>(d);
+  p->pcg = std::make_unique<JacobiPcg<double>>(d, s);
   ICB_CUDA(cudaStreamSynchronize(s));
   if(numeq)
     *numeq = hs.numeq;

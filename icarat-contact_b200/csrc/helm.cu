@@ -152,13 +152,13 @@ HelmFilter::HelmFilter(const Dims &dims, const double *h, double R, cudaStream_t
   nint = Nint[0];
   Dims sd = d;
   sd.dim = 1; // a scalar field on the same nodes: vectors of ld entries
-  pcg = std::make_unique<JacobiPcg<double>>(sd);
+  pcg = std::make_unique<JacobiPcg<double>>(sd, s);
   dinv.alloc(d.ld);
   rhs.alloc(d.ld);
   phi.alloc(d.ld);
-  ICB_CUDA(cudaMemset(dinv.p, 0, dinv.bytes()));
-  ICB_CUDA(cudaMemset(rhs.p, 0, rhs.bytes()));
-  ICB_CUDA(cudaMemset(phi.p, 0, phi.bytes()));
+  ICB_CUDA(cudaMemsetAsync(dinv.p, 0, dinv.bytes(), s));
+  ICB_CUDA(cudaMemsetAsync(rhs.p, 0, rhs.bytes(), s));
+  ICB_CUDA(cudaMemsetAsync(phi.p, 0, phi.bytes(), s));
   unsigned nb = unsigned((d.nnode + 255) / 256);
   if(d.dim == 3)
     k_helm_diag<3><<<nb, 256, 0, s>>>(K, d, dinv.p);

@@ -187,7 +187,6 @@ void launch_sensitivity(const Dims &d, const double *K, double y1, double y2, do
                         const double *rho, const double *u, double *dc, cudaStream_t s);
 
 // reductions / vector kernels (krylov.cu)
-void red_alloc(RedScratch &r, int maxBlocks, int nvals, std::vector<void *> &owned);
 void launch_dot(long long n, const double *a, const double *b, RedScratch &red,
                 double *out, cudaStream_t s);
 void launch_axpby(long long n, double a, const double *x, double b, double *y,

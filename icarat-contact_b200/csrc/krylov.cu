@@ -234,21 +234,23 @@ int reduction_blocks(const Dims &d)
 }
 
 // ------------------------------------------------------------ JacobiPcg --
-template <typename T> JacobiPcg<T>::JacobiPcg(const Dims &dims) : d(dims)
+template <typename T> JacobiPcg<T>::JacobiPcg(const Dims &dims, cudaStream_t s) : d(dims)
 {
   n = (long long)d.dim * d.ld;
   r.alloc(n);
   p.alloc(n);
   q.alloc(n);
-  ICB_CUDA(cudaMemset(r.p, 0, r.bytes()));
-  ICB_CUDA(cudaMemset(p.p, 0, p.bytes()));
-  ICB_CUDA(cudaMemset(q.p, 0, q.bytes()));
+  // every initialisation goes to the owner's stream: the blocking memset
+  // would run on the legacy stream, which non-blocking streams do not wait for
+  ICB_CUDA(cudaMemsetAsync(r.p, 0, r.bytes(), s));
+  ICB_CUDA(cudaMemsetAsync(p.p, 0, p.bytes(), s));
+  ICB_CUDA(cudaMemsetAsync(q.p, 0, q.bytes(), s));
   st.alloc(1);
   int mb = reduction_blocks(d);
   partials.alloc((size_t)mb * 2);
   dots.alloc(4);
   counter.alloc(1);
-  ICB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned)));
+  ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
   red.partials = partials.p;
   red.counter = counter.p;
   red.maxBlocks = mb;
@@ -390,18 +392,5 @@ int pcg_run_external(const Dims &d, const double *K, const double *E, const uint
   return hostState->status;
 }
 
-void red_alloc(RedScratch &r, int maxBlocks, int nvals, std::vector<void *> &owned)
-{
-  double *p = nullptr;
-  unsigned *c = nullptr;
-  ICB_CUDA(cudaMalloc(&p, sizeof(double) * (size_t)maxBlocks * nvals));
-  owned.push_back(p);
-  ICB_CUDA(cudaMalloc(&c, sizeof(unsigned)));
-  owned.push_back(c);
-  ICB_CUDA(cudaMemset(c, 0, sizeof(unsigned)));
-  r.partials = p;
-  r.counter = c;
-  r.maxBlocks = maxBlocks;
-}
 
 } // namespace icb

@@ -28,7 +28,7 @@ template <typename T> struct JacobiPcg
   int batch = 0;
   const void *graphKey[6] = {};
 
-  explicit JacobiPcg(const Dims &dims);
+  JacobiPcg(const Dims &dims, cudaStream_t s);
   ~JacobiPcg();
   /// solve K(E) x = b; K: host pointer to the unit element matrix of this
   /// level (captured by value into the batch graph: keep it stable).

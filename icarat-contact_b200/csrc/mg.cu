@@ -189,34 +189,47 @@ __global__ void k_jacobi0(long long n, T c, const T *__restrict__ dinv,
 }
 
 // --------------------------------------------------------- coarse level ----
+/// Dense coarse matrix, row by row: the thread of free DOF (node n, c) adds
+/// the rows of its <= 8 elements in element order.  Each row has one writer,
+/// so the sums are deterministic (no atomics).
 template <typename T>
 __global__ void k_dense_assemble(Dims d, KMat<double, 24> K, const T *__restrict__ E,
                                  const int *__restrict__ dense, int n, double *A)
 {
-  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if(e >= d.nel)
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(t >= (long long)d.nnode * d.dim)
     return;
-  const int ne = d.dim == 2 ? 4 : 8, nd = ne * d.dim;
-  int ei = int(e % d.nx), ej = int((e / d.nx) % d.ny), ek = int(e / ((long long)d.nx * d.ny));
-  long long sxy = (long long)d.sx * d.sy;
-  int idx[24];
-  for(int l = 0; l < ne; l++)
-  {
-    int q = l & 3, top = l >> 2;
-    long long node = ei + ((q == 1 || q == 2) ? 1 : 0) + (long long)(ej + (q >= 2 ? 1 : 0)) * d.sx +
-                     (long long)(ek + top) * sxy;
-    for(int c = 0; c < d.dim; c++)
-      idx[l * d.dim + c] = dense[c * d.ld + node];
-  }
-  double Ee = double(E[e]);
-  for(int a = 0; a < nd; a++)
-  {
-    if(idx[a] < 0)
-      continue;
-    for(int b = 0; b < nd; b++)
-      if(idx[b] >= 0)
-        atomicAdd(A + (long long)idx[a] * n + idx[b], Ee * K.k[a * nd + b]);
-  }
+  const int c = int(t % d.dim);
+  const long long nd = t / d.dim;
+  const int row = dense[c * d.ld + nd];
+  if(row < 0)
+    return;
+  const int ne = d.dim == 2 ? 4 : 8, ndof = ne * d.dim;
+  const long long sxy = (long long)d.sx * d.sy;
+  const int i = int(nd % d.sx), j = int((nd / d.sx) % d.sy), k = d.dim == 3 ? int(nd / sxy) : 0;
+  double *Arow = A + (long long)row * n;
+  for(int dk = (d.dim == 3 ? -1 : 0); dk <= 0; dk++)
+    for(int dj = -1; dj <= 0; dj++)
+      for(int di = -1; di <= 0; di++)
+      {
+        int ei = i + di, ej = j + dj, ek = k + dk;
+        if(ei < 0 || ej < 0 || ek < 0 || ei >= d.nx || ej >= d.ny || (d.dim == 3 && ek >= d.nz))
+          continue;
+        const int a = ((-di) ^ (-dj)) + 2 * (-dj) + (d.dim == 3 ? 4 * (-dk) : 0);
+        const double Ee = double(E[ei + (long long)ej * d.nx + (long long)ek * d.nx * d.ny]);
+        const long long base = ei + (long long)ej * d.sx + (long long)ek * sxy;
+        for(int l = 0; l < ne; l++)
+        {
+          int q = l & 3, top = l >> 2;
+          long long node = base + ((q == 1 || q == 2) ? 1 : 0) + (q >= 2 ? d.sx : 0) + top * sxy;
+          for(int c2 = 0; c2 < d.dim; c2++)
+          {
+            int col = dense[c2 * d.ld + node];
+            if(col >= 0)
+              Arow[col] += Ee * K.k[(a * d.dim + c) * ndof + l * d.dim + c2];
+          }
+        }
+      }
 }
 
 /// In-place Gauss-Jordan inversion of the SPD coarse matrix (no pivoting is
@@ -602,8 +615,13 @@ template <typename TK, typename TP> struct MgPcg
 
   /// level dims, element matrices and Dirichlet masks (host), device buffers
   void build(const HostSetup &hs, const TK *Kkrylov, const TK *Ekrylov, const TP *Kfine,
-             const TP *Efine, const uint8_t *fixFine, int coarseDofs, int smooth)
+             const TP *Efine, const uint8_t *fixFine, int coarseDofs, int smooth,
+             cudaStream_t s)
   {
+    // all device initialisation goes to the solve's stream (the blocking
+    // copies and memsets run on the legacy stream, which the library's
+    // non-blocking streams do not wait for); host staging is synchronised
+    // before it goes out of scope
     nu = smooth > 0 ? smooth : 2;
     lmax = element_lmax(hs.desc.dim, Kfine);
     // Chebyshev coefficients of steps 0..nu-1 (Saad, Iterative Methods for
@@ -673,7 +691,8 @@ template <typename TK, typename TP> struct MgPcg
               cm[I + J * c.d.sx + K * (long long)c.d.sx * c.d.sy] |= fm[nd];
       }
       c.fixOwn.alloc(c.d.nnode);
-      ICB_CUDA(cudaMemcpy(c.fixOwn.p, cm.data(), cm.size(), cudaMemcpyHostToDevice));
+      ICB_CUDA(cudaMemcpyAsync(c.fixOwn.p, cm.data(), cm.size(), cudaMemcpyHostToDevice, s));
+      ICB_CUDA(cudaStreamSynchronize(s));
       c.fix = c.fixOwn.p;
       c.Eown.alloc(c.d.nel);
       c.E = c.Eown.p;
@@ -694,12 +713,13 @@ template <typename TK, typename TP> struct MgPcg
       }
       for(DevBuf<TP> *v : {&lv[l].dinv, &lv[l].r, &lv[l].t, &lv[l].x, &lv[l].b, &lv[l].dv})
         if(v->p)
-          ICB_CUDA(cudaMemset(v->p, 0, v->bytes()));
+          ICB_CUDA(cudaMemsetAsync(v->p, 0, v->bytes(), s));
     }
     // coarsest dense index map
     const Level<TP> &C = lv.back();
     std::vector<uint8_t> cmask(C.d.nnode);
-    ICB_CUDA(cudaMemcpy(cmask.data(), C.fix, C.d.nnode, cudaMemcpyDeviceToHost));
+    ICB_CUDA(cudaMemcpyAsync(cmask.data(), C.fix, C.d.nnode, cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
     std::vector<int> dense((size_t)dim * C.d.ld, -1);
     std::vector<long long> soa;
     for(long long nd = 0; nd < C.d.nnode; nd++)
@@ -715,29 +735,31 @@ template <typename TK, typename TP> struct MgPcg
     cSoa.alloc(std::max(nc, 1));
     cDense.alloc(dense.size());
     if(nc)
-      ICB_CUDA(cudaMemcpy(cSoa.p, soa.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice));
-    ICB_CUDA(cudaMemcpy(cDense.p, dense.data(), sizeof(int) * dense.size(), cudaMemcpyHostToDevice));
+      ICB_CUDA(cudaMemcpyAsync(cSoa.p, soa.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaMemcpyAsync(cDense.p, dense.data(), sizeof(int) * dense.size(),
+                             cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
     cA.alloc((size_t)std::max(nc, 1) * std::max(nc, 1));
     cStatus.alloc(1);
     n = (long long)dim * lv[0].d.ld;
     for(DevBuf<TK> *v : {&r, &p, &q})
     {
       v->alloc(n);
-      ICB_CUDA(cudaMemset(v->p, 0, v->bytes()));
+      ICB_CUDA(cudaMemsetAsync(v->p, 0, v->bytes(), s));
     }
     z.alloc(n);
-    ICB_CUDA(cudaMemset(z.p, 0, z.bytes()));
+    ICB_CUDA(cudaMemsetAsync(z.p, 0, z.bytes(), s));
     if(!same())
     {
       rP.alloc(n);
-      ICB_CUDA(cudaMemset(rP.p, 0, rP.bytes()));
+      ICB_CUDA(cudaMemsetAsync(rP.p, 0, rP.bytes(), s));
     }
     st.alloc(1);
     int mb = reduction_blocks(lv[0].d);
     partials.alloc((size_t)mb * 2);
     dots.alloc(4);
     counter.alloc(1);
-    ICB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned)));
+    ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
     red = RedScratch{partials.p, counter.p, mb};
     ICB_CUDA(cudaMallocHost(&hst, sizeof(KState)));
   }
@@ -761,7 +783,8 @@ template <typename TK, typename TP> struct MgPcg
       KMat<double, 24> kd;
       for(int i = 0; i < 576; i++)
         kd.k[i] = double(C.K[i]);
-      k_dense_assemble<TP><<<nblocks(C.d.nel, 128), 128, 0, s>>>(C.d, kd, C.E, cDense.p, nc, cA.p);
+      k_dense_assemble<TP><<<nblocks(C.d.nnode * C.d.dim, 128), 128, 0, s>>>(C.d, kd, C.E,
+                                                                            cDense.p, nc, cA.p);
       k_invert_spd<<<1, 1024, 0, s>>>(nc, cA.p, cStatus.p);
       count_launch(2);
     }
@@ -938,7 +961,7 @@ int solve_multigrid(icb_problem p, const icb_solve_opts &o, const double *b, icb
     if(!M.mg64)
     {
       M.mg64 = std::make_unique<MgPcg<double, double>>();
-      M.mg64->build(hs, p->K0, p->E.p, p->K0, p->E.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth);
+      M.mg64->build(hs, p->K0, p->E.p, p->K0, p->E.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth, s);
     }
     M.mg64->refresh(s);
     status = M.mg64->solve(b, p->x.p, o.tol, o.maxit, s, &inf);
@@ -948,7 +971,8 @@ int solve_multigrid(icb_problem p, const icb_solve_opts &o, const double *b, icb
     if(!M.mgmx)
     {
       M.mgmx = std::make_unique<MgPcg<double, float>>();
-      M.mgmx->build(hs, p->K0, p->E.p, p->K0f, p->Ef.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth);
+      M.mgmx->build(hs, p->K0, p->E.p, p->K0f, p->Ef.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth,
+                    s);
     }
     M.mgmx->refresh(s);
     status = M.mgmx->solve(b, p->x.p, o.tol, o.maxit, s, &inf);

@@ -476,15 +476,14 @@ Dims make_dims(int dim, int nx, int ny, int nz)
 
 int num_sms()
 {
-  static int n = 0;
-  if(!n)
-  {
-    int dev = 0;
+  // thread-safe one-time query (worker threads of the batch runner and the
+  // server call it concurrently)
+  static const int n = [] {
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if(n <= 0)
-      n = 148;
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
   return n;
 }
 

@@ -479,12 +479,13 @@ ConeFilter::ConeFilter(const Dims &dims, const double *h, double radius, cudaStr
   nnb = int(w.size());
   offs.alloc(off.size());
   wts.alloc(w.size());
-  ICB_CUDA(cudaMemcpy(offs.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
-  ICB_CUDA(cudaMemcpy(wts.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
+  ICB_CUDA(cudaMemcpyAsync(offs.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(wts.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, s));
   aa.alloc(d.nel);
   k_cone_aa<<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d, offs.p, wts.p, nnb, aa.p);
   ICB_CUDA(cudaGetLastError());
   count_launch();
+  ICB_CUDA(cudaStreamSynchronize(s)); // off / w are host temporaries
 }
 
 void ConeFilter::forward(const double *in, double *out, double beta, double T, double *xhat,
@@ -513,13 +514,13 @@ void launch_threshold(long long n, const double *x, double beta, double T, doubl
 }
 
 // ================================================================= OC =====
-OcUpdater::OcUpdater(const Dims &dims) : d(dims)
+OcUpdater::OcUpdater(const Dims &dims, cudaStream_t s) : d(dims)
 {
   st.alloc(1);
   int nb = vblocks(d.nel);
   partials.alloc(nb);
   counter.alloc(1);
-  ICB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned)));
+  ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
   red = RedScratch{partials.p, counter.p, nb};
   ICB_CUDA(cudaMallocHost(&hst, sizeof(OcState)));
 }
@@ -582,18 +583,18 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
 }
 
 // ================================================================ MMA =====
-MmaUpdater::MmaUpdater(long long nvar) : n(nvar)
+MmaUpdater::MmaUpdater(long long nvar, cudaStream_t s) : n(nvar)
 {
   for(DevBuf<double> *b : {&low, &upp, &alpha, &beta, &p0, &q0, &pij, &qij, &xold1, &xold2})
   {
     b->alloc(n);
-    ICB_CUDA(cudaMemset(b->p, 0, b->bytes()));
+    ICB_CUDA(cudaMemsetAsync(b->p, 0, b->bytes(), s));
   }
   st.alloc(1);
   int nb = vblocks(n);
   partials.alloc((size_t)nb * 2);
   counter.alloc(1);
-  ICB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned)));
+  ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
   red = RedScratch{partials.p, counter.p, nb};
   ICB_CUDA(cudaMallocHost(&hst, sizeof(MmaState)));
   P.epsimin = std::sqrt(double(n + 1)) * 1e-9;

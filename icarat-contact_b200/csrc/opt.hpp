@@ -57,7 +57,7 @@ struct OcUpdater
   const void *key[9] = {};
   OcParams keyP;
 
-  explicit OcUpdater(const Dims &dims);
+  OcUpdater(const Dims &dims, cudaStream_t s);
   ~OcUpdater();
   /// x <- the OC update; returns the number of bisection steps
   int update(const ConeFilter *cone, double *x, const double *df, const double *dg, double g,
@@ -97,7 +97,7 @@ struct MmaUpdater
   cudaGraphExec_t exec = nullptr;
   const void *key[3] = {};
 
-  explicit MmaUpdater(long long nvar);
+  MmaUpdater(long long nvar, cudaStream_t s);
   ~MmaUpdater();
   /// MMASolver::Update(x, dfdx, &g, dgdx, xmin, xmax); returns the dual passes
   int update(double *x, const double *dfdx, double g, const double *dgdx, const double *xmin,

@@ -3,6 +3,7 @@
 // end to end on the device (opt_macro_oc.cpp:84-172,
 // opt_mma_Helmholtz.cpp:81-163).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -246,7 +247,7 @@ int icb_oc_update(icb_problem p, icb_cone cone, double *x, const double *dfdx, d
   ICB_CUDA(cudaMemcpyAsync(HI.p, xmax, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, p->hs->volume, V.p);
   count_launch();
-  OcUpdater oc(p->d);
+  OcUpdater oc(p->d, s);
   OcParams P;
   P.move = movelimit;
   P.beta = beta;
@@ -268,7 +269,7 @@ int icb_mma_create(icb_ctx ctx, long long n, int m, icb_mma *out)
   ICB_CUDA(cudaSetDevice(ctx->device));
   auto h = std::make_unique<icb_mma_s>();
   h->ctx = ctx;
-  h->m = std::make_unique<MmaUpdater>(n);
+  h->m = std::make_unique<MmaUpdater>(n, ctx->stream);
   for(DevBuf<double> *b : {&h->x, &h->df, &h->dg, &h->lo, &h->hi})
     b->alloc(n);
   *out = h.release();
@@ -316,7 +317,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   const long long n = p->d.nel;
   const double vol = p->hs->volume;
   ConeFilter cone(p->d, p->hs->h, o->filter_radius, s);
-  OcUpdater oc(p->d);
+  OcUpdater oc(p->d, s);
   DevBuf<double> x(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n), V(n);
   ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
@@ -329,6 +330,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   P.move = o->move_limit;
   for(int step = 1; step <= o->nsteps; step++)
   {
+    auto t0 = std::chrono::steady_clock::now();
     const double beta = o->use_threshold ? std::min(std::pow(2.0, (int)(step / 40)), 16.0) : 0.0;
     cone.forward(x.p, xf.p, beta, 0.5, xh.p, dxh.p, s); // beta 0: xh = xf, dxh = 1
     int rc = icb_set_density_device(p, xh.p);
@@ -354,6 +356,9 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
     cone.adjoint(dv.p, dvf.p, s);
     P.beta = beta;
     oc.update(&cone, x.p, dcf.p, dvf.p, V0, lo.p, hi.p, V.p, P, s);
+    if(o->iter_seconds)
+      o->iter_seconds[step - 1] =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -376,7 +381,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
   const long long n = p->d.nel;
   const double vol = p->hs->volume;
   HelmFilter helm(p->d, p->hs->h, o->filter_radius, s);
-  MmaUpdater mma(n);
+  MmaUpdater mma(n, s);
   DevBuf<double> x(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n);
   ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
@@ -386,6 +391,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
   double V0 = o->volume_ref;
   for(int step = 1; step <= o->nsteps; step++)
   {
+    auto t0 = std::chrono::steady_clock::now();
     icb_solve_info hi_{};
     int rc = helm.apply(x.p, xf.p, false, 1e-10, s, &hi_);
     if(rc)
@@ -420,6 +426,10 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     if(rc)
       throw Error{rc, "Helmholtz filter solve did not converge"};
     mma.update(x.p, dcf.p, g, dvf.p, lo.p, hi.p, s);
+    ICB_CUDA(cudaStreamSynchronize(s));
+    if(o->iter_seconds)
+      o->iter_seconds[step - 1] =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));

@@ -18,6 +18,7 @@ HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "icarat_b200.h")
 FP64, MIXED, TF32 = 0, 1, 2
 JACOBI, GMG = 0, 1
 PLANE_STRESS, PLANE_STRAIN, THREE_D = 0, 1, 2
+JOB_OC, JOB_MMA = 0, 1
 STATUS = {0: "OK", -1: "BAD_ARG", -2: "OOM", -3: "BREAKDOWN", -4: "MAXITER", -5: "TIMEOUT",
           -6: "NAN", -7: "CUDA", -8: "STATE", -9: "REJECTED"}
 
@@ -51,7 +52,19 @@ class SolveInfo(C.Structure):
 
 class LoopOpts(C.Structure):
     _fields_ = [("nsteps", C.c_int), ("filter_radius", C.c_double), ("move_limit", C.c_double),
-                ("use_threshold", C.c_int), ("volume_ref", C.c_double), ("solve", SolveOpts)]
+                ("use_threshold", C.c_int), ("volume_ref", C.c_double), ("solve", SolveOpts),
+                ("iter_seconds", _dp)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("grid", GridDesc), ("kind", C.c_int), ("loop", LoopOpts),
+                ("fixed", _u8p), ("load", _dp), ("rho0", _dp)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("submit_s", C.c_double),
+                ("start_s", C.c_double), ("end_s", C.c_double), ("bytes", C.c_longlong),
+                ("nsteps", C.c_int)]
 
 
 class IcbError(RuntimeError):
@@ -99,6 +112,16 @@ _SIGS = {
                                     C.POINTER(SolveInfo)]),
     "icb_noalloc_max_soa": (C.c_longlong, []),
     "icb_set_option": (C.c_int, [C.c_char_p, C.c_longlong]),
+    "icb_run_batch": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), _ip, C.POINTER(LoopOpts),
+                                C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.c_int, _ip]),
+    "icb_job_footprint": (C.c_longlong, [C.POINTER(GridDesc), C.c_int]),
+    "icb_server_create": (C.c_int, [C.c_int, C.c_longlong, C.c_int, C.POINTER(C.c_void_p)]),
+    "icb_server_submit": (C.c_int, [C.c_void_p, C.POINTER(JobDesc), _llp]),
+    "icb_server_wait": (C.c_int, [C.c_void_p, C.c_longlong, C.c_double, C.POINTER(JobInfo)]),
+    "icb_server_result": (C.c_int, [C.c_void_p, C.c_longlong, _dp, _dp, _dp]),
+    "icb_server_cancel": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "icb_server_forget": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "icb_server_destroy": (C.c_int, [C.c_void_p]),
     "icb_get_option": (C.c_longlong, [C.c_char_p]),
     "icb_cone_create": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_void_p)]),
     "icb_cone_destroy": (C.c_int, [C.c_void_p]),
@@ -414,10 +437,82 @@ def run_loop(prob, kind, rho0, nsteps, radius, move=0.15, use_threshold=True, vo
              precision=FP64, precond=GMG, tol=1e-8, maxit=20000):
     """icb_run_oc (kind "oc") or icb_run_mma (kind "mma"): compliance history, design."""
     o = LoopOpts(nsteps, radius, move, int(use_threshold), volume_ref,
-                 SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0))
+                 SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0), None)
     hist = np.zeros(nsteps)
     x = np.zeros(prob.nel)
     rho0 = np.ascontiguousarray(rho0, np.float64)
     f = lib().icb_run_oc if kind == "oc" else lib().icb_run_mma
     check(f(prob.h, C.byref(o), _p(rho0), _p(hist), _p(x)))
     return hist, x
+
+
+# ------------------------------------------------------------ batch/serve --
+def loop_opts(nsteps, radius, move=0.15, use_threshold=True, volume_ref=0.0, precision=FP64,
+              precond=GMG, tol=1e-8, maxit=20000):
+    return LoopOpts(nsteps, radius, move, int(use_threshold), volume_ref,
+                    SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0), None)
+
+
+def run_batch(probs, kinds, opts, rho0s, nworkers):
+    """icb_run_batch: returns (hists, xs, statuses)."""
+    n = len(probs)
+    H = [np.zeros(o.nsteps) for o in opts]
+    X = [np.zeros(p.nel) for p in probs]
+    R = [np.ascontiguousarray(r, np.float64) for r in rho0s]
+    ph = (C.c_void_p * n)(*[p.h.value for p in probs])
+    kk = np.asarray(kinds, np.int32)
+    oo = (LoopOpts * n)(*opts)
+    rr = (_dp * n)(*[_p(r) for r in R])
+    hh = (_dp * n)(*[_p(h) for h in H])
+    xx = (_dp * n)(*[_p(x) for x in X])
+    st = np.zeros(n, np.int32)
+    rc = lib().icb_run_batch(n, ph, _p(kk, _ip), oo, rr, hh, xx, nworkers, _p(st, _ip))
+    check(rc)
+    return H, X, st
+
+
+class Server:
+    """icb_server: continuous batching of app-loop jobs on one GPU."""
+
+    def __init__(self, device=0, budget_bytes=150 << 30, slots=8):
+        h = C.c_void_p()
+        check(lib().icb_server_create(device, int(budget_bytes), slots, C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, grid, kind, loop, fixed, load, rho0):
+        fixed = np.ascontiguousarray(fixed, np.uint8)
+        load = np.ascontiguousarray(load, np.float64)
+        rho0 = np.ascontiguousarray(rho0, np.float64)
+        jd = JobDesc(grid, kind, loop, _p(fixed, _u8p), _p(load), _p(rho0))
+        jid = C.c_longlong()
+        check(lib().icb_server_submit(self.h, C.byref(jd), C.byref(jid)))
+        self._keep[jid.value] = (loop.nsteps, grid)
+        return jid.value
+
+    def wait(self, jid, timeout=-1.0):
+        info = JobInfo()
+        rc = lib().icb_server_wait(self.h, jid, timeout, C.byref(info))
+        return rc, info
+
+    def result(self, jid):
+        nsteps, grid = self._keep[jid]
+        nel = grid.nx * grid.ny * (grid.nz if grid.dim == 3 else 1)
+        hist, x, it = np.zeros(nsteps), np.zeros(nel), np.zeros(nsteps)
+        check(lib().icb_server_result(self.h, jid, _p(hist), _p(x), _p(it)))
+        return hist, x, it
+
+    def cancel(self, jid):
+        return lib().icb_server_cancel(self.h, jid)
+
+    def forget(self, jid):
+        self._keep.pop(jid, None)
+        return lib().icb_server_forget(self.h, jid)
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.icb_server_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()

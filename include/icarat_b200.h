@@ -199,6 +199,7 @@ typedef struct
   int use_threshold;    /* beta = min(2^(step/40), 16) projection (icb_run_oc) */
   double volume_ref;    /* icb_run_mma: V0 of the constraint (<= 0: step-1 volume) */
   icb_solve_opts solve; /* the structural solve of every step                */
+  double *iter_seconds; /* optional [nsteps]: wall time of every step (or NULL) */
 } icb_loop_opts;
 /* opt-macro-oc/opt_macro_oc.cpp:84-172: cone filter, threshold, solve,
  * compliance, V0 at step 1, sensitivities, adjoint filter, OC; hist[nsteps]
@@ -209,6 +210,58 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
  * threshold, solve, volume constraint, sensitivities, adjoint filters, MMA. */
 int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
                 double *xout);
+
+/* ---- many runs on one GPU: batch runner and job server ------------------- */
+/* No counterpart in ICARAT (one problem per process).  Runs are independent
+ * icb_problems; give each one its own icb_ctx (stream) so their kernels
+ * overlap.  Results do not depend on what else runs. */
+#define ICB_JOB_OC 0  /* icb_run_oc: cone filter + OC (opt_macro_oc)              */
+#define ICB_JOB_MMA 1 /* icb_run_mma: Helmholtz filter + MMA (opt_mma_Helmholtz) */
+/* run n app loops with nworkers host threads; kinds may be NULL (all OC),
+ * xout may be NULL; status[n] (may be NULL) gets each run's status */
+int icb_run_batch(int n, const icb_problem *probs, const int *kinds, const icb_loop_opts *opts,
+                  const double *const *rho0, double *const *hist, double *const *xout,
+                  int nworkers, int *status);
+
+typedef struct icb_server_s *icb_server;
+#define ICB_JOB_QUEUED 0
+#define ICB_JOB_RUNNING 1
+#define ICB_JOB_DONE 2
+#define ICB_JOB_CANCELLED 3
+typedef struct
+{
+  icb_grid_desc grid;
+  int kind;                   /* ICB_JOB_OC | ICB_JOB_MMA                       */
+  icb_loop_opts loop;         /* iter_seconds is ignored (the server keeps them) */
+  const unsigned char *fixed; /* neq Dirichlet flags (node-major, interleaved)   */
+  const double *load;         /* neq nodal loads                                 */
+  const double *rho0;         /* nel initial design                              */
+} icb_job_desc;
+typedef struct
+{
+  int state, status;
+  double submit_s, start_s, end_s; /* seconds since the server was created */
+  long long bytes;                 /* device footprint the job was admitted with */
+  int nsteps;
+} icb_job_info;
+/* estimated device bytes of one run (what admission charges against the budget) */
+long long icb_job_footprint(const icb_grid_desc *g, int kind);
+/* a server with `slots` workers (one stream each) and an HBM budget: a queued
+ * job starts as soon as a worker is free and its footprint fits what the
+ * running jobs leave of the budget (the first queued job that fits) */
+int icb_server_create(int device, long long budget_bytes, int slots, icb_server *out);
+/* copies the job's arrays; ICB_ERR_REJECTED when it can never fit the budget */
+int icb_server_submit(icb_server s, const icb_job_desc *job, long long *id);
+/* waits up to timeout_s (< 0: forever) for the job; ICB_ERR_TIMEOUT if still running */
+int icb_server_wait(icb_server s, long long id, double timeout_s, icb_job_info *info);
+/* hist[nsteps], x[nel], iter_seconds[nsteps] (any may be NULL) of a finished job */
+int icb_server_result(icb_server s, long long id, double *hist, double *x, double *iter_seconds);
+/* cancels a job that has not started (ICB_ERR_STATE otherwise) */
+int icb_server_cancel(icb_server s, long long id);
+/* drops a finished job's record and results */
+int icb_server_forget(icb_server s, long long id);
+/* cancels queued jobs, waits for running ones, joins the workers */
+int icb_server_destroy(icb_server s);
 
 /* ---- device-level access (benchmarks, interop) --------------------------- */
 /* length of one SoA field vector on the device (dim * padded node count):

@@ -93,3 +93,75 @@ def build_gpu(ctx, kind, nx, ny, nz=1):
         p.nodal_load(n, f.reshape(-1, dim)[n])
     p.finalize()
     return p
+
+
+# ------------------------------------------------------- batched / served --
+def _edge_mask2d(nx, ny, edge):
+    fixed = np.zeros((ny + 1, nx + 1, 2), np.uint8)
+    if edge == 0:
+        fixed[:, 0, :] = 1
+    elif edge == 1:
+        fixed[:, nx, :] = 1
+    elif edge == 2:
+        fixed[0, :, :] = 1
+    else:
+        fixed[ny, :, :] = 1
+    return fixed
+
+
+def random_instance2d(rng, nelx_range=(64, 1024), aspect_range=(1.0, 4.0), vf_range=(0.2, 0.6),
+                      r_range=(1.2, 4.0), aspect_fixed=None):
+    """One batched/served 2D instance: nelx log-uniform, aspect uniform (or
+    fixed), a random clamped edge, 1-4 unit point loads (direction uniform on
+    the circle) at random boundary nodes off the clamped edge."""
+    lo, hi = nelx_range
+    nx = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+    a = aspect_fixed if aspect_fixed else rng.uniform(*aspect_range)
+    ny = max(1, int(round(nx / a)))
+    vf, r = rng.uniform(*vf_range), rng.uniform(*r_range)
+    edge = int(rng.integers(4))
+    fixed = _edge_mask2d(nx, ny, edge)
+    boundary = [(j, i) for j in range(ny + 1) for i in range(nx + 1)
+                if (i in (0, nx) or j in (0, ny)) and not fixed[j, i].any()]
+    load = np.zeros((ny + 1, nx + 1, 2))
+    for k in rng.choice(len(boundary), size=int(rng.integers(1, 5)), replace=False):
+        j, i = boundary[k]
+        th = rng.uniform(0, 2 * np.pi)
+        load[j, i] += (np.cos(th), np.sin(th))
+    return dict(dim=2, nx=nx, ny=ny, nz=1, vf=vf, r=r, fixed=fixed.reshape(-1),
+                load=load.reshape(-1))
+
+
+def random_instance3d(rng, nelx_range=(32, 128), vf_range=(0.2, 0.5), r_range=(1.5, 3.0)):
+    """A served 3D job: nelx uniform, nely = nelz = nelx/2, x = 0 clamped,
+    1-4 unit loads in random directions at random nodes of the x = L face."""
+    nx = int(rng.integers(nelx_range[0], nelx_range[1] + 1))
+    ny = nz = max(1, nx // 2)
+    fixed = np.zeros((nz + 1, ny + 1, nx + 1, 3), np.uint8)
+    fixed[:, :, 0, :] = 1
+    load = np.zeros((nz + 1, ny + 1, nx + 1, 3))
+    for _ in range(int(rng.integers(1, 5))):
+        v = rng.standard_normal(3)
+        load[rng.integers(nz + 1), rng.integers(ny + 1), nx] += v / np.linalg.norm(v)
+    return dict(dim=3, nx=nx, ny=ny, nz=nz, vf=rng.uniform(*vf_range), r=rng.uniform(*r_range),
+                fixed=fixed.reshape(-1), load=load.reshape(-1))
+
+
+def grid_desc(inst):
+    import icarat_b200 as icb
+    d = inst["dim"]
+    return icb.GridDesc(d, inst["nx"], inst["ny"], inst["nz"] if d == 3 else 1,
+                        float(inst["nx"]), float(inst["ny"]), float(inst["nz"] if d == 3 else 1),
+                        icb.THREE_D if d == 3 else icb.PLANE_STRESS, EMIN, E0, NU, PENAL)
+
+
+def build_instance(ctx, inst):
+    import icarat_b200 as icb
+    d = inst["dim"]
+    p = icb.Problem(ctx, d, inst["nx"], inst["ny"], inst["nz"], young=(EMIN, E0), nu=NU, penal=PENAL)
+    p.dirichlet_mask(inst["fixed"])
+    L = inst["load"].reshape(-1, d)
+    for n in np.nonzero(np.abs(L).sum(1))[0]:
+        p.nodal_load(n, L[n])
+    p.finalize()
+    return p
