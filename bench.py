@@ -266,21 +266,10 @@ def ours_arm(args):
            "h2d_bytes_per_step": 8 * prob.nel,
            "d2h_bytes_per_step": 8 * (numeq + prob.nel + 1)}
 
-    # ---- roofline of the dominant kernel (FP64 operator), timed live
-    nsoa = prob.soa_length()
-    x = torch.randn(nsoa, dtype=torch.float64, device=f"cuda:{local}")
-    y = torch.empty_like(x)
+    # ---- roofline of the dominant kernel (FP64 operator), timed live with
+    # an L2 flush before every launch
     prob.set_density_device(rho_d.data_ptr())
-    for _ in range(5):
-        prob.operator_apply_device(x.data_ptr(), y.data_ptr(), icb.FP64)
-    R = 50
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for _ in range(R):
-        prob.operator_apply_device(x.data_ptr(), y.data_ptr(), icb.FP64)
-    g1.record(stream)
-    torch.cuda.synchronize()
-    t_mv = g0.elapsed_time(g1) / R * 1e-3
+    t_mv = op_launch_seconds(prob, icb.FP64, stream, local)
     ndof = prob.neq
     alg_bytes = 8 * (2 * ndof + prob.nel)
     flops = 2 * 576 * prob.nel
@@ -338,6 +327,309 @@ def ours_arm(args):
     return 0
 
 
+# ------------------------------------------------------------- workloads --
+def _clock_wrap(fn):
+    clk = clocks_start(int(os.environ.get("LOCAL_RANK", "0")))
+    try:
+        return fn(), clocks_stop(clk)
+    except BaseException:
+        clocks_stop(clk)
+        raise
+
+
+def smooth_field(nx, ny, nz, seed, lo=0.001, hi=1.0, modes=16):
+    """Seeded smooth random density: affine map to [lo, hi] of
+    sum_k a_k cos(2 pi (k . x_c / L) + phi_k), k integer triples in [0,4]^3,
+    a_k ~ N(0,1), phi_k ~ U[0, 2 pi), at element centres."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+    f = np.zeros((nz, ny, nx))
+    for _ in range(modes):
+        k = rng.integers(0, 5, 3)
+        a, ph = rng.standard_normal(), rng.uniform(0, 2 * np.pi)
+        # separable evaluation of cos(2 pi (kx x + ky y + kz z) + ph)
+        cx, sx = np.cos(2 * np.pi * k[0] * x), np.sin(2 * np.pi * k[0] * x)
+        cy, sy = np.cos(2 * np.pi * k[1] * y), np.sin(2 * np.pi * k[1] * y)
+        cz, sz = np.cos(2 * np.pi * k[2] * z + ph), np.sin(2 * np.pi * k[2] * z + ph)
+        cxy = np.outer(cy, cx) - np.outer(sy, sx)
+        sxy = np.outer(sy, cx) + np.outer(cy, sx)
+        f += a * (cz[:, None, None] * cxy[None] - sz[:, None, None] * sxy[None])
+    f = (f - f.min()) / max(f.max() - f.min(), 1e-300)
+    return (lo + (hi - lo) * f).reshape(-1)
+
+
+def op_launch_seconds(prob, prec, stream, device=0, reps=30):
+    """Mean device time of one icb_operator_apply_device launch, each launch
+    bracketed by CUDA events on the problem's stream and preceded by a write
+    of 256 MiB (> L2) on that stream."""
+    import torch
+    import icarat_b200 as icb
+    dt = torch.float64 if prec == icb.FP64 else torch.float32
+    nsoa = prob.soa_length()
+    x = torch.randn(nsoa, dtype=dt, device=f"cuda:{device}")
+    y = torch.empty_like(x)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    torch.cuda.synchronize()
+    for _ in range(3):
+        prob.operator_apply_device(x.data_ptr(), y.data_ptr(), prec)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    with torch.cuda.stream(stream):
+        for a, b in ev:
+            flush.fill_(1)
+            a.record(stream)
+            prob.operator_apply_device(x.data_ptr(), y.data_ptr(), prec)
+            b.record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev) / reps * 1e-3
+
+
+def workload_operator(args):
+    """The Hex8 operator y = K(rho) x in each precision (FP64 SIMT, FP32 SIMT,
+    TF32 tcgen05) at 192x64x64 and 384x128x128, L2 flushed before every
+    launch; algorithmic bytes 8|4 x (2 x DOF + elements)."""
+    import torch
+    import cases
+    import icarat_b200 as icb
+    ctx = icb.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    peak, src = _peaks()
+    rows = []
+    for n in ((192, 64, 64), (384, 128, 128)):
+        g = cases.build_gpu(ctx, "cantilever3d", *n)
+        g.set_density(cases.uniform_density(g.nel, SEED))
+        for name, prec, tc, es in (("fp64", icb.FP64, 0, 8), ("fp32_simt", icb.MIXED, 0, 4),
+                                   ("tf32_tcgen05", icb.TF32, 1, 4)):
+            icb.set_option("tc_operator", tc)
+            t = op_launch_seconds(g, prec, stream)
+            B = es * (2 * g.neq + g.nel)
+            rows.append({"grid": "x".join(map(str, n)), "variant": name, "launch_us": t * 1e6,
+                         "alg_GBps": B / t / 1e9, "frac_of_" + src: B / t / 1e9 / peak,
+                         "elem_per_s": g.nel / t})
+        icb.set_option("tc_operator", 0)
+        g.close()
+    print(json.dumps({"metric": "Hex8 operator launch time", "unit": "us", "rows": rows,
+                      "tc_timeouts": icb.get_option("tc_timeouts"),
+                      "config": {"workload": "cantilever3d densities U[0.01,1], L2 flushed"}}), flush=True)
+    ctx.close()
+    return 0
+
+
+def workload_c1(args):
+    """c1: the opt-macro-oc loop, 120x40 Q4 cantilever, cone r = 1.5, move
+    0.2, threshold schedule, 50 steps; topopt iter/s on the GPU (FP64 GMG
+    solves) beside the oracle's loop on the host cores."""
+    import numpy as np
+    import cases
+    import icarat_b200 as icb
+    ctx = icb.Context(0)
+    g = cases.build_gpu(ctx, "cantilever2d", 120, 40)
+    rho0 = np.full(g.nel, 0.5)
+    icb.run_loop(g, "oc", rho0, 3, 1.5, move=0.2)
+    res = {}
+    for name, kw in (("fp64_jacobi", dict(precond=icb.JACOBI)), ("fp64_gmg", dict(precond=icb.GMG))):
+        o = icb.loop_opts(50, 1.5, move=0.2, precond=kw["precond"])
+        its = np.zeros(50)
+        o.iter_seconds = its.ctypes.data_as(icb._dp)
+        hist, x = np.zeros(50), np.zeros(g.nel)
+        t0 = time.perf_counter()
+        icb.check(icb.lib().icb_run_oc(g.h, icb.C.byref(o), icb._p(rho0), icb._p(hist), icb._p(x)))
+        dt = time.perf_counter() - t0
+        res[name] = {"iter_s": 50 / dt, "p50_ms": 1e3 * float(np.median(its)),
+                     "p99_ms": 1e3 * float(np.quantile(its, 0.99)), "c_first": hist[0], "c_last": hist[-1]}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    o = cases.build_oracle("cantilever2d", 120, 40)
+    t0 = time.perf_counter()
+    ho, xo, _ = o.oc_loop(rho0, 50, 1.5, 0.2, use_beta=True, tol=1e-8)
+    dt = time.perf_counter() - t0
+    best = max(v["iter_s"] for v in res.values())
+    print(json.dumps({"metric": "topopt iter/s (opt-macro-oc loop, c1 120x40 Q4, 50 steps)",
+                      "value": best, "unit": "iter/s", "n_gpus": 1, "higher_is_better": True,
+                      "dtype": "f64", "data": "synthetic (uniform 0.5 start)",
+                      "config": {"workload": "c1 cantilever2d 120x40, cone r=1.5, move 0.2, beta schedule"},
+                      "paths": res,
+                      "history_rel_diff_vs_oracle": float(np.max(np.abs(
+                          icb.run_loop(g, "oc", rho0, 50, 1.5, move=0.2)[0] - ho) / np.abs(ho))),
+                      "cpu_baseline": {"value": 50 / dt, "unit": "iter/s", "cores": po.lib().orc_num_threads(),
+                                       "kind": "port", "sample": "the full 50-step loop (assembled CSR Jacobi-PCG, tol 1e-8)"}}),
+          flush=True)
+    return 0
+
+
+def workload_c3(args):
+    """c3: 384x128x128 Hex8 half-MBB (19,220,355 DOF), smooth seeded density
+    field on [0.001, 1], Helmholtz R = 3, volume fraction 0.3, 20 MMA steps
+    with mixed-precision GMG solves; plus the mixed solve against the FP64
+    solve on the initial design."""
+    import numpy as np
+    import cases
+    import icarat_b200 as icb
+    n = tuple(args.size) if args.size else (384, 128, 128)
+    steps = args.mma_steps
+    ctx = icb.Context(0)
+    g = cases.build_gpu(ctx, "halfmbb3d", *n)
+    rho0 = smooth_field(*n, seed=SEED)
+    # mixed vs FP64 on the initial design (same densities, same tolerance)
+    g.set_density(rho0)
+    out = {}
+    for name, prec in (("fp64_gmg", icb.FP64), ("mixed_gmg", icb.MIXED)):
+        g.solve(precision=prec, precond=icb.GMG, tol=TOL, maxit=20000)
+        t0 = time.perf_counter()
+        inf = g.solve(precision=prec, precond=icb.GMG, tol=TOL, maxit=20000)
+        dt = time.perf_counter() - t0
+        out[name] = {"ms": 1e3 * dt, "iters": inf["iters"], "true_relres": inf["true_relres"],
+                     "compliance": g.compliance(), "dc": g.sensitivity()}
+    err = {"compliance_rel": abs(out["mixed_gmg"]["compliance"] - out["fp64_gmg"]["compliance"]) /
+                             abs(out["fp64_gmg"]["compliance"]),
+           "sens_linf_rel": float(np.abs(out["mixed_gmg"]["dc"] - out["fp64_gmg"]["dc"]).max() /
+                                  np.abs(out["fp64_gmg"]["dc"]).max())}
+    for v in out.values():
+        v.pop("dc")
+    vol = float(np.prod(n))
+    o = icb.loop_opts(steps, 3.0, precision=icb.MIXED, volume_ref=0.3 * vol)
+    its = np.zeros(steps)
+    o.iter_seconds = its.ctypes.data_as(icb._dp)
+    hist, x = np.zeros(steps), np.zeros(g.nel)
+    t0 = time.perf_counter()
+    icb.check(icb.lib().icb_run_mma(g.h, icb.C.byref(o), icb._p(rho0), icb._p(hist), icb._p(x)))
+    dt = time.perf_counter() - t0
+    print(json.dumps({"metric": "topopt iter/s (MMA + Helmholtz loop, c3 half-MBB, mixed precision)",
+                      "value": steps / dt, "unit": "iter/s", "n_gpus": 1, "higher_is_better": True,
+                      "dtype": "f64 Krylov / f32 multigrid", "data": "synthetic (seeded smooth field)",
+                      "config": {"workload": f"halfmbb3d {n[0]}x{n[1]}x{n[2]}", "dof": g.neq,
+                                 "helmholtz_R": 3.0, "volfrac": 0.3, "steps": steps, "tol": TOL},
+                      "latency_ms": {"p50": 1e3 * float(np.median(its)),
+                                     "p99": 1e3 * float(np.quantile(its, 0.99))},
+                      "solve_initial_design": out, "mixed_vs_fp64": err,
+                      "compliance_history": hist.tolist()}), flush=True)
+    return 0
+
+
+def workload_batched(args):
+    """c4: seeded 2D instances (nelx log-uniform 64-1024, aspect U[1,4], vf
+    U[0.2,0.6], r U[1.2,4], one clamped edge, 1-4 unit point loads), OC loop
+    with mixed-precision GMG solves, run by icb_run_batch with one stream per
+    instance; instance-iterations/s against the same runs one at a time."""
+    import numpy as np
+    import cases
+    import icarat_b200 as icb
+    N, steps = args.instances, args.loop_steps
+    rng = np.random.default_rng(4)
+    insts = [cases.random_instance2d(rng) for _ in range(N)]
+    nel_total = sum(i["nx"] * i["ny"] for i in insts)
+    runs, ref = {}, None
+    for W in args.workers:
+        ctxs = [icb.Context(0) for _ in range(N)]
+        probs = [cases.build_instance(c, i) for c, i in zip(ctxs, insts)]
+        opts = [icb.loop_opts(steps, i["r"], move=0.2, precision=icb.MIXED) for i in insts]
+        rho0 = [np.full(p.nel, i["vf"]) for p, i in zip(probs, insts)]
+        t0 = time.perf_counter()
+        H, X, S = icb.run_batch(probs, [icb.JOB_OC] * N, opts, rho0, nworkers=W)
+        dt = time.perf_counter() - t0
+        runs[W] = {"seconds": dt, "inst_iter_s": N * steps / dt, "all_ok": bool((S == 0).all())}
+        if ref is None:
+            ref = (H, X)
+        else:
+            runs[W]["bitwise_equal_to_first"] = all(np.array_equal(a, b) for a, b in zip(ref[0], H)) and \
+                all(np.array_equal(a, b) for a, b in zip(ref[1], X))
+        for p in probs:
+            p.close()
+        for c in ctxs:
+            c.close()
+    seq = runs.get(1, {}).get("inst_iter_s")
+    best_w = max(runs, key=lambda w: runs[w]["inst_iter_s"])
+    print(json.dumps({"metric": "instance-iterations/s (c4 batched 2D OC)", "value": runs[best_w]["inst_iter_s"],
+                      "unit": "instance-iter/s", "n_gpus": 1, "higher_is_better": True,
+                      "dtype": "f64 Krylov / f32 multigrid", "data": "synthetic (seeded instances)",
+                      "config": {"workload": f"{N} 2D Q4 instances, {nel_total} elements in total",
+                                 "oc_steps": steps, "workers": best_w},
+                      "speedup_vs_sequential": (runs[best_w]["inst_iter_s"] / seq) if seq else None,
+                      "runs": {str(k): v for k, v in runs.items()}}), flush=True)
+    return 0
+
+
+def workload_serving(args):
+    """c5: Poisson job arrivals at each rate lambda into one icb_server (HBM
+    budget 150 GB).  Jobs: 70 % 2D Q4 OC (nelx U[64,1024], aspect 2:1), 30 %
+    3D Hex8 MMA (nelx U[32,128], nely = nelz = nelx/2), vf U[0.2,0.5],
+    r U[1.5,3]; steps U[50,200] scaled by --iter-scale.  Per rate: jobs/s
+    (completed / makespan), p50/p99 job latency (submit to end) and
+    iteration latency; finally one job re-run alone against its mixed run."""
+    import numpy as np
+    import cases
+    import icarat_b200 as icb
+    rates = args.rates
+    out = {}
+    probe = None
+    for lam in rates:
+        rng = np.random.default_rng(5000 + int(lam))
+        jobs = []
+        for _ in range(args.jobs_per_rate):
+            if rng.uniform() < 0.7:
+                inst = cases.random_instance2d(rng, nelx_range=(64, 1024), aspect_fixed=2.0,
+                                               vf_range=(0.2, 0.5), r_range=(1.5, 3.0))
+                kind = icb.JOB_OC
+            else:
+                inst = cases.random_instance3d(rng, nelx_range=(32, 128), vf_range=(0.2, 0.5),
+                                               r_range=(1.5, 3.0))
+                kind = icb.JOB_MMA
+            nsteps = max(1, int(round(rng.integers(50, 201) * args.iter_scale)))
+            nel = inst["nx"] * inst["ny"] * (inst["nz"] if inst["dim"] == 3 else 1)
+            loop = icb.loop_opts(nsteps, inst["r"] if kind == icb.JOB_OC else 2.0 * inst["r"] / 1.5,
+                                 move=0.2, precision=icb.MIXED)
+            jobs.append((cases.grid_desc(inst), kind, loop, inst["fixed"], inst["load"],
+                         np.full(nel, inst["vf"])))
+        gaps = rng.exponential(1.0 / lam, len(jobs))
+        srv = icb.Server(budget_bytes=150 << 30, slots=args.slots)
+        t0 = time.perf_counter()
+        ids, tnext = [], t0
+        for j, gap in zip(jobs, gaps):
+            tnext += gap
+            while time.perf_counter() < tnext:
+                time.sleep(min(0.002, max(0.0, tnext - time.perf_counter())))
+            ids.append(srv.submit(*j))
+        lat, its, ends, starts, ok = [], [], [], [], 0
+        for k, jid in enumerate(ids):
+            rc, info = srv.wait(jid)
+            if rc == 0 and info.status == 0:
+                ok += 1
+                h, x, it = srv.result(jid)
+                lat.append(info.end_s - info.submit_s)
+                its.extend(it.tolist())
+                ends.append(info.end_s)
+                starts.append(info.submit_s)
+                if probe is None and jobs[k][1] == icb.JOB_OC:
+                    probe = (jobs[k], h, x)
+            srv.forget(jid)
+        srv.close()
+        span = max(ends) - min(starts) if ends else float("nan")
+        out[str(lam)] = {"jobs": len(jobs), "completed": ok, "jobs_per_s": ok / span,
+                         "job_latency_s": {"p50": float(np.median(lat)), "p99": float(np.quantile(lat, 0.99))},
+                         "iter_latency_ms": {"p50": 1e3 * float(np.median(its)),
+                                             "p99": 1e3 * float(np.quantile(its, 0.99))}}
+        print(json.dumps({"rate": lam, **out[str(lam)]}), file=sys.stderr, flush=True)
+    alone_equal = None
+    if probe is not None:
+        srv = icb.Server(budget_bytes=150 << 30, slots=1)
+        jid = srv.submit(*probe[0])
+        srv.wait(jid)
+        h, x, _ = srv.result(jid)
+        srv.close()
+        alone_equal = bool(np.array_equal(h, probe[1]) and np.array_equal(x, probe[2]))
+    best = max(out.values(), key=lambda v: v["jobs_per_s"])
+    print(json.dumps({"metric": "served jobs/s (c5 Poisson mix, 150 GB admission budget)",
+                      "value": best["jobs_per_s"], "unit": "jobs/s", "n_gpus": 1, "higher_is_better": True,
+                      "dtype": "f64 Krylov / f32 multigrid", "data": "synthetic (seeded job stream)",
+                      "config": {"workload": "70% 2D Q4 OC nelx 64-1024 aspect 2:1, 30% 3D Hex8 MMA nelx 32-128",
+                                 "jobs_per_rate": args.jobs_per_rate, "iter_scale": args.iter_scale,
+                                 "slots": args.slots},
+                      "rates": out, "alone_vs_mixed_bitwise_equal": alone_equal}), flush=True)
+    return 0
+
+
 def profile_operator(args):
     """Set up the bench problem and launch each operator variant 3 times (for
     an ncu capture of k_matvec_h8 on the full workload; no timing printed)."""
@@ -368,9 +660,23 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-operator", action="store_true",
                     help="only launch the operator kernels on the bench problem (for ncu)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "batched", "serving", "operator"],
+                    help="c2 (default): the bench line; the others print their own line")
+    ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 grid override")
+    ap.add_argument("--mma-steps", type=int, default=20)
+    ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--loop-steps", type=int, default=10, help="batched: OC steps per instance")
+    ap.add_argument("--workers", type=int, nargs="+", default=[1, 8, 16], help="batched: host workers")
+    ap.add_argument("--rates", type=float, nargs="+", default=[10, 20, 50, 100, 200, 500])
+    ap.add_argument("--jobs-per-rate", type=int, default=24)
+    ap.add_argument("--iter-scale", type=float, default=0.2, help="serving: scale on U[50,200] steps")
+    ap.add_argument("--slots", type=int, default=8)
     args = ap.parse_args()
     if args.profile_operator:
         return profile_operator(args)
+    if args.workload != "c2" and args.impl == "ours":
+        return {"c1": workload_c1, "c3": workload_c3, "batched": workload_batched,
+                "serving": workload_serving, "operator": workload_operator}[args.workload](args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

@@ -4,8 +4,9 @@
 
 Every .cu / .cpp under csrc/ is compiled by nvcc for
 ``-gencode arch=compute_100a,code=sm_100a`` into ``_build/`` and linked into
-``lib/libicarat_b200.so`` next to this file.  Objects are rebuilt only when
-their source or any header is newer.
+``lib/libicarat_b200.so`` next to this file.  The C++ app drivers under shim/
+(ICARAT's apps over the C++ class shim) are linked against it into lib/.
+Objects are rebuilt only when their source or any header is newer.
 """
 import argparse
 import concurrent.futures as cf
@@ -20,6 +21,8 @@ SRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libicarat_b200.so")
+SHIM = os.path.join(HERE, "shim")
+CXX = shutil.which("g++", path="/usr/bin:" + os.environ.get("PATH", "")) or "g++"
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -71,7 +74,28 @@ def build(jobs=None, verbose=False, clean=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    build_drivers(verbose)
     return LIB
+
+
+def build_drivers(verbose=False):
+    """shim/*_gpu.cpp -> lib/<name> (host C++, rpath to lib/)."""
+    hdrs = glob.glob(os.path.join(SHIM, "*.hpp")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    ht = max([os.path.getmtime(h) for h in hdrs] + [os.path.getmtime(LIB)])
+    out = []
+    for src in sorted(glob.glob(os.path.join(SHIM, "*_gpu.cpp"))):
+        exe = os.path.join(LIB_DIR, os.path.basename(src)[:-4])
+        out.append(exe)
+        if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(src), ht):
+            continue
+        cmd = [CXX, "-O2", "-std=c++17", "-Wall", "-I" + INCLUDE, "-I" + SHIM, src, "-o", exe,
+               "-L" + LIB_DIR, "-licarat_b200", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("driver build failed:\n" + r.stdout + r.stderr)
+    return out
 
 
 if __name__ == "__main__":

@@ -270,6 +270,24 @@ int icb_finalize(icb_problem p, long long *numeq)
   ICB_API_END
 }
 
+int icb_count_dof(icb_problem p, int *dof, long long *numeq)
+{
+  ICB_API_BEGIN
+  need(p && numeq, "NULL argument");
+  const HostSetup &hs = *p->hs;
+  long long cnt = 0;
+  for(long long i = 0; i < hs.neq; i++)
+    cnt += hs.fixed[i] ? 0 : 1;
+  *numeq = cnt;
+  if(dof)
+  {
+    long long f = 0, c = cnt;
+    for(long long i = 0; i < hs.neq; i++)
+      dof[i] = int(hs.fixed[i] ? c++ : f++);
+  }
+  ICB_API_END
+}
+
 int icb_get_dof_map(icb_problem p, int *dof)
 {
   ICB_API_BEGIN

@@ -90,6 +90,7 @@ _SIGS = {
     "icb_traction_box": (C.c_int, [C.c_void_p, _dp, _dp]),
     "icb_nodal_load": (C.c_int, [C.c_void_p, C.c_longlong, _dp]),
     "icb_finalize": (C.c_int, [C.c_void_p, _llp]),
+    "icb_count_dof": (C.c_int, [C.c_void_p, _ip, C.POINTER(C.c_longlong)]),
     "icb_get_dof_map": (C.c_int, [C.c_void_p, _ip]),
     "icb_get_load": (C.c_int, [C.c_void_p, _dp]),
     "icb_problem_sizes": (C.c_int, [C.c_void_p, _llp, _llp, _llp, _llp]),

@@ -118,6 +118,11 @@ int icb_nodal_load(icb_problem p, long long node, const double *f);
 /* BCIcarat::makeDOF -> countDOF (boundary_condition_base.hpp:35-88), load
  * assembly into Force::fext_org, upload to the device.  Returns numeq. */
 int icb_finalize(icb_problem p, long long *numeq);
+/* BCIcarat::makeDOF -> countDOF (boundary_condition_base.hpp:35-88) on the
+ * Dirichlet flags set so far, without freezing the problem: numeq and, when
+ * dof is not NULL, the neq-entry numbering.  Lets a caller follow ICARAT's
+ * order (makeDOF, then Force(numeq), then input_neumann, then icb_finalize). */
+int icb_count_dof(icb_problem p, int *dof, long long *numeq);
 /* node[i].dof[j] of countDOF, neq ints */
 int icb_get_dof_map(icb_problem p, int *dof);
 /* Force::fext_org (numeq) */
