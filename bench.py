@@ -397,7 +397,8 @@ def workload_operator(args):
     stream = torch.cuda.ExternalStream(ctx.stream())
     peak, src = _peaks()
     rows = []
-    for n in ((192, 64, 64), (384, 128, 128)):
+    grids = [tuple(args.size)] if args.size else [(192, 64, 64), (384, 128, 128)]
+    for n in grids:
         g = cases.build_gpu(ctx, "cantilever3d", *n)
         g.set_density(cases.uniform_density(g.nel, SEED))
         for name, prec, tc, es in (("fp64", icb.FP64, 0, 8), ("fp32_simt", icb.MIXED, 0, 4),
@@ -662,7 +663,7 @@ def main():
                     help="only launch the operator kernels on the bench problem (for ncu)")
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "batched", "serving", "operator"],
                     help="c2 (default): the bench line; the others print their own line")
-    ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 grid override")
+    ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 / operator grid override")
     ap.add_argument("--mma-steps", type=int, default=20)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--loop-steps", type=int, default=10, help="batched: OC steps per instance")

@@ -110,7 +110,7 @@ struct Device
   icb_problem prob = nullptr;
   icb_grid_desc desc{};
   bool finalized = false;
-  std::vector<double> volume; ///< element volumes
+  double volume = 0.0;        ///< element volume (uniform grid)
   std::vector<double> K0;     ///< unit-modulus element matrix
   Device() = default;
   Device(const Device &) = delete;
@@ -372,15 +372,14 @@ public:
     g.penalty = e0.pp();
     check(icb_ctx_create(fem_.device, &dev->ctx), "icb_ctx_create");
     check(icb_problem_create(dev->ctx, &g, &dev->prob), "icb_problem_create");
-    dev->volume.assign(fem_.nelx, 0.0);
-    check(icb_element_volume(dev->prob, dev->volume.data()), "icb_element_volume");
+    check(icb_element_volume(dev->prob, &dev->volume), "icb_element_volume");
     int nd = ne_ * d;
     dev->K0.assign(std::size_t(nd) * nd, 0.0);
     check(icb_get_K0(dev->prob, dev->K0.data()), "icb_get_K0");
     auto k0 = std::make_shared<const std::vector<double>>(dev->K0);
     for(long long e = 0; e < fem_.nelx; e++)
     {
-      element[e].volume = dev->volume[e];
+      element[e].volume = dev->volume;
       element[e].attachK0(k0);
     }
     fem_.gpu = dev;

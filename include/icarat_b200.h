@@ -133,7 +133,8 @@ int icb_problem_sizes(icb_problem p, long long *nel, long long *nnode, long long
 /* unit-modulus element matrix K0 (Ke of LinearElastic::makeKeFint,
  * elasticity.cpp:210-254, with E = 1), (d*ne)^2 row-major */
 int icb_get_K0(icb_problem p, double *K0);
-/* element volume: sum of Gauss jac (elasticity.cpp:249) */
+/* the element volume (one value: every element of the box grid has it),
+ * the sum of Gauss jac of elasticity.cpp:249 */
 int icb_element_volume(icb_problem p, double *v);
 
 /* ---- analysis ---------------------------------------------------------- */
