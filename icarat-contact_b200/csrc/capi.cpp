@@ -506,6 +506,39 @@ const double *icb_sensitivity_device(icb_problem p)
   return p->dc.p;
 }
 
+int icb_von_mises(icb_problem p, double *mises, double *stress)
+{
+  ICB_API_BEGIN
+  need(p && mises, "NULL argument");
+  needState(p->solved, "solve first");
+  setDevice(p);
+  cudaStream_t s = p->stream();
+  const long long nel = p->d.nel;
+  const int v = p->d.dim == 2 ? 3 : 6;
+  DevBuf<double> m(nel), st(stress ? nel * v : 0);
+  launch_von_mises(*p, m.p, stress ? st.p : nullptr, s);
+  ICB_CUDA(cudaMemcpyAsync(mises, m.p, sizeof(double) * nel, cudaMemcpyDeviceToHost, s));
+  if(stress)
+    ICB_CUDA(cudaMemcpyAsync(stress, st.p, sizeof(double) * nel * v, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  ICB_API_END
+}
+
+int icb_reactions(icb_problem p, double *reaction)
+{
+  ICB_API_BEGIN
+  need(p && reaction, "NULL argument");
+  needState(p->solved, "solve first");
+  setDevice(p);
+  cudaStream_t s = p->stream();
+  const long long n = p->d.nnode * p->d.dim;
+  DevBuf<double> r(n);
+  launch_reactions(*p, r.p, s);
+  ICB_CUDA(cudaMemcpyAsync(reaction, r.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  ICB_API_END
+}
+
 int icb_matvec(icb_problem p, const double *x, double *y)
 {
   ICB_API_BEGIN

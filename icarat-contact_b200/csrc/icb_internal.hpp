@@ -168,6 +168,10 @@ template <typename T>
 void launch_op(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,
                cudaStream_t s, const OpExtras<T> &x);
 
+// post-processing (post.cu); icb_problem_s is defined in problem.hpp
+void launch_von_mises(const icb_problem_s &p, double *mises, double *stress, cudaStream_t s);
+void launch_reactions(icb_problem_s &p, double *out, cudaStream_t s);
+
 // operators (operator.cu): every launcher takes the element matrix as a HOST
 // pointer and passes it by value.
 template <typename T>

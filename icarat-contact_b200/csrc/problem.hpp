@@ -30,6 +30,7 @@ struct icb_problem_s
   float K0f[576];
   // device arrays
   icb::DevBuf<uint8_t> fix;   ///< per-node Dirichlet bit mask
+  icb::DevBuf<uint8_t> fixNone; ///< all-zero mask (operator over every DOF, lazy)
   icb::DevBuf<double> f;      ///< load, SoA, zero on constrained DOFs
   icb::DevBuf<double> uD;     ///< Dirichlet values, SoA (empty if all zero)
   icb::DevBuf<double> u;      ///< displacement, SoA, Dirichlet values included

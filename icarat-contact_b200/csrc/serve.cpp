@@ -48,7 +48,7 @@ struct Job
   icb_grid_desc grid{};
   int kind = ICB_JOB_OC;
   icb_loop_opts loop{};
-  std::vector<unsigned char> fixed;
+  std::vector<unsigned char> fixed, nondesign, volumeSet;
   std::vector<double> load, rho0, hist, x, iters;
   long long bytes = 0;
   int state = ICB_JOB_QUEUED;
@@ -204,6 +204,18 @@ int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
   j->fixed.assign(jd->fixed, jd->fixed + neq);
   j->load.assign(jd->load, jd->load + neq);
   j->rho0.assign(jd->rho0, jd->rho0 + d.nel);
+  // the element masks are copied like the other arrays; on_step (if set) is
+  // called on the worker thread that runs the job
+  if(jd->loop.nondesign)
+  {
+    j->nondesign.assign(jd->loop.nondesign, jd->loop.nondesign + d.nel);
+    j->loop.nondesign = j->nondesign.data();
+  }
+  if(jd->loop.volume_set)
+  {
+    j->volumeSet.assign(jd->loop.volume_set, jd->loop.volume_set + d.nel);
+    j->loop.volume_set = j->volumeSet.data();
+  }
   j->hist.assign(jd->loop.nsteps, 0.0);
   j->iters.assign(jd->loop.nsteps, 0.0);
   j->x.assign(d.nel, 0.0);

@@ -92,6 +92,26 @@ __global__ void k_sum(long long n, const double *__restrict__ a, RedScratch red,
   block_reduce<1>(v, red, FinStore{out});
 }
 unsigned nb256(long long n) { return unsigned((n + 255) / 256); }
+__global__ void k_sum_masked(long long n, const double *__restrict__ a,
+                             const uint8_t *__restrict__ m, RedScratch red, double *out)
+{
+  double v[1] = {0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+    if(m[i])
+      v[0] += a[i];
+  block_reduce<1>(v, red, FinStore{out});
+}
+__global__ void k_zero_masked(long long n, const uint8_t *__restrict__ m, double *__restrict__ a,
+                              double *__restrict__ b)
+{
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if(i < n && m[i])
+  {
+    a[i] = 0.0;
+    b[i] = 0.0;
+  }
+}
 
 double deviceSum(icb_problem p, const double *a, long long n)
 {
@@ -104,6 +124,47 @@ double deviceSum(icb_problem p, const double *a, long long n)
   ICB_CUDA(cudaStreamSynchronize(p->stream()));
   return h;
 }
+
+/// sum of a over the flagged elements (all when m is NULL)
+double deviceSumMasked(icb_problem p, const double *a, const uint8_t *m, long long n)
+{
+  if(!m)
+    return deviceSum(p, a, n);
+  int nb = int(std::min<long long>(nb256(n), (long long)p->red.maxBlocks));
+  k_sum_masked<<<nb, 256, 0, p->stream()>>>(n, a, m, p->red, p->scal.p + 8);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+  double h;
+  ICB_CUDA(cudaMemcpyAsync(&h, p->scal.p + 8, sizeof(double), cudaMemcpyDeviceToHost, p->stream()));
+  ICB_CUDA(cudaStreamSynchronize(p->stream()));
+  return h;
+}
+
+/// the per-step callback of a device loop: host copies of the physical
+/// density, the node values and the von Mises stresses
+struct StepReport
+{
+  std::vector<double> rho, nodeval, mises;
+  void operator()(icb_problem p, const icb_loop_opts *o, int step, double comp,
+                  const double *rhoDev)
+  {
+    if(!o->on_step)
+      return;
+    const long long nel = p->d.nel, neq = p->d.nnode * p->d.dim;
+    rho.resize(nel);
+    nodeval.resize(neq);
+    mises.resize(nel);
+    cudaStream_t s = p->stream();
+    ICB_CUDA(cudaMemcpyAsync(rho.data(), rhoDev, sizeof(double) * nel, cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    int rc = icb_get_node_values(p, nodeval.data());
+    if(rc == ICB_OK)
+      rc = icb_von_mises(p, mises.data(), nullptr);
+    if(rc != ICB_OK)
+      throw Error{rc, "step report failed"};
+    o->on_step(o->step_user, step, comp, rho.data(), nodeval.data(), mises.data());
+  }
+};
 
 void toDev(DevBuf<double> &b, const double *h, long long n, cudaStream_t s)
 {
@@ -326,6 +387,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   count_launch(3);
   icb_solve_opts so = o->solve;
   double V0 = 0.0;
+  StepReport report;
   OcParams P;
   P.move = o->move_limit;
   for(int step = 1; step <= o->nsteps; step++)
@@ -342,6 +404,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
     rc = icb_compliance(p, &hist[step - 1]);
     if(rc)
       return rc;
+    report(p, o, step, hist[step - 1], xh.p);
     if(step == 1)
       V0 = deviceSum(p, xh.p, n) * vol;
     const double *dcd = icb_sensitivity_device(p);
@@ -376,42 +439,69 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
   needFinal(p);
   need(o && rho0 && hist, "NULL argument");
   need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
+  need(o->filter_type == ICB_FILTER_HELMHOLTZ || o->filter_type == ICB_FILTER_CONE,
+       "unknown filter_type");
   ICB_CUDA(cudaSetDevice(p->ctx->device));
   cudaStream_t s = p->stream();
   const long long n = p->d.nel;
   const double vol = p->hs->volume;
-  HelmFilter helm(p->d, p->hs->h, o->filter_radius, s);
+  const bool cone = o->filter_type == ICB_FILTER_CONE;
+  std::unique_ptr<HelmFilter> helm;
+  std::unique_ptr<ConeFilter> cf;
+  if(cone)
+    cf = std::make_unique<ConeFilter>(p->d, p->hs->h, o->filter_radius, s);
+  else
+    helm = std::make_unique<HelmFilter>(p->d, p->hs->h, o->filter_radius, s);
   MmaUpdater mma(n, s);
   DevBuf<double> x(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n);
+  DevBuf<uint8_t> nd(o->nondesign ? n : 0), vs(o->volume_set ? n : 0);
+  if(o->nondesign)
+    ICB_CUDA(cudaMemcpyAsync(nd.p, o->nondesign, n, cudaMemcpyHostToDevice, s));
+  if(o->volume_set)
+    ICB_CUDA(cudaMemcpyAsync(vs.p, o->volume_set, n, cudaMemcpyHostToDevice, s));
   ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);
   count_launch(2);
   icb_solve_opts so = o->solve;
   double V0 = o->volume_ref;
+  StepReport report;
+  auto filt = [&](const double *in, double *out, bool sens) {
+    if(cone)
+    {
+      if(sens)
+        cf->adjoint(in, out, s);
+      else
+        cf->forward(in, out, 0.0, 0.5, nullptr, nullptr, s);
+      return;
+    }
+    icb_solve_info hi_{};
+    int rc = helm->apply(in, out, sens, 1e-10, s, &hi_);
+    if(rc)
+      throw Error{rc, "Helmholtz filter solve did not converge"};
+  };
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
-    icb_solve_info hi_{};
-    int rc = helm.apply(x.p, xf.p, false, 1e-10, s, &hi_);
-    if(rc)
-      throw Error{rc, "Helmholtz filter solve did not converge"};
+    filt(x.p, xf.p, false);
     const double beta = std::min(std::pow(2.0, (int)(step / 40)), 16.0);
     launch_threshold(n, xf.p, beta, 0.5, xh.p, dxh.p, s);
-    rc = icb_set_density_device(p, xh.p);
+    int rc = icb_set_density_device(p, xh.p);
     if(rc)
       return rc;
     rc = icb_solve(p, &so, nullptr);
     if(rc)
       return rc;
     double g = 0.0;
+    const double vsum = deviceSumMasked(p, xh.p, o->volume_set ? vs.p : nullptr, n) * vol;
     if(step == 1 && o->volume_ref <= 0.0)
-      V0 = deviceSum(p, xh.p, n) * vol;
+      V0 = vsum;
     else
-      g = deviceSum(p, xh.p, n) * vol / V0 - 1.0;
+      g = vsum / V0 - 1.0;
     rc = icb_compliance(p, &hist[step - 1]);
     if(rc)
       return rc;
+    report(p, o, step, hist[step - 1], xh.p);
     const double *dcd = icb_sensitivity_device(p);
     if(!dcd)
       throw Error{ICB_ERR_STATE, "sensitivity failed"};
@@ -420,11 +510,13 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     k_fill_d<<<nb256(n), 256, 0, s>>>(n, vol / V0, dv.p);
     k_scale_mul<<<nb256(n), 256, 0, s>>>(n, dv.p, dxh.p, 1.0);
     count_launch(3);
-    rc = helm.apply(dc.p, dcf.p, true, 1e-10, s, &hi_);
-    if(rc == ICB_OK)
-      rc = helm.apply(dv.p, dvf.p, true, 1e-10, s, &hi_);
-    if(rc)
-      throw Error{rc, "Helmholtz filter solve did not converge"};
+    filt(dc.p, dcf.p, true);
+    filt(dv.p, dvf.p, true);
+    if(o->nondesign)
+    {
+      k_zero_masked<<<nb256(n), 256, 0, s>>>(n, nd.p, dcf.p, dvf.p);
+      count_launch();
+    }
     mma.update(x.p, dcf.p, g, dvf.p, lo.p, hi.p, s);
     ICB_CUDA(cudaStreamSynchronize(s));
     if(o->iter_seconds)

@@ -19,6 +19,7 @@ FP64, MIXED, TF32 = 0, 1, 2
 JACOBI, GMG = 0, 1
 PLANE_STRESS, PLANE_STRAIN, THREE_D = 0, 1, 2
 JOB_OC, JOB_MMA = 0, 1
+FILTER_HELMHOLTZ, FILTER_CONE = 0, 1
 STATUS = {0: "OK", -1: "BAD_ARG", -2: "OOM", -3: "BREAKDOWN", -4: "MAXITER", -5: "TIMEOUT",
           -6: "NAN", -7: "CUDA", -8: "STATE", -9: "REJECTED"}
 
@@ -50,10 +51,14 @@ class SolveInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+STEP_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_double, _dp, _dp, _dp)
+
+
 class LoopOpts(C.Structure):
     _fields_ = [("nsteps", C.c_int), ("filter_radius", C.c_double), ("move_limit", C.c_double),
                 ("use_threshold", C.c_int), ("volume_ref", C.c_double), ("solve", SolveOpts),
-                ("iter_seconds", _dp)]
+                ("iter_seconds", _dp), ("filter_type", C.c_int), ("nondesign", _u8p),
+                ("volume_set", _u8p), ("on_step", STEP_CB), ("step_user", C.c_void_p)]
 
 
 class JobDesc(C.Structure):
@@ -92,6 +97,8 @@ _SIGS = {
     "icb_finalize": (C.c_int, [C.c_void_p, _llp]),
     "icb_count_dof": (C.c_int, [C.c_void_p, _ip, C.POINTER(C.c_longlong)]),
     "icb_get_dof_map": (C.c_int, [C.c_void_p, _ip]),
+    "icb_von_mises": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "icb_reactions": (C.c_int, [C.c_void_p, _dp]),
     "icb_get_load": (C.c_int, [C.c_void_p, _dp]),
     "icb_problem_sizes": (C.c_int, [C.c_void_p, _llp, _llp, _llp, _llp]),
     "icb_get_K0": (C.c_int, [C.c_void_p, _dp]),
@@ -329,6 +336,18 @@ class Problem:
         check(lib().icb_sensitivity(self.h, _p(dc), None if dv is None else _p(dv)))
         return (dc, dv) if with_dv else dc
 
+    def von_mises(self, with_stress=False):
+        m = np.zeros(self.nel)
+        v = 3 if self.dim == 2 else 6
+        st = np.zeros(self.nel * v) if with_stress else None
+        check(lib().icb_von_mises(self.h, _p(m), None if st is None else _p(st)))
+        return (m, st.reshape(self.nel, v)) if with_stress else m
+
+    def reactions(self):
+        r = np.zeros(self.neq)
+        check(lib().icb_reactions(self.h, _p(r)))
+        return r
+
     def matvec(self, x):
         x = np.ascontiguousarray(x, np.float64)
         y = np.zeros(self.numeq)
@@ -435,10 +454,28 @@ class MMA:
 
 
 def run_loop(prob, kind, rho0, nsteps, radius, move=0.15, use_threshold=True, volume_ref=0.0,
-             precision=FP64, precond=GMG, tol=1e-8, maxit=20000):
-    """icb_run_oc (kind "oc") or icb_run_mma (kind "mma"): compliance history, design."""
+             precision=FP64, precond=GMG, tol=1e-8, maxit=20000, filter_type=0, nondesign=None,
+             volume_set=None, on_step=None):
+    """icb_run_oc (kind "oc") or icb_run_mma (kind "mma"): compliance history, design.
+    on_step(step, compliance, rho_phys, nodeval, mises) receives numpy copies."""
     o = LoopOpts(nsteps, radius, move, int(use_threshold), volume_ref,
                  SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0), None)
+    o.filter_type = filter_type
+    keep = []
+    for name, m in (("nondesign", nondesign), ("volume_set", volume_set)):
+        if m is not None:
+            a = np.ascontiguousarray(m, np.uint8)
+            keep.append(a)
+            setattr(o, name, _p(a, _u8p))
+    if on_step is not None:
+        nel, neq = prob.nel, prob.neq
+
+        def _cb(_u, step, comp, rho, nv, mi):
+            on_step(step, comp, np.ctypeslib.as_array(rho, (nel,)).copy(),
+                    np.ctypeslib.as_array(nv, (neq,)).copy(),
+                    np.ctypeslib.as_array(mi, (nel,)).copy())
+        o.on_step = STEP_CB(_cb)
+        keep.append(o.on_step)
     hist = np.zeros(nsteps)
     x = np.zeros(prob.nel)
     rho0 = np.ascontiguousarray(rho0, np.float64)

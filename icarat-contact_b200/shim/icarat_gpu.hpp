@@ -39,6 +39,8 @@
 //   * sensitivities come from sensitivity() below (the device computes
 //     -(E'/E) u_e^T Ke u_e and v_e), not from per-element Ke loops.
 //   * device failures throw icarat::gpu_error (ICARAT has none to report).
+//   * makeMisesStress computes every element's stress on the device once per
+//     solve; solve() also fills node[].reaction.
 #pragma once
 #include <cmath>
 #include <cstdlib>
@@ -112,6 +114,21 @@ struct Device
   bool finalized = false;
   double volume = 0.0;        ///< element volume (uniform grid)
   std::vector<double> K0;     ///< unit-modulus element matrix
+  long long solves = 0;       ///< solves so far
+  long long stressOf = -1;    ///< the solve the cached stresses belong to
+  std::vector<double> mises, stress;
+  /// element stresses of the last solve, fetched once per solve
+  void stresses(int voigt)
+  {
+    if(stressOf == solves)
+      return;
+    long long nel = 0;
+    check(icb_problem_sizes(prob, &nel, nullptr, nullptr, nullptr), "icb_problem_sizes");
+    mises.resize(std::size_t(nel));
+    stress.resize(std::size_t(nel) * voigt);
+    check(icb_von_mises(prob, mises.data(), stress.data()), "icb_von_mises");
+    stressOf = solves;
+  }
   Device() = default;
   Device(const Device &) = delete;
   Device &operator=(const Device &) = delete;
@@ -266,8 +283,23 @@ public:
   }
   void attachK0(std::shared_ptr<const std::vector<double>> k0) { K0_ = std::move(k0); }
 
+  /// Elastic::makeMisesStress (elasticity.cpp:165-208): the element's stress
+  /// and von Mises value from the last solve (all elements are computed on
+  /// the device on the first call after a solve)
+  template <class N> void makeMisesStress(FEM &fem, std::vector<N> &)
+  {
+    fem.gpu->stresses(voigt_);
+    mises_ = fem.gpu->mises[std::size_t(ID)];
+    stress_.assign(fem.gpu->stress.begin() + std::size_t(ID) * voigt_,
+                   fem.gpu->stress.begin() + std::size_t(ID + 1) * voigt_);
+  }
+  double mises() const { return mises_; }
+  const std::vector<double> &stress() const { return stress_; }
+
 private:
   int voigt_;
+  double mises_ = 0.0;
+  std::vector<double> stress_;
   double design_s_ = 0.0, pp_ = 3.0, young1_ = 0.0, young2_ = 1.0, poisson_ = 0.3;
   std::string mattype_ = "plane_stress";
   std::shared_ptr<const std::vector<double>> K0_;
@@ -548,12 +580,18 @@ public:
     else
       check(rc, "icb_solve");
     force.fext = force.fext_org;
+    g.solves++;
     check(icb_get_displacement(g.prob, value.val.data()), "icb_get_displacement");
     nodeval_.resize(std::size_t(fem.neq));
     check(icb_get_node_values(g.prob, nodeval_.data()), "icb_get_node_values");
     for(int n = 0; n < fem.numnp; n++)
       for(int c = 0; c < 3; c++)
         node[n].val[c] = c < fem.dofnp ? nodeval_[std::size_t(n) * fem.dofnp + c] : 0.0;
+    // node[].reaction (linear.hpp:89-91)
+    check(icb_reactions(g.prob, nodeval_.data()), "icb_reactions");
+    for(int n = 0; n < fem.numnp; n++)
+      for(int c = 0; c < 3; c++)
+        node[n].reaction[c] = c < fem.dofnp ? nodeval_[std::size_t(n) * fem.dofnp + c] : 0.0;
     if(log)
       std::cout << "#iterations: " << info_.iters << "  estimated error: " << info_.relres
                 << "  true ||f-Ku||/||f||: " << info_.true_relres << std::endl;

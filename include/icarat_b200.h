@@ -159,6 +159,16 @@ int icb_compliance(icb_problem p, double *c);
 int icb_sensitivity(icb_problem p, double *dc, double *dv);
 /* device pointers (valid until the problem is destroyed) */
 const double *icb_sensitivity_device(icb_problem p);
+/* Elastic::makeMisesStress (src/problem/elasticity.cpp:165-208) for every
+ * element of the last solve: mises[nel] and, when stress is not NULL, the
+ * element stress stress[nel * voigt] (voigt order [xx, yy, xy] in 2D,
+ * [xx, yy, zz, xy, yz, zx] in 3D), both from the physical density. */
+int icb_von_mises(icb_problem p, double *mises, double *stress);
+/* node[].reaction after LinearAnalysis::solve (linear.hpp:89-91,
+ * assembling.hpp:79-84, analysis_utility.hpp:34-51): the internal force
+ * sum_e Ke u_e at every DOF, node-major (neq), |r| < 1e-15 set to 0.  At a
+ * free DOF it equals the load; at a constrained DOF it is the reaction. */
+int icb_reactions(icb_problem p, double *reaction);
 /* K(rho) x over free DOFs (numeq in, numeq out): the product globalK * x of
  * the assembled LinearAnalysis::K() (linear.hpp:31), matrix-free. */
 int icb_matvec(icb_problem p, const double *x, double *y);
@@ -197,6 +207,16 @@ int icb_mma_update(icb_mma h, double *x, const double *dfdx, const double *gx,
                    const double *dgdx, const double *xmin, const double *xmax);
 
 /* ---- the ICARAT app loops on the device ----------------------------------- */
+#define ICB_FILTER_HELMHOLTZ 0 /* FilterHelmholtz (filter_helm.hpp)              */
+#define ICB_FILTER_CONE 1      /* Filter (filter.hpp)                            */
+
+/* Per-step results of a device loop, for the apps' output() (res<step>.vtk,
+ * function.csv): host arrays valid during the call.  rho_phys[nel] is the
+ * physical (filtered, thresholded) density, nodeval[neq] node[].val,
+ * mises[nel] the element von Mises stress. */
+typedef void (*icb_step_cb)(void *user, int step, double compliance, const double *rho_phys,
+                            const double *nodeval, const double *mises);
+
 typedef struct
 {
   int nsteps;           /* optimisation steps (fixed count, no I/O)          */
@@ -206,6 +226,16 @@ typedef struct
   double volume_ref;    /* icb_run_mma: V0 of the constraint (<= 0: step-1 volume) */
   icb_solve_opts solve; /* the structural solve of every step                */
   double *iter_seconds; /* optional [nsteps]: wall time of every step (or NULL) */
+  int filter_type;      /* icb_run_mma: ICB_FILTER_HELMHOLTZ (0) or ICB_FILTER_CONE */
+  /* icb_run_mma, opt-macro-mma-nondesign (opt_macro_mma_nondesign.cpp:120-166):
+   * nel flags; flagged elements get zero objective and constraint
+   * sensitivities after the filter (NULL: none) */
+  const unsigned char *nondesign;
+  /* icb_run_mma: nel flags of the elements summed into V0 and the volume
+   * constraint (the app's design IDs; NULL: every element) */
+  const unsigned char *volume_set;
+  icb_step_cb on_step;  /* optional, called after every step's solve      */
+  void *step_user;      /* passed to on_step                               */
 } icb_loop_opts;
 /* opt-macro-oc/opt_macro_oc.cpp:84-172: cone filter, threshold, solve,
  * compliance, V0 at step 1, sensitivities, adjoint filter, OC; hist[nsteps]

@@ -1582,6 +1582,169 @@ int orc_mma_loop(const OrcGrid *g, const uint8_t *fixed, const double *dval,
   return 0;
 }
 
+
+// ------------------------------------------------------ stress, reactions ----
+/// Elastic::makeMisesStress (elasticity.cpp:165-208): the element stress is
+/// the Gauss-point average of D(E(rho)) B u_e and the von Mises value is
+/// sqrt(s^T V s) with V = [[1,-.5,0],[-.5,1,0],[0,0,3]] in 2D (for plane
+/// strain too, as the reference does) and the 6x6 counterpart in 3D.
+/// stress (nel x voigt) may be NULL.
+void orc_von_mises(const OrcGrid *g, const double *rho, const double *nodeval, double *mises,
+                   double *stress)
+{
+  int d = g->dim, ne = nen(*g), nd = d * ne, v = d == 2 ? 3 : 6;
+  int64_t nel = nelx(*g);
+  double pts[8][3];
+  int nq = gaussPoints(*g, pts);
+  std::vector<double> Bq(size_t(nq) * v * nd);
+  for(int q = 0; q < nq; q++)
+  {
+    double dNdX[24], N[8];
+    shapeGrad(*g, pts[q], dNdX, N);
+    makeB(*g, dNdX, &Bq[size_t(q) * v * nd]);
+  }
+  const double fac = 1.0 / nq;
+#pragma omp parallel for schedule(static)
+  for(int64_t e = 0; e < nel; e++)
+  {
+    double D[36];
+    makeDe(*g, simp(g->young1, g->young2, rho[e], g->penal), D);
+    int64_t ndn[8];
+    elemNodes(*g, e, ndn);
+    double ue[24];
+    for(int a = 0; a < ne; a++)
+      for(int c = 0; c < d; c++)
+        ue[a * d + c] = nodeval[ndn[a] * d + c];
+    double sig[6] = {0, 0, 0, 0, 0, 0};
+    for(int q = 0; q < nq; q++)
+    {
+      const double *B = &Bq[size_t(q) * v * nd];
+      double eps[6];
+      for(int r = 0; r < v; r++)
+      {
+        double t = 0.0;
+        for(int j = 0; j < nd; j++)
+          t += B[r * nd + j] * ue[j];
+        eps[r] = t;
+      }
+      for(int r = 0; r < v; r++)
+      {
+        double t = 0.0;
+        for(int c = 0; c < v; c++)
+          t += D[r * v + c] * eps[c];
+        sig[r] += t * fac;
+      }
+    }
+    double m2;
+    if(d == 2)
+      m2 = sig[0] * sig[0] + sig[1] * sig[1] - sig[0] * sig[1] + 3.0 * sig[2] * sig[2];
+    else
+      m2 = sig[0] * sig[0] + sig[1] * sig[1] + sig[2] * sig[2] - sig[0] * sig[1] -
+           sig[1] * sig[2] - sig[0] * sig[2] +
+           3.0 * (sig[3] * sig[3] + sig[4] * sig[4] + sig[5] * sig[5]);
+    mises[e] = std::sqrt(m2);
+    if(stress)
+      for(int r = 0; r < v; r++)
+        stress[e * v + r] = sig[r];
+  }
+}
+
+/// The reaction of LinearAnalysis::assemblingK (linear.hpp:117-162,
+/// assembling.hpp:79-84) as divideReactionIntoNode stores it
+/// (analysis_utility.hpp:34-51): the internal force sum_e Ke u_e at every
+/// DOF, node-major (neq), entries below 1e-15 in magnitude set to 0.
+void orc_reactions(const OrcGrid *g, const double *rho, const double *nodeval, double *react)
+{
+  int d = g->dim, ne = nen(*g), nd = d * ne;
+  int64_t nel = nelx(*g), neq = numnp(*g) * d;
+  std::vector<double> K0(24 * 24);
+  unitK0(*g, K0.data());
+  std::fill(react, react + neq, 0.0);
+  for(int64_t e = 0; e < nel; e++)
+  {
+    double E = simp(g->young1, g->young2, rho[e], g->penal);
+    int64_t ndn[8];
+    elemNodes(*g, e, ndn);
+    double ue[24];
+    for(int a = 0; a < ne; a++)
+      for(int c = 0; c < d; c++)
+        ue[a * d + c] = nodeval[ndn[a] * d + c];
+    for(int i = 0; i < nd; i++)
+    {
+      double t = 0.0;
+      for(int j = 0; j < nd; j++)
+        t += K0[i * nd + j] * ue[j];
+      react[ndn[i / d] * d + i % d] += E * t;
+    }
+  }
+  for(int64_t i = 0; i < neq; i++)
+    if(std::fabs(react[i]) < 1.0e-15)
+      react[i] = 0.0;
+}
+
+/// The optimisation loop of opt-macro-mma-nondesign
+/// (opt_macro_mma_nondesign.cpp:82-178) without I/O: cone filter (radius
+/// rfil), threshold, solve, V0 over the elements flagged in `volset` (all when
+/// NULL) at step 1, constraint sum_volset x v / V0 - 1 (0 at step 1),
+/// sensitivities dv = v / V0 times the threshold derivative, adjoint cone
+/// filter, sensitivities of the `nondesign` elements set to 0, MMA update.
+int orc_mma_cone_loop(const OrcGrid *g, const uint8_t *fixed, const double *dval,
+                      const double *fext, const double *rho0, int nsteps, double rfil,
+                      const uint8_t *nondesign, const uint8_t *volset, double tol, double *hist,
+                      double *x)
+{
+  int d = g->dim;
+  int64_t nn = numnp(*g), nel = nelx(*g);
+  std::vector<int> dof(nn * d);
+  int64_t numeq = orc_count_dof(g, fixed, dof.data());
+  std::vector<double> u(numeq), nodeval(nn * d), xf(nel), xt(nel), dxt(nel), dc(nel), dv(nel),
+      xmin(nel, 1.0e-4), xmax(nel, 1.0), t1(nel), t2(nel);
+  std::copy(rho0, rho0 + nel, x);
+  double vol = orc_element_volume(g);
+  void *mma = orc_mma_create(nel, 1, 0.0, 1e5, 0.0);
+  void *cone = orc_cone_create(g, rfil);
+  double V0 = 0.0;
+  for(int step = 1; step <= nsteps; step++)
+  {
+    orc_cone_apply(cone, x, xf.data(), 0);
+    double beta = std::min(std::pow(2, (int)(step / 40)), 16.0);
+    orc_threshold(nel, xf.data(), beta, 0.5, xt.data());
+    orc_threshold_deriv(nel, xf.data(), beta, 0.5, dxt.data());
+    double comp, rr;
+    int it, mv;
+    orc_linear_solve(g, fixed, dval, dof.data(), numeq, fext, xt.data(), tol, 100000, u.data(),
+                     nodeval.data(), &comp, &it, &rr, &mv);
+    double gval = 0.0, vs = 0.0;
+    for(int64_t i = 0; i < nel; i++)
+      if(!volset || volset[i])
+        vs += xt[i] * vol;
+    if(step == 1)
+      V0 = vs;
+    else
+      gval = vs / V0 - 1.0;
+    hist[step - 1] = comp;
+    orc_sensitivity(g, xt.data(), nodeval.data(), dc.data());
+    for(int64_t i = 0; i < nel; i++)
+    {
+      dc[i] *= dxt[i];
+      dv[i] = vol / V0 * dxt[i];
+    }
+    orc_cone_apply(cone, dc.data(), t1.data(), 1);
+    orc_cone_apply(cone, dv.data(), t2.data(), 1);
+    if(nondesign)
+      for(int64_t i = 0; i < nel; i++)
+        if(nondesign[i])
+        {
+          t1[i] = 0.0;
+          t2[i] = 0.0;
+        }
+    orc_mma_update(mma, x, t1.data(), &gval, t2.data(), xmin.data(), xmax.data());
+  }
+  orc_cone_free(cone);
+  orc_mma_free(mma);
+  return 0;
+}
+
 int orc_num_threads()
 {
 #ifdef _OPENMP

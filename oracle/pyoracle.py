@@ -86,6 +86,10 @@ def lib():
                                       C.c_int, C.c_double, _dp, _dp, _ip]),
             "orc_mma_loop": (C.c_int, [G, _u8p, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double,
                                        C.c_double, _dp, _dp]),
+            "orc_von_mises": (None, [G, _dp, _dp, _dp, _dp]),
+            "orc_reactions": (None, [G, _dp, _dp, _dp]),
+            "orc_mma_cone_loop": (C.c_int, [G, _u8p, _dp, _dp, _dp, C.c_int, C.c_double, _u8p,
+                                            _u8p, C.c_double, _dp, _dp]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -240,6 +244,34 @@ class Problem:
                           _ptr(self.fext()), _ptr(np.ascontiguousarray(rho0, np.float64)), nsteps,
                           rfil, movelimit, int(use_beta), tol, _ptr(hist), _ptr(x), C.byref(tot))
         return hist, x, tot.value
+
+    def von_mises(self, rho, nodeval, with_stress=False):
+        """Element von Mises stress (and the nel x voigt stress) of a solution."""
+        m = np.zeros(self.nel)
+        v = 3 if self.dim == 2 else 6
+        st = np.zeros(self.nel * v) if with_stress else None
+        lib().orc_von_mises(C.byref(self.g), _ptr(np.ascontiguousarray(rho, np.float64)),
+                            _ptr(np.ascontiguousarray(nodeval, np.float64)), _ptr(m),
+                            None if st is None else _ptr(st))
+        return (m, st.reshape(self.nel, v)) if with_stress else m
+
+    def reactions(self, rho, nodeval):
+        """Internal force sum_e Ke u_e at every DOF, node-major (neq)."""
+        r = np.zeros(self.neq)
+        lib().orc_reactions(C.byref(self.g), _ptr(np.ascontiguousarray(rho, np.float64)),
+                            _ptr(np.ascontiguousarray(nodeval, np.float64)), _ptr(r))
+        return r
+
+    def mma_cone_loop(self, rho0, nsteps, rfil, nondesign=None, volset=None, tol=1e-8):
+        hist = np.zeros(nsteps)
+        x = np.zeros(self.nel)
+        nd = None if nondesign is None else np.ascontiguousarray(nondesign, np.uint8)
+        vs = None if volset is None else np.ascontiguousarray(volset, np.uint8)
+        lib().orc_mma_cone_loop(C.byref(self.g), _ptr(self.fixed, _u8p), _ptr(self.dval),
+                                _ptr(self.fext()), _ptr(np.ascontiguousarray(rho0, np.float64)),
+                                nsteps, rfil, None if nd is None else _ptr(nd, _u8p),
+                                None if vs is None else _ptr(vs, _u8p), tol, _ptr(hist), _ptr(x))
+        return hist, x
 
     def mma_loop(self, rho0, nsteps, R, Vref=0.0, tol=1e-8):
         hist = np.zeros(nsteps)
