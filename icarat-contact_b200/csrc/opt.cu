@@ -447,6 +447,139 @@ __global__ void k_mma_dip_init(MmaState *st, MmaParams P)
   st->passes = 0;
   st->z = 0.0; // z = max(0, 10 (lam a - 1)) with a = 0
 }
+/// GenSub of GCMMA (GCMMASolver.cpp:432-508 with asymp, 546-596): the
+/// asymptotes only in an outer update (then xold shifts), bounds without the
+/// final clamps, p/q with raa0 for the objective and raa for the constraint;
+/// the finisher stores r0 = f0x - S0, r = g - S1 and b = -r.
+struct FinGcSub
+{
+  MmaState *st;
+  __device__ void operator()(const double *t) const
+  {
+    st->r0 = st->f0x - t[0];
+    st->rr = st->g - t[1];
+    st->b = -st->rr;
+  }
+};
+
+__global__ void k_gc_gensub(long long n, MmaVec V, const double *__restrict__ x,
+                            const double *__restrict__ df0dx, const double *__restrict__ dfdx,
+                            const double *__restrict__ xmin, const double *__restrict__ xmax,
+                            MmaParams P, double raa0, double raa, int outerIter, int asymp,
+                            RedScratch red, MmaState *st)
+{
+  double v[2] = {0.0, 0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    const double xv = x[i], range = xmax[i] - xmin[i];
+    double lo = V.low[i], up = V.upp[i];
+    if(asymp)
+    {
+      if(outerIter < 3)
+      {
+        lo = xv - P.asyminit * range;
+        up = xv + P.asyminit * range;
+      }
+      else
+      {
+        const double o1 = V.xold1[i], o2 = V.xold2[i];
+        const double zzz = (xv - o1) * (o1 - o2);
+        const double gam = zzz < 0.0 ? P.asymdec : (zzz > 0.0 ? P.asyminc : 1.0);
+        lo = xv - gam * (o1 - lo);
+        up = xv + gam * (up - o1);
+        const double xmami = fmax(P.xmamieps, range);
+        lo = fmax(lo, xv - 100.0 * xmami);
+        lo = fmin(lo, xv - 1.0e-5 * xmami);
+        up = fmax(up, xv + 1.0e-5 * xmami);
+        up = fmin(up, xv + 100.0 * xmami);
+        const double xmi = xmin[i] - 1.0e-6, xma = xmax[i] + 1.0e-6;
+        if(xv < xmi)
+        {
+          lo = xv - (xma - xv) / 0.9;
+          up = xv + (xma - xv) / 0.9;
+        }
+        if(xv > xma)
+        {
+          lo = xv - (xv - xmi) / 0.9;
+          up = xv + (xv - xmi) / 0.9;
+        }
+      }
+      V.low[i] = lo;
+      V.upp[i] = up;
+    }
+    V.alpha[i] = fmax(fmax(xmin[i], lo + P.albefa * (xv - lo)), xv - P.move * range);
+    V.beta[i] = fmin(fmin(xmax[i], up - P.albefa * (up - xv)), xv + P.move * range);
+    const double uxinv = 1.0 / (up - xv), xlinv = 1.0 / (xv - lo);
+    const double inv = 1.0 / fmax(P.xmamieps, range);
+    const double u2 = pow(up - xv, 2.0), l2 = pow(xv - lo, 2.0);
+    const double df = df0dx[i], dg = dfdx[i];
+    const double pq = 0.001 * fabs(df) + raa0 * inv;
+    const double p0 = u2 * (fmax(0.0, df) + pq), q0 = l2 * (fmax(0.0, -df) + pq);
+    V.p0[i] = p0;
+    V.q0[i] = q0;
+    const double pqg = 0.001 * fabs(dg) + raa * inv;
+    const double pij = u2 * (fmax(0.0, dg) + pqg), qij = l2 * (fmax(0.0, -dg) + pqg);
+    V.pij[i] = pij;
+    V.qij[i] = qij;
+    v[0] += p0 * uxinv + q0 * xlinv;
+    v[1] += pij * uxinv + qij * xlinv;
+    if(asymp)
+    {
+      V.xold2[i] = V.xold1[i];
+      V.xold1[i] = xv;
+    }
+  }
+  block_reduce<2>(v, red, FinGcSub{st});
+}
+
+/// ComputeApprox (GCMMASolver.cpp:598-621)
+struct FinGcApprox
+{
+  MmaState *st;
+  __device__ void operator()(const double *t) const
+  {
+    st->f0app = t[0] + st->r0;
+    st->fapp = t[1] + st->rr;
+  }
+};
+__global__ void k_gc_approx(long long n, MmaVec V, const double *__restrict__ xm, RedScratch red,
+                            MmaState *st)
+{
+  double v[2] = {0.0, 0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    const double uxinv = 1.0 / (V.upp[i] - xm[i]), xlinv = 1.0 / (xm[i] - V.low[i]);
+    v[0] += V.p0[i] * uxinv + V.q0[i] * xlinv;
+    v[1] += V.pij[i] * uxinv + V.qij[i] * xlinv;
+  }
+  block_reduce<2>(v, red, FinGcApprox{st});
+}
+
+/// the raacof sum of RaaUpdate (GCMMASolver.cpp:513-523)
+struct FinRaacof
+{
+  MmaState *st;
+  __device__ void operator()(const double *t) const { st->raacof = t[0]; }
+};
+__global__ void k_gc_raacof(long long n, MmaVec V, const double *__restrict__ xm,
+                            const double *__restrict__ xv, const double *__restrict__ xmin,
+                            const double *__restrict__ xmax, MmaParams P, RedScratch red,
+                            MmaState *st)
+{
+  double v[1] = {0.0};
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+  {
+    const double xmami = fmax(P.xmamieps, xmax[i] - xmin[i]);
+    const double xxux = (xm[i] - xv[i]) / (V.upp[i] - xm[i]);
+    const double xxxl = (xm[i] - xv[i]) / (xm[i] - V.low[i]);
+    v[0] += xxux * xxxl * ((V.upp[i] - V.low[i]) / xmami);
+  }
+  block_reduce<1>(v, red, FinRaacof{st});
+}
+
 } // namespace
 
 // =============================================================== Cone =====
@@ -616,8 +749,16 @@ int MmaUpdater::update(double *x, const double *dfdx, double g, const double *dg
   // the constraint value for GenSub's b
   ICB_CUDA(cudaMemcpyAsync(&st.p->g, &g, sizeof(double), cudaMemcpyHostToDevice, s));
   k_mma_gensub<<<nb, VB, 0, s>>>(n, V, x, dfdx, dgdx, xmin, xmax, P, iter, red, st.p);
+  count_launch();
+  return solveDual(x, s);
+}
+
+int MmaUpdater::solveDual(double *x, cudaStream_t s)
+{
+  MmaVec V{low.p, upp.p, alpha.p, beta.p, p0.p, q0.p, pij.p, qij.p, xold1.p, xold2.p};
+  const int nb = vblocks(n);
   k_mma_dip_init<<<1, 1, 0, s>>>(st.p, P);
-  count_launch(2);
+  count_launch();
   const void *k[3] = {x, (const void *)s, nullptr};
   bool same = exec != nullptr;
   for(int i = 0; i < 3 && same; i++)
@@ -652,6 +793,76 @@ int MmaUpdater::update(double *x, const double *dfdx, double g, const double *dg
       break;
   }
   return hst->passes;
+}
+
+// ============================================================== GCMMA =====
+GcmmaUpdater::GcmmaUpdater(long long nvar, cudaStream_t s) : core(nvar, s)
+{
+  core.P.c = 1000.0; // GCMMASolver(n, m, a = 0, c = 1000, d = 0)
+}
+
+void GcmmaUpdater::subproblem(const double *xval, double f0x, const double *df0dx, double fx,
+                              const double *dfdx, const double *xmin, const double *xmax,
+                              bool asymp, cudaStream_t s)
+{
+  MmaVec V{core.low.p, core.upp.p, core.alpha.p, core.beta.p, core.p0.p,
+           core.q0.p,  core.pij.p, core.qij.p,   core.xold1.p, core.xold2.p};
+  double gf[2] = {fx, f0x};
+  ICB_CUDA(cudaMemcpyAsync(&core.st.p->g, &gf[0], sizeof(double), cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(&core.st.p->f0x, &gf[1], sizeof(double), cudaMemcpyHostToDevice, s));
+  k_gc_gensub<<<vblocks(core.n), VB, 0, s>>>(core.n, V, xval, df0dx, dfdx, xmin, xmax, core.P,
+                                              raa0, raa, outerIter, asymp ? 1 : 0, core.red,
+                                              core.st.p);
+  count_launch();
+  ICB_CUDA(cudaStreamSynchronize(s)); // gf is a host temporary
+}
+
+void GcmmaUpdater::approx(const double *xmma, cudaStream_t s)
+{
+  MmaVec V{core.low.p, core.upp.p, core.alpha.p, core.beta.p, core.p0.p,
+           core.q0.p,  core.pij.p, core.qij.p,   core.xold1.p, core.xold2.p};
+  k_gc_approx<<<vblocks(core.n), VB, 0, s>>>(core.n, V, xmma, core.red, core.st.p);
+  count_launch();
+  ICB_CUDA(cudaMemcpyAsync(core.hst, core.st.p, sizeof(MmaState), cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  f0app = core.hst->f0app;
+  fapp = core.hst->fapp;
+}
+
+void GcmmaUpdater::outer(double *xmma, const double *xval, double f0x, const double *df0dx,
+                         double fx, const double *dfdx, const double *xmin, const double *xmax,
+                         cudaStream_t s)
+{
+  // Asymp (GCMMASolver.cpp:432-508): iteration count, raa shrink
+  outerIter++;
+  raa0 = std::max(1e-6, 0.1 * raa0);
+  raa = std::max(1e-6, 0.1 * raa);
+  subproblem(xval, f0x, df0dx, fx, dfdx, xmin, xmax, true, s);
+  core.solveDual(xmma, s);
+  approx(xmma, s);
+}
+
+void GcmmaUpdater::inner(double *xmma, double f0xnew, double fxnew, const double *xval, double f0x,
+                         const double *df0dx, double fx, const double *dfdx, const double *xmin,
+                         const double *xmax, cudaStream_t s)
+{
+  // RaaUpdate (GCMMASolver.cpp:510-544)
+  MmaVec V{core.low.p, core.upp.p, core.alpha.p, core.beta.p, core.p0.p,
+           core.q0.p,  core.pij.p, core.qij.p,   core.xold1.p, core.xold2.p};
+  k_gc_raacof<<<vblocks(core.n), VB, 0, s>>>(core.n, V, xmma, xval, xmin, xmax, core.P, core.red,
+                                              core.st.p);
+  count_launch();
+  ICB_CUDA(cudaMemcpyAsync(core.hst, core.st.p, sizeof(MmaState), cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  const double raacof = std::max(1e-12, core.hst->raacof);
+  const double eps = core.P.epsimin;
+  if(f0xnew > f0app + 0.5 * eps)
+    raa0 = std::min(1.1 * (raa0 + (f0xnew - f0app) / raacof), 10.0 * raa0);
+  if(fxnew > fapp + 0.5 * eps)
+    raa = std::min(1.1 * (raa + (fxnew - fapp) / raacof), 10.0 * raa);
+  subproblem(xval, f0x, df0dx, fx, dfdx, xmin, xmax, false, s);
+  core.solveDual(xmma, s);
+  approx(xmma, s);
 }
 
 } // namespace icb

@@ -80,6 +80,8 @@ struct MmaState
 {
   double g, b, z, lam, mu, epsi, err;
   int outloop, loop, phase, done, passes, pad;
+  // GCMMA: objective at xval, constant terms, approximations at xmma, raacof
+  double f0x, r0, rr, f0app, fapp, raacof;
 };
 
 /// MMASolver (MMASolver.hpp:62-117) for one constraint
@@ -102,6 +104,39 @@ struct MmaUpdater
   /// MMASolver::Update(x, dfdx, &g, dgdx, xmin, xmax); returns the dual passes
   int update(double *x, const double *dfdx, double g, const double *dgdx, const double *xmin,
              const double *xmax, cudaStream_t s);
+  /// SolveDIP on the subproblem set up last: x <- x(lambda*); returns the passes
+  int solveDual(double *x, cudaStream_t s);
+};
+
+/// GCMMASolver (GCMMASolver.hpp:60-90, GCMMASolver.cpp:41-661) for one
+/// constraint: the MMA subproblem and dual of MmaUpdater with GCMMA's
+/// adaptive raa0 / raa, constant terms and approximation values
+struct GcmmaUpdater
+{
+  MmaUpdater core;
+  double raa0 = 1.0, raa = 1.0; ///< GCMMASolver.cpp:51
+  int outerIter = 0;
+  double f0app = 0.0, fapp = 0.0; ///< approximations at the last xmma
+
+  GcmmaUpdater(long long nvar, cudaStream_t s);
+  /// OuterUpdate (GCMMASolver.cpp:66-89)
+  void outer(double *xmma, const double *xval, double f0x, const double *df0dx, double fx,
+             const double *dfdx, const double *xmin, const double *xmax, cudaStream_t s);
+  /// InnerUpdate (GCMMASolver.cpp:91-112)
+  void inner(double *xmma, double f0xnew, double fxnew, const double *xval, double f0x,
+             const double *df0dx, double fx, const double *dfdx, const double *xmin,
+             const double *xmax, cudaStream_t s);
+  /// ConCheck (GCMMASolver.cpp:114-128)
+  bool concheck(double f0xnew, double fxnew) const
+  {
+    return !(f0app + core.P.epsimin < f0xnew) && !(fapp + core.P.epsimin < fxnew);
+  }
+
+private:
+  void subproblem(const double *xval, double f0x, const double *df0dx, double fx,
+                  const double *dfdx, const double *xmin, const double *xmax, bool asymp,
+                  cudaStream_t s);
+  void approx(const double *xmma, cudaStream_t s);
 };
 
 } // namespace icb

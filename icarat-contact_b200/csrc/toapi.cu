@@ -36,6 +36,12 @@ struct icb_mma_s
   std::unique_ptr<MmaUpdater> m;
   DevBuf<double> x, df, dg, lo, hi;
 };
+struct icb_gcmma_s
+{
+  icb_ctx ctx;
+  std::unique_ptr<GcmmaUpdater> g;
+  DevBuf<double> xm, xv, df, dg, lo, hi;
+};
 
 namespace
 {
@@ -363,6 +369,87 @@ int icb_mma_update(icb_mma h, double *x, const double *dfdx, const double *gx,
   API_CATCH
 }
 
+// --------------------------------------------------------------- GCMMA ----
+int icb_gcmma_create(icb_ctx ctx, long long n, int m, icb_gcmma *out)
+{
+  API_TRY
+  need(ctx && out && n > 0, "bad argument");
+  need(m == 1, "the device GCMMA supports one constraint (m = 1)");
+  ICB_CUDA(cudaSetDevice(ctx->device));
+  auto h = std::make_unique<icb_gcmma_s>();
+  h->ctx = ctx;
+  h->g = std::make_unique<GcmmaUpdater>(n, ctx->stream);
+  for(DevBuf<double> *b : {&h->xm, &h->xv, &h->df, &h->dg, &h->lo, &h->hi})
+    b->alloc(n);
+  ICB_CUDA(cudaStreamSynchronize(ctx->stream));
+  *out = h.release();
+  API_CATCH
+}
+
+int icb_gcmma_destroy(icb_gcmma h)
+{
+  API_TRY
+  delete h;
+  API_CATCH
+}
+
+namespace
+{
+void gcmmaUpload(icb_gcmma h, const double *xval, const double *df0dx, const double *dfdx,
+                 const double *xmin, const double *xmax)
+{
+  need(h && xval && df0dx && dfdx && xmin && xmax, "NULL argument");
+  ICB_CUDA(cudaSetDevice(h->ctx->device));
+  cudaStream_t s = h->ctx->stream;
+  const size_t b = sizeof(double) * h->g->core.n;
+  ICB_CUDA(cudaMemcpyAsync(h->xv.p, xval, b, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->df.p, df0dx, b, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->dg.p, dfdx, b, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->lo.p, xmin, b, cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(h->hi.p, xmax, b, cudaMemcpyHostToDevice, s));
+}
+} // namespace
+
+int icb_gcmma_outer(icb_gcmma h, double *xmma, const double *xval, double f0x,
+                    const double *df0dx, const double *fx, const double *dfdx, const double *xmin,
+                    const double *xmax)
+{
+  API_TRY
+  need(xmma && fx, "NULL argument");
+  gcmmaUpload(h, xval, df0dx, dfdx, xmin, xmax);
+  cudaStream_t s = h->ctx->stream;
+  h->g->outer(h->xm.p, h->xv.p, f0x, h->df.p, fx[0], h->dg.p, h->lo.p, h->hi.p, s);
+  ICB_CUDA(cudaMemcpyAsync(xmma, h->xm.p, sizeof(double) * h->g->core.n, cudaMemcpyDeviceToHost,
+                           s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+int icb_gcmma_inner(icb_gcmma h, double *xmma, double f0xnew, const double *fxnew,
+                    const double *xval, double f0x, const double *df0dx, const double *fx,
+                    const double *dfdx, const double *xmin, const double *xmax)
+{
+  API_TRY
+  need(xmma && fxnew && fx, "NULL argument");
+  gcmmaUpload(h, xval, df0dx, dfdx, xmin, xmax);
+  cudaStream_t s = h->ctx->stream;
+  const size_t b = sizeof(double) * h->g->core.n;
+  ICB_CUDA(cudaMemcpyAsync(h->xm.p, xmma, b, cudaMemcpyHostToDevice, s));
+  h->g->inner(h->xm.p, f0xnew, fxnew[0], h->xv.p, f0x, h->df.p, fx[0], h->dg.p, h->lo.p, h->hi.p,
+              s);
+  ICB_CUDA(cudaMemcpyAsync(xmma, h->xm.p, b, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+int icb_gcmma_concheck(icb_gcmma h, double f0xnew, const double *fxnew, int *conservative)
+{
+  API_TRY
+  need(h && fxnew && conservative, "NULL argument");
+  *conservative = h->g->concheck(f0xnew, fxnew[0]) ? 1 : 0;
+  API_CATCH
+}
+
 // ---------------------------------------------------------------- loops ----
 /// The opt-macro-oc loop (opt_macro_oc.cpp:84-172) on the device, without
 /// I/O and with a fixed number of steps.  hist[step] = compliance.
@@ -518,6 +605,91 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
       count_launch();
     }
     mma.update(x.p, dcf.p, g, dvf.p, lo.p, hi.p, s);
+    ICB_CUDA(cudaStreamSynchronize(s));
+    if(o->iter_seconds)
+      o->iter_seconds[step - 1] =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  if(xout)
+    ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  API_CATCH
+}
+
+/// The opt_macro_gcmma loop (opt_macro_gcmma.cpp:83-238) on the device:
+/// cone filter, threshold with beta = min(int(max((step - 100) / 40, 1)), 8),
+/// solve, V0 at step 1, constraint sum x v - V0, sensitivities times the
+/// threshold derivative (dv = v), adjoint filter, GCMMA outer update,
+/// evaluation of the candidate, at most 15 inner updates until ConCheck.
+int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
+                  int *inner, double *xout)
+{
+  API_TRY
+  needFinal(p);
+  need(o && rho0 && hist, "NULL argument");
+  need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
+  ICB_CUDA(cudaSetDevice(p->ctx->device));
+  cudaStream_t s = p->stream();
+  const long long n = p->d.nel;
+  const double vol = p->hs->volume;
+  ConeFilter cone(p->d, p->hs->h, o->filter_radius, s);
+  GcmmaUpdater gc(n, s);
+  DevBuf<double> x(n), xnew(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n),
+      V(n);
+  ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, vol, V.p);
+  count_launch(3);
+  icb_solve_opts so = o->solve;
+  double V0 = 0.0;
+  StepReport report;
+  // filter, threshold and solve at xx: compliance and sum x v
+  auto evaluate = [&](const double *xx, double beta, double &f, double &vs) {
+    cone.forward(xx, xf.p, beta, 0.5, xh.p, dxh.p, s);
+    int rc = icb_set_density_device(p, xh.p);
+    if(rc == ICB_OK)
+      rc = icb_solve(p, &so, nullptr);
+    if(rc == ICB_OK)
+      rc = icb_compliance(p, &f);
+    if(rc)
+      throw Error{rc, icb_last_error()};
+    vs = deviceSum(p, xh.p, n) * vol;
+  };
+  for(int step = 1; step <= o->nsteps; step++)
+  {
+    auto t0 = std::chrono::steady_clock::now();
+    const int btmp = int(std::max((step - 100) / 40.0, 1.0));
+    const double beta = std::min(double(btmp), 8.0);
+    double f, vs;
+    evaluate(x.p, beta, f, vs);
+    hist[step - 1] = f;
+    report(p, o, step, f, xh.p);
+    if(step == 1)
+      V0 = vs;
+    const double g = vs - V0;
+    const double *dcd = icb_sensitivity_device(p);
+    if(!dcd)
+      throw Error{ICB_ERR_STATE, "sensitivity failed"};
+    ICB_CUDA(cudaMemcpyAsync(dc.p, dcd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    k_scale_mul<<<nb256(n), 256, 0, s>>>(n, dc.p, dxh.p, 1.0);
+    ICB_CUDA(cudaMemcpyAsync(dv.p, V.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    k_scale_mul<<<nb256(n), 256, 0, s>>>(n, dv.p, dxh.p, 1.0);
+    count_launch(2);
+    cone.adjoint(dc.p, dcf.p, s);
+    cone.adjoint(dv.p, dvf.p, s);
+    gc.outer(xnew.p, x.p, f, dcf.p, g, dvf.p, lo.p, hi.p, s);
+    double fn, vn;
+    evaluate(xnew.p, beta, fn, vn);
+    int k = 0;
+    for(; !gc.concheck(fn, vn - V0) && k < 15; k++)
+    {
+      gc.inner(xnew.p, fn, vn - V0, x.p, f, dcf.p, g, dvf.p, lo.p, hi.p, s);
+      evaluate(xnew.p, beta, fn, vn);
+    }
+    if(inner)
+      inner[step - 1] = k;
+    ICB_CUDA(cudaMemcpyAsync(x.p, xnew.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     ICB_CUDA(cudaStreamSynchronize(s));
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =

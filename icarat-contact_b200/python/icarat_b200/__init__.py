@@ -98,6 +98,13 @@ _SIGS = {
     "icb_count_dof": (C.c_int, [C.c_void_p, _ip, C.POINTER(C.c_longlong)]),
     "icb_get_dof_map": (C.c_int, [C.c_void_p, _ip]),
     "icb_von_mises": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "icb_gcmma_create": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_void_p)]),
+    "icb_gcmma_destroy": (C.c_int, [C.c_void_p]),
+    "icb_gcmma_outer": (C.c_int, [C.c_void_p, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, _dp]),
+    "icb_gcmma_inner": (C.c_int, [C.c_void_p, _dp, C.c_double, _dp, _dp, C.c_double, _dp, _dp,
+                                  _dp, _dp, _dp]),
+    "icb_gcmma_concheck": (C.c_int, [C.c_void_p, C.c_double, _dp, _ip]),
+    "icb_run_gcmma": (C.c_int, [C.c_void_p, C.c_void_p, _dp, _dp, _ip, _dp]),
     "icb_reactions": (C.c_int, [C.c_void_p, _dp]),
     "icb_get_load": (C.c_int, [C.c_void_p, _dp]),
     "icb_problem_sizes": (C.c_int, [C.c_void_p, _llp, _llp, _llp, _llp]),
@@ -430,6 +437,54 @@ def oc_update(prob, cone, x, dfdx, g, dgdx, xmin, xmax, move, beta=0.0, T=0.5):
                               float(g), _p(args[1]), _p(args[2]), _p(args[3]), move, beta, T,
                               C.byref(steps)))
     return x, steps.value
+
+
+class GCMMA:
+    """icb_gcmma: GCMMASolver's outer / inner updates and ConCheck (m = 1)."""
+
+    def __init__(self, ctx, n, m=1):
+        h = C.c_void_p()
+        check(lib().icb_gcmma_create(ctx.h, n, m, C.byref(h)))
+        self.h, self.n = h, n
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.icb_gcmma_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def outer(self, xval, f0x, df0dx, fx, dfdx, xmin, xmax):
+        xm = np.zeros(self.n)
+        a = [np.ascontiguousarray(v, np.float64) for v in (xval, df0dx, np.atleast_1d(fx), dfdx,
+                                                           xmin, xmax)]
+        check(lib().icb_gcmma_outer(self.h, _p(xm), _p(a[0]), float(f0x), *[_p(v) for v in a[1:]]))
+        return xm
+
+    def inner(self, xmma, f0xnew, fxnew, xval, f0x, df0dx, fx, dfdx, xmin, xmax):
+        xm = np.array(xmma, np.float64)
+        a = [np.ascontiguousarray(v, np.float64) for v in (np.atleast_1d(fxnew), xval, df0dx,
+                                                           np.atleast_1d(fx), dfdx, xmin, xmax)]
+        check(lib().icb_gcmma_inner(self.h, _p(xm), float(f0xnew), _p(a[0]), _p(a[1]), float(f0x),
+                                    *[_p(v) for v in a[2:]]))
+        return xm
+
+    def concheck(self, f0xnew, fxnew):
+        ok = C.c_int()
+        fx = np.ascontiguousarray(np.atleast_1d(fxnew), np.float64)
+        check(lib().icb_gcmma_concheck(self.h, float(f0xnew), _p(fx), C.byref(ok)))
+        return bool(ok.value)
+
+
+def run_gcmma(prob, rho0, nsteps, radius, precision=FP64, precond=GMG, tol=1e-8, maxit=20000):
+    """icb_run_gcmma: (compliance history, inner iterations per step, design)."""
+    o = LoopOpts(nsteps, radius, 0.15, 1, 0.0, SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0),
+                 None)
+    hist, inner, x = np.zeros(nsteps), np.zeros(nsteps, np.int32), np.zeros(prob.nel)
+    rho0 = np.ascontiguousarray(rho0, np.float64)
+    check(lib().icb_run_gcmma(prob.h, C.byref(o), _p(rho0), _p(hist), _p(inner, _ip), _p(x)))
+    return hist, inner, x
 
 
 class MMA:

@@ -21,6 +21,7 @@
 //                     (src/optimization/filter_helm.hpp:28-137)
 //   OC::UpdateVariables (src/optimization/opt-solver/OCSolver.hpp:16-70)
 //   MMASolver::Update (src/optimization/opt-solver/MMASolver.hpp:62-80)
+//   GCMMASolver::OuterUpdate / InnerUpdate / ConCheck (GCMMASolver.hpp:60-90)
 //   Optimize          (src/optimization/opt_base.hpp:14-76)
 //
 // Differences a caller sees:
@@ -772,6 +773,44 @@ public:
 
 private:
   icb_mma h_ = nullptr;
+};
+
+/// GCMMASolver (src/optimization/opt-solver/GCMMASolver.hpp:60-90), one
+/// constraint: OuterUpdate, InnerUpdate, ConCheck on the device
+class GCMMASolver
+{
+public:
+  GCMMASolver(int n, int m, double a = 0.0, double c = 1000.0, double d = 0.0)
+  {
+    if(m != 1 || a != 0.0 || c != 1000.0 || d != 0.0)
+      detail::fatal("Error: the device GCMMA solves m = 1 with a = 0, c = 1000, d = 0");
+    check(icb_gcmma_create(detail::shared_context(), n, m, &h_), "icb_gcmma_create");
+  }
+  ~GCMMASolver() { icb_gcmma_destroy(h_); }
+  GCMMASolver(const GCMMASolver &) = delete;
+  GCMMASolver &operator=(const GCMMASolver &) = delete;
+
+  void OuterUpdate(double *xmma, const double *xval, double f0x, const double *df0dx,
+                   const double *fx, const double *dfdx, const double *xmin, const double *xmax)
+  {
+    check(icb_gcmma_outer(h_, xmma, xval, f0x, df0dx, fx, dfdx, xmin, xmax), "icb_gcmma_outer");
+  }
+  void InnerUpdate(double *xmma, double f0xnew, const double *fxnew, const double *xval,
+                   double f0x, const double *df0dx, const double *fx, const double *dfdx,
+                   const double *xmin, const double *xmax)
+  {
+    check(icb_gcmma_inner(h_, xmma, f0xnew, fxnew, xval, f0x, df0dx, fx, dfdx, xmin, xmax),
+          "icb_gcmma_inner");
+  }
+  bool ConCheck(double f0xnew, const double *fxnew) const
+  {
+    int ok = 0;
+    check(icb_gcmma_concheck(h_, f0xnew, fxnew, &ok), "icb_gcmma_concheck");
+    return ok != 0;
+  }
+
+private:
+  icb_gcmma h_ = nullptr;
 };
 
 /// design-variable bookkeeping (src/optimization/opt_base.hpp:14-76)

@@ -50,6 +50,7 @@ typedef struct icb_problem_s *icb_problem;
 typedef struct icb_cone_s *icb_cone;
 typedef struct icb_helm_s *icb_helm;
 typedef struct icb_mma_s *icb_mma;
+typedef struct icb_gcmma_s *icb_gcmma;
 
 /* Structured box problem: the `[mesh]` keys of MeshIcarat::setParameter
  * (src/io/mesh_icarat.hpp:69-128) and the `[material]` keys of
@@ -205,6 +206,20 @@ int icb_mma_create(icb_ctx ctx, long long n, int m, icb_mma *out);
 int icb_mma_destroy(icb_mma h);
 int icb_mma_update(icb_mma h, double *x, const double *dfdx, const double *gx,
                    const double *dgdx, const double *xmin, const double *xmax);
+/* GCMMASolver(n, m) (src/optimization/opt-solver/GCMMASolver.hpp:60-90) with
+ * a = 0, c = 1000, d = 0; m must be 1.  OuterUpdate (GCMMASolver.cpp:66-89),
+ * InnerUpdate (:91-112) and ConCheck (:114-128) as the GCMMA app calls them
+ * (opt_macro_gcmma.cpp:153-212). */
+int icb_gcmma_create(icb_ctx ctx, long long n, int m, icb_gcmma *out);
+int icb_gcmma_destroy(icb_gcmma h);
+int icb_gcmma_outer(icb_gcmma h, double *xmma, const double *xval, double f0x,
+                    const double *df0dx, const double *fx, const double *dfdx, const double *xmin,
+                    const double *xmax);
+int icb_gcmma_inner(icb_gcmma h, double *xmma, double f0xnew, const double *fxnew,
+                    const double *xval, double f0x, const double *df0dx, const double *fx,
+                    const double *dfdx, const double *xmin, const double *xmax);
+/* *conservative = 1 when the approximations at the last xmma bound f0xnew, fxnew */
+int icb_gcmma_concheck(icb_gcmma h, double f0xnew, const double *fxnew, int *conservative);
 
 /* ---- the ICARAT app loops on the device ----------------------------------- */
 #define ICB_FILTER_HELMHOLTZ 0 /* FilterHelmholtz (filter_helm.hpp)              */
@@ -246,6 +261,15 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
  * threshold, solve, volume constraint, sensitivities, adjoint filters, MMA. */
 int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
                 double *xout);
+
+/* opt-macro-gcmma (opt_macro_gcmma.cpp:83-238): cone filter of radius
+ * filter_radius, threshold beta = min(int(max((step - 100) / 40, 1)), 8),
+ * solve, constraint sum x v - V0, GCMMA outer update and up to 15 inner
+ * updates per step, each with a full evaluation.  hist[step] is the
+ * compliance of the step's design, inner[step] (may be NULL) its inner
+ * iterations. */
+int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
+                  int *inner, double *xout);
 
 /* ---- many runs on one GPU: batch runner and job server ------------------- */
 /* No counterpart in ICARAT (one problem per process).  Runs are independent

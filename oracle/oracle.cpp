@@ -1167,6 +1167,10 @@ struct Mma
   std::vector<double> a, c, low, upp, alpha, beta, p0, q0, pij, qij, b,
       xold1, xold2, lam, mu, y, grad, hess, s;
   double z = 0.0;
+  // GCMMA only: constraint raa, constant terms and approximation values
+  std::vector<double> raa, r, fapp;
+  double r0 = 0.0, f0app = 0.0;
+  int dualCap = 100; // outer-loop cap of the dual (none in GCMMA: 1 << 30)
 };
 
 void *orc_mma_create(int64_t n, int m, double a, double c, double d)
@@ -1231,79 +1235,14 @@ void mmaDualGrad(Mma &M, const double *x, std::vector<double> &g)
 }
 } // namespace
 
-void orc_mma_update(void *h, double *x, const double *dfdx, const double *gx,
-                    const double *dgdx, const double *xmin, const double *xmax)
+namespace
 {
-  Mma &M = *static_cast<Mma *>(h);
+/// SolveDIP (MMASolver.cpp:88-154; GCMMASolver.cpp:128-200): the dual of the
+/// subproblem by a primal-dual interior point iteration, x <- x(lambda)
+void mmaDual(Mma &M, double *x)
+{
   int64_t n = M.n;
   int m = M.m;
-  M.iter++;
-  // asymptotes
-  for(int64_t i = 0; i < n; i++)
-  {
-    double range = xmax[i] - xmin[i];
-    if(M.iter < 3)
-    {
-      M.low[i] = x[i] - M.asyminit * range;
-      M.upp[i] = x[i] + M.asyminit * range;
-      continue;
-    }
-    double t = (x[i] - M.xold1[i]) * (M.xold1[i] - M.xold2[i]);
-    double gam = t < 0.0 ? M.asymdec : (t > 0.0 ? M.asyminc : 1.0);
-    double lo = x[i] - gam * (M.xold1[i] - M.low[i]);
-    double up = x[i] + gam * (M.upp[i] - M.xold1[i]);
-    double xmami = std::max(M.xmamieps, range);
-    lo = std::min(std::max(lo, x[i] - 100.0 * xmami), x[i] - 1.0e-5 * xmami);
-    up = std::min(std::max(up, x[i] + 1.0e-5 * xmami), x[i] + 100.0 * xmami);
-    double xmi = xmin[i] - 1.0e-6, xma = xmax[i] + 1.0e-6;
-    if(x[i] < xmi)
-    {
-      lo = x[i] - (xma - x[i]) / 0.9;
-      up = x[i] + (xma - x[i]) / 0.9;
-    }
-    if(x[i] > xma)
-    {
-      lo = x[i] - (x[i] - xmi) / 0.9;
-      up = x[i] + (x[i] - xmi) / 0.9;
-    }
-    M.low[i] = lo;
-    M.upp[i] = up;
-  }
-  // bounds and approximation coefficients
-  for(int64_t i = 0; i < n; i++)
-  {
-    double range = xmax[i] - xmin[i];
-    double al = std::max(xmin[i], M.low[i] + M.albefa * (x[i] - M.low[i]));
-    al = std::min(std::max(al, x[i] - M.move * range), xmax[i]);
-    double be = std::min(xmax[i], M.upp[i] - M.albefa * (M.upp[i] - x[i]));
-    be = std::max(std::min(be, x[i] + M.move * range), xmin[i]);
-    M.alpha[i] = al;
-    M.beta[i] = be;
-    double inv = 1.0 / std::max(M.xmamieps, range);
-    double u2 = std::pow(M.upp[i] - x[i], 2.0), l2 = std::pow(x[i] - M.low[i], 2.0);
-    double pq = 0.001 * std::fabs(dfdx[i]) + M.raa0 * inv;
-    M.p0[i] = u2 * (std::max(0.0, dfdx[i]) + pq);
-    M.q0[i] = l2 * (std::max(0.0, -dfdx[i]) + pq);
-    for(int j = 0; j < m; j++)
-    {
-      double gg = dgdx[i * m + j];
-      double pqj = 0.001 * std::fabs(gg) + M.raa0 * inv;
-      M.pij[i * m + j] = u2 * (std::max(0.0, gg) + pqj);
-      M.qij[i * m + j] = l2 * (std::max(0.0, -gg) + pqj);
-    }
-  }
-  for(int j = 0; j < m; j++)
-  {
-    double s = -gx[j];
-    for(int64_t i = 0; i < n; i++)
-      s += M.pij[i * m + j] / (M.upp[i] - x[i]) +
-           M.qij[i * m + j] / (x[i] - M.low[i]);
-    M.b[j] = s;
-  }
-  M.xold2 = M.xold1;
-  std::copy(x, x + n, M.xold1.begin());
-
-  // dual interior point
   for(int j = 0; j < m; j++)
   {
     M.lam[j] = M.c[j] / 2.0;
@@ -1312,7 +1251,7 @@ void orc_mma_update(void *h, double *x, const double *dfdx, const double *gx,
   double epsi = 1.0, err = 1.0;
   int outer = 0;
   std::vector<double> df2(n), PQ(n * m);
-  while(epsi > M.epsimin && outer < 100)
+  while(epsi > M.epsimin && outer < M.dualCap)
   {
     outer++;
     int inner = 0;
@@ -1427,6 +1366,82 @@ void orc_mma_update(void *h, double *x, const double *dfdx, const double *gx,
     }
     epsi *= 0.1;
   }
+}
+} // namespace
+
+void orc_mma_update(void *h, double *x, const double *dfdx, const double *gx,
+                    const double *dgdx, const double *xmin, const double *xmax)
+{
+  Mma &M = *static_cast<Mma *>(h);
+  int64_t n = M.n;
+  int m = M.m;
+  M.iter++;
+  // asymptotes
+  for(int64_t i = 0; i < n; i++)
+  {
+    double range = xmax[i] - xmin[i];
+    if(M.iter < 3)
+    {
+      M.low[i] = x[i] - M.asyminit * range;
+      M.upp[i] = x[i] + M.asyminit * range;
+      continue;
+    }
+    double t = (x[i] - M.xold1[i]) * (M.xold1[i] - M.xold2[i]);
+    double gam = t < 0.0 ? M.asymdec : (t > 0.0 ? M.asyminc : 1.0);
+    double lo = x[i] - gam * (M.xold1[i] - M.low[i]);
+    double up = x[i] + gam * (M.upp[i] - M.xold1[i]);
+    double xmami = std::max(M.xmamieps, range);
+    lo = std::min(std::max(lo, x[i] - 100.0 * xmami), x[i] - 1.0e-5 * xmami);
+    up = std::min(std::max(up, x[i] + 1.0e-5 * xmami), x[i] + 100.0 * xmami);
+    double xmi = xmin[i] - 1.0e-6, xma = xmax[i] + 1.0e-6;
+    if(x[i] < xmi)
+    {
+      lo = x[i] - (xma - x[i]) / 0.9;
+      up = x[i] + (xma - x[i]) / 0.9;
+    }
+    if(x[i] > xma)
+    {
+      lo = x[i] - (x[i] - xmi) / 0.9;
+      up = x[i] + (x[i] - xmi) / 0.9;
+    }
+    M.low[i] = lo;
+    M.upp[i] = up;
+  }
+  // bounds and approximation coefficients
+  for(int64_t i = 0; i < n; i++)
+  {
+    double range = xmax[i] - xmin[i];
+    double al = std::max(xmin[i], M.low[i] + M.albefa * (x[i] - M.low[i]));
+    al = std::min(std::max(al, x[i] - M.move * range), xmax[i]);
+    double be = std::min(xmax[i], M.upp[i] - M.albefa * (M.upp[i] - x[i]));
+    be = std::max(std::min(be, x[i] + M.move * range), xmin[i]);
+    M.alpha[i] = al;
+    M.beta[i] = be;
+    double inv = 1.0 / std::max(M.xmamieps, range);
+    double u2 = std::pow(M.upp[i] - x[i], 2.0), l2 = std::pow(x[i] - M.low[i], 2.0);
+    double pq = 0.001 * std::fabs(dfdx[i]) + M.raa0 * inv;
+    M.p0[i] = u2 * (std::max(0.0, dfdx[i]) + pq);
+    M.q0[i] = l2 * (std::max(0.0, -dfdx[i]) + pq);
+    for(int j = 0; j < m; j++)
+    {
+      double gg = dgdx[i * m + j];
+      double pqj = 0.001 * std::fabs(gg) + M.raa0 * inv;
+      M.pij[i * m + j] = u2 * (std::max(0.0, gg) + pqj);
+      M.qij[i * m + j] = l2 * (std::max(0.0, -gg) + pqj);
+    }
+  }
+  for(int j = 0; j < m; j++)
+  {
+    double s = -gx[j];
+    for(int64_t i = 0; i < n; i++)
+      s += M.pij[i * m + j] / (M.upp[i] - x[i]) +
+           M.qij[i * m + j] / (x[i] - M.low[i]);
+    M.b[j] = s;
+  }
+  M.xold2 = M.xold1;
+  std::copy(x, x + n, M.xold1.begin());
+
+  mmaDual(M, x);
 }
 
 // ---------------------------------------------------------------- loops ----
@@ -1742,6 +1757,248 @@ int orc_mma_cone_loop(const OrcGrid *g, const uint8_t *fixed, const double *dval
   }
   orc_cone_free(cone);
   orc_mma_free(mma);
+  return 0;
+}
+
+// ---------------------------------------------------------------- GCMMA ----
+/// GCMMA, the globally convergent MMA with conservative inner iterations, as
+/// GCMMASolver sets it up (src/optimization/opt-solver/GCMMASolver.cpp:41-58):
+/// raa0 = raa_j = 1 at start, raa0eps = raaeps = 1e-6, xmamieps 1e-5,
+/// epsimin sqrt(n+m) 1e-9, move 0.15, albefa 0.2, asymptotes 0.2 / 0.7 /
+/// 1.2, c = 1000 by default; the dual has no outer-loop cap.  Outer update
+/// (:66-89): asymptotes and raa shrink (:432-508), subproblem (:546-596),
+/// xold shift, dual, approximation values (:598-621).  Inner update
+/// (:91-112): raa growth from the non-conservative misfit (:510-544), then
+/// the same subproblem, dual and approximation.  Written from Svanberg's
+/// published method with these constants.
+void *orc_gcmma_create(int64_t n, int m, double a, double c, double d)
+{
+  Mma *M = static_cast<Mma *>(orc_mma_create(n, m, a, c, d));
+  M->raa0 = 1.0;
+  M->raa.assign(m, 1.0);
+  M->r.assign(m, 0.0);
+  M->fapp.assign(m, 0.0);
+  M->dualCap = 1 << 30;
+  return M;
+}
+void orc_gcmma_free(void *h) { delete static_cast<Mma *>(h); }
+
+namespace
+{
+void gcAsymp(Mma &M, const double *x, const double *xmin, const double *xmax)
+{
+  M.iter++;
+  for(int64_t i = 0; i < M.n; i++)
+  {
+    double range = xmax[i] - xmin[i];
+    if(M.iter < 3)
+    {
+      M.low[i] = x[i] - M.asyminit * range;
+      M.upp[i] = x[i] + M.asyminit * range;
+      continue;
+    }
+    double t = (x[i] - M.xold1[i]) * (M.xold1[i] - M.xold2[i]);
+    double gam = t < 0.0 ? M.asymdec : (t > 0.0 ? M.asyminc : 1.0);
+    double lo = x[i] - gam * (M.xold1[i] - M.low[i]);
+    double up = x[i] + gam * (M.upp[i] - M.xold1[i]);
+    double xmami = std::max(M.xmamieps, range);
+    lo = std::min(std::max(lo, x[i] - 100.0 * xmami), x[i] - 1.0e-5 * xmami);
+    up = std::min(std::max(up, x[i] + 1.0e-5 * xmami), x[i] + 100.0 * xmami);
+    double xmi = xmin[i] - 1.0e-6, xma = xmax[i] + 1.0e-6;
+    if(x[i] < xmi)
+    {
+      lo = x[i] - (xma - x[i]) / 0.9;
+      up = x[i] + (xma - x[i]) / 0.9;
+    }
+    if(x[i] > xma)
+    {
+      lo = x[i] - (x[i] - xmi) / 0.9;
+      up = x[i] + (x[i] - xmi) / 0.9;
+    }
+    M.low[i] = lo;
+    M.upp[i] = up;
+  }
+  M.raa0 = std::max(1e-6, 0.1 * M.raa0);
+  for(int j = 0; j < M.m; j++)
+    M.raa[j] = std::max(1e-6, 0.1 * M.raa[j]);
+}
+
+void gcSub(Mma &M, const double *x, double f0x, const double *df0dx, const double *fx,
+           const double *dfdx, const double *xmin, const double *xmax)
+{
+  int m = M.m;
+  double r0 = 0.0;
+  std::vector<double> r(m, 0.0);
+  for(int64_t i = 0; i < M.n; i++)
+  {
+    double range = xmax[i] - xmin[i];
+    double al = std::max(xmin[i], M.low[i] + M.albefa * (x[i] - M.low[i]));
+    M.alpha[i] = std::max(al, x[i] - M.move * range);
+    double be = std::min(xmax[i], M.upp[i] - M.albefa * (M.upp[i] - x[i]));
+    M.beta[i] = std::min(be, x[i] + M.move * range);
+    double uxinv = 1.0 / (M.upp[i] - x[i]), xlinv = 1.0 / (x[i] - M.low[i]);
+    double inv = 1.0 / std::max(M.xmamieps, range);
+    double u2 = std::pow(M.upp[i] - x[i], 2.0), l2 = std::pow(x[i] - M.low[i], 2.0);
+    double pq = 0.001 * std::fabs(df0dx[i]) + M.raa0 * inv;
+    M.p0[i] = u2 * (std::max(0.0, df0dx[i]) + pq);
+    M.q0[i] = l2 * (std::max(0.0, -df0dx[i]) + pq);
+    r0 += M.p0[i] * uxinv + M.q0[i] * xlinv;
+    for(int j = 0; j < m; j++)
+    {
+      double gg = dfdx[i * m + j];
+      double pqj = 0.001 * std::fabs(gg) + M.raa[j] * inv;
+      M.pij[i * m + j] = u2 * (std::max(0.0, gg) + pqj);
+      M.qij[i * m + j] = l2 * (std::max(0.0, -gg) + pqj);
+      r[j] += M.pij[i * m + j] * uxinv + M.qij[i * m + j] * xlinv;
+    }
+  }
+  M.r0 = f0x - r0;
+  for(int j = 0; j < m; j++)
+  {
+    M.r[j] = fx[j] - r[j];
+    M.b[j] = -M.r[j];
+  }
+}
+
+void gcApprox(Mma &M, const double *xmma)
+{
+  double f0 = 0.0;
+  std::vector<double> f(M.m, 0.0);
+  for(int64_t i = 0; i < M.n; i++)
+  {
+    double uxinv = 1.0 / (M.upp[i] - xmma[i]), xlinv = 1.0 / (xmma[i] - M.low[i]);
+    f0 += M.p0[i] * uxinv + M.q0[i] * xlinv;
+    for(int j = 0; j < M.m; j++)
+      f[j] += M.pij[i * M.m + j] * uxinv + M.qij[i * M.m + j] * xlinv;
+  }
+  M.f0app = f0 + M.r0;
+  for(int j = 0; j < M.m; j++)
+    M.fapp[j] = f[j] + M.r[j];
+}
+} // namespace
+
+void orc_gcmma_outer(void *h, double *xmma, const double *xval, double f0x, const double *df0dx,
+                     const double *fx, const double *dfdx, const double *xmin, const double *xmax)
+{
+  Mma &M = *static_cast<Mma *>(h);
+  gcAsymp(M, xval, xmin, xmax);
+  gcSub(M, xval, f0x, df0dx, fx, dfdx, xmin, xmax);
+  M.xold2 = M.xold1;
+  std::copy(xval, xval + M.n, M.xold1.begin());
+  std::copy(xval, xval + M.n, xmma);
+  mmaDual(M, xmma);
+  gcApprox(M, xmma);
+}
+
+void orc_gcmma_inner(void *h, double *xmma, double f0xnew, const double *fxnew, const double *xval,
+                     double f0x, const double *df0dx, const double *fx, const double *dfdx,
+                     const double *xmin, const double *xmax)
+{
+  Mma &M = *static_cast<Mma *>(h);
+  double raacof = 0.0;
+  for(int64_t i = 0; i < M.n; i++)
+  {
+    double xmami = std::max(M.xmamieps, xmax[i] - xmin[i]);
+    double xxux = (xmma[i] - xval[i]) / (M.upp[i] - xmma[i]);
+    double xxxl = (xmma[i] - xval[i]) / (xmma[i] - M.low[i]);
+    raacof += xxux * xxxl * ((M.upp[i] - M.low[i]) / xmami);
+  }
+  raacof = std::max(1e-12, raacof);
+  if(f0xnew > M.f0app + 0.5 * M.epsimin)
+    M.raa0 = std::min(1.1 * (M.raa0 + (f0xnew - M.f0app) / raacof), 10.0 * M.raa0);
+  for(int j = 0; j < M.m; j++)
+    if(fxnew[j] > M.fapp[j] + 0.5 * M.epsimin)
+      M.raa[j] = std::min(1.1 * (M.raa[j] + (fxnew[j] - M.fapp[j]) / raacof), 10.0 * M.raa[j]);
+  gcSub(M, xval, f0x, df0dx, fx, dfdx, xmin, xmax);
+  std::copy(xval, xval + M.n, xmma);
+  mmaDual(M, xmma);
+  gcApprox(M, xmma);
+}
+
+/// ConCheck (GCMMASolver.cpp:114-128): 1 when the approximations at xmma
+/// are conservative for the new values
+int orc_gcmma_concheck(void *h, double f0xnew, const double *fxnew)
+{
+  Mma &M = *static_cast<Mma *>(h);
+  if(M.f0app + M.epsimin < f0xnew)
+    return 0;
+  for(int j = 0; j < M.m; j++)
+    if(M.fapp[j] + M.epsimin < fxnew[j])
+      return 0;
+  return 1;
+}
+
+/// The optimisation loop of opt_macro_gcmma.cpp (:83-238) without I/O: cone
+/// filter (radius rfil), threshold with beta = min(int(max((step - 100) / 40,
+/// 1)), 8), solve, V0 at step 1, constraint sum x v - V0 (not normalised),
+/// sensitivities times the threshold derivative (dv = v), adjoint filter,
+/// GCMMA outer update, evaluation at the candidate, at most 15 inner updates
+/// until the approximation is conservative.  hist[step] is the compliance of
+/// the step's design; inner[step] the number of inner iterations.
+int orc_gcmma_loop(const OrcGrid *g, const uint8_t *fixed, const double *dval, const double *fext,
+                   const double *rho0, int nsteps, double rfil, double tol, double *hist, int *inner,
+                   double *x)
+{
+  int d = g->dim;
+  int64_t nn = numnp(*g), nel = nelx(*g);
+  std::vector<int> dof(nn * d);
+  int64_t numeq = orc_count_dof(g, fixed, dof.data());
+  std::vector<double> u(numeq), nodeval(nn * d), xf(nel), xt(nel), dxt(nel), dc(nel), dv(nel),
+      xmin(nel, 1.0e-4), xmax(nel, 1.0), t1(nel), t2(nel), xnew(nel);
+  std::copy(rho0, rho0 + nel, x);
+  double vol = orc_element_volume(g);
+  void *gc = orc_gcmma_create(nel, 1, 0.0, 1000.0, 0.0);
+  void *cone = orc_cone_create(g, rfil);
+  double V0 = 0.0;
+  auto evaluate = [&](const double *xx, double beta, double &f, double &gv) {
+    orc_cone_apply(cone, xx, xf.data(), 0);
+    orc_threshold(nel, xf.data(), beta, 0.5, xt.data());
+    double rr;
+    int it, mv;
+    orc_linear_solve(g, fixed, dval, dof.data(), numeq, fext, xt.data(), tol, 100000, u.data(),
+                     nodeval.data(), &f, &it, &rr, &mv);
+    double vs = 0.0;
+    for(int64_t i = 0; i < nel; i++)
+      vs += xt[i] * vol;
+    gv = vs;
+  };
+  for(int step = 1; step <= nsteps; step++)
+  {
+    int btmp = int(std::max((step - 100) / 40.0, 1.0));
+    double beta = std::min(double(btmp), 8.0);
+    double f, vs;
+    evaluate(x, beta, f, vs);
+    orc_threshold_deriv(nel, xf.data(), beta, 0.5, dxt.data());
+    if(step == 1)
+      V0 = vs;
+    double gv = vs - V0;
+    hist[step - 1] = f;
+    orc_sensitivity(g, xt.data(), nodeval.data(), dc.data());
+    for(int64_t i = 0; i < nel; i++)
+    {
+      dc[i] *= dxt[i];
+      dv[i] = vol * dxt[i];
+    }
+    orc_cone_apply(cone, dc.data(), t1.data(), 1);
+    orc_cone_apply(cone, dv.data(), t2.data(), 1);
+    orc_gcmma_outer(gc, xnew.data(), x, f, t1.data(), &gv, t2.data(), xmin.data(), xmax.data());
+    double fn, vn;
+    evaluate(xnew.data(), beta, fn, vn);
+    double gn = vn - V0;
+    int k = 0;
+    for(; !orc_gcmma_concheck(gc, fn, &gn) && k < 15; k++)
+    {
+      orc_gcmma_inner(gc, xnew.data(), fn, &gn, x, f, t1.data(), &gv, t2.data(), xmin.data(),
+                      xmax.data());
+      evaluate(xnew.data(), beta, fn, vn);
+      gn = vn - V0;
+    }
+    if(inner)
+      inner[step - 1] = k;
+    std::copy(xnew.begin(), xnew.end(), x);
+  }
+  orc_cone_free(cone);
+  orc_gcmma_free(gc);
   return 0;
 }
 

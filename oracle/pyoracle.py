@@ -90,6 +90,15 @@ def lib():
             "orc_reactions": (None, [G, _dp, _dp, _dp]),
             "orc_mma_cone_loop": (C.c_int, [G, _u8p, _dp, _dp, _dp, C.c_int, C.c_double, _u8p,
                                             _u8p, C.c_double, _dp, _dp]),
+            "orc_gcmma_create": (C.c_void_p, [C.c_int64, C.c_int, C.c_double, C.c_double,
+                                              C.c_double]),
+            "orc_gcmma_free": (None, [C.c_void_p]),
+            "orc_gcmma_outer": (None, [C.c_void_p, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, _dp]),
+            "orc_gcmma_inner": (None, [C.c_void_p, _dp, C.c_double, _dp, _dp, C.c_double, _dp, _dp,
+                                       _dp, _dp, _dp]),
+            "orc_gcmma_concheck": (C.c_int, [C.c_void_p, C.c_double, _dp]),
+            "orc_gcmma_loop": (C.c_int, [G, _u8p, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double,
+                                         _dp, _ip, _dp]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -120,6 +129,17 @@ def ref():
         L.ref_mma_update.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_mma_free.restype = None
         L.ref_mma_free.argtypes = [C.c_void_p]
+        L.ref_gcmma_create.restype = C.c_void_p
+        L.ref_gcmma_create.argtypes = [C.c_int, C.c_int]
+        L.ref_gcmma_outer.restype = None
+        L.ref_gcmma_outer.argtypes = [C.c_void_p, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, _dp]
+        L.ref_gcmma_inner.restype = None
+        L.ref_gcmma_inner.argtypes = [C.c_void_p, _dp, C.c_double, _dp, _dp, C.c_double, _dp, _dp,
+                                      _dp, _dp, _dp]
+        L.ref_gcmma_concheck.restype = C.c_int
+        L.ref_gcmma_concheck.argtypes = [C.c_void_p, C.c_double, _dp]
+        L.ref_gcmma_free.restype = None
+        L.ref_gcmma_free.argtypes = [C.c_void_p]
         _ref = L
     return _ref
 
@@ -273,6 +293,15 @@ class Problem:
                                 None if vs is None else _ptr(vs, _u8p), tol, _ptr(hist), _ptr(x))
         return hist, x
 
+    def gcmma_loop(self, rho0, nsteps, rfil, tol=1e-8):
+        hist = np.zeros(nsteps)
+        inner = np.zeros(nsteps, np.int32)
+        x = np.zeros(self.nel)
+        lib().orc_gcmma_loop(C.byref(self.g), _ptr(self.fixed, _u8p), _ptr(self.dval),
+                             _ptr(self.fext()), _ptr(np.ascontiguousarray(rho0, np.float64)),
+                             nsteps, rfil, tol, _ptr(hist), _ptr(inner, _ip), _ptr(x))
+        return hist, inner, x
+
     def mma_loop(self, rho0, nsteps, R, Vref=0.0, tol=1e-8):
         hist = np.zeros(nsteps)
         x = np.zeros(self.nel)
@@ -357,3 +386,43 @@ class MMA:
         f = ref().ref_mma_update if self.use_ref else lib().orc_mma_update
         f(self.h, _ptr(x), *[_ptr(v) for v in a])
         return x
+
+
+class GCMMA:
+    """GCMMA outer / inner updates and ConCheck; ``use_ref`` selects ICARAT's
+    own GCMMASolver (oracle/_ref)."""
+
+    def __init__(self, n, m=1, use_ref=False):
+        self.n, self.m, self.use_ref = n, m, use_ref
+        self.h = ref().ref_gcmma_create(n, m) if use_ref else lib().orc_gcmma_create(
+            n, m, 0.0, 1000.0, 0.0)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            (ref().ref_gcmma_free if self.use_ref else lib().orc_gcmma_free)(self.h)
+            self.h = None
+
+    def _L(self):
+        return ref() if self.use_ref else lib()
+
+    def outer(self, xval, f0x, df0dx, fx, dfdx, xmin, xmax):
+        xmma = np.zeros(self.n)
+        a = [np.ascontiguousarray(v, np.float64) for v in (xval, df0dx, np.atleast_1d(fx), dfdx,
+                                                           xmin, xmax)]
+        f = self._L().ref_gcmma_outer if self.use_ref else lib().orc_gcmma_outer
+        f(self.h, _ptr(xmma), _ptr(a[0]), float(f0x), *[_ptr(v) for v in a[1:]])
+        return xmma
+
+    def inner(self, xmma, f0xnew, fxnew, xval, f0x, df0dx, fx, dfdx, xmin, xmax):
+        xmma = np.array(xmma, np.float64)
+        a = [np.ascontiguousarray(v, np.float64) for v in (np.atleast_1d(fxnew), xval, df0dx,
+                                                           np.atleast_1d(fx), dfdx, xmin, xmax)]
+        f = self._L().ref_gcmma_inner if self.use_ref else lib().orc_gcmma_inner
+        f(self.h, _ptr(xmma), float(f0xnew), _ptr(a[0]), _ptr(a[1]), float(f0x),
+          *[_ptr(v) for v in a[2:]])
+        return xmma
+
+    def concheck(self, f0xnew, fxnew):
+        fx = np.ascontiguousarray(np.atleast_1d(fxnew), np.float64)
+        f = self._L().ref_gcmma_concheck if self.use_ref else lib().orc_gcmma_concheck
+        return bool(f(self.h, float(f0xnew), _ptr(fx)))

@@ -1,12 +1,17 @@
 """Generate the committed golden fixtures under tests/golden/.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--small-fem]
 
 ref_opt.npz -- outputs of ICARAT's own OC and MMA updates (OCSolver.hpp,
     MMASolver.cpp compiled from the ICARAT sources into oracle/_ref by
     oracle/Makefile) on seeded inputs: one OC update with a plain-volume
     callback, one OC update whose callback filters and thresholds (as
     opt_macro_oc.cpp:155-164 does), and a 6-step MMA trajectory with m = 1.
+ref_gcmma.npz -- ICARAT's own GCMMASolver (GCMMASolver.cpp from the ICARAT
+    sources, same build) driven through 8 outer updates with inner
+    iterations on the analytic problem min sum c / x^3 s.t. sum v x^2 / V
+    <= 1 (steep enough that several approximations are not conservative):
+    every update's output design and every ConCheck verdict.
 small_fem.npz -- oracle outputs on small structured problems (K0 matrices,
     loads of ICARAT's fdm.toml boundary conditions, a solve and its
     sensitivities), kept as regression vectors for the oracle itself.
@@ -67,6 +72,48 @@ def ref_opt():
     return out
 
 
+def gcmma_problem(n, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.5, 2.0, n)
+    v = rng.uniform(0.5, 1.5, n)
+    V = 0.35 * 0.25 * v.sum()
+    return c, v, V
+
+
+def gcmma_run(gc, n, c, v, V, x0, outers=8):
+    """Outer / inner GCMMA sequence of the GCMMA app (opt_macro_gcmma.cpp:
+    153-212) on f0 = sum c / x^3, f = sum v x^2 / V - 1; returns the designs
+    after every update and the ConCheck verdicts, in order."""
+    f0 = lambda x: float((c / x ** 3).sum())  # noqa: E731
+    f = lambda x: float(v @ x ** 2 / V - 1.0)  # noqa: E731
+    xmin, xmax = np.full(n, 1e-4), np.ones(n)
+    x = x0.copy()
+    outs, checks = [], []
+    for _ in range(outers):
+        df0, df = -3.0 * c / x ** 4, 2.0 * v * x / V
+        xm = gc.outer(x, f0(x), df0, f(x), df, xmin, xmax)
+        outs.append(xm.copy())
+        ok = gc.concheck(f0(xm), f(xm))
+        checks.append(ok)
+        k = 0
+        while not ok and k < 15:
+            xm = gc.inner(xm, f0(xm), f(xm), x, f0(x), df0, f(x), df, xmin, xmax)
+            outs.append(xm.copy())
+            ok = gc.concheck(f0(xm), f(xm))
+            checks.append(ok)
+            k += 1
+        x = xm
+    return np.array(outs), np.array(checks)
+
+
+def ref_gcmma():
+    n = 96
+    c, v, V = gcmma_problem(n, 7)
+    x0 = np.full(n, 0.5)
+    outs, checks = gcmma_run(po.GCMMA(n, 1, use_ref=True), n, c, v, V, x0)
+    return {"c": c, "v": v, "V": V, "x0": x0, "outs": outs, "checks": checks}
+
+
 def small_fem():
     out = {}
     out["K0_q4_stress"] = po.Problem(2, 2, 2).K0()
@@ -97,7 +144,10 @@ if __name__ == "__main__":
     if po.ref_available():
         np.savez_compressed(os.path.join(HERE, "ref_opt.npz"), **ref_opt())
         print("wrote ref_opt.npz (ICARAT OC/MMA from oracle/_ref)")
+        np.savez_compressed(os.path.join(HERE, "ref_gcmma.npz"), **ref_gcmma())
+        print("wrote ref_gcmma.npz (ICARAT GCMMA from oracle/_ref)")
     else:
         print("oracle/_ref not built: ref_opt.npz left as it is")
-    np.savez_compressed(os.path.join(HERE, "small_fem.npz"), **small_fem())
-    print("wrote small_fem.npz")
+    if "--small-fem" in sys.argv:
+        np.savez_compressed(os.path.join(HERE, "small_fem.npz"), **small_fem())
+        print("wrote small_fem.npz")
