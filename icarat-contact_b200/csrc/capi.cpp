@@ -141,6 +141,7 @@ int icb_problem_create(icb_ctx ctx, const icb_grid_desc *desc, icb_problem *out)
 {
   ICB_API_BEGIN
   need(ctx && desc && out, "NULL argument");
+  need(desc->state != ICB_HEAT, "heat conduction problems are created with icb_heat_create");
   auto p = std::make_unique<icb_problem_s>();
   p->ctx = ctx;
   p->hs = std::make_unique<HostSetup>(*desc);

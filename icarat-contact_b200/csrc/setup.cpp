@@ -62,6 +62,20 @@ void lame_constants(int state, double nu, double &lam, double &mu)
     lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
 }
 
+void heat_element(int dim, const double *h, const double *D, double *K)
+{
+  int ne = dim == 2 ? 4 : 8;
+  for(int a = 0; a < ne; a++)
+    for(int b = 0; b < ne; b++)
+    {
+      double v = 0.0;
+      for(int i = 0; i < dim; i++)
+        for(int j = 0; j < dim; j++)
+          v += D[i * dim + j] * gradInt(dim, h, a, b, i, j);
+      K[a * ne + b] = v;
+    }
+}
+
 void unit_stiffness(int dim, int state, double nu, const double *h, double *K)
 {
   double lam, mu;
@@ -115,21 +129,26 @@ HostSetup::HostSetup(const icb_grid_desc &g) : desc(g)
     throw Error{ICB_ERR_BAD_ARG, "division must be >= 1"};
   if(!(g.lx > 0 && g.ly > 0 && (g.dim == 2 || g.lz > 0)))
     throw Error{ICB_ERR_BAD_ARG, "length must be > 0"};
-  if(g.dim == 3 && g.state != ICB_3D)
+  const bool heat = g.state == ICB_HEAT;
+  if(!heat && g.dim == 3 && g.state != ICB_3D)
     throw Error{ICB_ERR_BAD_ARG, "3D problems need state ICB_3D"};
-  if(g.dim == 2 && g.state != ICB_PLANE_STRESS && g.state != ICB_PLANE_STRAIN)
+  if(!heat && g.dim == 2 && g.state != ICB_PLANE_STRESS && g.state != ICB_PLANE_STRAIN)
     throw Error{ICB_ERR_BAD_ARG, "2D problems need plane_stress or plane_strain"};
-  if(!(g.poisson > -1.0 && g.poisson < 0.5))
+  if(!heat && !(g.poisson > -1.0 && g.poisson < 0.5))
     throw Error{ICB_ERR_BAD_ARG, "poisson out of range"};
+  dofnp = heat ? 1 : g.dim; // mesh_icarat.hpp:77 (probTypeToDofnpVoigt)
   dims = make_dims(g.dim, g.nx, g.ny, g.dim == 3 ? g.nz : 1);
   h[0] = g.lx / g.nx;
   h[1] = g.ly / g.ny;
   h[2] = g.dim == 3 ? g.lz / g.nz : 1.0;
-  neq = dims.nnode * g.dim;
+  neq = dims.nnode * dofnp;
   fixed.assign(neq, 0);
   dval.assign(neq, 0.0);
   nodal.assign(neq, 0.0);
-  unit_stiffness(g.dim, g.state, g.poisson, h, K0);
+  for(double &k : K0)
+    k = 0.0;
+  if(!heat)
+    unit_stiffness(g.dim, g.state, g.poisson, h, K0);
   volume = h[0] * h[1] * (g.dim == 3 ? h[2] : 1.0);
 }
 
@@ -164,7 +183,7 @@ void HostSetup::dirichletBox(const int *flag, const double *val, const double *r
   const double tol = 1.0e-7; // boundary_condition_icarat.hpp:73
   double lo[3] = {range[0] - tol, range[2] - tol, range[4] - tol};
   double hi[3] = {range[1] + tol, range[3] + tol, range[5] + tol};
-  int d = desc.dim;
+  const int d = desc.dim, nd = dofnp;
   for(long long n = 0; n < dims.nnode; n++)
   {
     double x[3];
@@ -174,10 +193,10 @@ void HostSetup::dirichletBox(const int *flag, const double *val, const double *r
       in = in && x[c] >= lo[c] && x[c] <= hi[c];
     if(!in)
       continue;
-    for(int c = 0; c < d; c++)
+    for(int c = 0; c < nd; c++)
     {
-      fixed[n * d + c] = flag[c] != 0;
-      dval[n * d + c] = val[c];
+      fixed[n * nd + c] = flag[c] != 0;
+      dval[n * nd + c] = val[c];
     }
   }
 }
@@ -211,8 +230,8 @@ void HostSetup::nodalLoad(long long node, const double *f)
     throw Error{ICB_ERR_STATE, "loads are frozen after icb_finalize"};
   if(node < 0 || node >= dims.nnode)
     throw Error{ICB_ERR_BAD_ARG, "node index out of range"};
-  for(int c = 0; c < desc.dim; c++)
-    nodal[node * desc.dim + c] += f[c];
+  for(int c = 0; c < dofnp; c++)
+    nodal[node * dofnp + c] += f[c];
 }
 
 /// countDOF (boundary_condition_base.hpp:35-88) then the loads: nodal loads
@@ -321,9 +340,9 @@ void HostSetup::finalize()
           }
         }
         for(int s = 0; s < ns; s++)
-          for(int c = 0; c < d; c++)
+          for(int c = 0; c < dofnp; c++)
           {
-            long long gi = sn[s] * d + c;
+            long long gi = sn[s] * dofnp + c;
             if(!fixed[gi])
               fext[dof[gi]] += share[s] * t.val[c];
           }

@@ -11,6 +11,10 @@ void lame_constants(int state, double nu, double &lam, double &mu);
 /// unit-modulus element stiffness (E = 1) of a box element with sides h,
 /// (d*ne)^2 row-major, DOFs node-major with interleaved components
 void unit_stiffness(int dim, int state, double nu, const double *h, double *K);
+/// heat element matrix int grad N^T D grad N over the box element (the
+/// Gauss sum of LinearHeat::makeKeFint, heat.cpp:67-111, done exactly), for a
+/// dim x dim conductivity D; ne x ne row-major
+void heat_element(int dim, const double *h, const double *D, double *K);
 /// Helmholtz filter element matrix (M + re^2 K_grad, re = R/(2 sqrt 3)) and
 /// the load integrals int N_a of FilterHelmholtz::makeKeFint
 /// (src/optimization/filter_helm.hpp:178-222)
@@ -28,6 +32,7 @@ struct HostSetup
 {
   icb_grid_desc desc;
   Dims dims;
+  int dofnp = 0; ///< DOFs per node: dim (elasticity) or 1 (heat)
   double h[3];
   long long neq = 0, numeq = 0;
   std::vector<unsigned char> fixed; ///< neq

@@ -98,6 +98,18 @@ _SIGS = {
     "icb_count_dof": (C.c_int, [C.c_void_p, _ip, C.POINTER(C.c_longlong)]),
     "icb_get_dof_map": (C.c_int, [C.c_void_p, _ip]),
     "icb_von_mises": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "icb_heat_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "icb_heat_destroy": (C.c_int, [C.c_void_p]),
+    "icb_heat_dirichlet_box": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _dp]),
+    "icb_heat_flux_box": (C.c_int, [C.c_void_p, C.c_double, _dp]),
+    "icb_heat_nodal_source": (C.c_int, [C.c_void_p, C.c_longlong, C.c_double]),
+    "icb_heat_finalize": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "icb_heat_set_density": (C.c_int, [C.c_void_p, _dp]),
+    "icb_heat_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "icb_heat_get_temperature": (C.c_int, [C.c_void_p, _dp]),
+    "icb_heat_objective": (C.c_int, [C.c_void_p, _dp]),
+    "icb_heat_sensitivity": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "icb_run_heat": (C.c_int, [C.c_void_p, C.c_void_p, _dp, _dp, _dp]),
     "icb_gcmma_create": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_void_p)]),
     "icb_gcmma_destroy": (C.c_int, [C.c_void_p]),
     "icb_gcmma_outer": (C.c_int, [C.c_void_p, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, _dp]),
@@ -437,6 +449,83 @@ def oc_update(prob, cone, x, dfdx, g, dgdx, xmin, xmax, move, beta=0.0, T=0.5):
                               float(g), _p(args[1]), _p(args[2]), _p(args[3]), move, beta, T,
                               C.byref(steps)))
     return x, steps.value
+
+
+class HeatDesc(C.Structure):
+    _fields_ = [("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("cond1", C.c_double * 6), ("cond2", C.c_double * 6), ("penalty", C.c_double)]
+
+
+class Heat:
+    """icb_heat: steady heat conduction with SIMP conductivity (LinearHeat)."""
+
+    def __init__(self, ctx, dim, nx, ny, nz=1, lx=None, ly=None, lz=None,
+                 cond1=(1.0, 1.0, 1.0, 0, 0, 0), cond2=(1e-3, 1e-3, 1e-3, 0, 0, 0), penal=3.0):
+        self.desc = HeatDesc(dim, nx, ny, nz if dim == 3 else 1, float(lx or nx), float(ly or ny),
+                             float((lz or nz) if dim == 3 else 1.0), (C.c_double * 6)(*cond1),
+                             (C.c_double * 6)(*cond2), penal)
+        h = C.c_void_p()
+        check(lib().icb_heat_create(ctx.h, C.byref(self.desc), C.byref(h)))
+        self.h, self.ctx, self.dim = h, ctx, dim
+        self.nel = nx * ny * (nz if dim == 3 else 1)
+        self.nnode = (nx + 1) * (ny + 1) * ((nz + 1) if dim == 3 else 1)
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.icb_heat_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def dirichlet_box(self, flag, val, rng):
+        check(lib().icb_heat_dirichlet_box(self.h, int(flag), float(val), _p(np.asarray(rng, np.float64))))
+
+    def flux_box(self, q, rng):
+        check(lib().icb_heat_flux_box(self.h, float(q), _p(np.asarray(rng, np.float64))))
+
+    def nodal_source(self, node, q):
+        check(lib().icb_heat_nodal_source(self.h, int(node), float(q)))
+
+    def finalize(self):
+        n = C.c_longlong()
+        check(lib().icb_heat_finalize(self.h, C.byref(n)))
+        self.numeq = n.value
+        return n.value
+
+    def set_density(self, rho):
+        check(lib().icb_heat_set_density(self.h, _p(np.ascontiguousarray(rho, np.float64))))
+
+    def solve(self, tol=1e-10, maxit=10000):
+        o = SolveOpts(FP64, JACOBI, tol, maxit, 0.0, 0, 0)
+        info = SolveInfo()
+        check(lib().icb_heat_solve(self.h, C.byref(o), C.byref(info)))
+        return info.as_dict()
+
+    def temperature(self):
+        t = np.zeros(self.nnode)
+        check(lib().icb_heat_get_temperature(self.h, _p(t)))
+        return t
+
+    def objective(self):
+        f = C.c_double()
+        check(lib().icb_heat_objective(self.h, C.byref(f)))
+        return f.value
+
+    def sensitivity(self, rho):
+        dc = np.zeros(self.nel)
+        check(lib().icb_heat_sensitivity(self.h, _p(np.ascontiguousarray(rho, np.float64)), _p(dc),
+                                         None))
+        return dc
+
+    def run(self, rho0, nsteps, radius, tol=1e-10, maxit=100000):
+        o = LoopOpts(nsteps, radius, 0.15, 1, 0.0, SolveOpts(FP64, JACOBI, tol, maxit, 0.0, 0, 0),
+                     None)
+        hist, x = np.zeros(nsteps), np.zeros(self.nel)
+        check(lib().icb_run_heat(self.h, C.byref(o), _p(np.ascontiguousarray(rho0, np.float64)),
+                                 _p(hist), _p(x)))
+        return hist, x
 
 
 class GCMMA:

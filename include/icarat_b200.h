@@ -37,6 +37,7 @@ extern "C" {
 #define ICB_PLANE_STRESS 0
 #define ICB_PLANE_STRAIN 1
 #define ICB_3D 2
+#define ICB_HEAT 3 /* icb_heat problems: scalar heat conduction, one DOF per node */
 
 #define ICB_FP64 0  /* plain FP64 path: the drop-in for Solvers "Eigen_CG"   */
 #define ICB_MIXED 1 /* FP64 Krylov + operator, FP32 multigrid preconditioner */
@@ -270,6 +271,44 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
  * iterations. */
 int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
                   int *inner, double *xout);
+
+/* ---- heat conduction (LinearHeat, opt-heat) ------------------------------ */
+typedef struct icb_heat_s *icb_heat;
+/* src/problem/heat.{hpp,cpp}: a structured box of quad4 / hexa8 elements with
+ * one temperature per node; conductivities of the two materials as ICARAT's
+ * [material] conductivity rows [xx, yy, zz, xy, yz, xz]; SIMP
+ * De = rho^p D1 + (1 - rho^p) D2 (heat.cpp:53-64), cond1[0] >= cond2[0]. */
+typedef struct
+{
+  int dim, nx, ny, nz;
+  double lx, ly, lz;
+  double cond1[6], cond2[6];
+  double penalty;
+} icb_heat_desc;
+int icb_heat_create(icb_ctx ctx, const icb_heat_desc *desc, icb_heat *out);
+int icb_heat_destroy(icb_heat h);
+/* input_dirich with dofnp 1: fixed temperature `val` where flag != 0 in the box */
+int icb_heat_dirichlet_box(icb_heat h, int flag, double val, const double *range);
+/* input_neumann with dofnp 1: constant flux q on the element sides of the box */
+int icb_heat_flux_box(icb_heat h, double q, const double *range);
+int icb_heat_nodal_source(icb_heat h, long long node, double q);
+int icb_heat_finalize(icb_heat h, long long *numeq);
+int icb_heat_set_density(icb_heat h, const double *rho);
+/* LinearAnalysis<LinearHeat>::solve with Eigen_CG: FP64 Jacobi-PCG (opts NULL:
+ * tol 1e-10, 10000 iterations) */
+int icb_heat_solve(icb_heat h, const icb_solve_opts *opts, icb_solve_info *info);
+/* node[].val[0] (nnode) */
+int icb_heat_get_temperature(icb_heat h, double *nodeval);
+/* the app's objective u^T K u over the free DOFs (opt_heat.cpp:116) */
+int icb_heat_objective(icb_heat h, double *f);
+/* opt_heat.cpp:155-190 without the threshold factor: dc_e = -u_e^T
+ * (p rho^(p-1) (K1 - K2)) u_e at the density rho of the solve; dv_e = v_e */
+int icb_heat_sensitivity(icb_heat h, const double *rho, double *dc, double *dv);
+/* the opt-heat loop (opt_heat.cpp:79-151): Helmholtz filter (filter_radius),
+ * threshold, solve, objective, constraint sum x v - V0, MMA; hist[step] is
+ * the objective */
+int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double *hist,
+                 double *xout);
 
 /* ---- many runs on one GPU: batch runner and job server ------------------- */
 /* No counterpart in ICARAT (one problem per process).  Runs are independent

@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -47,6 +48,9 @@ struct OrcGrid
 
 namespace
 {
+/// DOFs per node: dim for elasticity, 1 for heat conduction (state 3)
+inline int dofnp(const OrcGrid &g) { return g.state == 3 ? 1 : g.dim; }
+
 inline int64_t numnp(const OrcGrid &g)
 {
   return g.dim == 2 ? int64_t(g.nx + 1) * (g.ny + 1)
@@ -590,7 +594,7 @@ void orc_dirichlet_box(const OrcGrid *g, const int *flag, const double *val,
   double lo[3] = {range[0] - tol, range[2] - tol, range[4] - tol};
   double hi[3] = {range[1] + tol, range[3] + tol, range[5] + tol};
   int64_t nn = numnp(*g);
-  int d = g->dim;
+  int d = g->dim, nd = dofnp(*g);
   for(int64_t n = 0; n < nn; n++)
   {
     double x[3];
@@ -601,10 +605,10 @@ void orc_dirichlet_box(const OrcGrid *g, const int *flag, const double *val,
     if(!in)
       continue;
     // setDirichValue (boundary_condition_base.hpp:17-33): copies flag & value
-    for(int c = 0; c < d; c++)
+    for(int c = 0; c < nd; c++)
     {
-      fixed[n * d + c] = uint8_t(flag[c] != 0);
-      dval[n * d + c] = val[c];
+      fixed[n * nd + c] = uint8_t(flag[c] != 0);
+      dval[n * nd + c] = val[c];
     }
   }
 }
@@ -614,7 +618,7 @@ void orc_dirichlet_box(const OrcGrid *g, const int *flag, const double *val,
 int64_t orc_count_dof(const OrcGrid *g, const uint8_t *fixed, int *dof)
 {
   int64_t nn = numnp(*g);
-  int d = g->dim;
+  int d = dofnp(*g);
   int64_t cnt = 0;
   for(int64_t n = 0; n < nn; n++)
     for(int c = 0; c < d; c++)
@@ -701,9 +705,9 @@ void orc_traction_box(const OrcGrid *g, const double *val, const double *range,
         double L = std::sqrt(std::pow(xb[0] - xa[0], 2) + std::pow(xb[1] - xa[1], 2));
         share = 0.5 * L; // sum over 2 points of N * (L/2)
         for(int s = 0; s < 2; s++)
-          for(int c = 0; c < d; c++)
+          for(int c = 0; c < dofnp(*g); c++)
           {
-            int dd = dof[nd[q4side[side][s]] * d + c];
+            int dd = dof[nd[q4side[side][s]] * dofnp(*g) + c];
             if(dd < numeq)
               fext[dd] += share * val[c];
           }
@@ -741,9 +745,9 @@ void orc_traction_box(const OrcGrid *g, const double *val, const double *range,
             fe[s] += Nq[s] * jac;
         }
         for(int s = 0; s < 4; s++)
-          for(int c = 0; c < d; c++)
+          for(int c = 0; c < dofnp(*g); c++)
           {
-            int dd = dof[nd[h8side[side][s]] * d + c];
+            int dd = dof[nd[h8side[side][s]] * dofnp(*g) + c];
             if(dd < numeq)
               fext[dd] += fe[s] * val[c];
           }
@@ -1999,6 +2003,201 @@ int orc_gcmma_loop(const OrcGrid *g, const uint8_t *fixed, const double *dval, c
   }
   orc_cone_free(cone);
   orc_gcmma_free(gc);
+  return 0;
+}
+
+// ----------------------------------------------------------------- heat ----
+namespace
+{
+/// conductivity tensor from ICARAT's [xx, yy, zz, xy, yz, xz] (heat.cpp:31-51;
+/// the 3D branch of the reference assigns De1_ twice, overwriting material
+/// 1 with material 2 and leaving De2_ unset: here each material gets its own
+/// tensor, the evident intent)
+void condTensor(int dim, const double *c, double *D)
+{
+  if(dim == 2)
+  {
+    D[0] = c[0];
+    D[1] = c[3];
+    D[2] = c[3];
+    D[3] = c[1];
+  }
+  else
+  {
+    const double v[9] = {c[0], c[3], c[5], c[3], c[1], c[4], c[5], c[4], c[2]};
+    for(int i = 0; i < 9; i++)
+      D[i] = v[i];
+  }
+}
+
+/// LinearHeat::makeKeFint (heat.cpp:67-111) for a conductivity D: Ke =
+/// sum over the Gauss points of B^T D B jac, B = dN/dX
+void heatKe(const OrcGrid &g, const double *D, double *Ke)
+{
+  int ne = nen(g), d = g.dim;
+  for(int i = 0; i < ne * ne; i++)
+    Ke[i] = 0.0;
+  double pts[8][3];
+  int nq = gaussPoints(g, pts);
+  for(int q = 0; q < nq; q++)
+  {
+    double dNdX[24], N[8];
+    double jac = shapeGrad(g, pts[q], dNdX, N);
+    for(int a = 0; a < ne; a++)
+      for(int b = 0; b < ne; b++)
+      {
+        double t = 0.0;
+        for(int i = 0; i < d; i++)
+          for(int j = 0; j < d; j++)
+            t += dNdX[i * ne + a] * D[i * d + j] * dNdX[j * ne + b];
+        Ke[a * ne + b] += t * jac;
+      }
+  }
+}
+} // namespace
+
+/// the element matrices K1, K2 of the two materials (ne x ne each)
+void orc_heat_Ke(const OrcGrid *g, const double *cond1, const double *cond2, double *K1, double *K2)
+{
+  double D1[9], D2[9];
+  condTensor(g->dim, cond1, D1);
+  condTensor(g->dim, cond2, D2);
+  heatKe(*g, D1, K1);
+  heatKe(*g, D2, K2);
+}
+
+/// LinearAnalysis<LinearHeat, Node>::solve with Eigen_CG on the assembled
+/// free-DOF matrix of Ke(rho) = rho^p K1 + (1 - rho^p) K2 (heat.cpp:53-64):
+/// fres = fext - K_fd u_d, Jacobi-PCG from 0 to tol; nodeval[nnode] gets the
+/// temperatures (Dirichlet values included, |T| < 1e-15 set to 0) and
+/// *objective the app's u^T K u over the free DOFs (opt_heat.cpp:116).
+int orc_heat_solve(const OrcGrid *g, const double *cond1, const double *cond2, const uint8_t *fixed,
+                   const double *dval, const double *fext, const double *rho, double tol,
+                   double *nodeval, double *objective, int *iters)
+{
+  int ne = nen(*g);
+  int64_t nn = numnp(*g), nel = nelx(*g);
+  std::vector<int> dof(nn);
+  int64_t numeq = orc_count_dof(g, fixed, dof.data());
+  std::vector<double> K1(ne * ne), K2(ne * ne);
+  orc_heat_Ke(g, cond1, cond2, K1.data(), K2.data());
+  std::vector<std::map<int, double>> rows(numeq);
+  std::vector<double> b(fext, fext + numeq);
+  for(int64_t e = 0; e < nel; e++)
+  {
+    double a = std::pow(rho[e], g->penal);
+    int64_t nd[8];
+    elemNodes(*g, e, nd);
+    for(int i = 0; i < ne; i++)
+    {
+      int di = dof[nd[i]];
+      if(di >= numeq)
+        continue;
+      for(int j = 0; j < ne; j++)
+      {
+        double k = a * K1[i * ne + j] + (1.0 - a) * K2[i * ne + j];
+        int dj = dof[nd[j]];
+        if(dj < numeq)
+          rows[di][dj] += k;
+        else
+          b[di] -= k * dval[nd[j]];
+      }
+    }
+  }
+  Csr A;
+  A.n = numeq;
+  A.rowptr.assign(numeq + 1, 0);
+  A.diag.assign(numeq, 0.0);
+  for(int64_t r = 0; r < numeq; r++)
+  {
+    A.rowptr[r + 1] = A.rowptr[r] + int64_t(rows[r].size());
+    for(auto &kv : rows[r])
+    {
+      A.col.push_back(kv.first);
+      A.val.push_back(kv.second);
+      if(kv.first == r)
+        A.diag[r] = kv.second;
+    }
+  }
+  std::vector<double> u(numeq);
+  double rr;
+  int mv;
+  int rc = pcgCsr(A, b.data(), u.data(), tol, 100000, iters, &rr, &mv);
+  std::vector<double> Ku(numeq);
+  spmv(A, u.data(), Ku.data());
+  *objective = dot(numeq, u.data(), Ku.data());
+  for(int64_t n = 0; n < nn; n++)
+  {
+    double v = dof[n] < numeq ? u[dof[n]] : dval[n];
+    nodeval[n] = std::fabs(v) < 1.0e-15 ? 0.0 : v;
+  }
+  return rc;
+}
+
+/// the heat app's sensitivity (opt_heat.cpp:155-190) without the threshold
+/// factor: dc_e = -u_e^T (p rho^(p-1) (K1 - K2)) u_e
+void orc_heat_sensitivity(const OrcGrid *g, const double *cond1, const double *cond2,
+                          const double *rho, const double *nodeval, double *dc)
+{
+  int ne = nen(*g);
+  int64_t nel = nelx(*g);
+  std::vector<double> K1(ne * ne), K2(ne * ne);
+  orc_heat_Ke(g, cond1, cond2, K1.data(), K2.data());
+  for(int64_t e = 0; e < nel; e++)
+  {
+    double dk = g->penal * std::pow(rho[e], g->penal - 1.0);
+    int64_t nd[8];
+    elemNodes(*g, e, nd);
+    double q = 0.0;
+    for(int i = 0; i < ne; i++)
+      for(int j = 0; j < ne; j++)
+        q += nodeval[nd[i]] * dk * (K1[i * ne + j] - K2[i * ne + j]) * nodeval[nd[j]];
+    dc[e] = -q;
+  }
+}
+
+/// The opt-heat loop (opt_heat.cpp:79-151) without I/O: Helmholtz filter of
+/// radius R, threshold (beta = min(2^(step/40), 16)), solve, V0 at step 1,
+/// objective u^T K u, constraint sum x v - V0, sensitivities times the
+/// threshold derivative (dv = derivative * v), adjoint Helmholtz filters, MMA.
+int orc_heat_loop(const OrcGrid *g, const double *cond1, const double *cond2, const uint8_t *fixed,
+                  const double *dval, const double *fext, const double *rho0, int nsteps, double R,
+                  double tol, double *hist, double *x)
+{
+  int64_t nn = numnp(*g), nel = nelx(*g);
+  std::vector<double> nodeval(nn), xf(nel), xt(nel), dxt(nel), dc(nel), dv(nel),
+      xmin(nel, 1.0e-4), xmax(nel, 1.0), t1(nel), t2(nel);
+  std::copy(rho0, rho0 + nel, x);
+  double vol = orc_element_volume(g);
+  void *mma = orc_mma_create(nel, 1, 0.0, 1e5, 0.0);
+  double V0 = 0.0;
+  for(int step = 1; step <= nsteps; step++)
+  {
+    int it;
+    orc_helmholtz(g, R, x, xf.data(), 0, 1e-10, &it);
+    double beta = std::min(std::pow(2, (int)(step / 40)), 16.0);
+    orc_threshold(nel, xf.data(), beta, 0.5, xt.data());
+    double obj;
+    orc_heat_solve(g, cond1, cond2, fixed, dval, fext, xt.data(), tol, nodeval.data(), &obj, &it);
+    double vs = 0.0;
+    for(int64_t i = 0; i < nel; i++)
+      vs += xt[i] * vol;
+    if(step == 1)
+      V0 = vs;
+    double gval = vs - V0;
+    hist[step - 1] = obj;
+    orc_threshold_deriv(nel, xf.data(), beta, 0.5, dxt.data());
+    orc_heat_sensitivity(g, cond1, cond2, xt.data(), nodeval.data(), dc.data());
+    for(int64_t i = 0; i < nel; i++)
+    {
+      dc[i] *= dxt[i];
+      dv[i] = dxt[i] * vol;
+    }
+    orc_helmholtz(g, R, dc.data(), t1.data(), 1, 1e-10, &it);
+    orc_helmholtz(g, R, dv.data(), t2.data(), 1, 1e-10, &it);
+    orc_mma_update(mma, x, t1.data(), &gval, t2.data(), xmin.data(), xmax.data());
+  }
+  orc_mma_free(mma);
   return 0;
 }
 

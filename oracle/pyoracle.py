@@ -99,6 +99,12 @@ def lib():
             "orc_gcmma_concheck": (C.c_int, [C.c_void_p, C.c_double, _dp]),
             "orc_gcmma_loop": (C.c_int, [G, _u8p, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double,
                                          _dp, _ip, _dp]),
+            "orc_heat_Ke": (None, [G, _dp, _dp, _dp, _dp]),
+            "orc_heat_solve": (C.c_int, [G, _dp, _dp, _u8p, _dp, _dp, _dp, C.c_double, _dp, _dp,
+                                         _ip]),
+            "orc_heat_sensitivity": (None, [G, _dp, _dp, _dp, _dp, _dp]),
+            "orc_heat_loop": (C.c_int, [G, _dp, _dp, _u8p, _dp, _dp, _dp, C.c_int, C.c_double,
+                                        C.c_double, _dp, _dp]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -164,7 +170,8 @@ class Problem:
         self.dim = dim
         self.nnode = int(lib().orc_numnp(C.byref(self.g)))
         self.nel = int(lib().orc_nelx(C.byref(self.g)))
-        self.neq = self.nnode * dim
+        self.dofnp = 1 if state == 3 else dim  # heat conduction: one DOF per node
+        self.neq = self.nnode * self.dofnp
         self.fixed = np.zeros(self.neq, np.uint8)
         self.dval = np.zeros(self.neq)
         self.fext_full = np.zeros(self.neq)
@@ -291,6 +298,42 @@ class Problem:
                                 _ptr(self.fext()), _ptr(np.ascontiguousarray(rho0, np.float64)),
                                 nsteps, rfil, None if nd is None else _ptr(nd, _u8p),
                                 None if vs is None else _ptr(vs, _u8p), tol, _ptr(hist), _ptr(x))
+        return hist, x
+
+    # heat conduction (state 3) ------------------------------------------
+    def heat_Ke(self, cond1, cond2):
+        ne = 4 if self.dim == 2 else 8
+        K1, K2 = np.zeros((ne, ne)), np.zeros((ne, ne))
+        lib().orc_heat_Ke(C.byref(self.g), _ptr(np.asarray(cond1, np.float64)),
+                          _ptr(np.asarray(cond2, np.float64)), _ptr(K1), _ptr(K2))
+        return K1, K2
+
+    def heat_solve(self, cond1, cond2, rho, tol=1e-10):
+        nv = np.zeros(self.nnode)
+        obj = C.c_double()
+        it = C.c_int()
+        rc = lib().orc_heat_solve(C.byref(self.g), _ptr(np.asarray(cond1, np.float64)),
+                                  _ptr(np.asarray(cond2, np.float64)), _ptr(self.fixed, _u8p),
+                                  _ptr(self.dval), _ptr(self.fext()),
+                                  _ptr(np.ascontiguousarray(rho, np.float64)), tol, _ptr(nv),
+                                  C.byref(obj), C.byref(it))
+        return {"nodeval": nv, "objective": obj.value, "iters": it.value, "rc": rc}
+
+    def heat_sensitivity(self, cond1, cond2, rho, nodeval):
+        dc = np.zeros(self.nel)
+        lib().orc_heat_sensitivity(C.byref(self.g), _ptr(np.asarray(cond1, np.float64)),
+                                   _ptr(np.asarray(cond2, np.float64)),
+                                   _ptr(np.ascontiguousarray(rho, np.float64)),
+                                   _ptr(np.ascontiguousarray(nodeval, np.float64)), _ptr(dc))
+        return dc
+
+    def heat_loop(self, cond1, cond2, rho0, nsteps, R, tol=1e-10):
+        hist, x = np.zeros(nsteps), np.zeros(self.nel)
+        lib().orc_heat_loop(C.byref(self.g), _ptr(np.asarray(cond1, np.float64)),
+                            _ptr(np.asarray(cond2, np.float64)), _ptr(self.fixed, _u8p),
+                            _ptr(self.dval), _ptr(self.fext()),
+                            _ptr(np.ascontiguousarray(rho0, np.float64)), nsteps, R, tol,
+                            _ptr(hist), _ptr(x))
         return hist, x
 
     def gcmma_loop(self, rho0, nsteps, rfil, tol=1e-8):
