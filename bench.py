@@ -137,6 +137,19 @@ def run_cpu_sample(nit, reps=1):
     return times, numeq, po.lib().orc_num_threads(), t_asm
 
 
+def reduce_over_ranks(ms, units, dist, device):
+    """Whole-job figures of a replica run: the slowest rank's time and the
+    units every rank processed (max and sum over ranks)."""
+    if dist is None:
+        return ms, units
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    u = torch.tensor([units], dtype=torch.float64, device=device)
+    dist.all_reduce(u)
+    return float(t.item()), float(u.item())
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -218,14 +231,7 @@ def ours_arm(args):
     lat = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps))
     clocks = clocks_stop(clk)
     launches = icb.launch_count() - l0
-    ms = e0.elapsed_time(e1)
-    units = float(numeq) * mv
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        u = torch.tensor([units], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(u)
-        ms, units = float(t.item()), float(u.item())
+    ms, units = reduce_over_ranks(e0.elapsed_time(e1), float(numeq) * mv, dist, f"cuda:{local}")
     value = units / (ms * 1e-3)
 
     # ---- e2e through the C ABI with pinned host buffers
@@ -254,14 +260,7 @@ def ours_arm(args):
         mv2 += step_e2e()["matvecs"]
     f1.record(stream)
     barrier()
-    ms2 = f0.elapsed_time(f1)
-    units2 = float(numeq) * mv2
-    if dist is not None:
-        t = torch.tensor([ms2], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        u = torch.tensor([units2], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(u)
-        ms2, units2 = float(t.item()), float(u.item())
+    ms2, units2 = reduce_over_ranks(f0.elapsed_time(f1), float(numeq) * mv2, dist, f"cuda:{local}")
     e2e = {"value": units2 / (ms2 * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": 8 * prob.nel,
            "d2h_bytes_per_step": 8 * (numeq + prob.nel + 1)}
@@ -489,6 +488,31 @@ def workload_c3(args):
                                   np.abs(out["fp64_gmg"]["dc"]).max())}
     for v in out.values():
         v.pop("dc")
+    # the plain FP64 GPU path (the Eigen_CG drop-in: Jacobi-PCG) on the same design
+    t0 = time.perf_counter()
+    inf = g.solve(precision=icb.FP64, precond=icb.JACOBI, tol=TOL, maxit=200000)
+    t_j = time.perf_counter() - t0
+    out["fp64_jacobi"] = {"ms": 1e3 * t_j, "iters": inf["iters"], "true_relres": inf["true_relres"],
+                          "compliance": g.compliance()}
+    speed = {"mixed_gmg_vs_fp64_jacobi": out["fp64_jacobi"]["ms"] / out["mixed_gmg"]["ms"],
+             "mixed_gmg_vs_fp64_gmg": out["fp64_gmg"]["ms"] / out["mixed_gmg"]["ms"]}
+    # host-CPU reference: the assembled matrix of this grid would need ~58 GB of
+    # triplets, so the oracle's matrix-free Jacobi-PCG is timed for a few
+    # iterations and scaled by the iteration count of the same FP64 Jacobi solve
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        o = cases.build_oracle("halfmbb3d", *n)
+        nit = 3
+        t_it = min(o.ebe_pcg_time(rho0, nit)[0] for _ in range(2)) / nit
+        cpu_ttsol = t_it * out["fp64_jacobi"]["iters"]
+        cpu = {"value": nit * o.neq / (t_it * nit), "unit": "DOF*iter/s",
+               "cores": po.lib().orc_num_threads(), "kind": "port",
+               "sample": f"{nit} matrix-free Jacobi-PCG iterations of the oracle on the host cores "
+                         f"({t_it:.3f} s per iteration); time to the FP64 solve estimated as "
+                         f"per-iteration time x {out['fp64_jacobi']['iters']} iterations = {cpu_ttsol:.0f} s"}
+        speed["mixed_gmg_vs_cpu_estimate"] = cpu_ttsol / (out["mixed_gmg"]["ms"] * 1e-3)
     vol = float(np.prod(n))
     o = icb.loop_opts(steps, 3.0, precision=icb.MIXED, volume_ref=0.3 * vol)
     its = np.zeros(steps)
@@ -504,8 +528,8 @@ def workload_c3(args):
                                  "helmholtz_R": 3.0, "volfrac": 0.3, "steps": steps, "tol": TOL},
                       "latency_ms": {"p50": 1e3 * float(np.median(its)),
                                      "p99": 1e3 * float(np.quantile(its, 0.99))},
-                      "solve_initial_design": out, "mixed_vs_fp64": err,
-                      "compliance_history": hist.tolist()}), flush=True)
+                      "solve_initial_design": out, "mixed_vs_fp64": err, "speedups": speed,
+                      "cpu_baseline": cpu, "compliance_history": hist.tolist()}), flush=True)
     return 0
 
 
@@ -520,16 +544,37 @@ def workload_batched(args):
     N, steps = args.instances, args.loop_steps
     rng = np.random.default_rng(4)
     insts = [cases.random_instance2d(rng) for _ in range(N)]
+    # several GPUs: every rank runs its footprint-balanced share, no exchange
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        fp = [icb.job_footprint(cases.grid_desc(i), icb.JOB_OC) for i in insts]
+        insts = [insts[k] for k in icb.shard_by_footprint(fp, world)[rank]]
+    Nloc = len(insts)
     nel_total = sum(i["nx"] * i["ny"] for i in insts)
     runs, ref = {}, None
     for W in args.workers:
-        ctxs = [icb.Context(0) for _ in range(N)]
+        dev = int(os.environ.get("LOCAL_RANK", "0"))
+        ctxs = [icb.Context(dev) for _ in range(Nloc)]
         probs = [cases.build_instance(c, i) for c, i in zip(ctxs, insts)]
         opts = [icb.loop_opts(steps, i["r"], move=0.2, precision=icb.MIXED) for i in insts]
         rho0 = [np.full(p.nel, i["vf"]) for p, i in zip(probs, insts)]
+        if dist is not None:
+            dist.barrier()
         t0 = time.perf_counter()
-        H, X, S = icb.run_batch(probs, [icb.JOB_OC] * N, opts, rho0, nworkers=W)
+        H, X, S = icb.run_batch(probs, [icb.JOB_OC] * Nloc, opts, rho0, nworkers=W)
         dt = time.perf_counter() - t0
+        if dist is not None:
+            import torch
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
         runs[W] = {"seconds": dt, "inst_iter_s": N * steps / dt, "all_ok": bool((S == 0).all())}
         if ref is None:
             ref = (H, X)
@@ -540,12 +585,17 @@ def workload_batched(args):
             p.close()
         for c in ctxs:
             c.close()
+    if dist is not None:
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     seq = runs.get(1, {}).get("inst_iter_s")
     best_w = max(runs, key=lambda w: runs[w]["inst_iter_s"])
     print(json.dumps({"metric": "instance-iterations/s (c4 batched 2D OC)", "value": runs[best_w]["inst_iter_s"],
-                      "unit": "instance-iter/s", "n_gpus": 1, "higher_is_better": True,
+                      "unit": "instance-iter/s", "n_gpus": world, "higher_is_better": True,
+                      "scaling": "strong (the 256 instances are split over the GPUs by footprint)",
                       "dtype": "f64 Krylov / f32 multigrid", "data": "synthetic (seeded instances)",
-                      "config": {"workload": f"{N} 2D Q4 instances, {nel_total} elements in total",
+                      "config": {"workload": f"{N} 2D Q4 instances, {nel_total} elements on rank 0",
                                  "oc_steps": steps, "workers": best_w},
                       "speedup_vs_sequential": (runs[best_w]["inst_iter_s"] / seq) if seq else None,
                       "runs": {str(k): v for k, v in runs.items()}}), flush=True)

@@ -653,6 +653,25 @@ def run_batch(probs, kinds, opts, rho0s, nworkers):
     return H, X, st
 
 
+def job_footprint(grid, kind):
+    """icb_job_footprint: device bytes one run of this grid needs."""
+    return lib().icb_job_footprint(C.byref(grid), kind)
+
+
+def shard_by_footprint(footprints, nshards):
+    """Split jobs over GPUs with no exchange between them: longest-first
+    greedy assignment to the least-loaded shard (by device footprint, a proxy
+    for work).  Returns one sorted index list per shard; every rank computes
+    the same split from the same list."""
+    loads = [0] * nshards
+    shards = [[] for _ in range(nshards)]
+    for i in sorted(range(len(footprints)), key=lambda k: (-footprints[k], k)):
+        r = min(range(nshards), key=lambda k: (loads[k], k))
+        shards[r].append(i)
+        loads[r] += footprints[i]
+    return [sorted(s) for s in shards]
+
+
 class Server:
     """icb_server: continuous batching of app-loop jobs on one GPU."""
 

@@ -18,6 +18,7 @@
 // file:line) whose behaviour it restates.
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -2199,6 +2200,118 @@ int orc_heat_loop(const OrcGrid *g, const double *cond1, const double *cond2, co
   }
   orc_mma_free(mma);
   return 0;
+}
+
+// ------------------------------------------------- matrix-free CPU sample ----
+/// Jacobi-PCG iterations with a matrix-free element-by-element operator on
+/// the host cores (OpenMP over nodes: every node gathers the rows of its <= 8
+/// elements, so no two threads write one entry), on full-grid node-major
+/// vectors with constrained DOFs held at 0.  For grids whose assembled
+/// matrix does not fit in host memory this is the CPU path that can run; it
+/// is timed over `nit` iterations from x = 0 with b = the load `fneq` (neq).
+/// Returns the seconds of the iterations (set-up excluded); *rr the final
+/// ||r||^2.
+double orc_ebe_pcg_time(const OrcGrid *g, const uint8_t *fixed, const double *rho,
+                        const double *fneq, int nit, double *rr)
+{
+  const int d = g->dim, ne = nen(*g), nd = d * ne;
+  const int64_t nn = numnp(*g), neq = nn * d;
+  const int64_t sx = g->nx + 1, sy = g->ny + 1, nx = g->nx, ny = g->ny,
+                nz = d == 3 ? g->nz : 1;
+  std::vector<double> K0(24 * 24), E(nelx(*g));
+  unitK0(*g, K0.data());
+  for(int64_t e = 0; e < nelx(*g); e++)
+    E[e] = simp(g->young1, g->young2, rho[e], g->penal);
+  auto apply = [&](const double *u, double *y) {
+#pragma omp parallel for schedule(static)
+    for(int64_t n = 0; n < nn; n++)
+    {
+      const int64_t i = n % sx, j = (n / sx) % sy, k = d == 3 ? n / (sx * sy) : 0;
+      double acc[3] = {0, 0, 0};
+      for(int dk = (d == 3 ? -1 : 0); dk <= 0; dk++)
+        for(int dj = -1; dj <= 0; dj++)
+          for(int di = -1; di <= 0; di++)
+          {
+            const int64_t ei = i + di, ej = j + dj, ek = k + dk;
+            if(ei < 0 || ej < 0 || ek < 0 || ei >= nx || ej >= ny || ek >= nz)
+              continue;
+            const int64_t e = ei + ej * nx + ek * nx * ny;
+            int64_t nd8[8];
+            elemNodes(*g, e, nd8);
+            int ln = 0;
+            for(int a = 0; a < ne; a++)
+              if(nd8[a] == n)
+                ln = a;
+            for(int c = 0; c < d; c++)
+            {
+              double s = 0.0;
+              const double *row = &K0[size_t(ln * d + c) * nd];
+              for(int b = 0; b < ne; b++)
+                for(int c2 = 0; c2 < d; c2++)
+                  s += row[b * d + c2] * u[nd8[b] * d + c2];
+              acc[c] += E[e] * s;
+            }
+          }
+      for(int c = 0; c < d; c++)
+        y[n * d + c] = fixed[n * d + c] ? 0.0 : acc[c];
+    }
+  };
+  std::vector<double> x(neq, 0.0), r(neq), z(neq), p(neq), q(neq), inv(neq, 1.0), ones(neq, 0.0);
+  // inverse diagonal from e_i probes would cost neq operator rows; use the
+  // per-node diagonal of the element sums
+#pragma omp parallel for schedule(static)
+  for(int64_t n = 0; n < nn; n++)
+  {
+    const int64_t i = n % sx, j = (n / sx) % sy, k = d == 3 ? n / (sx * sy) : 0;
+    for(int c = 0; c < d; c++)
+    {
+      double s = 0.0;
+      for(int dk = (d == 3 ? -1 : 0); dk <= 0; dk++)
+        for(int dj = -1; dj <= 0; dj++)
+          for(int di = -1; di <= 0; di++)
+          {
+            const int64_t ei = i + di, ej = j + dj, ek = k + dk;
+            if(ei < 0 || ej < 0 || ek < 0 || ei >= nx || ej >= ny || ek >= nz)
+              continue;
+            const int64_t e = ei + ej * nx + ek * nx * ny;
+            int64_t nd8[8];
+            elemNodes(*g, e, nd8);
+            for(int a = 0; a < ne; a++)
+              if(nd8[a] == n)
+                s += E[e] * K0[size_t(a * d + c) * nd + a * d + c];
+          }
+      inv[n * d + c] = (fixed[n * d + c] || s == 0.0) ? 1.0 : 1.0 / s;
+    }
+  }
+  for(int64_t i = 0; i < neq; i++)
+    r[i] = fixed[i] ? 0.0 : fneq[i];
+  auto t0 = std::chrono::steady_clock::now();
+  for(int64_t i = 0; i < neq; i++)
+    p[i] = inv[i] * r[i];
+  double absNew = dot(neq, r.data(), p.data()), r2 = 0.0;
+  for(int it = 0; it < nit; it++)
+  {
+    apply(p.data(), q.data());
+    const double alpha = absNew / dot(neq, p.data(), q.data());
+#pragma omp parallel for schedule(static)
+    for(int64_t i = 0; i < neq; i++)
+    {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+      z[i] = inv[i] * r[i];
+    }
+    r2 = dot(neq, r.data(), r.data());
+    const double absOld = absNew;
+    absNew = dot(neq, r.data(), z.data());
+    const double beta = absNew / absOld;
+#pragma omp parallel for schedule(static)
+    for(int64_t i = 0; i < neq; i++)
+      p[i] = z[i] + beta * p[i];
+  }
+  double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if(rr)
+    *rr = r2;
+  return sec;
 }
 
 int orc_num_threads()

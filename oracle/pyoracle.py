@@ -105,6 +105,7 @@ def lib():
             "orc_heat_sensitivity": (None, [G, _dp, _dp, _dp, _dp, _dp]),
             "orc_heat_loop": (C.c_int, [G, _dp, _dp, _u8p, _dp, _dp, _dp, C.c_int, C.c_double,
                                         C.c_double, _dp, _dp]),
+            "orc_ebe_pcg_time": (C.c_double, [G, _u8p, _dp, _dp, C.c_int, _dp]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -299,6 +300,15 @@ class Problem:
                                 nsteps, rfil, None if nd is None else _ptr(nd, _u8p),
                                 None if vs is None else _ptr(vs, _u8p), tol, _ptr(hist), _ptr(x))
         return hist, x
+
+    def ebe_pcg_time(self, rho, nit):
+        """Seconds of nit matrix-free Jacobi-PCG iterations on the host cores."""
+        rr = C.c_double()
+        t = lib().orc_ebe_pcg_time(C.byref(self.g), _ptr(self.fixed, _u8p),
+                                   _ptr(np.ascontiguousarray(rho, np.float64)),
+                                   _ptr(np.ascontiguousarray(self.fext_full, np.float64)), nit,
+                                   C.byref(rr))
+        return t, rr.value
 
     # heat conduction (state 3) ------------------------------------------
     def heat_Ke(self, cond1, cond2):
