@@ -27,6 +27,7 @@
 #include "reduce.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace icb
 {
@@ -60,10 +61,29 @@ __device__ __forceinline__ T epilogue(T Au, T uself, long long i, const Epi<T> &
   return uself + dn;
 }
 
+/// upper triangle of the symmetric 24x24 K0, row-major (300 doubles).  The
+/// full FP64 matrix (4608 bytes) is past the 4 KB of kernel parameters that
+/// live in the constant bank; packed, every entry stays a constant operand of
+/// its FMA instead of a value the kernel must load into a register.
+struct KSym24
+{
+  double k[300];
+};
+__host__ __device__ constexpr int symIdx(int r, int c)
+{
+  return r <= c ? r * 24 - r * (r - 1) / 2 + (c - r) : c * 24 - c * (c - 1) / 2 + (r - c);
+}
+template <typename T>
+__device__ __forceinline__ T kget(const KMat<T, 24> &K, int r, int c)
+{
+  return K.k[r * 24 + c];
+}
+__device__ __forceinline__ double kget(const KSym24 &K, int r, int c) { return K.k[symIdx(r, c)]; }
+
 // ----------------------------------------------------------------- Hex8 ----
-template <typename T, bool DOT, int MODE>
+template <typename T, typename KT, bool DOT, int MODE>
 __global__ void __launch_bounds__(TX *TY3)
-    k_matvec_h8(const KMat<T, 24> K, const Dims d, const int zchunk,
+    k_matvec_h8(const KT K, const Dims d, const int zchunk,
                 const T *__restrict__ E, const T *__restrict__ u, T *__restrict__ y,
                 const uint8_t *__restrict__ fix, RedScratch red, double *dotOut,
                 const KState *gate, const int gateConv, const Epi<T> ep)
@@ -139,12 +159,12 @@ __global__ void __launch_bounds__(TX *TY3)
         for(int q2 = 0; q2 < 4; q2++)
 #pragma unroll
           for(int c2 = 0; c2 < 3; c2++)
-            s = fma(K.k[row * 24 + q2 * 3 + c2], ub[c2][q2], s);
+            s = fma(kget(K, row, q2 * 3 + c2), ub[c2][q2], s);
 #pragma unroll
         for(int q2 = 0; q2 < 4; q2++)
 #pragma unroll
           for(int c2 = 0; c2 < 3; c2++)
-            s = fma(K.k[row * 24 + 12 + q2 * 3 + c2], ut[c2][q2], s);
+            s = fma(kget(K, row, 12 + q2 * 3 + c2), ut[c2][q2], s);
         acc[c][q] = fma(Ee, s, carry[c][q]);
       }
     if(ek >= Z0)
@@ -193,12 +213,12 @@ __global__ void __launch_bounds__(TX *TY3)
         for(int q2 = 0; q2 < 4; q2++)
 #pragma unroll
           for(int c2 = 0; c2 < 3; c2++)
-            s = fma(K.k[row * 24 + q2 * 3 + c2], ub[c2][q2], s);
+            s = fma(kget(K, row, q2 * 3 + c2), ub[c2][q2], s);
 #pragma unroll
         for(int q2 = 0; q2 < 4; q2++)
 #pragma unroll
           for(int c2 = 0; c2 < 3; c2++)
-            s = fma(K.k[row * 24 + 12 + q2 * 3 + c2], ut[c2][q2], s);
+            s = fma(kget(K, row, 12 + q2 * 3 + c2), ut[c2][q2], s);
         carry[c][q] = Ee * s;
       }
 #pragma unroll
@@ -521,14 +541,27 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
     bz = (d.sz + zchunk - 1) / zchunk;
     dim3 grid(bx, by, bz), block(TX, TY3);
     if(x.dotRed)
-    {
       ICB_REQUIRE(bx * by * bz <= red.maxBlocks, "reduction scratch too small");
-      k_matvec_h8<T, true, MODE><<<grid, block, 0, s>>>(km, d, zchunk, E, u, y, fix, red,
-                                                        x.dotOut, x.gate, x.gateConv, ep);
+    if constexpr(std::is_same<T, double>::value)
+    {
+      KSym24 ks;
+      for(int r = 0; r < 24; r++)
+        for(int c = r; c < 24; c++)
+          ks.k[symIdx(r, c)] = K[r * 24 + c];
+      if(x.dotRed)
+        k_matvec_h8<T, KSym24, true, MODE><<<grid, block, 0, s>>>(ks, d, zchunk, E, u, y, fix, red,
+                                                                  x.dotOut, x.gate, x.gateConv, ep);
+      else
+        k_matvec_h8<T, KSym24, false, MODE><<<grid, block, 0, s>>>(ks, d, zchunk, E, u, y, fix,
+                                                                   red, x.dotOut, x.gate,
+                                                                   x.gateConv, ep);
     }
+    else if(x.dotRed)
+      k_matvec_h8<T, KMat<T, 24>, true, MODE><<<grid, block, 0, s>>>(
+          km, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
     else
-      k_matvec_h8<T, false, MODE><<<grid, block, 0, s>>>(km, d, zchunk, E, u, y, fix, red,
-                                                         x.dotOut, x.gate, x.gateConv, ep);
+      k_matvec_h8<T, KMat<T, 24>, false, MODE><<<grid, block, 0, s>>>(
+          km, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
   }
   else
   {
