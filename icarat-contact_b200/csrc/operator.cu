@@ -81,8 +81,8 @@ __device__ __forceinline__ T kget(const KMat<T, 24> &K, int r, int c)
 __device__ __forceinline__ double kget(const KSym24 &K, int r, int c) { return K.k[symIdx(r, c)]; }
 
 // ----------------------------------------------------------------- Hex8 ----
-template <typename T, typename KT, bool DOT, int MODE>
-__global__ void __launch_bounds__(TX *TY3)
+template <typename T, typename KT, int TYK, bool DOT, int MODE>
+__global__ void __launch_bounds__(TX *TYK)
     k_matvec_h8(const KT K, const Dims d, const int zchunk,
                 const T *__restrict__ E, const T *__restrict__ u, T *__restrict__ y,
                 const uint8_t *__restrict__ fix, RedScratch red, double *dotOut,
@@ -90,9 +90,9 @@ __global__ void __launch_bounds__(TX *TY3)
 {
   if(gate && (gate->stop || (gateConv && gate->conv)))
     return;
-  __shared__ T sB[2][3][TY3][TX];
+  __shared__ T sB[2][3][TYK][TX];
   const int lx = threadIdx.x, ly = threadIdx.y;
-  const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TY3 - 1);
+  const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TYK - 1);
   const int ei = X0 - 1 + lx, ej = Y0 - 1 + ly;
   const int Z0 = blockIdx.z * zchunk;
   const int Z1 = min(Z0 + zchunk, d.sz) - 1;
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(TX *TY3)
       }
       __syncthreads();
       const int ni = ei + 1, nj = ej + 1;
-      if(lx < TX - 1 && ly < TY3 - 1 && ni < d.sx && nj < d.sy)
+      if(lx < TX - 1 && ly < TYK - 1 && ni < d.sx && nj < d.sy)
       {
         const long long node = (long long)ni + (long long)nj * d.sx + (long long)ek * sxy;
         const unsigned f = __ldg(fix + node);
@@ -512,10 +512,15 @@ int matvec_blocks(const Dims &d)
   const int target = num_sms() * 4;
   if(d.dim == 3)
   {
-    int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TY3 - 2) / (TY3 - 1);
-    int bz = std::max(1, std::min(d.sz, (target + bx * by - 1) / (bx * by)));
-    int zchunk = (d.sz + bz - 1) / bz;
-    return bx * by * ((d.sz + zchunk - 1) / zchunk);
+    int most = 0;
+    for(int ty : {TY3})
+    {
+      int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + ty - 2) / (ty - 1);
+      int bz = std::max(1, std::min(d.sz, (target + bx * by - 1) / (bx * by)));
+      int zchunk = (d.sz + bz - 1) / bz;
+      most = std::max(most, bx * by * ((d.sz + zchunk - 1) / zchunk));
+    }
+    return most;
   }
   int strips = (d.sx + TX - 2) / (TX - 1);
   int bx = (strips + TY2 - 1) / TY2;
@@ -535,11 +540,14 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   {
     KMat<T, 24> km;
     std::copy(K, K + 576, km.k);
-    int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TY3 - 2) / (TY3 - 1);
+    // 8 element rows per tile for FP64 and FP32 (16-row FP64 tiles were
+    // measured: faster at 384x128x128, slower at 192x64x64)
+    constexpr int TYK = TY3;
+    int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TYK - 2) / (TYK - 1);
     int bz = std::max(1, std::min(d.sz, (target + bx * by - 1) / (bx * by)));
     int zchunk = (d.sz + bz - 1) / bz;
     bz = (d.sz + zchunk - 1) / zchunk;
-    dim3 grid(bx, by, bz), block(TX, TY3);
+    dim3 grid(bx, by, bz), block(TX, TYK);
     if(x.dotRed)
       ICB_REQUIRE(bx * by * bz <= red.maxBlocks, "reduction scratch too small");
     if constexpr(std::is_same<T, double>::value)
@@ -549,18 +557,17 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
         for(int c = r; c < 24; c++)
           ks.k[symIdx(r, c)] = K[r * 24 + c];
       if(x.dotRed)
-        k_matvec_h8<T, KSym24, true, MODE><<<grid, block, 0, s>>>(ks, d, zchunk, E, u, y, fix, red,
-                                                                  x.dotOut, x.gate, x.gateConv, ep);
+        k_matvec_h8<T, KSym24, TYK, true, MODE><<<grid, block, 0, s>>>(
+            ks, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
       else
-        k_matvec_h8<T, KSym24, false, MODE><<<grid, block, 0, s>>>(ks, d, zchunk, E, u, y, fix,
-                                                                   red, x.dotOut, x.gate,
-                                                                   x.gateConv, ep);
+        k_matvec_h8<T, KSym24, TYK, false, MODE><<<grid, block, 0, s>>>(
+            ks, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
     }
     else if(x.dotRed)
-      k_matvec_h8<T, KMat<T, 24>, true, MODE><<<grid, block, 0, s>>>(
+      k_matvec_h8<T, KMat<T, 24>, TYK, true, MODE><<<grid, block, 0, s>>>(
           km, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
     else
-      k_matvec_h8<T, KMat<T, 24>, false, MODE><<<grid, block, 0, s>>>(
+      k_matvec_h8<T, KMat<T, 24>, TYK, false, MODE><<<grid, block, 0, s>>>(
           km, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
   }
   else
