@@ -2,11 +2,10 @@
 // that must not allocate device memory.
 //
 // Some callers cannot call cudaMalloc at the point where they need a solve:
-// code running while a stream is being captured into a CUDA graph (the
-// allocator is not capturable), hosts that hand the whole GPU memory to their
-// own pool up front and treat any outside allocation as a failure, and
-// real-time or serving loops that must not risk an allocator stall or an
-// out-of-memory error in the middle of a request.  For them this entry point
+// hosts that hand the whole GPU memory to their own pool up front and treat
+// any allocation from outside it as a failure, and real-time or serving loops
+// that must not risk an allocator stall or an out-of-memory error in the
+// middle of a request.  For them this entry point
 // takes its scratch (three Krylov vectors, the reduction partials, the
 // completion counter and the device-side solver state) from one file-scope
 // device array instead of allocating it.

@@ -383,10 +383,9 @@ long long icb_get_option(const char *name);
 
 /* ---- solve without device allocation ------------------------------------ */
 /* No counterpart in ICARAT.  For callers that cannot allocate device memory
- * when they solve: code running under CUDA stream capture (cudaMalloc cannot
- * be captured), hosts that give all GPU memory to their own pool and treat
- * outside allocations as failures, and real-time or serving loops that must
- * not stall on the allocator or hit out-of-memory mid-request.
+ * when they solve: hosts that give all GPU memory to their own pool and treat
+ * any allocation from outside it as a failure, and real-time or serving loops
+ * that must not stall on the allocator or hit out-of-memory mid-request.
  * The same FP64 Jacobi-PCG as icb_solve with ICB_FP64 / ICB_PRECOND_JACOBI
  * (Eigen_CG semantics), on caller-provided device SoA vectors: b_dev holds
  * the right-hand side (0 on constrained DOFs), x_dev receives the solution;

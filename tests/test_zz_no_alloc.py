@@ -1,6 +1,6 @@
 """icb_solve_noalloc: the Jacobi-PCG solve for callers that cannot allocate
-device memory (code under CUDA stream capture, hosts that own all GPU memory
-through their own pool, serving loops that must not touch the allocator).
+device memory (hosts that own all GPU memory through their own pool, serving
+loops that must not touch the allocator).
 
 It must give the same displacement as the allocating entry point
 (icb_solve, FP64 Jacobi), within the parity bars the other tests use, on
