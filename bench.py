@@ -271,15 +271,16 @@ def ours_arm(args):
     t_mv = op_launch_seconds(prob, icb.FP64, stream, local)
     ndof = prob.neq
     alg_bytes = 8 * (2 * ndof + prob.nel)
-    flops = 2 * 576 * prob.nel
+    flops = 207 * prob.nel
     peak, peak_kind = _peaks()
     achieved = alg_bytes / t_mv / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": _traffic("matvec_fp64_cantilever3d"),
-                "kernel": "k_matvec_h8<double>", "launch_us": t_mv * 1e6,
+                "frac": achieved / peak, "traffic": _traffic("matvec_h8m_fp64_cantilever3d_192x64x64"),
+                "kernel": "k_matvec_h8m<double>", "launch_us": t_mv * 1e6,
                 "peak_source": peak_kind,
                 "fp64_tflops": flops / t_mv / 1e12,
-                "note": "FP64 element contraction: 1152 flop per element"}
+                "note": "FP64 corner-mode element operator: 207 flop per element "
+                        "(two butterflies + 45 multiply-adds; the dense 24x24 form is 1152)"}
 
     # ---- the same solve with the multigrid paths (time to solution)
     alt = {}
@@ -386,9 +387,10 @@ def op_launch_seconds(prob, prec, stream, device=0, reps=30):
 
 
 def workload_operator(args):
-    """The Hex8 operator y = K(rho) x in each precision (FP64 SIMT, FP32 SIMT,
-    TF32 tcgen05) at 192x64x64 and 384x128x128, L2 flushed before every
-    launch; algorithmic bytes 8|4 x (2 x DOF + elements)."""
+    """The Hex8 operator y = K(rho) x in each precision and form (FP64 and
+    FP32 on CUDA cores in the corner-mode and the dense form, TF32 tcgen05)
+    at 192x64x64 and 384x128x128, L2 flushed before every launch;
+    algorithmic bytes 8|4 x (2 x DOF + elements)."""
     import torch
     import cases
     import icarat_b200 as icb
@@ -400,15 +402,20 @@ def workload_operator(args):
     for n in grids:
         g = cases.build_gpu(ctx, "cantilever3d", *n)
         g.set_density(cases.uniform_density(g.nel, SEED))
-        for name, prec, tc, es in (("fp64", icb.FP64, 0, 8), ("fp32_simt", icb.MIXED, 0, 4),
-                                   ("tf32_tcgen05", icb.TF32, 1, 4)):
+        for name, prec, tc, modal, es in (("fp64_modal", icb.FP64, 0, 1, 8),
+                                          ("fp64_dense", icb.FP64, 0, 0, 8),
+                                          ("fp32_modal", icb.MIXED, 0, 1, 4),
+                                          ("fp32_dense", icb.MIXED, 0, 0, 4),
+                                          ("tf32_tcgen05", icb.TF32, 1, 1, 4)):
             icb.set_option("tc_operator", tc)
+            icb.set_option("hex8_modal", modal)
             t = op_launch_seconds(g, prec, stream)
             B = es * (2 * g.neq + g.nel)
             rows.append({"grid": "x".join(map(str, n)), "variant": name, "launch_us": t * 1e6,
                          "alg_GBps": B / t / 1e9, "frac_of_" + src: B / t / 1e9 / peak,
                          "elem_per_s": g.nel / t})
         icb.set_option("tc_operator", 0)
+        icb.set_option("hex8_modal", 1)
         g.close()
     print(json.dumps({"metric": "Hex8 operator launch time", "unit": "us", "rows": rows,
                       "tc_timeouts": icb.get_option("tc_timeouts"),
@@ -681,6 +688,35 @@ def workload_serving(args):
     return 0
 
 
+def workload_solve(args):
+    """One solve on the c3 geometry (half-MBB, seeded smooth densities), for
+    profiling: a warm-up solve that builds the hierarchy, then the timed one.
+    --size sets the grid (default 384 128 128), --solver fp64_jacobi |
+    fp64_gmg | mixed_gmg (default mixed_gmg), --tc 1 puts the mixed
+    V-cycle's fine-level operator on the tensor cores."""
+    import numpy as np
+    import cases
+    import icarat_b200 as icb
+    n = tuple(args.size) if args.size else (384, 128, 128)
+    prec, pc = {"fp64_jacobi": (icb.FP64, icb.JACOBI), "fp64_gmg": (icb.FP64, icb.GMG),
+                "mixed_gmg": (icb.MIXED, icb.GMG)}[args.solver]
+    ctx = icb.Context(0)
+    icb.set_option("tc_operator", args.tc)
+    g = cases.build_gpu(ctx, "halfmbb3d", *n)
+    g.set_density(smooth_field(*n, seed=SEED))
+    g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000)
+    t0 = time.perf_counter()
+    inf = g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000)
+    dt = time.perf_counter() - t0
+    print(json.dumps({"metric": "solve time", "value": 1e3 * dt, "unit": "ms", "solver": args.solver,
+                      "tc_operator": args.tc, "tc_timeouts": icb.get_option("tc_timeouts"),
+                      "config": {"workload": f"halfmbb3d {n[0]}x{n[1]}x{n[2]}", "dof": g.neq},
+                      "iters": inf["iters"], "true_relres": inf["true_relres"]}), flush=True)
+    g.close()
+    ctx.close()
+    return 0
+
+
 def profile_operator(args):
     """Set up the bench problem and launch each operator variant 3 times (for
     an ncu capture of k_matvec_h8 on the full workload; no timing printed)."""
@@ -711,10 +747,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-operator", action="store_true",
                     help="only launch the operator kernels on the bench problem (for ncu)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "batched", "serving", "operator"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "batched", "serving", "operator", "solve"],
                     help="c2 (default): the bench line; the others print their own line")
     ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 / operator grid override")
     ap.add_argument("--mma-steps", type=int, default=20)
+    ap.add_argument("--tc", type=int, default=0, choices=[0, 1],
+                    help="solve workload: fine-level V-cycle operator on the tensor cores")
+    ap.add_argument("--solver", default="mixed_gmg", choices=["fp64_jacobi", "fp64_gmg", "mixed_gmg"],
+                    help="solve workload: which solver")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--loop-steps", type=int, default=10, help="batched: OC steps per instance")
     ap.add_argument("--workers", type=int, nargs="+", default=[1, 8, 16], help="batched: host workers")
@@ -727,7 +767,8 @@ def main():
         return profile_operator(args)
     if args.workload != "c2" and args.impl == "ours":
         return {"c1": workload_c1, "c3": workload_c3, "batched": workload_batched,
-                "serving": workload_serving, "operator": workload_operator}[args.workload](args)
+                "serving": workload_serving, "operator": workload_operator,
+                "solve": workload_solve}[args.workload](args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

@@ -591,6 +591,8 @@ int icb_set_option(const char *name, long long value)
   std::string n(name);
   if(n == "tc_operator")
     set_tc_operator(value != 0);
+  else if(n == "hex8_modal")
+    set_hex8_modal(value != 0);
   else
     need(false, "unknown option");
   ICB_API_END
@@ -603,6 +605,8 @@ long long icb_get_option(const char *name)
   std::string n(name);
   if(n == "tc_operator")
     return tc_operator_enabled() ? 1 : 0;
+  if(n == "hex8_modal")
+    return hex8_modal_enabled() ? 1 : 0;
   if(n == "tc_timeouts")
     return (long long)tc_timeouts();
   return -1;

@@ -161,6 +161,9 @@ unsigned tc_timeouts();
 /// whether FP32 Hex8 operator launches use the tensor-core kernel
 bool tc_operator_enabled();
 void set_tc_operator(bool on);
+/// whether Hex8 operator launches use the corner-mode kernel when K0 allows it
+bool hex8_modal_enabled();
+void set_hex8_modal(bool on);
 
 /// K: HOST pointer to the unit element matrix ((d*ne)^2 entries); it is
 /// passed by value, so the kernel's FMAs take it from the constant bank.

@@ -27,6 +27,9 @@
 #include "reduce.cuh"
 
 #include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <unordered_map>
 #include <type_traits>
 
 namespace icb
@@ -226,6 +229,238 @@ __global__ void __launch_bounds__(TX *TYK)
 #pragma unroll
       for(int q = 0; q < 4; q++)
         ub[c][q] = ut[c][q];
+  }
+  if(DOT)
+  {
+    double v[1] = {dot};
+    block_reduce<1>(v, red, FinStore{dotOut});
+  }
+}
+
+// ------------------------------------------------ Hex8, corner-mode form ----
+// The 8 corners of a box element are the vertices of a unit cube, so the
+// 8-point Hadamard transform  h_s = sum_a (-1)^(s.o_a) u_a  (s, o_a in {0,1}^3)
+// takes a component's corner values to the element's corner modes: the mean,
+// the three first differences, the three mixed second differences and the
+// xyz twist.  For an isotropic material on a box (every Hex8 element of the
+// structured grids) K0 is block-diagonal in that basis: the 24 x 24 matrix
+// Kt = H K0 H / 64 (H = H8 (x) I3, DOF s*3+c) has 45 nonzeros in 11 dense
+// blocks -- {e_xx, e_yy, e_zz}, the three shear pairs, four blocks of mixed
+// second differences and the three twist modes; the rigid translations (s = 0)
+// are its null rows.  So  K0 u = H (Kt (H u))  costs two butterflies and 45
+// FMAs instead of 576.  The host builds Kt from K0 and checks that every entry
+// outside the blocks vanishes (to rounding); an element matrix that fails the
+// check runs on the dense kernel above.
+//
+// The marching column shares the butterflies between layers: the x-y half of
+// the transform is applied once per node plane (the top plane of element k is
+// the bottom plane of element k+1), and the top-face result is carried up in
+// x-y mode form, where the next element's bottom-face result is added to it
+// before the one inverse x-y butterfly per plane.
+constexpr int kModalNnz = 45;
+template <typename T> struct KModal
+{
+  T v[kModalNnz]; ///< Kt entries, block by block, row-major within a block
+};
+/// the 11 blocks of Kt (modal DOF s*3+c), listed by their modal DOFs
+struct ModalBlocks
+{
+  int n[11];
+  int dof[11][3];
+};
+__host__ __device__ constexpr ModalBlocks modal_blocks()
+{
+  return ModalBlocks{{3, 2, 2, 2, 2, 2, 3, 2, 1, 1, 1},
+                     {{3, 7, 14},
+                      {4, 6, 0},
+                      {5, 12, 0},
+                      {8, 13, 0},
+                      {9, 20, 0},
+                      {10, 17, 0},
+                      {11, 16, 18},
+                      {15, 19, 0},
+                      {21, 0, 0},
+                      {22, 0, 0},
+                      {23, 0, 0}}};
+}
+
+/// yh = Kt uh, block B onwards (OFF: offset of block B in K.v); every index
+/// is a compile-time constant, so uh and yh stay in registers
+template <int B, int OFF, typename T>
+__device__ __forceinline__ void modal_blocks_apply(const KModal<T> &K, const T (&uh)[24],
+                                                   T (&yh)[24])
+{
+  if constexpr(B < 11)
+  {
+    constexpr ModalBlocks MB = modal_blocks();
+    constexpr int n = MB.n[B];
+    constexpr int a = MB.dof[B][0], b = MB.dof[B][1], c = MB.dof[B][2];
+    if constexpr(n == 1)
+      yh[a] = K.v[OFF] * uh[a];
+    else if constexpr(n == 2)
+    {
+      yh[a] = fma(K.v[OFF + 1], uh[b], K.v[OFF] * uh[a]);
+      yh[b] = fma(K.v[OFF + 3], uh[b], K.v[OFF + 2] * uh[a]);
+    }
+    else
+    {
+      yh[a] = fma(K.v[OFF + 2], uh[c], fma(K.v[OFF + 1], uh[b], K.v[OFF] * uh[a]));
+      yh[b] = fma(K.v[OFF + 5], uh[c], fma(K.v[OFF + 4], uh[b], K.v[OFF + 3] * uh[a]));
+      yh[c] = fma(K.v[OFF + 8], uh[c], fma(K.v[OFF + 7], uh[b], K.v[OFF + 6] * uh[a]));
+    }
+    modal_blocks_apply<B + 1, OFF + n * n>(K, uh, yh);
+  }
+}
+
+/// x-y half of the transform on one plane, corners in lnode order
+/// (q0 (0,0), q1 (1,0), q2 (1,1), q3 (0,1)) -> modes h[sx + 2 sy]
+template <typename T> __device__ __forceinline__ void plane_modes(const T u[4], T h[4])
+{
+  const T a = u[0] + u[1], b = u[0] - u[1], c = u[3] + u[2], e = u[3] - u[2];
+  h[0] = a + c;
+  h[1] = b + e;
+  h[2] = a - c;
+  h[3] = b - e;
+}
+/// its inverse up to a factor 4 (the factors of both butterflies, 64 in all,
+/// are folded into Kt): modes -> corners
+template <typename T> __device__ __forceinline__ void plane_corners(const T h[4], T u[4])
+{
+  const T p = h[0] + h[2], m = h[0] - h[2], r = h[1] + h[3], n = h[1] - h[3];
+  u[0] = p + r;
+  u[1] = p - r;
+  u[2] = m - n;
+  u[3] = m + n;
+}
+
+template <typename T, int TYK, bool DOT, int MODE, int MINB>
+__global__ void __launch_bounds__(TX *TYK, MINB)
+    k_matvec_h8m(const KModal<T> K, const Dims d, const int zchunk,
+                 const T *__restrict__ E, const T *__restrict__ u, T *__restrict__ y,
+                 const uint8_t *__restrict__ fix, RedScratch red, double *dotOut,
+                 const KState *gate, const int gateConv, const Epi<T> ep)
+{
+  if(gate && (gate->stop || (gateConv && gate->conv)))
+    return;
+  __shared__ T sB[2][3][TYK][TX];
+  const int lx = threadIdx.x, ly = threadIdx.y;
+  const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TYK - 1);
+  const int ei = X0 - 1 + lx, ej = Y0 - 1 + ly;
+  const int Z0 = blockIdx.z * zchunk;
+  const int Z1 = min(Z0 + zchunk, d.sz) - 1;
+  const bool col = ei >= 0 && ei < d.nx && ej >= 0 && ej < d.ny;
+  const long long sxy = (long long)d.sx * d.sy;
+  const long long ld = d.ld;
+  const long long nb = col ? (long long)ei + (long long)ej * d.sx : 0;
+  const long long qoff[4] = {0, 1, 1 + (long long)d.sx, (long long)d.sx};
+
+  // x-y modes of the bottom plane and the carried top-face result
+  T bh[3][4], carry[3][4];
+#pragma unroll
+  for(int c = 0; c < 3; c++)
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+    {
+      carry[c][q] = T(0);
+      bh[c][q] = T(0);
+    }
+  if(col && Z0 - 1 >= 0)
+  {
+    const long long base = nb + (long long)(Z0 - 1) * sxy;
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      T v[4];
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+        v[q] = __ldg(u + c * ld + base + qoff[q]);
+      plane_modes(v, bh[c]);
+    }
+  }
+  double dot = 0.0;
+  for(int ek = Z0 - 1; ek <= Z1; ++ek)
+  {
+    const bool lay = col && ek >= 0 && ek < d.nz;
+    const bool topok = col && ek + 1 >= 0 && ek + 1 <= d.nz;
+    T th[3][4];
+    {
+      T v[3][4];
+      const long long base = nb + (long long)(ek + 1) * sxy;
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+#pragma unroll
+        for(int q = 0; q < 4; q++)
+          v[c][q] = topok ? __ldg(u + c * ld + base + qoff[q]) : T(0);
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+        plane_modes(v[c], th[c]);
+    }
+    const T Ee = lay ? __ldg(E + (long long)ei + (long long)ej * d.nx +
+                             (long long)ek * d.nx * d.ny)
+                     : T(0);
+    // element modes: z butterfly of the two planes' x-y modes
+    T uh[24], yh[24];
+#pragma unroll
+    for(int s = 0; s < 4; s++)
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        uh[s * 3 + c] = bh[c][s] + th[c][s];
+        uh[(s + 4) * 3 + c] = bh[c][s] - th[c][s];
+      }
+    yh[0] = yh[1] = yh[2] = T(0); // rigid translations
+    modal_blocks_apply<0, 0>(K, uh, yh);
+    // inverse z butterfly: bottom face completes plane ek, top face is carried
+    T acc[3][4];
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      T hb[4];
+#pragma unroll
+      for(int s = 0; s < 4; s++)
+      {
+        hb[s] = fma(Ee, yh[s * 3 + c] + yh[(s + 4) * 3 + c], carry[c][s]);
+        carry[c][s] = Ee * (yh[s * 3 + c] - yh[(s + 4) * 3 + c]);
+      }
+      plane_corners(hb, acc[c]);
+    }
+    if(ek >= Z0)
+    {
+      T A[3];
+      const int buf = ek & 1;
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        A[c] = acc[c][lnode(1, 1)] + __shfl_down_sync(0xffffffffu, acc[c][lnode(0, 1)], 1);
+        sB[buf][c][ly][lx] =
+            acc[c][lnode(1, 0)] + __shfl_down_sync(0xffffffffu, acc[c][lnode(0, 0)], 1);
+      }
+      __syncthreads();
+      const int ni = ei + 1, nj = ej + 1;
+      if(lx < TX - 1 && ly < TYK - 1 && ni < d.sx && nj < d.sy)
+      {
+        const long long node = (long long)ni + (long long)nj * d.sx + (long long)ek * sxy;
+        const unsigned f = __ldg(fix + node);
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          T o = A[c] + sB[buf][c][ly + 1][lx];
+          if((f >> c) & 1u)
+            o = T(0);
+          T us = T(0);
+          if(DOT || MODE >= OP_JACOBI)
+            us = __ldg(u + c * ld + node);
+          if(DOT)
+            dot += double(us) * double(o);
+          y[c * ld + node] = epilogue<T, MODE>(o, us, c * ld + node, ep);
+        }
+      }
+    }
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+        bh[c][q] = th[c][q];
   }
   if(DOT)
   {
@@ -507,26 +742,144 @@ int num_sms()
   return n;
 }
 
+/// CTAs of a kernel resident at once on the device (occupancy queried once
+/// per kernel)
+static int resident_ctas(const void *kern, int threads)
+{
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> memo;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = memo.find(kern);
+  if(it != memo.end())
+    return it->second;
+  int n = 0;
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, 0) != cudaSuccess || n < 1)
+  {
+    (void)cudaGetLastError();
+    n = 1;
+  }
+  return memo[kern] = n * num_sms();
+}
+
+/// z planes per CTA of the Hex8 kernels: `tiles` x-y tiles, `resident` CTAs
+/// in flight.  A CTA marches zchunk + 1 element layers (the layer below its
+/// chunk is recomputed), and the launch takes ceil(CTAs / resident) rounds,
+/// so the split minimises rounds x (zchunk + 1).
+static int h8_zchunk(const Dims &d, long long tiles, int resident)
+{
+  int best = d.sz;
+  long long bestCost = -1;
+  for(int bz = 1; bz <= d.sz; bz++)
+  {
+    const int zc = (d.sz + bz - 1) / bz;
+    const long long n = tiles * ((d.sz + zc - 1) / zc);
+    const long long cost = (n + resident - 1) / resident * (zc + 1);
+    if(bestCost < 0 || cost < bestCost)
+    {
+      bestCost = cost;
+      best = zc;
+    }
+  }
+  return best;
+}
+
 int matvec_blocks(const Dims &d)
 {
-  const int target = num_sms() * 4;
   if(d.dim == 3)
   {
-    int most = 0;
-    for(int ty : {TY3})
+    // the largest CTA count h8_zchunk picks for any occupancy of 1..8 CTAs/SM
+    const long long tiles = (long long)((d.sx + TX - 2) / (TX - 1)) * ((d.sy + TY3 - 2) / (TY3 - 1));
+    long long most = 0;
+    for(int k = 1; k <= 8; k++)
     {
-      int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + ty - 2) / (ty - 1);
-      int bz = std::max(1, std::min(d.sz, (target + bx * by - 1) / (bx * by)));
-      int zchunk = (d.sz + bz - 1) / bz;
-      most = std::max(most, bx * by * ((d.sz + zchunk - 1) / zchunk));
+      const int zc = h8_zchunk(d, tiles, k * num_sms());
+      most = std::max(most, tiles * ((d.sz + zc - 1) / zc));
     }
-    return most;
+    return int(most);
   }
+  const int target = num_sms() * 4;
   int strips = (d.sx + TX - 2) / (TX - 1);
   int bx = (strips + TY2 - 1) / TY2;
   int by = std::max(1, std::min(d.sy, (target + bx - 1) / bx));
   int ychunk = (d.sy + by - 1) / by;
   return bx * ((d.sy + ychunk - 1) / ychunk);
+}
+
+static bool g_hex8_modal = true;
+
+/// Kt = H K0 H / 64 on the 11 blocks of the corner-mode form.  False when an
+/// entry outside the blocks is above rounding (|Kt_rc| > tol max |Kt|, tol
+/// 1e-12 for an FP64 K0, 1e-5 for its FP32 copy).
+template <typename T> static bool modal_form(const T *K, KModal<T> &m)
+{
+  auto sign = [](int s, int a) {
+    const int q = a & 3;
+    const int o = ((q == 1 || q == 2) ? 1 : 0) | (q >= 2 ? 2 : 0) | ((a >> 2) << 2);
+    return (__builtin_popcount(unsigned(s & o)) & 1) ? -1.0 : 1.0;
+  };
+  double hk[24][24], kt[24][24];
+  for(int r = 0; r < 24; r++)
+    for(int c = 0; c < 24; c++)
+    {
+      double v = 0.0;
+      for(int a = 0; a < 8; a++)
+        v += sign(r / 3, a) * double(K[(a * 3 + r % 3) * 24 + c]);
+      hk[r][c] = v;
+    }
+  double big = 0.0;
+  for(int r = 0; r < 24; r++)
+    for(int c = 0; c < 24; c++)
+    {
+      double v = 0.0;
+      for(int b = 0; b < 8; b++)
+        v += hk[r][b * 3 + c % 3] * sign(c / 3, b);
+      kt[r][c] = v / 64.0;
+      big = std::max(big, std::fabs(kt[r][c]));
+    }
+  constexpr ModalBlocks MB = modal_blocks();
+  bool in[24][24] = {};
+  int k = 0;
+  for(int b = 0; b < 11; b++)
+    for(int i = 0; i < MB.n[b]; i++)
+      for(int j = 0; j < MB.n[b]; j++, k++)
+      {
+        in[MB.dof[b][i]][MB.dof[b][j]] = true;
+        m.v[k] = T(kt[MB.dof[b][i]][MB.dof[b][j]]);
+      }
+  const double tol = sizeof(T) == 8 ? 1e-12 : 1e-5;
+  for(int r = 0; r < 24; r++)
+    for(int c = 0; c < 24; c++)
+      if(!in[r][c] && std::fabs(kt[r][c]) > tol * big)
+        return false;
+  return big > 0.0;
+}
+
+/// modal_form with a small per-thread cache keyed by K0's entries (the
+/// multigrid levels each have their own K0; launchers run on several host
+/// threads in the batch runner and the server)
+template <typename T> static bool modal_form_cached(const T *K, KModal<T> &m)
+{
+  struct Entry
+  {
+    T K[576];
+    KModal<T> m;
+    bool ok = false, used = false;
+  };
+  thread_local Entry cache[8];
+  thread_local int next = 0;
+  for(Entry &e : cache)
+    if(e.used && std::equal(K, K + 576, e.K))
+    {
+      m = e.m;
+      return e.ok;
+    }
+  Entry &e = cache[next];
+  next = (next + 1) % 8;
+  std::copy(K, K + 576, e.K);
+  e.used = true;
+  e.ok = modal_form(K, e.m);
+  m = e.m;
+  return e.ok;
 }
 
 template <typename T, int MODE>
@@ -538,37 +891,49 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   Epi<T> ep{x.b, x.dinv, T(x.omega), x.d, T(x.c1), T(x.c2)};
   if(d.dim == 3)
   {
-    KMat<T, 24> km;
-    std::copy(K, K + 576, km.k);
     // 8 element rows per tile for FP64 and FP32 (16-row FP64 tiles were
     // measured: faster at 384x128x128, slower at 192x64x64)
     constexpr int TYK = TY3;
-    int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TYK - 2) / (TYK - 1);
-    int bz = std::max(1, std::min(d.sz, (target + bx * by - 1) / (bx * by)));
-    int zchunk = (d.sz + bz - 1) / bz;
-    bz = (d.sz + zchunk - 1) / zchunk;
-    dim3 grid(bx, by, bz), block(TX, TYK);
-    if(x.dotRed)
-      ICB_REQUIRE(bx * by * bz <= red.maxBlocks, "reduction scratch too small");
-    if constexpr(std::is_same<T, double>::value)
+    const int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TYK - 2) / (TYK - 1);
+    auto run = [&](auto kern, const auto &kp) {
+      const int zchunk = h8_zchunk(d, (long long)bx * by, resident_ctas((const void *)kern, TX * TYK));
+      const int bz = (d.sz + zchunk - 1) / zchunk;
+      if(x.dotRed)
+        ICB_REQUIRE((long long)bx * by * bz <= red.maxBlocks, "reduction scratch too small");
+      kern<<<dim3(bx, by, bz), dim3(TX, TYK), 0, s>>>(kp, d, zchunk, E, u, y, fix, red, x.dotOut,
+                                                      x.gate, x.gateConv, ep);
+    };
+    KModal<T> kmod;
+    if(g_hex8_modal && modal_form_cached(K, kmod))
+    {
+      // FP64: 2 CTAs per SM at 128 registers (a few spill to L1) beat 1 CTA
+      // at 164 registers: 248.7 vs 378.4 us at 384x128x128
+      constexpr int MB = sizeof(T) == 8 ? 2 : 4;
+      if(x.dotRed)
+        run(k_matvec_h8m<T, TYK, true, MODE, MB>, kmod);
+      else
+        run(k_matvec_h8m<T, TYK, false, MODE, MB>, kmod);
+    }
+    else if constexpr(std::is_same<T, double>::value)
     {
       KSym24 ks;
       for(int r = 0; r < 24; r++)
         for(int c = r; c < 24; c++)
           ks.k[symIdx(r, c)] = K[r * 24 + c];
       if(x.dotRed)
-        k_matvec_h8<T, KSym24, TYK, true, MODE><<<grid, block, 0, s>>>(
-            ks, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
+        run(k_matvec_h8<T, KSym24, TYK, true, MODE>, ks);
       else
-        k_matvec_h8<T, KSym24, TYK, false, MODE><<<grid, block, 0, s>>>(
-            ks, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
+        run(k_matvec_h8<T, KSym24, TYK, false, MODE>, ks);
     }
-    else if(x.dotRed)
-      k_matvec_h8<T, KMat<T, 24>, TYK, true, MODE><<<grid, block, 0, s>>>(
-          km, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
     else
-      k_matvec_h8<T, KMat<T, 24>, TYK, false, MODE><<<grid, block, 0, s>>>(
-          km, d, zchunk, E, u, y, fix, red, x.dotOut, x.gate, x.gateConv, ep);
+    {
+      KMat<T, 24> km;
+      std::copy(K, K + 576, km.k);
+      if(x.dotRed)
+        run(k_matvec_h8<T, KMat<T, 24>, TYK, true, MODE>, km);
+      else
+        run(k_matvec_h8<T, KMat<T, 24>, TYK, false, MODE>, km);
+    }
   }
   else
   {
@@ -597,6 +962,8 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
 static bool g_tc_operator = false;
 bool tc_operator_enabled() { return g_tc_operator; }
 void set_tc_operator(bool on) { g_tc_operator = on; }
+bool hex8_modal_enabled() { return g_hex8_modal; }
+void set_hex8_modal(bool on) { g_hex8_modal = on; }
 
 template <typename T>
 void launch_op(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,

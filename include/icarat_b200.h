@@ -376,8 +376,11 @@ int icb_operator_apply_device(icb_problem p, int precision, const void *x, void 
 long long icb_launch_count(void);
 /* process-wide switches: "tc_operator" (1: the FP32 Hex8 operator inside the
  * ICB_MIXED V-cycle runs on the tcgen05 tensor cores in TF32; 0: CUDA
- * cores).  icb_get_option also reports "tc_timeouts" (tensor-core waits that
- * gave up; 0 in a healthy run).  Unknown names: ICB_ERR_BAD_ARG / -1. */
+ * cores); "hex8_modal" (1, the default: CUDA-core Hex8 operators apply K0 in
+ * the element's corner-mode basis, 45 multiply-adds per element instead of
+ * 576; 0: the dense 24 x 24 product).  icb_get_option also reports
+ * "tc_timeouts" (tensor-core waits that gave up; 0 in a healthy run).
+ * Unknown names: ICB_ERR_BAD_ARG / -1. */
 int icb_set_option(const char *name, long long value);
 long long icb_get_option(const char *name);
 
