@@ -333,6 +333,24 @@ template <typename T> __device__ __forceinline__ void plane_corners(const T h[4]
   u[3] = m + n;
 }
 
+/// the epilogue's per-node inputs (the node's own value, b, D^-1, the
+/// Chebyshev direction), loaded ahead of their use
+template <typename T> struct EpiIn
+{
+  T b[3], dinv[3], d[3], us[3];
+};
+
+/// dynamic shared memory of k_matvec_h8m: the carry, and for FP64 the
+/// bottom plane's modes (12 values per thread each)
+template <typename T, int TYK> constexpr int h8m_smem_bytes()
+{
+  return int(sizeof(T)) * 12 * TYK * TX * (sizeof(T) == 8 ? 2 : 1);
+}
+
+/// Each layer issues the loads of the next layer's top plane and modulus
+/// ahead of its own element work, so the arithmetic covers their latency.
+/// The carried top-face result lives in shared memory (each thread its own
+/// 12 values), which keeps the registers for the prefetched plane.
 template <typename T, int TYK, bool DOT, int MODE, int MINB>
 __global__ void __launch_bounds__(TX *TYK, MINB)
     k_matvec_h8m(const KModal<T> K, const Dims d, const int zchunk,
@@ -342,6 +360,12 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
 {
   if(gate && (gate->stop || (gateConv && gate->conv)))
     return;
+  // FP64 also keeps the bottom plane's modes in shared memory (kSmemModes);
+  // carry and modes take h8m_smem_bytes of dynamic shared memory
+  constexpr bool kSmemModes = sizeof(T) == 8;
+  extern __shared__ __align__(16) unsigned char h8m_dyn[];
+  auto sC = reinterpret_cast<T(*)[TYK][TX]>(h8m_dyn);
+  auto sH = reinterpret_cast<T(*)[TYK][TX]>(h8m_dyn + sizeof(T) * 12 * TYK * TX);
   __shared__ T sB[2][3][TYK][TX];
   const int lx = threadIdx.x, ly = threadIdx.y;
   const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TYK - 1);
@@ -349,55 +373,91 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
   const int Z0 = blockIdx.z * zchunk;
   const int Z1 = min(Z0 + zchunk, d.sz) - 1;
   const bool col = ei >= 0 && ei < d.nx && ej >= 0 && ej < d.ny;
-  const long long sxy = (long long)d.sx * d.sy;
+  const long long sxy = (long long)d.sx * d.sy, exy = (long long)d.nx * d.ny;
   const long long ld = d.ld;
+  // component c of this column's corner q in node plane k: u[c*ld + nb + qoff[q] + k*sxy]
   const long long nb = col ? (long long)ei + (long long)ej * d.sx : 0;
   const long long qoff[4] = {0, 1, 1 + (long long)d.sx, (long long)d.sx};
+  const long long eb = col ? (long long)ei + (long long)ej * d.nx : 0;
+  auto load_plane = [&](int k, T (&v)[3][4]) {
+    const bool ok = col && k >= 0 && k <= d.nz;
+    const T *p = u + nb + (long long)k * sxy;
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+        v[c][q] = ok ? __ldg(p + c * ld + qoff[q]) : T(0);
+  };
+  auto load_E = [&](int k) {
+    return col && k >= 0 && k < d.nz ? __ldg(E + eb + (long long)k * exy) : T(0);
+  };
 
-  // x-y modes of the bottom plane and the carried top-face result
-  T bh[3][4], carry[3][4];
-#pragma unroll
-  for(int c = 0; c < 3; c++)
-#pragma unroll
-    for(int q = 0; q < 4; q++)
-    {
-      carry[c][q] = T(0);
-      bh[c][q] = T(0);
-    }
-  if(col && Z0 - 1 >= 0)
+  // the bottom plane's x-y modes; the top-face result carried up (sC)
+  T bh[3][4], nxt[3][4];
   {
-    const long long base = nb + (long long)(Z0 - 1) * sxy;
+    T v[3][4];
+    load_plane(Z0 - 1, v);
 #pragma unroll
     for(int c = 0; c < 3; c++)
     {
-      T v[4];
+      plane_modes(v[c], bh[c]);
 #pragma unroll
       for(int q = 0; q < 4; q++)
-        v[q] = __ldg(u + c * ld + base + qoff[q]);
-      plane_modes(v, bh[c]);
+      {
+        sC[c * 4 + q][ly][lx] = T(0);
+        if(kSmemModes)
+          sH[c * 4 + q][ly][lx] = bh[c][q];
+      }
     }
   }
+  load_plane(Z0, nxt);
+  T Enxt = load_E(Z0 - 1);
   double dot = 0.0;
   for(int ek = Z0 - 1; ek <= Z1; ++ek)
   {
-    const bool lay = col && ek >= 0 && ek < d.nz;
-    const bool topok = col && ek + 1 >= 0 && ek + 1 <= d.nz;
     T th[3][4];
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+      plane_modes(nxt[c], th[c]);
+    const T Ee = Enxt;
+    // next layer's inputs: FP32 at the top of the layer, FP64 after the
+    // element product (its registers are the limit)
+    constexpr bool kLateNext = sizeof(T) == 8;
+    if(!kLateNext)
     {
-      T v[3][4];
-      const long long base = nb + (long long)(ek + 1) * sxy;
-#pragma unroll
-      for(int c = 0; c < 3; c++)
-#pragma unroll
-        for(int q = 0; q < 4; q++)
-          v[c][q] = topok ? __ldg(u + c * ld + base + qoff[q]) : T(0);
-#pragma unroll
-      for(int c = 0; c < 3; c++)
-        plane_modes(v[c], th[c]);
+      load_plane(ek + 2, nxt);
+      Enxt = load_E(ek + 1);
     }
-    const T Ee = lay ? __ldg(E + (long long)ei + (long long)ej * d.nx +
-                             (long long)ek * d.nx * d.ny)
-                     : T(0);
+    const bool out = ek >= Z0;
+    const int ni = ei + 1, nj = ej + 1;
+    const bool own = out && lx < TX - 1 && ly < TYK - 1 && ni < d.sx && nj < d.sy;
+    const long long node = (long long)ni + (long long)nj * d.sx + (long long)ek * sxy;
+    unsigned f = 0;
+    EpiIn<T> in;
+    auto load_in = [&]() {
+      if(own)
+      {
+        f = __ldg(fix + node);
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          if(DOT || MODE >= OP_JACOBI)
+            in.us[c] = __ldg(u + c * ld + node);
+          if(MODE != OP_APPLY)
+            in.b[c] = __ldg(ep.b + c * ld + node);
+          if(MODE >= OP_JACOBI)
+            in.dinv[c] = __ldg(ep.dinv + c * ld + node);
+          if(MODE == OP_CHEB)
+            in.d[c] = ep.c1 != T(0) ? ep.d[c * ld + node] : T(0);
+        }
+      }
+    };
+    // FP32: before the element work; FP64: after it, where the registers
+    // of the element work are free again (the exchange barrier covers part
+    // of the latency)
+    constexpr bool kEarly = sizeof(T) == 4;
+    if(kEarly)
+      load_in();
     // element modes: z butterfly of the two planes' x-y modes
     T uh[24], yh[24];
 #pragma unroll
@@ -405,11 +465,19 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
 #pragma unroll
       for(int c = 0; c < 3; c++)
       {
-        uh[s * 3 + c] = bh[c][s] + th[c][s];
-        uh[(s + 4) * 3 + c] = bh[c][s] - th[c][s];
+        const T b = kSmemModes ? sH[c * 4 + s][ly][lx] : bh[c][s];
+        uh[s * 3 + c] = b + th[c][s];
+        uh[(s + 4) * 3 + c] = b - th[c][s];
+        if(kSmemModes)
+          sH[c * 4 + s][ly][lx] = th[c][s];
       }
     yh[0] = yh[1] = yh[2] = T(0); // rigid translations
     modal_blocks_apply<0, 0>(K, uh, yh);
+    if(kLateNext)
+    {
+      load_plane(ek + 2, nxt);
+      Enxt = load_E(ek + 1);
+    }
     // inverse z butterfly: bottom face completes plane ek, top face is carried
     T acc[3][4];
 #pragma unroll
@@ -419,12 +487,20 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
 #pragma unroll
       for(int s = 0; s < 4; s++)
       {
-        hb[s] = fma(Ee, yh[s * 3 + c] + yh[(s + 4) * 3 + c], carry[c][s]);
-        carry[c][s] = Ee * (yh[s * 3 + c] - yh[(s + 4) * 3 + c]);
+        hb[s] = fma(Ee, yh[s * 3 + c] + yh[(s + 4) * 3 + c], sC[c * 4 + s][ly][lx]);
+        sC[c * 4 + s][ly][lx] = Ee * (yh[s * 3 + c] - yh[(s + 4) * 3 + c]);
       }
       plane_corners(hb, acc[c]);
     }
-    if(ek >= Z0)
+    if(!kSmemModes)
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+#pragma unroll
+        for(int q = 0; q < 4; q++)
+          bh[c][q] = th[c][q];
+    if(!kEarly)
+      load_in();
+    if(out)
     {
       T A[3];
       const int buf = ek & 1;
@@ -436,31 +512,41 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
             acc[c][lnode(1, 0)] + __shfl_down_sync(0xffffffffu, acc[c][lnode(0, 0)], 1);
       }
       __syncthreads();
-      const int ni = ei + 1, nj = ej + 1;
-      if(lx < TX - 1 && ly < TYK - 1 && ni < d.sx && nj < d.sy)
+      if(own)
       {
-        const long long node = (long long)ni + (long long)nj * d.sx + (long long)ek * sxy;
-        const unsigned f = __ldg(fix + node);
 #pragma unroll
         for(int c = 0; c < 3; c++)
         {
           T o = A[c] + sB[buf][c][ly + 1][lx];
           if((f >> c) & 1u)
             o = T(0);
-          T us = T(0);
-          if(DOT || MODE >= OP_JACOBI)
-            us = __ldg(u + c * ld + node);
+          const T us = in.us[c];
           if(DOT)
             dot += double(us) * double(o);
-          y[c * ld + node] = epilogue<T, MODE>(o, us, c * ld + node, ep);
+          const long long i = c * ld + node;
+          T w;
+          if(MODE == OP_APPLY)
+            w = o;
+          else
+          {
+            const T r = in.b[c] - o;
+            if(MODE == OP_RESIDUAL)
+              w = r;
+            else if(MODE == OP_JACOBI)
+              w = us + ep.omega * in.dinv[c] * r;
+            else
+            {
+              T dn = ep.c2 * in.dinv[c] * r;
+              if(ep.c1 != T(0))
+                dn += ep.c1 * in.d[c];
+              ep.d[i] = dn;
+              w = us + dn;
+            }
+          }
+          y[i] = w;
         }
       }
     }
-#pragma unroll
-    for(int c = 0; c < 3; c++)
-#pragma unroll
-      for(int q = 0; q < 4; q++)
-        bh[c][q] = th[c][q];
   }
   if(DOT)
   {
@@ -744,7 +830,7 @@ int num_sms()
 
 /// CTAs of a kernel resident at once on the device (occupancy queried once
 /// per kernel)
-static int resident_ctas(const void *kern, int threads)
+static int resident_ctas(const void *kern, int threads, int smem)
 {
   static std::mutex mu;
   static std::unordered_map<const void *, int> memo;
@@ -752,8 +838,11 @@ static int resident_ctas(const void *kern, int threads)
   auto it = memo.find(kern);
   if(it != memo.end())
     return it->second;
+  // static + dynamic shared memory past 48 KB needs the opt-in
+  if(smem > 0)
+    ICB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int n = 0;
-  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, 0) != cudaSuccess || n < 1)
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess || n < 1)
   {
     (void)cudaGetLastError();
     n = 1;
@@ -895,24 +984,27 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
     // measured: faster at 384x128x128, slower at 192x64x64)
     constexpr int TYK = TY3;
     const int bx = (d.sx + TX - 2) / (TX - 1), by = (d.sy + TYK - 2) / (TYK - 1);
-    auto run = [&](auto kern, const auto &kp) {
-      const int zchunk = h8_zchunk(d, (long long)bx * by, resident_ctas((const void *)kern, TX * TYK));
+    auto run = [&](auto kern, const auto &kp, int smem) {
+      const int zchunk =
+          h8_zchunk(d, (long long)bx * by, resident_ctas((const void *)kern, TX * TYK, smem));
       const int bz = (d.sz + zchunk - 1) / zchunk;
       if(x.dotRed)
         ICB_REQUIRE((long long)bx * by * bz <= red.maxBlocks, "reduction scratch too small");
-      kern<<<dim3(bx, by, bz), dim3(TX, TYK), 0, s>>>(kp, d, zchunk, E, u, y, fix, red, x.dotOut,
-                                                      x.gate, x.gateConv, ep);
+      kern<<<dim3(bx, by, bz), dim3(TX, TYK), smem, s>>>(kp, d, zchunk, E, u, y, fix, red,
+                                                         x.dotOut, x.gate, x.gateConv, ep);
     };
     KModal<T> kmod;
     if(g_hex8_modal && modal_form_cached(K, kmod))
     {
-      // FP64: 2 CTAs per SM at 128 registers (a few spill to L1) beat 1 CTA
-      // at 164 registers: 248.7 vs 378.4 us at 384x128x128
-      constexpr int MB = sizeof(T) == 8 ? 2 : 4;
+      // 2 (FP64) / 3 (FP32) CTAs of 256 threads per SM.  The carry (and for
+      // FP64 the bottom plane's modes) live in shared memory: FP64 with both
+      // in registers spills, and the dot-fused FP64 Jacobi-PCG on
+      // halfmbb3d 192x64x64 took 208 ms against 172 ms for 2374 iterations
+      constexpr int MB = sizeof(T) == 8 ? 2 : 3;
       if(x.dotRed)
-        run(k_matvec_h8m<T, TYK, true, MODE, MB>, kmod);
+        run(k_matvec_h8m<T, TYK, true, MODE, MB>, kmod, h8m_smem_bytes<T, TYK>());
       else
-        run(k_matvec_h8m<T, TYK, false, MODE, MB>, kmod);
+        run(k_matvec_h8m<T, TYK, false, MODE, MB>, kmod, h8m_smem_bytes<T, TYK>());
     }
     else if constexpr(std::is_same<T, double>::value)
     {
@@ -921,18 +1013,18 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
         for(int c = r; c < 24; c++)
           ks.k[symIdx(r, c)] = K[r * 24 + c];
       if(x.dotRed)
-        run(k_matvec_h8<T, KSym24, TYK, true, MODE>, ks);
+        run(k_matvec_h8<T, KSym24, TYK, true, MODE>, ks, 0);
       else
-        run(k_matvec_h8<T, KSym24, TYK, false, MODE>, ks);
+        run(k_matvec_h8<T, KSym24, TYK, false, MODE>, ks, 0);
     }
     else
     {
       KMat<T, 24> km;
       std::copy(K, K + 576, km.k);
       if(x.dotRed)
-        run(k_matvec_h8<T, KMat<T, 24>, TYK, true, MODE>, km);
+        run(k_matvec_h8<T, KMat<T, 24>, TYK, true, MODE>, km, 0);
       else
-        run(k_matvec_h8<T, KMat<T, 24>, TYK, false, MODE>, km);
+        run(k_matvec_h8<T, KMat<T, 24>, TYK, false, MODE>, km, 0);
     }
   }
   else
