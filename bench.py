@@ -482,6 +482,8 @@ def workload_c3(args):
     # mixed vs FP64 on the initial design (same densities, same tolerance)
     g.set_density(rho0)
     out = {}
+    if args.loop_only:
+        return _c3_loop(args, icb, g, n, steps, rho0, None, None, None, None)
     for name, prec in (("fp64_gmg", icb.FP64), ("mixed_gmg", icb.MIXED)):
         g.solve(precision=prec, precond=icb.GMG, tol=TOL, maxit=20000)
         t0 = time.perf_counter()
@@ -520,6 +522,12 @@ def workload_c3(args):
                          f"({t_it:.3f} s per iteration); time to the FP64 solve estimated as "
                          f"per-iteration time x {out['fp64_jacobi']['iters']} iterations = {cpu_ttsol:.0f} s"}
         speed["mixed_gmg_vs_cpu_estimate"] = cpu_ttsol / (out["mixed_gmg"]["ms"] * 1e-3)
+    return _c3_loop(args, icb, g, n, steps, rho0, out, err, speed, cpu)
+
+
+def _c3_loop(args, icb, g, n, steps, rho0, out, err, speed, cpu):
+    """the c3 MMA + Helmholtz loop and its JSON line"""
+    import numpy as np
     vol = float(np.prod(n))
     o = icb.loop_opts(steps, 3.0, precision=icb.MIXED, volume_ref=0.3 * vol)
     its = np.zeros(steps)
@@ -751,6 +759,8 @@ def main():
                     help="c2 (default): the bench line; the others print their own line")
     ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 / operator grid override")
     ap.add_argument("--mma-steps", type=int, default=20)
+    ap.add_argument("--loop-only", action="store_true",
+                    help="c3: only the MMA loop (no initial-design solves, no CPU sample)")
     ap.add_argument("--tc", type=int, default=0, choices=[0, 1],
                     help="solve workload: fine-level V-cycle operator on the tensor cores")
     ap.add_argument("--solver", default="mixed_gmg", choices=["fp64_jacobi", "fp64_gmg", "mixed_gmg"],

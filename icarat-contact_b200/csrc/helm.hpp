@@ -14,6 +14,7 @@ struct HelmFilter
   int ne = 8;
   KMat<double, 8> K; ///< M + re^2 K_grad of one element (ne x ne)
   double nint = 0.0; ///< int N_a over an element (the same for every node)
+  double h[3] = {1.0, 1.0, 1.0}; ///< element edge lengths
   std::unique_ptr<JacobiPcg<double>> pcg;
   DevBuf<double> dinv, rhs, phi;
 

@@ -45,6 +45,13 @@ inline int vblocks(long long n)
   return int(std::max<long long>(1, std::min<long long>((n + VB - 1) / VB, num_sms() * 8LL)));
 }
 inline unsigned nblocks(long long n, int bs) { return unsigned((n + bs - 1) / bs); }
+/// transfer kernels: kTB threads along x, one grid row per (y, z) node line
+constexpr int kTB = 128;
+inline dim3 grid3(const Dims &d)
+{
+  ICB_REQUIRE(d.sy <= 65535 && d.sz <= 65535, "grid too large for the transfer launch");
+  return dim3(unsigned((d.sx + kTB - 1) / kTB), unsigned(d.sy), unsigned(d.sz));
+}
 __device__ __forceinline__ bool gated(const KState *g)
 {
   return g && (g->stop || g->conv);
@@ -71,104 +78,86 @@ __global__ void k_coarsen_E(Dims df, Dims dc, const T *__restrict__ Ef, T *__res
   Ec[e] = T(s / (df.dim == 3 ? 8.0 : 4.0));
 }
 
-/// b_c = R r_f (R = P^T), constrained coarse DOFs zeroed
+/// b_c = R r_f (R = P^T), constrained coarse DOFs zeroed.  One thread per
+/// coarse node (x along threads, y and z along the grid, so no index
+/// division): the 1-D weights of the fine neighbours 2I-1, 2I, 2I+1 are
+/// 1/2, 1, 1/2 (those inside the fine grid), applied row by row.
 template <typename T>
 __global__ void k_restrict(Dims df, Dims dc, const T *__restrict__ rf, T *__restrict__ bc,
                            const uint8_t *__restrict__ fixc, const KState *gate)
 {
   if(gated(gate))
     return;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if(n >= dc.nnode)
+  const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y, K = blockIdx.z;
+  if(I >= dc.sx)
     return;
-  long long sxy = (long long)dc.sx * dc.sy;
-  int I = int(n % dc.sx), J = int((n / dc.sx) % dc.sy), K = int(n / sxy);
-  long long fsxy = (long long)df.sx * df.sy;
-  double s[3] = {0, 0, 0};
-  int kr = df.dim == 3 ? 1 : 0;
+  const long long fsxy = (long long)df.sx * df.sy;
+  const int kr = df.dim == 3 ? 1 : 0;
+  const T h = T(0.5);
+  T s[3] = {T(0), T(0), T(0)};
   for(int dk = -kr; dk <= kr; dk++)
   {
-    int k = 2 * K + dk;
+    const int k = 2 * K + dk;
     if(k < 0 || k >= df.sz)
       continue;
-    double wk = dk ? 0.5 : 1.0;
+    T sk[3] = {T(0), T(0), T(0)};
     for(int dj = -1; dj <= 1; dj++)
     {
-      int j = 2 * J + dj;
+      const int j = 2 * J + dj;
       if(j < 0 || j >= df.sy)
         continue;
-      double wj = wk * (dj ? 0.5 : 1.0);
-      for(int di = -1; di <= 1; di++)
-      {
-        int i = 2 * I + di;
-        if(i < 0 || i >= df.sx)
-          continue;
-        double w = wj * (di ? 0.5 : 1.0);
-        long long f = i + (long long)j * df.sx + (long long)k * fsxy;
-        for(int c = 0; c < df.dim; c++)
-          s[c] += w * double(rf[c * df.ld + f]);
-      }
+      const long long row = (long long)j * df.sx + (long long)k * fsxy;
+      const int i = 2 * I;
+      const bool lo = i - 1 >= 0, mid = i < df.sx, hi = i + 1 < df.sx;
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+        if(c < df.dim)
+        {
+          const T *r = rf + c * df.ld + row;
+          const T v = (mid ? r[i] : T(0)) + h * ((lo ? r[i - 1] : T(0)) + (hi ? r[i + 1] : T(0)));
+          sk[c] = dj ? fma(h, v, sk[c]) : sk[c] + v;
+        }
     }
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+      s[c] = dk ? fma(h, sk[c], s[c]) : s[c] + sk[c];
   }
-  unsigned fx = fixc[n];
+  const long long n = I + (long long)J * dc.sx + (long long)K * dc.sx * dc.sy;
+  const unsigned fx = fixc[n];
   for(int c = 0; c < dc.dim; c++)
-    bc[c * dc.ld + n] = ((fx >> c) & 1u) ? T(0) : T(s[c]);
+    bc[c * dc.ld + n] = ((fx >> c) & 1u) ? T(0) : s[c];
 }
 
-/// x_f += P x_c, constrained fine DOFs untouched (they stay 0)
+/// x_f += P x_c, constrained fine DOFs untouched (they stay 0).  One thread
+/// per fine node (x along threads, y and z along the grid): the trilinear
+/// interpolant as three nested midpoints; an even index takes the same
+/// coarse node twice, which the midpoint returns exactly.
 template <typename T>
 __global__ void k_prolong_add(Dims df, Dims dc, const T *__restrict__ xc, T *__restrict__ xf,
                               const uint8_t *__restrict__ fixf, const KState *gate)
 {
   if(gated(gate))
     return;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if(n >= df.nnode)
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if(i >= df.sx)
     return;
-  long long sxy = (long long)df.sx * df.sy;
-  int i = int(n % df.sx), j = int((n / df.sx) % df.sy), k = int(n / sxy);
-  int I[2], J[2], K[2], ni, nj, nk;
-  double wi[2], wj[2], wk[2];
-  auto split = [](int v, int *C, double *w, int &cnt) {
-    if(v & 1)
+  const int I0 = i >> 1, I1 = (i + 1) >> 1, J0 = j >> 1, J1 = (j + 1) >> 1;
+  const int K0 = k >> 1, K1 = df.dim == 3 ? (k + 1) >> 1 : K0;
+  const long long csxy = (long long)dc.sx * dc.sy;
+  const long long r00 = (long long)J0 * dc.sx + K0 * csxy, r10 = (long long)J1 * dc.sx + K0 * csxy;
+  const long long r01 = (long long)J0 * dc.sx + K1 * csxy, r11 = (long long)J1 * dc.sx + K1 * csxy;
+  const long long n = i + (long long)j * df.sx + (long long)k * df.sx * df.sy;
+  const unsigned fx = fixf[n];
+  const T h = T(0.5);
+#pragma unroll
+  for(int c = 0; c < 3; c++)
+    if(c < df.dim && !((fx >> c) & 1u))
     {
-      C[0] = (v - 1) / 2;
-      C[1] = (v + 1) / 2;
-      w[0] = w[1] = 0.5;
-      cnt = 2;
+      const T *x = xc + c * dc.ld;
+      const T a = h * (x[r00 + I0] + x[r00 + I1]), b = h * (x[r10 + I0] + x[r10 + I1]);
+      const T a2 = h * (x[r01 + I0] + x[r01 + I1]), b2 = h * (x[r11 + I0] + x[r11 + I1]);
+      xf[c * df.ld + n] += h * (h * (a + b) + h * (a2 + b2));
     }
-    else
-    {
-      C[0] = v / 2;
-      w[0] = 1.0;
-      cnt = 1;
-    }
-  };
-  split(i, I, wi, ni);
-  split(j, J, wj, nj);
-  if(df.dim == 3)
-    split(k, K, wk, nk);
-  else
-  {
-    K[0] = 0;
-    wk[0] = 1.0;
-    nk = 1;
-  }
-  long long csxy = (long long)dc.sx * dc.sy;
-  double s[3] = {0, 0, 0};
-  for(int c3 = 0; c3 < nk; c3++)
-    for(int b = 0; b < nj; b++)
-      for(int a = 0; a < ni; a++)
-      {
-        double w = wi[a] * wj[b] * wk[c3];
-        long long cn = I[a] + (long long)J[b] * dc.sx + (long long)K[c3] * csxy;
-        for(int c = 0; c < df.dim; c++)
-          s[c] += w * double(xc[c * dc.ld + cn]);
-      }
-  unsigned fx = fixf[n];
-  for(int c = 0; c < df.dim; c++)
-    if(!((fx >> c) & 1u))
-      xf[c * df.ld + n] += T(s[c]);
 }
 
 /// first smoothing step from a zero guess: x = d = c D^-1 b
@@ -837,10 +826,10 @@ template <typename TK, typename TP> struct MgPcg
     res.gateConv = 1;
     launch_op<TP>(L.d, L.K, L.E, cur, L.r.p, L.fix, s, res);
     Level<TP> &Cn = lv[l + 1];
-    k_restrict<TP><<<nblocks(Cn.d.nnode, 256), 256, 0, s>>>(L.d, Cn.d, L.r.p, Cn.b.p, Cn.fix, gate);
+    k_restrict<TP><<<grid3(Cn.d), kTB, 0, s>>>(L.d, Cn.d, L.r.p, Cn.b.p, Cn.fix, gate);
     count_launch();
     level(l + 1, Cn.b.p, Cn.x.p, s, gate);
-    k_prolong_add<TP><<<nblocks(L.d.nnode, 256), 256, 0, s>>>(L.d, Cn.d, Cn.x.p, cur, L.fix, gate);
+    k_prolong_add<TP><<<grid3(L.d), kTB, 0, s>>>(L.d, Cn.d, Cn.x.p, cur, L.fix, gate);
     count_launch();
     for(int k = 0; k < nu; k++)
     {

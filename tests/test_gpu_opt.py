@@ -44,7 +44,8 @@ def test_threshold_matches_oracle(ctx):
         assert np.abs(b - po.threshold_deriv(x, beta)).max() <= 1e-12 * beta
 
 
-@pytest.mark.parametrize("dims,R", [((2, 40, 20), 2.0), ((2, 25, 10), 3.0), ((3, 12, 8, 6), 3.0)])
+@pytest.mark.parametrize("dims,R", [((2, 40, 20), 2.0), ((2, 25, 10), 3.0), ((3, 12, 8, 6), 3.0),
+                                    ((3, 70, 17, 9), 2.5), ((3, 33, 40, 3), 4.0)])
 def test_helmholtz_filter_matches_oracle(ctx, dims, R):
     o = po.Problem(*dims)
     g = icb.Problem(ctx, *dims)
