@@ -23,8 +23,9 @@
 //    when the fine DOF at the same point is);
 //  * smoother: damped Jacobi with the fused operator epilogue (one kernel per
 //    sweep), nu sweeps before and after the coarse correction;
-//  * coarsest level: dense FP64 inverse built on the device (one CTA,
-//    Gauss-Jordan), applied as a dense product.
+//  * coarsest level (<= 160 DOFs by default): dense FP64 inverse built on
+//    the device (one CTA, Gauss-Jordan in shared memory), applied as a
+//    dense product.
 // The whole V-cycle is a fixed kernel sequence, so a batch of PCG
 // iterations including their V-cycles is captured as one CUDA graph.
 #include <algorithm>
@@ -224,12 +225,26 @@ __global__ void k_dense_assemble(Dims d, KMat<double, 24> K, const T *__restrict
 /// In-place Gauss-Jordan inversion of the SPD coarse matrix (no pivoting is
 /// needed for SPD).  One CTA; a non-positive pivot is recorded in *status
 /// and replaced by a tiny positive value so the preconditioner stays usable.
-__global__ void __launch_bounds__(1024) k_invert_spd(int n, double *A, int *status)
+/// SMEM: the matrix is worked on in shared memory (n^2 doubles, n <=
+/// kInvSmemMax) and copied back once; otherwise in place in global memory
+/// (L2-resident).  Warp w updates rows w, w + 32, ..., its lanes the columns.
+constexpr int kInvSmemMax = 160;
+template <bool SMEM>
+__global__ void __launch_bounds__(1024) k_invert_spd(int n, double *Ag, int *status)
 {
+  extern __shared__ double sA[];
   __shared__ double rowk[1024];
   __shared__ double colk[1024];
   __shared__ double piv;
   const int tid = threadIdx.x, nth = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nwarp = nth >> 5;
+  double *A = SMEM ? sA : Ag;
+  if(SMEM)
+  {
+    for(int t = tid; t < n * n; t += nth)
+      sA[t] = Ag[t];
+    __syncthreads();
+  }
   double dmax = 0.0;
   for(int i = 0; i < n; i++)
     dmax = fmax(dmax, A[(long long)i * n + i]);
@@ -253,19 +268,22 @@ __global__ void __launch_bounds__(1024) k_invert_spd(int n, double *A, int *stat
       colk[j] = A[(long long)j * n + k];
     }
     __syncthreads();
-    for(long long t = tid; t < (long long)n * n; t += nth)
+    for(int i = warp; i < n; i += nwarp)
     {
-      int i = int(t / n), j = int(t % n);
+      double *Ai = A + (long long)i * n;
+      const double f = colk[i];
       if(i == k)
-        A[t] = rowk[j];
+        for(int j = lane; j < n; j += 32)
+          Ai[j] = rowk[j];
       else
-      {
-        double f = colk[i];
-        A[t] = (j == k ? 0.0 : A[t]) - f * rowk[j];
-      }
+        for(int j = lane; j < n; j += 32)
+          Ai[j] = (j == k ? 0.0 : Ai[j]) - f * rowk[j];
     }
     __syncthreads();
   }
+  if(SMEM)
+    for(int t = tid; t < n * n; t += nth)
+      Ag[t] = sA[t];
 }
 
 /// x_c = A^-1 b_c over the free coarse DOFs (warp per row)
@@ -645,7 +663,9 @@ template <typename TK, typename TP> struct MgPcg
         if(hs.fixed[nd * hs.desc.dim + c])
           fm[nd] |= uint8_t(1u << c);
     const int dim = hs.desc.dim;
-    const int cd = coarseDofs > 0 ? coarseDofs : 600;
+    // default: coarsen until the grid has <= 160 DOFs, so the coarsest
+    // matrix is inverted in shared memory (600 DOFs cost 14.6 ms a density)
+    const int cd = coarseDofs > 0 ? coarseDofs : kInvSmemMax;
     while(true)
     {
       const Dims &f = lv.back().d;
@@ -774,7 +794,18 @@ template <typename TK, typename TP> struct MgPcg
         kd.k[i] = double(C.K[i]);
       k_dense_assemble<TP><<<nblocks(C.d.nnode * C.d.dim, 128), 128, 0, s>>>(C.d, kd, C.E,
                                                                             cDense.p, nc, cA.p);
-      k_invert_spd<<<1, 1024, 0, s>>>(nc, cA.p, cStatus.p);
+      if(nc <= kInvSmemMax)
+      {
+        // the shared-memory opt-in is a per-device function attribute shared by
+        // every host thread: always set it to the largest size, so threads of
+        // the batch runner never shrink it under one another's launch
+        ICB_CUDA(cudaFuncSetAttribute(k_invert_spd<true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(sizeof(double)) * kInvSmemMax * kInvSmemMax));
+        k_invert_spd<true><<<1, 1024, int(sizeof(double)) * nc * nc, s>>>(nc, cA.p, cStatus.p);
+      }
+      else
+        k_invert_spd<false><<<1, 1024, 0, s>>>(nc, cA.p, cStatus.p);
       count_launch(2);
     }
     ICB_CUDA(cudaGetLastError());

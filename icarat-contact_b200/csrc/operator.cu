@@ -833,10 +833,14 @@ int num_sms()
 static int resident_ctas(const void *kern, int threads, int smem)
 {
   static std::mutex mu;
-  static std::unordered_map<const void *, int> memo;
+  // keyed by kernel and device: the shared-memory opt-in is per device
+  static std::unordered_map<const void *, int> memo[64];
+  int dev = 0;
+  ICB_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
-  auto it = memo.find(kern);
-  if(it != memo.end())
+  auto &m = memo[dev & 63];
+  auto it = m.find(kern);
+  if(it != m.end())
     return it->second;
   // static + dynamic shared memory past 48 KB needs the opt-in
   if(smem > 0)
@@ -847,7 +851,7 @@ static int resident_ctas(const void *kern, int threads, int smem)
     (void)cudaGetLastError();
     n = 1;
   }
-  return memo[kern] = n * num_sms();
+  return m[kern] = n * num_sms();
 }
 
 /// z planes per CTA of the Hex8 kernels: `tiles` x-y tiles, `resident` CTAs

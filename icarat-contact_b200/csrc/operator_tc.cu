@@ -547,12 +547,10 @@ void launch_tc_mode(const Dims &d, const float *K, const float *E, const float *
   KMat<float, 24> km;
   std::copy(K, K + 576, km.k);
   auto kern = x.dotRed ? k_matvec_h8_tc<true, MODE> : k_matvec_h8_tc<false, MODE>;
-  static const int smem = [&] {
-    const int bytes = int(sizeof(TcSmem)) + 1024;
-    cudaFuncSetAttribute(k_matvec_h8_tc<true, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_matvec_h8_tc<false, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    return bytes;
-  }();
+  // the shared-memory opt-in is a per-device attribute: set it on every call
+  // (same value from every thread, so concurrent launches never see less)
+  const int smem = int(sizeof(TcSmem)) + 1024;
+  ICB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   ICB_REQUIRE(3 * d.ld < (1LL << 31), "grid too large for the tensor-core operator's 32-bit offsets");
   TcWork w;
   w.bx = (d.sx + TX - 2) / (TX - 1);

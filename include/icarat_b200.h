@@ -76,7 +76,7 @@ typedef struct
   int maxit;      /* Solvers maxIter_ (10000)                               */
   double inner_tol; /* reserved (0)                                       */
   int mg_smooth;  /* GMG: Jacobi sweeps before and after (0 = default)      */
-  int mg_coarse_dofs; /* GMG: coarsen while the grid has more DOFs (0 = default) */
+  int mg_coarse_dofs; /* GMG: coarsen while the grid has more DOFs (0 = 160, at most 1024) */
 } icb_solve_opts;
 
 typedef struct
