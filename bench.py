@@ -557,6 +557,8 @@ def workload_batched(args):
     import cases
     import icarat_b200 as icb
     N, steps = args.instances, args.loop_steps
+    if args.blocking_sync:
+        icb.set_option("blocking_sync", 1)
     rng = np.random.default_rng(4)
     insts = [cases.random_instance2d(rng) for _ in range(N)]
     # several GPUs: every rank runs its footprint-balanced share, no exchange
@@ -759,6 +761,8 @@ def main():
                     help="c2 (default): the bench line; the others print their own line")
     ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 / operator grid override")
     ap.add_argument("--mma-steps", type=int, default=20)
+    ap.add_argument("--blocking-sync", action="store_true",
+                    help="batched: host waits sleep instead of spinning")
     ap.add_argument("--loop-only", action="store_true",
                     help="c3: only the MMA loop (no initial-design solves, no CPU sample)")
     ap.add_argument("--tc", type=int, default=0, choices=[0, 1],

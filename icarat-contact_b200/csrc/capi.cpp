@@ -21,7 +21,13 @@ namespace icb
 static thread_local std::string g_err;
 static std::atomic<long long> g_launches{0};
 void set_error(const std::string &m) { g_err = m; }
-void count_launch(long long n) { g_launches += n; }
+static thread_local long long t_launches = 0;
+void count_launch(long long n)
+{
+  g_launches += n;
+  t_launches += n;
+}
+long long thread_launch_count() { return t_launches; }
 } // namespace icb
 
 #define ICB_API_BEGIN try {
@@ -593,6 +599,14 @@ int icb_set_option(const char *name, long long value)
     set_tc_operator(value != 0);
   else if(n == "hex8_modal")
     set_hex8_modal(value != 0);
+  else if(n == "blocking_sync")
+  {
+    // host waits sleep instead of spinning (cudaDeviceScheduleBlockingSync);
+    // a device flag, so it must precede the first context on this device
+    int dev = 0;
+    ICB_CUDA(cudaGetDevice(&dev));
+    ICB_CUDA(cudaSetDeviceFlags(value ? cudaDeviceScheduleBlockingSync : cudaDeviceScheduleAuto));
+  }
   else
     need(false, "unknown option");
   ICB_API_END

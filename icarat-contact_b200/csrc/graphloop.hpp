@@ -1,0 +1,60 @@
+// graphloop.hpp -- a CUDA graph whose body repeats on the device while a
+// kernel at the end of the body says so (a conditional WHILE node): one
+// graph launch and one host wait run a Krylov solve or a bisection to its
+// end, with no wasted gated iterations and no host round trip in between.
+#pragma once
+#include <functional>
+
+#include "icb_internal.hpp"
+
+namespace icb
+{
+/// the loop condition as the last kernel of a body sees it: `on` is 0 when
+/// the kernel runs outside a WHILE graph
+struct LoopCtl
+{
+  cudaGraphConditionalHandle h = 0;
+  int on = 0;
+};
+
+struct WhileGraph
+{
+  cudaGraphExec_t exec = nullptr;
+  long long bodyNodes = 0; ///< nodes of one pass of the body (for icb_launch_count)
+
+  WhileGraph() = default;
+  WhileGraph(const WhileGraph &) = delete;
+  WhileGraph &operator=(const WhileGraph &) = delete;
+  ~WhileGraph() { reset(); }
+  void reset();
+  /// record the body by stream capture: body(cs, L) launches one pass on cs;
+  /// its last kernel sets the condition through L (loop_end_* / loop_stop)
+  void build(const std::function<void(cudaStream_t, const LoopCtl &)> &body);
+  void launch(cudaStream_t s) const;
+};
+
+#ifdef __CUDACC__
+/// one thread, at the end of a Krylov body: count the pass (st->pad, zeroed by
+/// the solver's init kernel), stop a loop that ran st->maxit + 2 passes
+/// without stopping (ICB_ERR_MAXITER), and repeat while !st->stop
+__device__ __forceinline__ void loop_end_krylov(const LoopCtl &L, KState *st)
+{
+  if(!L.on)
+    return;
+  const int n = ++st->pad;
+  if(!st->stop && (long long)n >= (long long)st->maxit + 2)
+  {
+    st->stop = 1;
+    st->status = ICB_ERR_MAXITER;
+  }
+  cudaGraphSetConditional(L.h, st->stop ? 0u : 1u);
+}
+/// one thread of a body's last kernel that found the loop already finished
+__device__ __forceinline__ void loop_stop(const LoopCtl &L)
+{
+  if(L.on)
+    cudaGraphSetConditional(L.h, 0u);
+}
+#endif
+
+} // namespace icb

@@ -17,6 +17,8 @@ namespace icb
 void set_error(const std::string &msg);
 /// add to the process-wide count of kernel launches (icb_launch_count)
 void count_launch(long long n = 1);
+/// this host thread's share of that count (to undo launches recorded by a capture)
+long long thread_launch_count();
 struct Error
 {
   int code;

@@ -4,9 +4,9 @@
 //   B  r -= alpha q       (fused r.r and r.D^-1 r reductions, convergence test)
 //   C  x += alpha p ; p = D^-1 r + beta p
 // All scalars live in a device KState; the last block of each reduction
-// updates them, so no host round trip is needed inside the loop.  A batch of
-// iterations is captured once as a CUDA graph and relaunched; kernels after
-// convergence see `stop` and return at once.
+// updates them, so no host round trip is needed inside the loop.  One
+// iteration is captured once as the body of a CUDA graph's conditional WHILE
+// node, which the device repeats until `stop` is set.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -41,6 +41,7 @@ struct FinInit
     st->tol = tol;
     st->thr = fmax(tol * tol * t[0], DBL_MIN);
     st->iter = 0;
+    st->pad = 0;
     st->matvecs = 0;
     st->maxit = maxit;
     st->conv = 0;
@@ -139,29 +140,37 @@ __global__ void k_pcg_r(long long n, T *__restrict__ r, const T *__restrict__ q,
 struct FinXP
 {
   KState *st;
+  LoopCtl L;
   __device__ void operator()(const double *) const
   {
     if(st->conv)
-    {
       st->stop = 1;
-      return;
-    }
-    st->iter++;
-    if(st->iter >= st->maxit)
+    else
     {
-      st->status = ICB_ERR_MAXITER;
-      st->stop = 1;
+      st->iter++;
+      if(st->iter >= st->maxit)
+      {
+        st->status = ICB_ERR_MAXITER;
+        st->stop = 1;
+      }
     }
+    loop_end_krylov(L, st);
   }
 };
 
+/// the last kernel of an iteration; inside the solve graph it also decides
+/// whether the device runs the next one
 template <typename T>
 __global__ void k_pcg_xp(long long n, T *__restrict__ x, T *__restrict__ p,
                          const T *__restrict__ r, const T *__restrict__ dinv, RedScratch red,
-                         KState *st)
+                         KState *st, LoopCtl L)
 {
   if(st->stop)
+  {
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+      loop_stop(L);
     return;
+  }
   const T a = T(st->alpha), bt = T(st->beta);
   const bool conv = st->conv;
   for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -173,7 +182,7 @@ __global__ void k_pcg_xp(long long n, T *__restrict__ x, T *__restrict__ p,
       p[i] = dinv[i] * r[i] + bt * pi;
   }
   double v[1] = {0.0};
-  block_reduce<1>(v, red, FinXP{st});
+  block_reduce<1>(v, red, FinXP{st, L});
 }
 
 __global__ void k_dot(long long n, const double *__restrict__ a, const double *__restrict__ b,
@@ -259,8 +268,6 @@ template <typename T> JacobiPcg<T>::JacobiPcg(const Dims &dims, cudaStream_t s) 
 
 template <typename T> JacobiPcg<T>::~JacobiPcg()
 {
-  if(exec)
-    cudaGraphExecDestroy(exec);
   if(hst)
     cudaFreeHost(hst);
 }
@@ -281,6 +288,9 @@ int JacobiPcg<T>::solve(const T *K, const T *E, const uint8_t *fix, const T *inv
   return solveOp(op, K, E, fix, invdiag, b, x, tol, maxit, s, info);
 }
 
+/// Jacobi-PCG iterations per pass of the solve graph's WHILE body
+constexpr int kUnroll = 4;
+
 template <typename T>
 int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const void *opKey0,
                           const void *opKey1, const void *opKey2, const T *invdiag, const T *b,
@@ -295,49 +305,37 @@ int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const voi
   ICB_CUDA(cudaGetLastError());
   count_launch();
 
-  // (re)capture the batch graph when the operands changed
+  // (re)capture the solve graph when the operands changed
   const void *key[6] = {opKey0, opKey1, opKey2, invdiag, x, (const void *)s};
-  bool same = exec != nullptr;
+  bool same = loop.exec != nullptr;
   for(int i = 0; i < 6 && same; i++)
     same = key[i] == graphKey[i];
   if(!same)
   {
-    if(exec)
-      cudaGraphExecDestroy(exec);
-    exec = nullptr;
-    batch = 16;
-    cudaStream_t cs;
-    ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    cudaGraph_t g;
-    ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    for(int it = 0; it < batch; it++)
-    {
-      op(cs); // q = K p with the fused p.q reduction into dots[0]
-      k_pcg_r<T><<<nb, VB, 0, cs>>>(n, r.p, q.p, invdiag, dots.p, red, st.p);
-      k_pcg_xp<T><<<nb, VB, 0, cs>>>(n, x, p.p, r.p, invdiag, red, st.p);
-    }
-    ICB_CUDA(cudaStreamEndCapture(cs, &g));
-    count_launch(-(long long)batch); // operator launches recorded during capture
-    ICB_CUDA(cudaGraphInstantiate(&exec, g, 0));
-    cudaGraphDestroy(g);
-    cudaStreamDestroy(cs);
+    KState *stp = st.p;
+    const long long before = thread_launch_count();
+    // four iterations per pass of the WHILE body: the device's turn-around
+    // between passes (~3.4 us) would otherwise cost ~5 % of an iteration of
+    // three kernels; the iterations after the stop inside a pass are gated
+    loop.build([&](cudaStream_t cs, const LoopCtl &L) {
+      for(int u = 0; u < kUnroll; u++)
+      {
+        op(cs); // q = K p with the fused p.q reduction into dots[0]
+        k_pcg_r<T><<<nb, VB, 0, cs>>>(n, r.p, q.p, invdiag, dots.p, red, stp);
+        k_pcg_xp<T><<<nb, VB, 0, cs>>>(n, x, p.p, r.p, invdiag, red, stp,
+                                       u == kUnroll - 1 ? L : LoopCtl{});
+      }
+    });
+    count_launch(before - thread_launch_count()); // recorded, not launched
     for(int i = 0; i < 6; i++)
       graphKey[i] = key[i];
   }
-  // the batches: poll the device stop flag once per graph launch
-  long long launched = 0;
-  for(;;)
-  {
-    ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
-    ICB_CUDA(cudaStreamSynchronize(s));
-    if(hst->stop)
-      break;
-    if(launched > (long long)maxit + batch)
-      break; // device bookkeeping stops at maxit; this is a host-side backstop
-    ICB_CUDA(cudaGraphLaunch(exec, s));
-    launched += batch;
-    count_launch(3LL * batch);
-  }
+  // the whole solve: one launch, one wait (the device stops at maxit, and the
+  // loop itself after maxit + 2 passes)
+  loop.launch(s);
+  ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
+  count_launch((long long)hst->pad * loop.bodyNodes);
   ICB_CUDA(cudaEventRecord(e1, s));
   ICB_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -383,7 +381,7 @@ int pcg_run_external(const Dims &d, const double *K, const double *E, const uint
     {
       launch_matvec<double>(d, K, E, p, q, fix, s, &red, dotOut, st);
       k_pcg_r<double><<<nb, VB, 0, s>>>(n, r, q, invdiag, dotOut, red, st);
-      k_pcg_xp<double><<<nb, VB, 0, s>>>(n, x, p, r, invdiag, red, st);
+      k_pcg_xp<double><<<nb, VB, 0, s>>>(n, x, p, r, invdiag, red, st, LoopCtl{});
       count_launch(2);
     }
     ICB_CUDA(cudaGetLastError());

@@ -2,6 +2,7 @@
 #pragma once
 #include <functional>
 
+#include "graphloop.hpp"
 #include "icb_internal.hpp"
 
 namespace icb
@@ -12,8 +13,9 @@ namespace icb
 /// called by Solvers::EigenCG (src/analysis/solver/solvers.cpp:64-92):
 /// x0 = 0, stop when ||r||^2 < max(tol^2 ||b||^2, DBL_MIN), the iteration
 /// count excludes the converging iteration.  Every scalar stays on the device;
-/// the host only polls the stop flag once per batch of iterations, and a
-/// batch is one CUDA-graph launch.
+/// the iterations run in a CUDA graph whose conditional WHILE node repeats
+/// them until the device's stop flag is set: one launch and one host wait
+/// per solve.
 template <typename T> struct JacobiPcg
 {
   Dims d;
@@ -24,14 +26,13 @@ template <typename T> struct JacobiPcg
   DevBuf<unsigned> counter;
   RedScratch red;
   KState *hst = nullptr; ///< pinned mirror
-  cudaGraphExec_t exec = nullptr;
-  int batch = 0;
+  WhileGraph loop;
   const void *graphKey[6] = {};
 
   JacobiPcg(const Dims &dims, cudaStream_t s);
   ~JacobiPcg();
   /// solve K(E) x = b; K: host pointer to the unit element matrix of this
-  /// level (captured by value into the batch graph: keep it stable).
+  /// level (captured by value into the solve graph: keep it stable).
   int solve(const T *K, const T *E, const uint8_t *fix, const T *invdiag, const T *b, T *x,
             double tol, int maxit, cudaStream_t s, icb_solve_info *info);
   /// the same iteration with any operator: `op(stream)` must compute q = A p

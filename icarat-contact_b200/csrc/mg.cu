@@ -26,13 +26,15 @@
 //  * coarsest level (<= 160 DOFs by default): dense FP64 inverse built on
 //    the device (one CTA, Gauss-Jordan in shared memory), applied as a
 //    dense product.
-// The whole V-cycle is a fixed kernel sequence, so a batch of PCG
-// iterations including their V-cycles is captured as one CUDA graph.
+// The whole V-cycle is a fixed kernel sequence, so one PCG iteration with
+// its V-cycle is captured as the body of a CUDA graph's conditional WHILE
+// node, which the device repeats until the stop flag is set.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
 
+#include "graphloop.hpp"
 #include "mg.hpp"
 #include "reduce.cuh"
 
@@ -337,6 +339,7 @@ struct FinInitMg
     st->tol = tol;
     st->thr = fmax(tol * tol * t[0], DBL_MIN);
     st->iter = 0;
+    st->pad = 0;
     st->matvecs = 0;
     st->maxit = maxit;
     st->conv = 0;
@@ -496,28 +499,36 @@ __global__ void k_mg_rz(long long n, const TK *__restrict__ r, const TP *__restr
 struct FinXPmg
 {
   KState *st;
+  LoopCtl L;
   __device__ void operator()(const double *) const
   {
     if(st->conv)
-    {
       st->stop = 1;
-      return;
-    }
-    st->iter++;
-    if(st->iter >= st->maxit)
+    else
     {
-      st->status = ICB_ERR_MAXITER;
-      st->stop = 1;
+      st->iter++;
+      if(st->iter >= st->maxit)
+      {
+        st->status = ICB_ERR_MAXITER;
+        st->stop = 1;
+      }
     }
+    loop_end_krylov(L, st);
   }
 };
 
+/// the last kernel of an iteration; inside the solve graph it also decides
+/// whether the device runs the next one
 template <typename TK, typename TP>
 __global__ void k_mg_xp(long long n, TK *__restrict__ x, TK *__restrict__ p,
-                        const TP *__restrict__ z, RedScratch red, KState *st)
+                        const TP *__restrict__ z, RedScratch red, KState *st, LoopCtl L)
 {
   if(st->stop)
+  {
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+      loop_stop(L);
     return;
+  }
   const TK a = TK(st->alpha), bt = TK(st->beta);
   const bool conv = st->conv;
   for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -529,7 +540,7 @@ __global__ void k_mg_xp(long long n, TK *__restrict__ x, TK *__restrict__ p,
       p[i] = TK(z[i]) + bt * pi;
   }
   double v[1] = {0.0};
-  block_reduce<1>(v, red, FinXPmg{st});
+  block_reduce<1>(v, red, FinXPmg{st, L});
 }
 } // namespace
 
@@ -604,15 +615,11 @@ template <typename TK, typename TP> struct MgPcg
   DevBuf<unsigned> counter;
   RedScratch red;
   KState *hst = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  WhileGraph loop; ///< one FCG iteration, repeated on the device until stop
   const void *key[4] = {};
-  int batch = 8;
-  long long graphNodes = 0;
 
   ~MgPcg()
   {
-    if(exec)
-      cudaGraphExecDestroy(exec);
     if(hst)
       cudaFreeHost(hst);
   }
@@ -873,7 +880,7 @@ template <typename TK, typename TP> struct MgPcg
       ICB_CUDA(cudaMemcpyAsync(out, cur, sizeof(TP) * m, cudaMemcpyDeviceToDevice, s));
   }
 
-  void iteration(TK *x, cudaStream_t s)
+  void iteration(TK *x, cudaStream_t s, const LoopCtl &L)
   {
     const Dims &d = lv[0].d;
     int nb = vblocks(n);
@@ -885,7 +892,7 @@ template <typename TK, typename TP> struct MgPcg
     k_mg_r<TK, TP><<<nb, VB, 0, s>>>(n, r.p, same() ? nullptr : rP.p, q.p, z.p, dots.p, red, st.p);
     level(0, rin(), z.p, s, st.p);
     k_mg_rz<TK, TP><<<nb, VB, 0, s>>>(n, r.p, z.p, red, st.p);
-    k_mg_xp<TK, TP><<<nb, VB, 0, s>>>(n, x, p.p, z.p, red, st.p);
+    k_mg_xp<TK, TP><<<nb, VB, 0, s>>>(n, x, p.p, z.p, red, st.p, L);
     count_launch(3);
   }
 
@@ -900,43 +907,22 @@ template <typename TK, typename TP> struct MgPcg
     count_launch();
     ICB_CUDA(cudaGetLastError());
     const void *k[4] = {x, Ek, lv[0].E, (const void *)s};
-    bool same_ = exec != nullptr;
+    bool same_ = loop.exec != nullptr;
     for(int i = 0; i < 4 && same_; i++)
       same_ = k[i] == key[i];
     if(!same_)
     {
-      if(exec)
-        cudaGraphExecDestroy(exec);
-      exec = nullptr;
-      cudaStream_t cs;
-      ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-      long long before = 0;
-      cudaGraph_t g;
-      ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      for(int it = 0; it < batch; it++)
-        iteration(x, cs);
-      ICB_CUDA(cudaStreamEndCapture(cs, &g));
-      ICB_CUDA(cudaGraphInstantiate(&exec, g, 0));
-      size_t nn = 0;
-      cudaGraphGetNodes(g, nullptr, &nn);
-      cudaGraphDestroy(g);
-      cudaStreamDestroy(cs);
-      (void)before;
-      graphNodes = (long long)nn;
+      const long long before = thread_launch_count();
+      loop.build([&](cudaStream_t cs, const LoopCtl &L) { iteration(x, cs, L); });
+      count_launch(before - thread_launch_count()); // recorded, not launched
       for(int i = 0; i < 4; i++)
         key[i] = k[i];
     }
-    long long launched = 0;
-    for(;;)
-    {
-      ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
-      ICB_CUDA(cudaStreamSynchronize(s));
-      if(hst->stop || launched > (long long)maxit + batch)
-        break;
-      ICB_CUDA(cudaGraphLaunch(exec, s));
-      launched += batch;
-      count_launch(graphNodes);
-    }
+    // the whole solve: one launch, one wait
+    loop.launch(s);
+    ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    count_launch((long long)hst->pad * loop.bodyNodes);
     if(info)
     {
       info->iters = hst->iter;

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <vector>
 
+#include "graphloop.hpp"
 #include "opt.hpp"
 #include "reduce.cuh"
 
@@ -139,8 +140,11 @@ __device__ __forceinline__ double oc_candidate(double x, double df, double dg, d
 struct FinOc
 {
   OcState *st;
+  LoopCtl L;
   __device__ void operator()(const double *t) const
   {
+    // the lambda just evaluated, before the bisection moves it
+    st->lastLam = st->lam;
     // OCSolver.hpp:52-60: lambda goes up while the candidate's volume exceeds g
     if(t[0] - st->g > 0.0)
       st->l0 = st->lam;
@@ -152,6 +156,14 @@ struct FinOc
       st->done = 1;
     else
       st->lam = 0.5 * (st->l1 + st->l0);
+    // inside the update graph: repeat while not done (at most maxiter + 1
+    // passes, counted in pad)
+    if(L.on)
+    {
+      if(++st->pad > st->maxiter)
+        st->done = 1;
+      cudaGraphSetConditional(L.h, st->done ? 0u : 1u);
+    }
   }
 };
 
@@ -161,10 +173,14 @@ __global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__r
                           const double *__restrict__ df, const double *__restrict__ dg,
                           const double *__restrict__ xmin, const double *__restrict__ xmax,
                           const double *__restrict__ vol, OcParams P, RedScratch red,
-                          OcState *st)
+                          OcState *st, LoopCtl L)
 {
   if(st->done)
+  {
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+      loop_stop(L);
     return;
+  }
   const double lam = st->lam;
   double v[1] = {0.0};
   for(long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < d.nel;
@@ -191,7 +207,7 @@ __global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__r
     double xh = P.beta > 0.0 ? thresh(xf, P.beta, P.T) : xf;
     v[0] += xh * vol[e];
   }
-  block_reduce<1>(v, red, FinOc{st});
+  block_reduce<1>(v, red, FinOc{st, L});
 }
 
 __global__ void k_oc_init(OcState *st, double g, OcParams P)
@@ -201,6 +217,7 @@ __global__ void k_oc_init(OcState *st, double g, OcParams P)
   st->lambdaeps = 1.0e-5;
   st->maxiter = 100;
   st->counter = 0;
+  st->pad = 0;
   st->g = g;
   st->done = 0;
   st->vol = 0.0;
@@ -225,12 +242,6 @@ __global__ void k_oc_final(long long n, double *__restrict__ x, const double *__
   x[e] = oc_candidate(x[e], df[e], dg[e], lam, P.eta, P.move, xmin[e], xmax[e]);
 }
 
-__global__ void k_oc_latch(OcState *st)
-{
-  // record the lambda just evaluated before the bisection moves it
-  if(!st->done)
-    st->lastLam = st->lam;
-}
 
 // ----------------------------------------------------------------- MMA ----
 struct FinSum2
@@ -659,8 +670,6 @@ OcUpdater::OcUpdater(const Dims &dims, cudaStream_t s) : d(dims)
 }
 OcUpdater::~OcUpdater()
 {
-  if(exec)
-    cudaGraphExecDestroy(exec);
   if(hst)
     cudaFreeHost(hst);
 }
@@ -678,40 +687,29 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
   int nnb = cone ? cone->nnb : 0;
   OcParams Pp = P;
   Pp.useFilter = cone != nullptr;
-  // graph of the 100 bisection steps (each gated on done), rebuilt when the
-  // operands or parameters change
+  // graph of the bisection: one step as the body of a conditional WHILE node
+  // that the device repeats until done (at most maxiter = 100 steps), rebuilt
+  // when the operands or parameters change
   const void *k[9] = {cone, x, df, dg, xmin, xmax, vol, (const void *)s, nullptr};
-  bool same = exec != nullptr && std::memcmp(&Pp, &keyP, sizeof(OcParams)) == 0;
+  bool same = loop.exec != nullptr && std::memcmp(&Pp, &keyP, sizeof(OcParams)) == 0;
   for(int i = 0; i < 9 && same; i++)
     same = k[i] == key[i];
   if(!same)
   {
-    if(exec)
-      cudaGraphExecDestroy(exec);
-    exec = nullptr;
-    cudaStream_t cs;
-    ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    cudaGraph_t gr;
-    ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    for(int it = 0; it < 100; it++)
-    {
-      k_oc_latch<<<1, 1, 0, cs>>>(st.p);
-      k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, Pp, red, st.p);
-    }
-    k_oc_final<<<unsigned((d.nel + 255) / 256), 256, 0, cs>>>(d.nel, x, df, dg, xmin, xmax, Pp,
-                                                             st.p);
-    ICB_CUDA(cudaStreamEndCapture(cs, &gr));
-    ICB_CUDA(cudaGraphInstantiate(&exec, gr, 0));
-    cudaGraphDestroy(gr);
-    cudaStreamDestroy(cs);
+    loop.build([&](cudaStream_t cs, const LoopCtl &L) {
+      k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, Pp, red, st.p,
+                                   L);
+    });
     for(int i = 0; i < 9; i++)
       key[i] = k[i];
     keyP = Pp;
   }
-  ICB_CUDA(cudaGraphLaunch(exec, s));
-  count_launch(201);
+  loop.launch(s);
+  k_oc_final<<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d.nel, x, df, dg, xmin, xmax, Pp, st.p);
+  ICB_CUDA(cudaGetLastError());
   ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(OcState), cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
+  count_launch(1 + (long long)hst->pad * loop.bodyNodes);
   return hst->counter;
 }
 

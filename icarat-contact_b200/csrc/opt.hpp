@@ -2,6 +2,7 @@
 #pragma once
 #include <cstring>
 
+#include "graphloop.hpp"
 #include "icb_internal.hpp"
 
 namespace icb
@@ -53,7 +54,7 @@ struct OcUpdater
   DevBuf<unsigned> counter;
   RedScratch red;
   OcState *hst = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  WhileGraph loop; ///< one bisection step, repeated on the device until done
   const void *key[9] = {};
   OcParams keyP;
 
