@@ -543,6 +543,7 @@ def _c3_loop(args, icb, g, n, steps, rho0, out, err, speed, cpu):
                                  "helmholtz_R": 3.0, "volfrac": 0.3, "steps": steps, "tol": TOL},
                       "latency_ms": {"p50": 1e3 * float(np.median(its)),
                                      "p99": 1e3 * float(np.quantile(its, 0.99))},
+                      "loop_seconds": dt, "step_seconds_sum": float(its.sum()),
                       "solve_initial_design": out, "mixed_vs_fp64": err, "speedups": speed,
                       "cpu_baseline": cpu, "compliance_history": hist.tolist()}), flush=True)
     return 0
@@ -557,8 +558,6 @@ def workload_batched(args):
     import cases
     import icarat_b200 as icb
     N, steps = args.instances, args.loop_steps
-    if args.blocking_sync:
-        icb.set_option("blocking_sync", 1)
     rng = np.random.default_rng(4)
     insts = [cases.random_instance2d(rng) for _ in range(N)]
     # several GPUs: every rank runs its footprint-balanced share, no exchange
@@ -761,8 +760,9 @@ def main():
                     help="c2 (default): the bench line; the others print their own line")
     ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 / operator grid override")
     ap.add_argument("--mma-steps", type=int, default=20)
-    ap.add_argument("--blocking-sync", action="store_true",
-                    help="batched: host waits sleep instead of spinning")
+    ap.add_argument("--host-loops", action="store_true",
+                    help="run the multigrid PCG and OC loops as host-polled graph batches "
+                         "(icb option device_loops = 0), so a profiler sees every kernel")
     ap.add_argument("--loop-only", action="store_true",
                     help="c3: only the MMA loop (no initial-design solves, no CPU sample)")
     ap.add_argument("--tc", type=int, default=0, choices=[0, 1],
@@ -777,6 +777,9 @@ def main():
     ap.add_argument("--iter-scale", type=float, default=0.2, help="serving: scale on U[50,200] steps")
     ap.add_argument("--slots", type=int, default=8)
     args = ap.parse_args()
+    if args.host_loops and args.impl == "ours":
+        import icarat_b200 as icb
+        icb.set_option("device_loops", 0)
     if args.profile_operator:
         return profile_operator(args)
     if args.workload != "c2" and args.impl == "ours":

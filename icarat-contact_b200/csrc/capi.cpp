@@ -9,6 +9,7 @@
 #include <cstring>
 #include <string>
 
+#include "graphloop.hpp"
 #include "mg.hpp"
 #include "problem.hpp"
 
@@ -599,14 +600,8 @@ int icb_set_option(const char *name, long long value)
     set_tc_operator(value != 0);
   else if(n == "hex8_modal")
     set_hex8_modal(value != 0);
-  else if(n == "blocking_sync")
-  {
-    // host waits sleep instead of spinning (cudaDeviceScheduleBlockingSync);
-    // a device flag, so it must precede the first context on this device
-    int dev = 0;
-    ICB_CUDA(cudaGetDevice(&dev));
-    ICB_CUDA(cudaSetDeviceFlags(value ? cudaDeviceScheduleBlockingSync : cudaDeviceScheduleAuto));
-  }
+  else if(n == "device_loops")
+    set_device_loops(value != 0);
   else
     need(false, "unknown option");
   ICB_API_END
@@ -621,6 +616,8 @@ long long icb_get_option(const char *name)
     return tc_operator_enabled() ? 1 : 0;
   if(n == "hex8_modal")
     return hex8_modal_enabled() ? 1 : 0;
+  if(n == "device_loops")
+    return device_loops_enabled() ? 1 : 0;
   if(n == "tc_timeouts")
     return (long long)tc_timeouts();
   return -1;

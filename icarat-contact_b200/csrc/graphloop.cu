@@ -1,20 +1,60 @@
 // graphloop.cu -- conditional WHILE graphs for the device-side solver loops.
+#include <algorithm>
+#include <atomic>
+
 #include "graphloop.hpp"
 
 namespace icb
 {
+
+static std::atomic<bool> g_device_loops{true};
+bool device_loops_enabled() { return g_device_loops.load(); }
+void set_device_loops(bool on) { g_device_loops = on; }
 
 void WhileGraph::reset()
 {
   if(exec)
     cudaGraphExecDestroy(exec);
   exec = nullptr;
-  bodyNodes = 0;
+  graphNodes = 0;
 }
 
-void WhileGraph::build(const std::function<void(cudaStream_t, const LoopCtl &)> &body)
+void WhileGraph::build(const std::function<void(cudaStream_t, const LoopCtl &)> &body,
+                       bool onDevice, int hostBatch)
 {
   reset();
+  device = onDevice;
+  batch = onDevice ? 1 : std::max(1, hostBatch);
+  if(!onDevice)
+  {
+    cudaStream_t cs = nullptr;
+    ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    try
+    {
+      ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      for(int k = 0; k < batch; k++)
+        body(cs, LoopCtl{});
+      ICB_CUDA(cudaStreamEndCapture(cs, &g));
+      size_t nn = 0;
+      ICB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+      graphNodes = (long long)nn;
+      ICB_CUDA(cudaGraphInstantiate(&exec, g, 0));
+    }
+    catch(...)
+    {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(cs, &junk);
+      if(g)
+        cudaGraphDestroy(g);
+      cudaStreamDestroy(cs);
+      exec = nullptr;
+      throw;
+    }
+    cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    return;
+  }
   cudaGraph_t g = nullptr;
   ICB_CUDA(cudaGraphCreate(&g, 0));
   cudaStream_t cs = nullptr;
@@ -40,7 +80,7 @@ void WhileGraph::build(const std::function<void(cudaStream_t, const LoopCtl &)> 
     ICB_CUDA(cudaStreamEndCapture(cs, &captured));
     size_t nn = 0;
     ICB_CUDA(cudaGraphGetNodes(bodyG, nullptr, &nn));
-    bodyNodes = (long long)nn;
+    graphNodes = (long long)nn;
     ICB_CUDA(cudaGraphInstantiate(&exec, g, 0));
   }
   catch(...)

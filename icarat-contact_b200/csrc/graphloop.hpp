@@ -17,10 +17,19 @@ struct LoopCtl
   int on = 0;
 };
 
+/// A solver loop as a CUDA graph, in one of two forms: on the device, the
+/// body is a conditional WHILE node that repeats until the body's last kernel
+/// clears the condition (one launch and one host wait per solve); from the
+/// host, the graph holds `batch` passes of the body and is relaunched until
+/// a polled device flag says stop (the kernels after the stop are gated).
+/// Profilers that cannot follow conditional nodes see every kernel of the
+/// host form.
 struct WhileGraph
 {
   cudaGraphExec_t exec = nullptr;
-  long long bodyNodes = 0; ///< nodes of one pass of the body (for icb_launch_count)
+  bool device = true;      ///< the WHILE-node form
+  int batch = 1;           ///< passes per launch in the host form
+  long long graphNodes = 0; ///< nodes per launch (host) or per pass (device)
 
   WhileGraph() = default;
   WhileGraph(const WhileGraph &) = delete;
@@ -28,10 +37,17 @@ struct WhileGraph
   ~WhileGraph() { reset(); }
   void reset();
   /// record the body by stream capture: body(cs, L) launches one pass on cs;
-  /// its last kernel sets the condition through L (loop_end_* / loop_stop)
-  void build(const std::function<void(cudaStream_t, const LoopCtl &)> &body);
+  /// its last kernel sets the condition through L (loop_end_* / loop_stop;
+  /// L.on is 0 in the host form)
+  void build(const std::function<void(cudaStream_t, const LoopCtl &)> &body, bool onDevice,
+             int hostBatch);
   void launch(cudaStream_t s) const;
 };
+
+/// process-wide choice of the loop form for the multigrid PCG and the OC
+/// bisection (icb_set_option "device_loops"; default on)
+bool device_loops_enabled();
+void set_device_loops(bool on);
 
 #ifdef __CUDACC__
 /// one thread, at the end of a Krylov body: count the pass (st->pad, zeroed by

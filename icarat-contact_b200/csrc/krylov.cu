@@ -4,9 +4,9 @@
 //   B  r -= alpha q       (fused r.r and r.D^-1 r reductions, convergence test)
 //   C  x += alpha p ; p = D^-1 r + beta p
 // All scalars live in a device KState; the last block of each reduction
-// updates them, so no host round trip is needed inside the loop.  One
-// iteration is captured once as the body of a CUDA graph's conditional WHILE
-// node, which the device repeats until `stop` is set.
+// updates them, so no host round trip is needed inside the loop.  A batch of
+// iterations is captured once as a CUDA graph and relaunched; kernels after
+// convergence see `stop` and return at once.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -288,9 +288,6 @@ int JacobiPcg<T>::solve(const T *K, const T *E, const uint8_t *fix, const T *inv
   return solveOp(op, K, E, fix, invdiag, b, x, tol, maxit, s, info);
 }
 
-/// Jacobi-PCG iterations per pass of the solve graph's WHILE body
-constexpr int kUnroll = 4;
-
 template <typename T>
 int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const void *opKey0,
                           const void *opKey1, const void *opKey2, const T *invdiag, const T *b,
@@ -305,7 +302,10 @@ int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const voi
   ICB_CUDA(cudaGetLastError());
   count_launch();
 
-  // (re)capture the solve graph when the operands changed
+  // (re)capture the batch graph when the operands changed: 16 iterations per
+  // launch, polled from the host (a device-side WHILE loop was measured at
+  // the same speed here, 251 against 249 ms for the c2 solve, and profilers
+  // cannot follow its kernels)
   const void *key[6] = {opKey0, opKey1, opKey2, invdiag, x, (const void *)s};
   bool same = loop.exec != nullptr;
   for(int i = 0; i < 6 && same; i++)
@@ -314,28 +314,30 @@ int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const voi
   {
     KState *stp = st.p;
     const long long before = thread_launch_count();
-    // four iterations per pass of the WHILE body: the device's turn-around
-    // between passes (~3.4 us) would otherwise cost ~5 % of an iteration of
-    // three kernels; the iterations after the stop inside a pass are gated
-    loop.build([&](cudaStream_t cs, const LoopCtl &L) {
-      for(int u = 0; u < kUnroll; u++)
-      {
-        op(cs); // q = K p with the fused p.q reduction into dots[0]
-        k_pcg_r<T><<<nb, VB, 0, cs>>>(n, r.p, q.p, invdiag, dots.p, red, stp);
-        k_pcg_xp<T><<<nb, VB, 0, cs>>>(n, x, p.p, r.p, invdiag, red, stp,
-                                       u == kUnroll - 1 ? L : LoopCtl{});
-      }
-    });
+    loop.build(
+        [&](cudaStream_t cs, const LoopCtl &L) {
+          op(cs); // q = K p with the fused p.q reduction into dots[0]
+          k_pcg_r<T><<<nb, VB, 0, cs>>>(n, r.p, q.p, invdiag, dots.p, red, stp);
+          k_pcg_xp<T><<<nb, VB, 0, cs>>>(n, x, p.p, r.p, invdiag, red, stp, L);
+        },
+        false, 16);
     count_launch(before - thread_launch_count()); // recorded, not launched
     for(int i = 0; i < 6; i++)
       graphKey[i] = key[i];
   }
-  // the whole solve: one launch, one wait (the device stops at maxit, and the
-  // loop itself after maxit + 2 passes)
-  loop.launch(s);
-  ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
-  ICB_CUDA(cudaStreamSynchronize(s));
-  count_launch((long long)hst->pad * loop.bodyNodes);
+  long long launched = 0;
+  for(;;)
+  {
+    ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    if(hst->stop)
+      break;
+    if(launched > (long long)maxit + loop.batch)
+      break; // device bookkeeping stops at maxit; this is a host-side backstop
+    loop.launch(s);
+    launched += loop.batch;
+    count_launch(loop.graphNodes);
+  }
   ICB_CUDA(cudaEventRecord(e1, s));
   ICB_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;

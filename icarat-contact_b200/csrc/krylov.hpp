@@ -13,9 +13,8 @@ namespace icb
 /// called by Solvers::EigenCG (src/analysis/solver/solvers.cpp:64-92):
 /// x0 = 0, stop when ||r||^2 < max(tol^2 ||b||^2, DBL_MIN), the iteration
 /// count excludes the converging iteration.  Every scalar stays on the device;
-/// the iterations run in a CUDA graph whose conditional WHILE node repeats
-/// them until the device's stop flag is set: one launch and one host wait
-/// per solve.
+/// the host only polls the stop flag once per batch of iterations, and a
+/// batch is one CUDA-graph launch.
 template <typename T> struct JacobiPcg
 {
   Dims d;
@@ -26,13 +25,13 @@ template <typename T> struct JacobiPcg
   DevBuf<unsigned> counter;
   RedScratch red;
   KState *hst = nullptr; ///< pinned mirror
-  WhileGraph loop;
+  WhileGraph loop; ///< host form: 16 iterations per launch
   const void *graphKey[6] = {};
 
   JacobiPcg(const Dims &dims, cudaStream_t s);
   ~JacobiPcg();
   /// solve K(E) x = b; K: host pointer to the unit element matrix of this
-  /// level (captured by value into the solve graph: keep it stable).
+  /// level (captured by value into the batch graph: keep it stable).
   int solve(const T *K, const T *E, const uint8_t *fix, const T *invdiag, const T *b, T *x,
             double tol, int maxit, cudaStream_t s, icb_solve_info *info);
   /// the same iteration with any operator: `op(stream)` must compute q = A p

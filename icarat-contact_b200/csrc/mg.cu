@@ -35,6 +35,7 @@
 #include <cstring>
 
 #include "graphloop.hpp"
+#include "loopcache.hpp"
 #include "mg.hpp"
 #include "reduce.cuh"
 
@@ -907,22 +908,40 @@ template <typename TK, typename TP> struct MgPcg
     count_launch();
     ICB_CUDA(cudaGetLastError());
     const void *k[4] = {x, Ek, lv[0].E, (const void *)s};
-    bool same_ = loop.exec != nullptr;
+    const bool dev = device_loops_enabled();
+    bool same_ = loop.exec != nullptr && loop.device == dev;
     for(int i = 0; i < 4 && same_; i++)
       same_ = k[i] == key[i];
     if(!same_)
     {
       const long long before = thread_launch_count();
-      loop.build([&](cudaStream_t cs, const LoopCtl &L) { iteration(x, cs, L); });
+      loop.build([&](cudaStream_t cs, const LoopCtl &L) { iteration(x, cs, L); }, dev, 8);
       count_launch(before - thread_launch_count()); // recorded, not launched
       for(int i = 0; i < 4; i++)
         key[i] = k[i];
     }
-    // the whole solve: one launch, one wait
-    loop.launch(s);
-    ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
-    ICB_CUDA(cudaStreamSynchronize(s));
-    count_launch((long long)hst->pad * loop.bodyNodes);
+    if(loop.device)
+    {
+      // the whole solve: one launch, one wait
+      loop.launch(s);
+      ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+      ICB_CUDA(cudaStreamSynchronize(s));
+      count_launch((long long)hst->pad * loop.graphNodes);
+    }
+    else
+    {
+      long long launched = 0;
+      for(;;)
+      {
+        ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+        ICB_CUDA(cudaStreamSynchronize(s));
+        if(hst->stop || launched > (long long)maxit + loop.batch)
+          break;
+        loop.launch(s);
+        launched += loop.batch;
+        count_launch(loop.graphNodes);
+      }
+    }
     if(info)
     {
       info->iters = hst->iter;

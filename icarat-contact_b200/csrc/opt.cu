@@ -691,15 +691,20 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
   // that the device repeats until done (at most maxiter = 100 steps), rebuilt
   // when the operands or parameters change
   const void *k[9] = {cone, x, df, dg, xmin, xmax, vol, (const void *)s, nullptr};
-  bool same = loop.exec != nullptr && std::memcmp(&Pp, &keyP, sizeof(OcParams)) == 0;
+  const bool dev = device_loops_enabled();
+  bool same = loop.exec != nullptr && loop.device == dev &&
+              std::memcmp(&Pp, &keyP, sizeof(OcParams)) == 0;
   for(int i = 0; i < 9 && same; i++)
     same = k[i] == key[i];
   if(!same)
   {
-    loop.build([&](cudaStream_t cs, const LoopCtl &L) {
-      k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, Pp, red, st.p,
-                                   L);
-    });
+    // host form: all of ICARAT's 100 steps in one launch, gated after done
+    loop.build(
+        [&](cudaStream_t cs, const LoopCtl &L) {
+          k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, Pp, red,
+                                       st.p, L);
+        },
+        dev, 100);
     for(int i = 0; i < 9; i++)
       key[i] = k[i];
     keyP = Pp;
@@ -709,7 +714,7 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
   ICB_CUDA(cudaGetLastError());
   ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(OcState), cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  count_launch(1 + (long long)hst->pad * loop.bodyNodes);
+  count_launch(1 + (loop.device ? (long long)hst->pad : 1) * loop.graphNodes);
   return hst->counter;
 }
 
@@ -717,18 +722,22 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
 MmaUpdater::MmaUpdater(long long nvar, cudaStream_t s) : n(nvar)
 {
   for(DevBuf<double> *b : {&low, &upp, &alpha, &beta, &p0, &q0, &pij, &qij, &xold1, &xold2})
-  {
     b->alloc(n);
-    ICB_CUDA(cudaMemsetAsync(b->p, 0, b->bytes(), s));
-  }
   st.alloc(1);
   int nb = vblocks(n);
   partials.alloc((size_t)nb * 2);
   counter.alloc(1);
-  ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
   red = RedScratch{partials.p, counter.p, nb};
   ICB_CUDA(cudaMallocHost(&hst, sizeof(MmaState)));
   P.epsimin = std::sqrt(double(n + 1)) * 1e-9;
+  reset(s);
+}
+void MmaUpdater::reset(cudaStream_t s)
+{
+  iter = 0;
+  for(DevBuf<double> *b : {&low, &upp, &alpha, &beta, &p0, &q0, &pij, &qij, &xold1, &xold2})
+    ICB_CUDA(cudaMemsetAsync(b->p, 0, b->bytes(), s));
+  ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
 }
 MmaUpdater::~MmaUpdater()
 {

@@ -102,6 +102,8 @@ struct MmaUpdater
 
   MmaUpdater(long long nvar, cudaStream_t s);
   ~MmaUpdater();
+  /// back to the state of a new solver (iteration 0, zero history)
+  void reset(cudaStream_t s);
   /// MMASolver::Update(x, dfdx, &g, dgdx, xmin, xmax); returns the dual passes
   int update(double *x, const double *dfdx, double g, const double *dgdx, const double *xmin,
              const double *xmax, cudaStream_t s);
@@ -120,6 +122,14 @@ struct GcmmaUpdater
   double f0app = 0.0, fapp = 0.0; ///< approximations at the last xmma
 
   GcmmaUpdater(long long nvar, cudaStream_t s);
+  /// back to the state of a new solver
+  void reset(cudaStream_t s)
+  {
+    core.reset(s);
+    raa0 = raa = 1.0;
+    outerIter = 0;
+    f0app = fapp = 0.0;
+  }
   /// OuterUpdate (GCMMASolver.cpp:66-89)
   void outer(double *xmma, const double *xval, double f0x, const double *df0dx, double fx,
              const double *dfdx, const double *xmin, const double *xmax, cudaStream_t s);

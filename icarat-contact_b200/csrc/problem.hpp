@@ -14,7 +14,8 @@ struct icb_ctx_s
 
 namespace icb
 {
-struct Mixed; // multigrid / mixed-precision machinery (mg.cu)
+struct Mixed;     // multigrid / mixed-precision machinery (mg.cu)
+struct LoopCache; // work space of the app loops (loopcache.hpp)
 }
 
 /// One LinearAnalysis-equivalent: mesh, BCs, loads and the device arrays the
@@ -51,6 +52,7 @@ struct icb_problem_s
   icb::RedScratch red;
   std::unique_ptr<icb::JacobiPcg<double>> pcg;
   std::unique_ptr<icb::Mixed> mixed;
+  std::unique_ptr<icb::LoopCache> loops; ///< filters, updaters, vectors of the app loops
   bool hasDirichletValues = false;
   bool hasDensity = false;
   bool solved = false;
@@ -59,5 +61,5 @@ struct icb_problem_s
 
   cudaStream_t stream() const { return ctx->stream; }
   icb_problem_s();
-  ~icb_problem_s(); ///< defined where icb::Mixed is complete (mg.cu)
+  ~icb_problem_s(); ///< defined where icb::Mixed and icb::LoopCache are complete (mg.cu)
 };

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "helm.hpp"
+#include "loopcache.hpp"
 #include "mg.hpp"
 #include "opt.hpp"
 #include "problem.hpp"
@@ -179,6 +180,17 @@ void toDev(DevBuf<double> &b, const double *h, long long n, cudaStream_t s)
   ICB_CUDA(cudaMemcpyAsync(b.p, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
 }
 } // namespace
+
+namespace icb
+{
+/// the problem's loop work space, created on first use
+static LoopCache &loop_cache(icb_problem p)
+{
+  if(!p->loops)
+    p->loops = std::make_unique<LoopCache>();
+  return *p->loops;
+}
+} // namespace icb
 
 extern "C" {
 
@@ -464,9 +476,12 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   cudaStream_t s = p->stream();
   const long long n = p->d.nel;
   const double vol = p->hs->volume;
-  ConeFilter cone(p->d, p->hs->h, o->filter_radius, s);
-  OcUpdater oc(p->d, s);
-  DevBuf<double> x(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n), V(n);
+  LoopCache &LC = loop_cache(p);
+  ConeFilter &cone = LC.coneFilter(p->d, p->hs->h, o->filter_radius, s);
+  OcUpdater &oc = LC.ocUpdater(p->d, s);
+  DevBuf<double> &x = LC.buf(0, n), &xf = LC.buf(1, n), &xh = LC.buf(2, n), &dxh = LC.buf(3, n),
+                 &dc = LC.buf(4, n), &dv = LC.buf(5, n), &dcf = LC.buf(6, n), &dvf = LC.buf(7, n),
+                 &lo = LC.buf(8, n), &hi = LC.buf(9, n), &V = LC.buf(10, n);
   ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);
@@ -533,14 +548,17 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
   const long long n = p->d.nel;
   const double vol = p->hs->volume;
   const bool cone = o->filter_type == ICB_FILTER_CONE;
-  std::unique_ptr<HelmFilter> helm;
-  std::unique_ptr<ConeFilter> cf;
+  LoopCache &LC = loop_cache(p);
+  HelmFilter *helm = nullptr;
+  ConeFilter *cf = nullptr;
   if(cone)
-    cf = std::make_unique<ConeFilter>(p->d, p->hs->h, o->filter_radius, s);
+    cf = &LC.coneFilter(p->d, p->hs->h, o->filter_radius, s);
   else
-    helm = std::make_unique<HelmFilter>(p->d, p->hs->h, o->filter_radius, s);
-  MmaUpdater mma(n, s);
-  DevBuf<double> x(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n);
+    helm = &LC.helmholtz(p->d, p->hs->h, o->filter_radius, s);
+  MmaUpdater &mma = LC.mmaUpdater(n, s);
+  DevBuf<double> &x = LC.buf(0, n), &xf = LC.buf(1, n), &xh = LC.buf(2, n), &dxh = LC.buf(3, n),
+                 &dc = LC.buf(4, n), &dv = LC.buf(5, n), &dcf = LC.buf(6, n), &dvf = LC.buf(7, n),
+                 &lo = LC.buf(8, n), &hi = LC.buf(9, n);
   DevBuf<uint8_t> nd(o->nondesign ? n : 0), vs(o->volume_set ? n : 0);
   if(o->nondesign)
     ICB_CUDA(cudaMemcpyAsync(nd.p, o->nondesign, n, cudaMemcpyHostToDevice, s));
@@ -632,10 +650,12 @@ int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, dou
   cudaStream_t s = p->stream();
   const long long n = p->d.nel;
   const double vol = p->hs->volume;
-  ConeFilter cone(p->d, p->hs->h, o->filter_radius, s);
-  GcmmaUpdater gc(n, s);
-  DevBuf<double> x(n), xnew(n), xf(n), xh(n), dxh(n), dc(n), dv(n), dcf(n), dvf(n), lo(n), hi(n),
-      V(n);
+  LoopCache &LC = loop_cache(p);
+  ConeFilter &cone = LC.coneFilter(p->d, p->hs->h, o->filter_radius, s);
+  GcmmaUpdater &gc = LC.gcmmaUpdater(n, s);
+  DevBuf<double> &x = LC.buf(0, n), &xnew = LC.buf(1, n), &xf = LC.buf(2, n), &xh = LC.buf(3, n),
+                 &dxh = LC.buf(4, n), &dc = LC.buf(5, n), &dv = LC.buf(6, n), &dcf = LC.buf(7, n),
+                 &dvf = LC.buf(8, n), &lo = LC.buf(9, n), &hi = LC.buf(10, n), &V = LC.buf(11, n);
   ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);

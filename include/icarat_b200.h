@@ -378,9 +378,13 @@ long long icb_launch_count(void);
  * ICB_MIXED V-cycle runs on the tcgen05 tensor cores in TF32; 0: CUDA
  * cores); "hex8_modal" (1, the default: CUDA-core Hex8 operators apply K0 in
  * the element's corner-mode basis, 45 multiply-adds per element instead of
- * 576; 0: the dense 24 x 24 product).  icb_get_option also reports
- * "tc_timeouts" (tensor-core waits that gave up; 0 in a healthy run).
- * Unknown names: ICB_ERR_BAD_ARG / -1. */
+ * 576; 0: the dense 24 x 24 product); "device_loops" (1, the default: the
+ * multigrid PCG and the OC bisection run their iterations in a CUDA graph's
+ * conditional WHILE node, one launch and one host wait each; 0: batches of
+ * iterations polled from the host, for profilers that cannot follow
+ * conditional graph nodes).  icb_get_option also reports "tc_timeouts"
+ * (tensor-core waits that gave up; 0 in a healthy run).  Unknown names:
+ * ICB_ERR_BAD_ARG / -1. */
 int icb_set_option(const char *name, long long value);
 long long icb_get_option(const char *name);
 

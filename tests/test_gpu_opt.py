@@ -109,3 +109,20 @@ def test_mma_helmholtz_loop_history(ctx):
     rel = np.abs(hg - ho) / np.abs(ho)
     assert rel.max() <= 1e-4, rel
     assert np.abs(xg - xo).max() <= 1e-3
+
+
+def test_repeated_loops_on_one_problem_agree(ctx):
+    """The app loops keep their filters, updaters and work vectors with the
+    problem: a second run (and one with another filter radius in between)
+    starts from a fresh solver state and repeats the first bitwise."""
+    g = cases.build_gpu(ctx, "halfmbb2d", 40, 16)
+    rho0 = np.full(g.nel, 0.4)
+    for kind in ("mma", "oc"):
+        h1, x1 = icb.run_loop(g, kind, rho0, 6, 2.0, tol=1e-10)
+        icb.run_loop(g, kind, rho0, 2, 3.0, tol=1e-10)
+        h2, x2 = icb.run_loop(g, kind, rho0, 6, 2.0, tol=1e-10)
+        assert np.array_equal(h1, h2) and np.array_equal(x1, x2), kind
+    a = icb.run_gcmma(g, rho0, 4, 1.5)
+    b = icb.run_gcmma(g, rho0, 4, 1.5)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)

@@ -206,3 +206,28 @@ def test_mixed_full_size_cantilever3d(ctx):
     assert imx["true_relres"] <= 2e-8 and i64["true_relres"] <= 2e-8
     assert abs(g.compliance() - c64) <= COMPLIANCE_RTOL * c64
     assert np.abs(g.sensitivity() - dc64).max() <= SENS_RTOL * np.abs(dc64).max()
+
+
+@pytest.mark.parametrize("kind,n", [("cantilever2d", (61, 20)), ("halfmbb3d", (16, 8, 8))])
+def test_device_and_host_loop_forms_agree(ctx, kind, n):
+    """The multigrid PCG and the OC bisection give bitwise-identical results
+    whether their iterations run in a conditional WHILE graph on the device
+    or in host-polled batches (the kernels after the stop are gated)."""
+    rho = cases.uniform_density(int(np.prod(n)), 11)
+    out = {}
+    for dev in (1, 0):
+        icb.set_option("device_loops", dev)
+        try:
+            g = cases.build_gpu(ctx, kind, *n)
+            g.set_density(rho)
+            info = g.solve(precision=icb.MIXED, precond=icb.GMG, tol=1e-8)
+            u = g.displacement()
+            hist, x = icb.run_loop(g, "oc", np.full(g.nel, 0.4), 3, 1.5, move=0.2)
+            out[dev] = (info["iters"], u, hist, x)
+            g.close()
+        finally:
+            icb.set_option("device_loops", 1)
+    assert icb.get_option("device_loops") == 1
+    assert out[0][0] == out[1][0]
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert np.array_equal(a, b)
