@@ -163,18 +163,24 @@ __global__ void __launch_bounds__(HTX *HTY)
   // u at this node of plane k-1 (for the fused dot product)
   double Gm = 0.0, Hm = 0.0, G0 = 0.0, H0 = 0.0, U0 = 0.0;
   double dot = 0.0;
-  double v[2];
+  // plane k's values (v) and plane k+1's (w) are in flight: loads are issued
+  // two planes ahead of their use
+  double v[2], w[2];
   fetch(Z0 - 1, v);
+  fetch(Z0, w);
   for(int k = Z0 - 1; k <= Z1 + 1; ++k)
   {
     const int b = k & 1;
 #pragma unroll
     for(int t = 0; t < 2; t++)
+    {
       if(tid + t * NT < NP)
         (&sP[b][0][0])[tid + t * NT] = v[t];
+      v[t] = w[t];
+    }
     __syncthreads();
-    if(k + 1 <= Z1 + 1)
-      fetch(k + 1, v);
+    if(k + 2 <= Z1 + 1)
+      fetch(k + 2, w);
     // in-plane sums of plane k at this node
     double mx[3], sx[3];
 #pragma unroll
@@ -317,10 +323,34 @@ int HelmFilter::apply(const double *in, double *out, bool sens, double tol, cuda
   }
   const int tx = (d.sx + HTX - 1) / HTX, ty = (d.sy + HTY - 1) / HTY;
   const long long tiles = (long long)tx * ty;
-  int bz = int(std::max(1LL, std::min<long long>(d.sz, (4LL * num_sms() + tiles - 1) / tiles)));
-  bz = int(std::min<long long>(bz, std::max(1LL, P.red.maxBlocks / tiles)));
-  const int zc = (d.sz + bz - 1) / bz;
-  bz = (d.sz + zc - 1) / zc;
+  // planes per CTA: fewest rounds x (planes + 2) for the CTAs resident at once
+  // (a CTA also stages the planes just below and above its chunk), within the
+  // reduction scratch
+  int per = 0;
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_helm_apply3<true>, HTX * HTY, 0) !=
+         cudaSuccess ||
+     per < 1)
+  {
+    (void)cudaGetLastError();
+    per = 1;
+  }
+  const long long resident = (long long)per * num_sms();
+  int zc = d.sz;
+  long long best = -1;
+  for(int bzt = 1; bzt <= d.sz; bzt++)
+  {
+    const int z = (d.sz + bzt - 1) / bzt;
+    const long long nb3 = tiles * ((d.sz + z - 1) / z);
+    if(nb3 > P.red.maxBlocks)
+      break;
+    const long long cost = (nb3 + resident - 1) / resident * (z + 2);
+    if(best < 0 || cost < best)
+    {
+      best = cost;
+      zc = z;
+    }
+  }
+  int bz = (d.sz + zc - 1) / zc;
   const bool tensor = d.dim == 3 && tiles * bz <= P.red.maxBlocks;
   const dim3 tgrid(tx, ty, bz), tblock(HTX, HTY);
   auto op = [=](cudaStream_t cs) {
