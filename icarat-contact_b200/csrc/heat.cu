@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <vector>
 #include <memory>
 
 #include "helm.hpp"
@@ -557,6 +558,10 @@ int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double 
     if(rc)
       throw Error{rc, "Helmholtz filter solve did not converge"};
   };
+  // the apps' Optimize::isConvergence stop rule (conv_eps > 0) and step
+  // reports (on_step: design, temperature, no stress)
+  double fold = 0.0;
+  std::vector<double> hostRho, hostT, hostU;
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
@@ -571,6 +576,28 @@ int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double 
     if(inf.status != ICB_OK)
       return inf.status;
     hist[step - 1] = heatObjective(*h);
+    if(o->on_step)
+    {
+      hostRho.resize(n);
+      hostU.resize(h->d.ld);
+      hostT.resize(h->d.nnode);
+      ICB_CUDA(cudaMemcpyAsync(hostRho.data(), xh.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      ICB_CUDA(cudaMemcpyAsync(hostU.data(), h->u.p, sizeof(double) * h->d.ld,
+                               cudaMemcpyDeviceToHost, s));
+      ICB_CUDA(cudaStreamSynchronize(s));
+      for(long long nd = 0; nd < h->d.nnode; nd++)
+        hostT[nd] = std::fabs(hostU[nd]) < 1.0e-15 ? 0.0 : hostU[nd];
+      o->on_step(o->step_user, step, hist[step - 1], hostRho.data(), hostT.data(), nullptr);
+    }
+    if(o->steps_done)
+      *o->steps_done = step;
+    bool last = false;
+    if(o->conv_eps > 0.0)
+    {
+      last = std::fabs(fold - hist[step - 1]) / hist[step - 1] < o->conv_eps &&
+             step > o->conv_min_steps;
+      fold = hist[step - 1];
+    }
     const double vs = device_dot(n, xh.p, hi.p, h->pcg->red, h->pcg->dots.p, s) * vol; // hi = 1
     if(step == 1)
       V0 = vs;
@@ -588,6 +615,8 @@ int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double 
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if(last)
+      break;
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));

@@ -199,6 +199,7 @@ int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
   j->kind = jd->kind;
   j->loop = jd->loop;
   j->loop.iter_seconds = nullptr;
+  j->loop.steps_done = nullptr; // the caller's memory is not written later
   Dims d = make_dims(g.dim, g.nx, g.ny, g.dim == 3 ? g.nz : 1);
   long long neq = d.nnode * g.dim;
   j->fixed.assign(jd->fixed, jd->fixed + neq);

@@ -173,6 +173,23 @@ struct StepReport
   }
 };
 
+/// Optimize::isConvergence (optimize.hpp) as the loops apply it: `done` once
+/// |f_old - f| / f < eps after step minstep; every step reports steps_done
+struct StopRule
+{
+  double fold = 0.0;
+  bool check(const icb_loop_opts *o, int step, double f)
+  {
+    if(o->steps_done)
+      *o->steps_done = step;
+    if(!(o->conv_eps > 0.0))
+      return false;
+    const bool done = std::fabs(fold - f) / f < o->conv_eps && step > o->conv_min_steps;
+    fold = f;
+    return done;
+  }
+};
+
 void toDev(DevBuf<double> &b, const double *h, long long n, cudaStream_t s)
 {
   if((long long)b.n < n)
@@ -492,6 +509,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   StepReport report;
   OcParams P;
   P.move = o->move_limit;
+  StopRule stop;
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
@@ -507,6 +525,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
     if(rc)
       return rc;
     report(p, o, step, hist[step - 1], xh.p);
+    const bool last = stop.check(o, step, hist[step - 1]);
     if(step == 1)
       V0 = deviceSum(p, xh.p, n) * vol;
     const double *dcd = icb_sensitivity_device(p);
@@ -524,6 +543,8 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if(last)
+      break;
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -585,6 +606,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     if(rc)
       throw Error{rc, "Helmholtz filter solve did not converge"};
   };
+  StopRule stop;
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
@@ -607,6 +629,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     if(rc)
       return rc;
     report(p, o, step, hist[step - 1], xh.p);
+    const bool last = stop.check(o, step, hist[step - 1]);
     const double *dcd = icb_sensitivity_device(p);
     if(!dcd)
       throw Error{ICB_ERR_STATE, "sensitivity failed"};
@@ -627,6 +650,8 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if(last)
+      break;
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -676,6 +701,7 @@ int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, dou
       throw Error{rc, icb_last_error()};
     vs = deviceSum(p, xh.p, n) * vol;
   };
+  StopRule stop;
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
@@ -685,6 +711,7 @@ int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, dou
     evaluate(x.p, beta, f, vs);
     hist[step - 1] = f;
     report(p, o, step, f, xh.p);
+    const bool last = stop.check(o, step, f);
     if(step == 1)
       V0 = vs;
     const double g = vs - V0;
@@ -714,6 +741,8 @@ int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, dou
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if(last)
+      break;
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));

@@ -58,7 +58,8 @@ class LoopOpts(C.Structure):
     _fields_ = [("nsteps", C.c_int), ("filter_radius", C.c_double), ("move_limit", C.c_double),
                 ("use_threshold", C.c_int), ("volume_ref", C.c_double), ("solve", SolveOpts),
                 ("iter_seconds", _dp), ("filter_type", C.c_int), ("nondesign", _u8p),
-                ("volume_set", _u8p), ("on_step", STEP_CB), ("step_user", C.c_void_p)]
+                ("volume_set", _u8p), ("on_step", STEP_CB), ("step_user", C.c_void_p),
+                ("conv_eps", C.c_double), ("conv_min_steps", C.c_int), ("steps_done", _ip)]
 
 
 class JobDesc(C.Structure):
@@ -599,12 +600,18 @@ class MMA:
 
 def run_loop(prob, kind, rho0, nsteps, radius, move=0.15, use_threshold=True, volume_ref=0.0,
              precision=FP64, precond=GMG, tol=1e-8, maxit=20000, filter_type=0, nondesign=None,
-             volume_set=None, on_step=None):
+             volume_set=None, on_step=None, conv_eps=0.0, conv_min_steps=0, steps_done=None):
     """icb_run_oc (kind "oc") or icb_run_mma (kind "mma"): compliance history, design.
-    on_step(step, compliance, rho_phys, nodeval, mises) receives numpy copies."""
+    on_step(step, compliance, rho_phys, nodeval, mises) receives numpy copies;
+    conv_eps > 0 applies the apps' isConvergence(conv_eps, conv_min_steps)
+    stop rule, steps_done (a one-element int32 array) receives the steps run."""
     o = LoopOpts(nsteps, radius, move, int(use_threshold), volume_ref,
                  SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0), None)
     o.filter_type = filter_type
+    o.conv_eps = conv_eps
+    o.conv_min_steps = conv_min_steps
+    if steps_done is not None:
+        o.steps_done = _p(steps_done, _ip)
     keep = []
     for name, m in (("nondesign", nondesign), ("volume_set", volume_set)):
         if m is not None:

@@ -252,6 +252,15 @@ typedef struct
   const unsigned char *volume_set;
   icb_step_cb on_step;  /* optional, called after every step's solve      */
   void *step_user;      /* passed to on_step                               */
+  /* optional stop rule of the apps' Optimize::isConvergence(eps, minstep)
+   * (opt_heat.cpp:121, opt_mma_Helmholtz.cpp:128): once a step's objective
+   * differs from the previous step's by less than conv_eps (relative) and
+   * step > conv_min_steps, that step's update is completed and the loop
+   * ends.  conv_eps <= 0: all nsteps run.  steps_done (may be NULL) receives
+   * the number of steps run (icb_server ignores it). */
+  double conv_eps;
+  int conv_min_steps;
+  int *steps_done;
 } icb_loop_opts;
 /* opt-macro-oc/opt_macro_oc.cpp:84-172: cone filter, threshold, solve,
  * compliance, V0 at step 1, sensitivities, adjoint filter, OC; hist[nsteps]
@@ -306,7 +315,8 @@ int icb_heat_objective(icb_heat h, double *f);
 int icb_heat_sensitivity(icb_heat h, const double *rho, double *dc, double *dv);
 /* the opt-heat loop (opt_heat.cpp:79-151): Helmholtz filter (filter_radius),
  * threshold, solve, objective, constraint sum x v - V0, MMA; hist[step] is
- * the objective */
+ * the objective; on_step receives the thresholded design, the temperatures
+ * (nnode) and no stress (NULL) */
 int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double *hist,
                  double *xout);
 

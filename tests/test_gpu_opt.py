@@ -126,3 +126,20 @@ def test_repeated_loops_on_one_problem_agree(ctx):
     b = icb.run_gcmma(g, rho0, 4, 1.5)
     for u, v in zip(a, b):
         assert np.array_equal(u, v)
+
+
+@pytest.mark.parametrize("kind", ["oc", "mma"])
+def test_loop_stop_rule(ctx, kind):
+    """conv_eps applies Optimize::isConvergence(eps, minstep): the step whose
+    objective changed by less than eps (relative) after minstep ends the loop
+    (its update still runs); the history up to there equals the full run's."""
+    g = cases.build_gpu(ctx, "halfmbb2d", 40, 16)
+    rho0 = np.full(g.nel, 0.4)
+    full, _ = icb.run_loop(g, kind, rho0, 8, 2.0, tol=1e-10)
+    done = np.zeros(1, np.int32)
+    h, _ = icb.run_loop(g, kind, rho0, 8, 2.0, tol=1e-10, conv_eps=0.9, conv_min_steps=3,
+                        steps_done=done)
+    rel = np.abs(np.diff(full)) / np.abs(full[1:])
+    expect = next(s for s in range(4, 9) if rel[s - 2] < 0.9)
+    assert done[0] == expect
+    assert np.array_equal(h[:expect], full[:expect]) and not h[expect:].any()

@@ -93,7 +93,7 @@ def test_reader_rejects_outside_subset(toml_dump, tmp_path, body, what):
 
 
 def test_drivers_are_built():
-    for name in ("opt_macro_oc_gpu", "opt_mma_helmholtz_gpu"):
+    for name in ("opt_macro_oc_gpu", "opt_mma_helmholtz_gpu", "opt_heat_gpu"):
         assert os.access(os.path.join(LIB, name), os.X_OK), name
 
 
@@ -160,3 +160,41 @@ def test_mma_app_on_shim_matches_oracle():
     rel = np.abs(out[:, 1] - hist) / np.abs(hist)
     assert rel.max() <= 1e-4, rel
     assert out[0, 2] == 0.0  # step-1 constraint: V0 is the step-1 volume
+
+
+@pytest.mark.gpu
+def test_heat_app_on_shim_matches_oracle(tmp_path):
+    """opt_heat_gpu (the opt-heat app on the library) against the oracle's
+    heat loop, and the app's outputs: function.csv and res<step>.vtk with the
+    temperature, threshold_s and design_s arrays."""
+    toml = os.path.join(TOMLS, "heat2d.toml")
+    with open(toml, "rb") as fh:
+        cfg = tomllib.load(fh)
+    m, mat, bc, tp = cfg["mesh"], cfg["material"], cfg["boundary_condition"], cfg["this_problem"]
+    r = subprocess.run([os.path.join(LIB, "opt_heat_gpu"), toml], capture_output=True, text=True,
+                       timeout=600, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    out = np.array([[float(v) for v in ln.split(",")] for ln in r.stdout.split()])
+    steps = tp["steps"]
+    assert out.shape == (steps, 2)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as po
+    nx, ny, _ = m["division"]
+    lx, ly, _ = m["length"]
+    o = po.Problem(2, nx, ny, 1, lx, ly, 1.0, state=3)
+    for flag, val, rng in bc["dirichlet"]:
+        o.dirichlet_box([flag[0], 0, 0, 0, 0, 0], [val[0], 0, 0, 0, 0, 0],
+                        np.asarray(rng, float).reshape(6))
+    for val, rng in bc["neumann"]:
+        o.traction_box([val[0], 0, 0], np.asarray(rng, float).reshape(6))
+    c1, c2 = mat["conductivity"]
+    ho, _ = o.heat_loop(c1, c2, np.full(nx * ny, mat["designs_0"]), steps, tp["filterR"],
+                        tol=1e-12)
+    assert np.abs(out[:, 1] - ho).max() / np.abs(ho).max() <= 1e-4
+    fn = np.loadtxt(tmp_path / "function.csv")
+    assert fn.shape == (steps, 2) and np.allclose(fn[:, 1], out[:, 1], rtol=1e-5)
+    vtk = (tmp_path / "res1.vtk").read_text()
+    for key in ("POINT_DATA", "SCALARS temperature", "SCALARS threshold_s", "CELL_DATA",
+                "SCALARS design_s", f"CELLS {nx * ny}"):
+        assert key in vtk, key
+    assert os.path.exists(tmp_path / f"res{steps}.vtk")
