@@ -796,6 +796,63 @@ __global__ void k_sensitivity(const KMat<double, 24> K, const Dims d, double y1,
   dc[e] = -(dyoung / young) * q;
 }
 
+/// the same sensitivity for a Hex8 element in the corner-mode form:
+/// u_e^T K0 u_e = (H u_e)^T Kt (H u_e), 45 multiply-adds instead of 576; one
+/// thread per element on a 3D launch (x along threads, y and z along the grid)
+__global__ void k_sensitivity_h8m(const KModal<double> K, const Dims d, double y1, double y2,
+                                  double p, const double *__restrict__ rho,
+                                  const double *__restrict__ u, double *__restrict__ dc)
+{
+  const int ei = blockIdx.x * blockDim.x + threadIdx.x, ej = blockIdx.y, ek = blockIdx.z;
+  if(ei >= d.nx)
+    return;
+  const long long e = ei + (long long)ej * d.nx + (long long)ek * d.nx * d.ny;
+  const long long sxy = (long long)d.sx * d.sy;
+  const long long base = ei + (long long)ej * d.sx + (long long)ek * sxy;
+  const long long qoff[4] = {0, 1, 1 + (long long)d.sx, (long long)d.sx};
+  double uh[24], yh[24];
+#pragma unroll
+  for(int c = 0; c < 3; c++)
+  {
+    double vb[4], vt[4], hb[4], ht[4];
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+    {
+      // node values with |u| < 1e-15 zeroed, as divideValIntoNode leaves them
+      const double b = u[c * d.ld + base + qoff[q]], t = u[c * d.ld + base + qoff[q] + sxy];
+      vb[q] = fabs(b) < 1.0e-15 ? 0.0 : b;
+      vt[q] = fabs(t) < 1.0e-15 ? 0.0 : t;
+    }
+    plane_modes(vb, hb);
+    plane_modes(vt, ht);
+#pragma unroll
+    for(int s = 0; s < 4; s++)
+    {
+      uh[s * 3 + c] = hb[s] + ht[s];
+      uh[(s + 4) * 3 + c] = hb[s] - ht[s];
+    }
+  }
+  yh[0] = yh[1] = yh[2] = 0.0;
+  modal_blocks_apply<0, 0>(K, uh, yh);
+  double q = 0.0;
+#pragma unroll
+  for(int r = 3; r < 24; r++)
+    q = fma(uh[r], yh[r], q);
+  const double s = rho[e];
+  double young, dyoung;
+  if(y2 >= y1)
+  {
+    young = (1.0 - pow(s, p)) * y1 + pow(s, p) * y2;
+    dyoung = p * pow(s, p - 1.0) * (y2 - y1);
+  }
+  else
+  {
+    young = pow(1.0 - s, p) * y1 + (1.0 - pow(1.0 - s, p)) * y2;
+    dyoung = (y2 - y1) * p * pow(1.0 - s, p - 1.0);
+  }
+  dc[e] = -(dyoung / young) * (young * q);
+}
+
 inline unsigned blocks_for(long long n, int bs) { return unsigned((n + bs - 1) / bs); }
 } // namespace
 
@@ -1156,7 +1213,11 @@ void launch_sensitivity(const Dims &d, const double *K, double y1, double y2, do
   KMat<double, 24> km;
   int nd = d.dim == 2 ? 8 : 24;
   std::copy(K, K + nd * nd, km.k);
-  if(d.dim == 3)
+  KModal<double> kmod;
+  if(d.dim == 3 && g_hex8_modal && d.ny <= 65535 && d.nz <= 65535 && modal_form_cached(K, kmod))
+    k_sensitivity_h8m<<<dim3(unsigned((d.nx + 127) / 128), unsigned(d.ny), unsigned(d.nz)), 128,
+                        0, s>>>(kmod, d, y1, y2, p, rho, u, dc);
+  else if(d.dim == 3)
     k_sensitivity<3><<<blocks_for(d.nel, 128), 128, 0, s>>>(km, d, y1, y2, p, rho, u, dc);
   else
     k_sensitivity<2><<<blocks_for(d.nel, 128), 128, 0, s>>>(km, d, y1, y2, p, rho, u, dc);
