@@ -133,14 +133,15 @@ enum OpMode
   OP_APPLY = 0,    ///< y = K u
   OP_RESIDUAL = 1, ///< y = b - K u
   OP_JACOBI = 2,   ///< y = u + omega D^-1 (b - K u)
-  OP_CHEB = 3      ///< d = c1 d + c2 D^-1 (b - K u); y = u + d (Chebyshev step)
+  /// Chebyshev step in three-term form: y = u + c1 (u - y_in) + c2 D^-1 (b - K u),
+  /// y_in the previous iterate that y holds on entry (not read when c1 = 0)
+  OP_CHEB = 3
 };
 template <typename T> struct Epi
 {
   const T *b;
   const T *dinv;
   T omega;
-  T *d;
   T c1, c2;
 };
 template <typename T> struct OpExtras
@@ -149,7 +150,6 @@ template <typename T> struct OpExtras
   const T *b = nullptr;
   const T *dinv = nullptr;
   double omega = 0.0;
-  T *d = nullptr; ///< OP_CHEB direction vector (read and written at each node)
   double c1 = 0.0, c2 = 0.0;
   RedScratch *dotRed = nullptr; ///< fused u.y reduction (OP_APPLY) into *dotOut
   double *dotOut = nullptr;

@@ -164,10 +164,10 @@ __global__ void k_prolong_add(Dims df, Dims dc, const T *__restrict__ xc, T *__r
     }
 }
 
-/// first smoothing step from a zero guess: x = d = c D^-1 b
+/// first smoothing step from a zero guess: x = c D^-1 b, x0 = 0
 template <typename T>
 __global__ void k_jacobi0(long long n, T c, const T *__restrict__ dinv,
-                          const T *__restrict__ b, T *__restrict__ x, T *__restrict__ d,
+                          const T *__restrict__ b, T *__restrict__ x, T *__restrict__ x0,
                           const KState *gate)
 {
   if(gated(gate))
@@ -175,9 +175,8 @@ __global__ void k_jacobi0(long long n, T c, const T *__restrict__ dinv,
   for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)gridDim.x * blockDim.x)
   {
-    T v = c * dinv[i] * b[i];
-    x[i] = v;
-    d[i] = v;
+    x[i] = c * dinv[i] * b[i];
+    x0[i] = T(0); // the iterate before x, for the next three-term step
   }
 }
 
@@ -585,7 +584,7 @@ template <typename T> struct Level
   const T *E = nullptr;
   DevBuf<uint8_t> fixOwn;
   const uint8_t *fix = nullptr;
-  DevBuf<T> dinv, x, b, r, t, dv;
+  DevBuf<T> dinv, x, b, r, t;
 };
 
 /// Flexible CG in TK with a TP V-cycle (see the kernels above).
@@ -722,13 +721,12 @@ template <typename TK, typename TP> struct MgPcg
       lv[l].dinv.alloc(m);
       lv[l].r.alloc(m);
       lv[l].t.alloc(m);
-      lv[l].dv.alloc(m);
       if(l > 0)
       {
         lv[l].x.alloc(m);
         lv[l].b.alloc(m);
       }
-      for(DevBuf<TP> *v : {&lv[l].dinv, &lv[l].r, &lv[l].t, &lv[l].x, &lv[l].b, &lv[l].dv})
+      for(DevBuf<TP> *v : {&lv[l].dinv, &lv[l].r, &lv[l].t, &lv[l].x, &lv[l].b})
         if(v->p)
           ICB_CUDA(cudaMemsetAsync(v->p, 0, v->bytes(), s));
     }
@@ -842,13 +840,12 @@ template <typename TK, typename TP> struct MgPcg
     // step 0 from zero, then 2nu-1 operator steps: an odd number of
     // ping-pongs ends in out
     TP *cur = L.t.p, *oth = out;
-    k_jacobi0<TP><<<vblocks(m), VB, 0, s>>>(m, TP(cc2[0]), L.dinv.p, b, cur, L.dv.p, gate);
+    k_jacobi0<TP><<<vblocks(m), VB, 0, s>>>(m, TP(cc2[0]), L.dinv.p, b, cur, oth, gate);
     count_launch();
     OpExtras<TP> ch;
     ch.mode = OP_CHEB;
     ch.b = b;
     ch.dinv = L.dinv.p;
-    ch.d = L.dv.p;
     ch.gate = gate;
     ch.gateConv = 1;
     for(int k = 1; k < nu; k++)

@@ -44,10 +44,11 @@ constexpr int TY2 = 4; // warps per CTA (2D: independent x strips)
 __host__ __device__ constexpr int lnode(int a, int b) { return (a ^ b) + 2 * b; }
 
 /// fused output stage: y = Au (OP_APPLY), b - Au (OP_RESIDUAL), a damped
-/// Jacobi sweep u + w D^-1 (b - Au) (OP_JACOBI) or a Chebyshev step
-/// (OP_CHEB); Au is already 0 on constrained DOFs and so are b and D^-1.
+/// Jacobi sweep u + w D^-1 (b - Au) (OP_JACOBI) or a three-term Chebyshev
+/// step (OP_CHEB, which reads the previous iterate from y at this DOF before
+/// overwriting it); Au is already 0 on constrained DOFs and so are b and D^-1.
 template <typename T, int MODE>
-__device__ __forceinline__ T epilogue(T Au, T uself, long long i, const Epi<T> &ep)
+__device__ __forceinline__ T epilogue(T Au, T uself, long long i, const Epi<T> &ep, const T *y)
 {
   if(MODE == OP_APPLY)
     return Au;
@@ -56,11 +57,9 @@ __device__ __forceinline__ T epilogue(T Au, T uself, long long i, const Epi<T> &
     return r;
   if(MODE == OP_JACOBI)
     return uself + ep.omega * __ldg(ep.dinv + i) * r;
-  // OP_CHEB: the direction is read and written only at this node
   T dn = ep.c2 * __ldg(ep.dinv + i) * r;
   if(ep.c1 != T(0))
-    dn += ep.c1 * ep.d[i];
-  ep.d[i] = dn;
+    dn += ep.c1 * (uself - y[i]);
   return uself + dn;
 }
 
@@ -200,7 +199,7 @@ __global__ void __launch_bounds__(TX *TYK)
             us = __ldg(u + c * ld + node);
           if(DOT)
             dot += double(us) * double(o);
-          y[c * ld + node] = epilogue<T, MODE>(o, us, c * ld + node, ep);
+          y[c * ld + node] = epilogue<T, MODE>(o, us, c * ld + node, ep, y);
         }
       }
     }
@@ -334,7 +333,7 @@ template <typename T> __device__ __forceinline__ void plane_corners(const T h[4]
 }
 
 /// the epilogue's per-node inputs (the node's own value, b, D^-1, the
-/// Chebyshev direction), loaded ahead of their use
+/// previous Chebyshev iterate), loaded ahead of their use
 template <typename T> struct EpiIn
 {
   T b[3], dinv[3], d[3], us[3];
@@ -448,7 +447,7 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
           if(MODE >= OP_JACOBI)
             in.dinv[c] = __ldg(ep.dinv + c * ld + node);
           if(MODE == OP_CHEB)
-            in.d[c] = ep.c1 != T(0) ? ep.d[c * ld + node] : T(0);
+            in.d[c] = ep.c1 != T(0) ? y[c * ld + node] : T(0); // the previous iterate
         }
       }
     };
@@ -538,8 +537,7 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
             {
               T dn = ep.c2 * in.dinv[c] * r;
               if(ep.c1 != T(0))
-                dn += ep.c1 * in.d[c];
-              ep.d[i] = dn;
+                dn += ep.c1 * (us - in.d[c]);
               w = us + dn;
             }
           }
@@ -644,7 +642,7 @@ __global__ void __launch_bounds__(TX *TY2)
             us = __ldg(u + c * ld + node); // node i = 0 belongs to a halo column
           if(DOT)
             dot += double(us) * double(v);
-          y[c * ld + node] = epilogue<T, MODE>(v, us, c * ld + node, ep);
+          y[c * ld + node] = epilogue<T, MODE>(v, us, c * ld + node, ep, y);
         }
       }
     }
@@ -1038,7 +1036,7 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
 {
   RedScratch red = x.dotRed ? *x.dotRed : RedScratch{};
   const int target = num_sms() * 4;
-  Epi<T> ep{x.b, x.dinv, T(x.omega), x.d, T(x.c1), T(x.c2)};
+  Epi<T> ep{x.b, x.dinv, T(x.omega), T(x.c1), T(x.c2)};
   if(d.dim == 3)
   {
     // 8 element rows per tile for FP64 and FP32 (16-row FP64 tiles were

@@ -241,8 +241,9 @@ template <bool DOT, int MODE> struct LayerOps
   float bb[3] = {0.f, 0.f, 0.f}, dv[3] = {0.f, 0.f, 0.f}, dp[3] = {0.f, 0.f, 0.f};
   __device__ __forceinline__ void load(bool lay, const float *__restrict__ E, long long e, bool outp,
                                        const uint8_t *__restrict__ fix,
-                                       const float *__restrict__ u, const Epi<float> &ep,
-                                       long long node, long long ld, bool col)
+                                       const float *__restrict__ u, const float *y,
+                                       const Epi<float> &ep, long long node, long long ld,
+                                       bool col)
   {
     Ee = lay ? __ldg(E + e) : 0.f;
     if(!outp)
@@ -258,7 +259,7 @@ template <bool DOT, int MODE> struct LayerOps
       if(MODE >= OP_JACOBI)
         dv[c] = __ldg(ep.dinv + c * ld + node);
       if(MODE == OP_CHEB && ep.c1 != 0.f)
-        dp[c] = ep.d[c * ld + node];
+        dp[c] = y[c * ld + node]; // the previous iterate (y is written after)
     }
   }
 };
@@ -388,7 +389,7 @@ __global__ void __launch_bounds__(TX *TY, kBlocksPerSm)
     const long long nBase = (long long)ni + (long long)nj * d.sx;
     LayerOps<DOT, MODE> cur, nxt;
     cur.load(col && Z0 - 1 >= 0 && Z0 - 1 < d.nz, E, eBase + (long long)(Z0 - 1) * nxy, false, fix,
-             u, ep, nBase, ld, col);
+             u, y, ep, nBase, ld, col);
     for(int ek = Z0 - 1; ek <= Z1; ++ek)
     {
       const int kt = ek + 1;
@@ -396,7 +397,7 @@ __global__ void __launch_bounds__(TX *TY, kBlocksPerSm)
       const bool outp = ek >= Z0 && outCol;
       const long long node = nBase + (long long)ek * sxy;
       if(ek + 1 <= Z1)
-        nxt.load(col && ek + 1 < d.nz, E, eBase + (long long)(ek + 1) * nxy, outCol, fix, u, ep,
+        nxt.load(col && ek + 1 < d.nz, E, eBase + (long long)(ek + 1) * nxy, outCol, fix, u, y, ep,
                  nBase + (long long)(ek + 1) * sxy, ld, col);
       const float Ee = cur.Ee;
       // ---- top corners from the staged plane
@@ -500,8 +501,7 @@ __global__ void __launch_bounds__(TX *TY, kBlocksPerSm)
             {
               float dn = ep.c2 * cur.dv[c] * (cur.bb[c] - o);
               if(ep.c1 != 0.f)
-                dn += ep.c1 * cur.dp[c];
-              ep.d[c * ld + node] = dn;
+                dn += ep.c1 * (us - cur.dp[c]);
               outv = us + dn;
             }
             y[c * ld + node] = outv;
@@ -563,7 +563,7 @@ void launch_tc_mode(const Dims &d, const float *K, const float *E, const float *
   w.items = w.bx * w.by * w.bz;
   const int grid = std::min(w.items, slots);
   RedScratch red = x.dotRed ? *x.dotRed : RedScratch{};
-  Epi<float> ep{x.b, x.dinv, float(x.omega), x.d, float(x.c1), float(x.c2)};
+  Epi<float> ep{x.b, x.dinv, float(x.omega), float(x.c1), float(x.c2)};
   if(x.dotRed)
     ICB_REQUIRE(grid <= red.maxBlocks, "reduction scratch too small");
   kern<<<grid, dim3(TX, TY), smem, s>>>(km, d, w, E, u, y, fix, red, x.dotOut, x.gate,
