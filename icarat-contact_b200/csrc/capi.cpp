@@ -31,26 +31,6 @@ void count_launch(long long n)
 long long thread_launch_count() { return t_launches; }
 } // namespace icb
 
-#define ICB_API_BEGIN try {
-#define ICB_API_END                                                                         \
-  return ICB_OK;                                                                            \
-  }                                                                                         \
-  catch(const icb::Error &e)                                                                \
-  {                                                                                         \
-    icb::set_error(e.msg);                                                                  \
-    return e.code;                                                                          \
-  }                                                                                         \
-  catch(const std::bad_alloc &)                                                             \
-  {                                                                                         \
-    icb::set_error("host allocation failed");                                               \
-    return ICB_ERR_OOM;                                                                     \
-  }                                                                                         \
-  catch(const std::exception &e)                                                            \
-  {                                                                                         \
-    icb::set_error(e.what());                                                               \
-    return ICB_ERR_STATE;                                                                   \
-  }
-
 namespace
 {
 void need(bool c, const char *m)

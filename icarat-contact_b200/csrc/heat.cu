@@ -231,21 +231,6 @@ void needH(icb_heat h, bool final)
     throw Error{ICB_ERR_STATE, "call icb_heat_finalize first"};
 }
 
-#define HEAT_TRY try {
-#define HEAT_CATCH                                                                                 \
-  }                                                                                                \
-  catch(const Error &e)                                                                            \
-  {                                                                                                \
-    set_error(e.msg);                                                                              \
-    return e.code;                                                                                 \
-  }                                                                                                \
-  catch(const std::bad_alloc &)                                                                    \
-  {                                                                                                \
-    set_error("host allocation failed");                                                           \
-    return ICB_ERR_OOM;                                                                            \
-  }                                                                                                \
-  return ICB_OK;
-
 void solveHeat(icb_heat_s &H, const icb_solve_opts *opts, icb_solve_info *info)
 {
   cudaStream_t s = H.stream();
@@ -323,7 +308,7 @@ extern "C" {
 
 int icb_heat_create(icb_ctx ctx, const icb_heat_desc *desc, icb_heat *out)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   if(!ctx || !desc || !out)
     throw Error{ICB_ERR_BAD_ARG, "NULL argument"};
   if(desc->cond1[0] < desc->cond2[0])
@@ -362,12 +347,12 @@ int icb_heat_create(icb_ctx ctx, const icb_heat_desc *desc, icb_heat *out)
   }
   ctx->refs++;
   *out = H.release();
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_destroy(icb_heat h)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   if(!h)
     return ICB_OK;
   icb_ctx c = h->ctx;
@@ -375,43 +360,43 @@ int icb_heat_destroy(icb_heat h)
   cudaStreamSynchronize(c->stream);
   delete h;
   icb_ctx_destroy(c);
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_dirichlet_box(icb_heat h, int flag, double val, const double *range)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, false);
   if(!range)
     throw Error{ICB_ERR_BAD_ARG, "NULL range"};
   const int f[6] = {flag, 0, 0, 0, 0, 0};
   const double v[6] = {val, 0, 0, 0, 0, 0};
   h->hs->dirichletBox(f, v, range);
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_flux_box(icb_heat h, double q, const double *range)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, false);
   if(!range)
     throw Error{ICB_ERR_BAD_ARG, "NULL range"};
   const double v[3] = {q, 0, 0};
   h->hs->tractionBox(v, range);
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_nodal_source(icb_heat h, long long node, double q)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, false);
   h->hs->nodalLoad(node, &q);
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_finalize(icb_heat h, long long *numeq)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, false);
   if(h->finalized)
     throw Error{ICB_ERR_STATE, "icb_heat_finalize called twice"};
@@ -446,12 +431,12 @@ int icb_heat_finalize(icb_heat h, long long *numeq)
   h->finalized = true;
   if(numeq)
     *numeq = hs.numeq;
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_set_density(icb_heat h, const double *rho)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, true);
   if(!rho)
     throw Error{ICB_ERR_BAD_ARG, "NULL rho"};
@@ -463,12 +448,12 @@ int icb_heat_set_density(icb_heat h, const double *rho)
   count_launch();
   ICB_CUDA(cudaStreamSynchronize(s));
   h->hasDensity = true;
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_solve(icb_heat h, const icb_solve_opts *opts, icb_solve_info *info)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, true);
   if(!h->hasDensity)
     throw Error{ICB_ERR_STATE, "set the density first"};
@@ -479,12 +464,12 @@ int icb_heat_solve(icb_heat h, const icb_solve_opts *opts, icb_solve_info *info)
     *info = inf;
   if(inf.status != ICB_OK)
     return inf.status;
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_get_temperature(icb_heat h, double *nodeval)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, true);
   if(!nodeval || !h->solved)
     throw Error{ICB_ERR_STATE, "solve first"};
@@ -494,22 +479,22 @@ int icb_heat_get_temperature(icb_heat h, double *nodeval)
   ICB_CUDA(cudaStreamSynchronize(s));
   for(long long n = 0; n < h->d.nnode; n++)
     nodeval[n] = std::fabs(t[n]) < 1.0e-15 ? 0.0 : t[n];
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_objective(icb_heat h, double *f)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, true);
   if(!f || !h->solved)
     throw Error{ICB_ERR_STATE, "solve first"};
   *f = heatObjective(*h);
-  HEAT_CATCH
+  ICB_API_END
 }
 
 int icb_heat_sensitivity(icb_heat h, const double *rho, double *dc, double *dv)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, true);
   if(!rho || !dc || !h->solved)
     throw Error{ICB_ERR_STATE, "solve first (and pass the density of the solve)"};
@@ -523,7 +508,7 @@ int icb_heat_sensitivity(icb_heat h, const double *rho, double *dc, double *dv)
   if(dv)
     for(long long e = 0; e < n; e++)
       dv[e] = h->hs->volume;
-  HEAT_CATCH
+  ICB_API_END
 }
 
 /// The opt-heat loop (opt_heat.cpp:79-151) on the device: Helmholtz filter,
@@ -532,7 +517,7 @@ int icb_heat_sensitivity(icb_heat h, const double *rho, double *dc, double *dv)
 /// Helmholtz filters, MMA (c = 1e5).  hist[step] = the objective.
 int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double *hist, double *xout)
 {
-  HEAT_TRY
+  ICB_API_BEGIN
   needH(h, true);
   if(!o || !rho0 || !hist || o->nsteps <= 0 || !(o->filter_radius > 0.0))
     throw Error{ICB_ERR_BAD_ARG, "bad loop options"};
@@ -621,7 +606,7 @@ int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double 
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  HEAT_CATCH
+  ICB_API_END
 }
 
 } // extern "C"

@@ -4,7 +4,9 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <exception>
 #include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -39,6 +41,28 @@ struct Error
     if(!(cond))                                                                 \
       throw ::icb::Error{ICB_ERR_BAD_ARG, msg};                                 \
   } while(0)
+/// the body of every extern "C" entry point: no C++ exception crosses the C
+/// ABI; an Error returns its code, a failed host allocation ICB_ERR_OOM, any
+/// other exception ICB_ERR_STATE, each with its message in icb_last_error
+#define ICB_API_BEGIN try {
+#define ICB_API_END                                                             \
+  }                                                                             \
+  catch(const ::icb::Error &e)                                                  \
+  {                                                                             \
+    ::icb::set_error(e.msg);                                                    \
+    return e.code;                                                              \
+  }                                                                             \
+  catch(const std::bad_alloc &)                                                 \
+  {                                                                             \
+    ::icb::set_error("host allocation failed");                                 \
+    return ICB_ERR_OOM;                                                         \
+  }                                                                             \
+  catch(const std::exception &e)                                                \
+  {                                                                             \
+    ::icb::set_error(e.what());                                                 \
+    return ICB_ERR_STATE;                                                       \
+  }                                                                             \
+  return ICB_OK;
 
 // ---------------------------------------------------------- device memory --
 template <typename T> struct DevBuf

@@ -23,6 +23,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -89,9 +90,11 @@ struct icb_server_s
 
   void worker()
   {
+    // a worker without a context still takes jobs and fails them with the
+    // context's error, so no admitted job waits for ever
     icb_ctx ctx = nullptr;
-    if(icb_ctx_create(device, &ctx) != ICB_OK)
-      return;
+    const int ctxStatus = icb_ctx_create(device, &ctx);
+    const std::string ctxError = ctxStatus == ICB_OK ? "" : icb_last_error();
     for(;;)
     {
       std::shared_ptr<Job> j;
@@ -104,9 +107,10 @@ struct icb_server_s
         j->state = ICB_JOB_RUNNING;
         j->start = now();
       }
-      int st = ICB_OK;
+      int st = ctxStatus;
       icb_problem p = nullptr;
-      st = icb_problem_create(ctx, &j->grid, &p);
+      if(st == ICB_OK)
+        st = icb_problem_create(ctx, &j->grid, &p);
       if(st == ICB_OK)
         st = icb_dirichlet_mask(p, j->fixed.data(), nullptr);
       if(st == ICB_OK)
@@ -131,7 +135,7 @@ struct icb_server_s
         o.iter_seconds = j->iters.data();
         st = runOne(p, j->kind, o, j->rho0.data(), j->hist.data(), j->x.data());
       }
-      std::string err = st == ICB_OK ? "" : icb_last_error();
+      std::string err = st == ICB_OK ? "" : ctxStatus != ICB_OK ? ctxError : icb_last_error();
       icb_problem_destroy(p);
       {
         std::lock_guard<std::mutex> lk(mu);
@@ -147,6 +151,29 @@ struct icb_server_s
     icb_ctx_destroy(ctx);
   }
 };
+
+namespace
+{
+/// cancels the queued jobs, lets the running ones finish and joins the workers
+void stopAll(icb_server_s &s)
+{
+  {
+    std::lock_guard<std::mutex> lk(s.mu);
+    s.stopping = true;
+    for(auto &j : s.queue)
+    {
+      j->state = ICB_JOB_CANCELLED;
+      j->status = ICB_ERR_STATE;
+      j->error = "server stopped";
+    }
+    s.queue.clear();
+  }
+  s.cv.notify_all();
+  s.doneCv.notify_all();
+  for(auto &t : s.workers)
+    t.join();
+}
+} // namespace
 
 extern "C" {
 
@@ -166,34 +193,41 @@ long long icb_job_footprint(const icb_grid_desc *g, int kind)
 
 int icb_server_create(int device, long long budget_bytes, int slots, icb_server *out)
 {
+  ICB_API_BEGIN
   if(!out || slots < 1 || budget_bytes <= 0)
-  {
-    set_error("bad server arguments");
-    return ICB_ERR_BAD_ARG;
-  }
-  auto s = new icb_server_s;
+    throw Error{ICB_ERR_BAD_ARG, "bad server arguments"};
+  auto s = std::make_unique<icb_server_s>();
   s->device = device;
   s->budget = budget_bytes;
   s->slots = slots;
-  for(int i = 0; i < slots; i++)
-    s->workers.emplace_back([s] { s->worker(); });
-  *out = s;
-  return ICB_OK;
+  try
+  {
+    for(int i = 0; i < slots; i++)
+    {
+      icb_server_s *raw = s.get();
+      s->workers.emplace_back([raw] { raw->worker(); });
+    }
+  }
+  catch(...)
+  {
+    // a thread that could not start: stop and join the ones that did
+    stopAll(*s);
+    throw;
+  }
+  *out = s.release();
+  ICB_API_END
 }
 
 int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
 {
+  ICB_API_BEGIN
   if(!s || !jd || !jd->fixed || !jd->load || !jd->rho0 || jd->loop.nsteps <= 0)
-  {
-    set_error("bad job");
-    return ICB_ERR_BAD_ARG;
-  }
+    throw Error{ICB_ERR_BAD_ARG, "bad job"};
+  if(jd->kind != ICB_JOB_OC && jd->kind != ICB_JOB_MMA)
+    throw Error{ICB_ERR_BAD_ARG, "job kind must be ICB_JOB_OC or ICB_JOB_MMA"};
   const icb_grid_desc &g = jd->grid;
   if((g.dim != 2 && g.dim != 3) || g.nx < 1 || g.ny < 1 || (g.dim == 3 && g.nz < 1))
-  {
-    set_error("bad grid");
-    return ICB_ERR_BAD_ARG;
-  }
+    throw Error{ICB_ERR_BAD_ARG, "bad grid"};
   auto j = std::make_shared<Job>();
   j->grid = g;
   j->kind = jd->kind;
@@ -224,10 +258,7 @@ int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if(j->bytes > s->budget)
-    {
-      set_error("job needs more device memory than the server budget");
-      return ICB_ERR_REJECTED;
-    }
+      throw Error{ICB_ERR_REJECTED, "job needs more device memory than the server budget"};
     j->id = s->nextId++;
     j->submit = s->now();
     s->jobs[j->id] = j;
@@ -236,7 +267,7 @@ int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
   s->cv.notify_all();
   if(id)
     *id = j->id;
-  return ICB_OK;
+  ICB_API_END
 }
 
 int icb_server_wait(icb_server s, long long id, double timeout_s, icb_job_info *info)
@@ -345,20 +376,7 @@ int icb_server_destroy(icb_server s)
 {
   if(!s)
     return ICB_OK;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->stopping = true;
-    for(auto &j : s->queue)
-    {
-      j->state = ICB_JOB_CANCELLED;
-      j->status = ICB_ERR_STATE;
-    }
-    s->queue.clear();
-  }
-  s->cv.notify_all();
-  s->doneCv.notify_all();
-  for(auto &t : s->workers)
-    t.join();
+  stopAll(*s);
   delete s;
   return ICB_OK;
 }
@@ -367,11 +385,9 @@ int icb_run_batch(int n, const icb_problem *probs, const int *kinds, const icb_l
                   const double *const *rho0, double *const *hist, double *const *xout,
                   int nworkers, int *status)
 {
+  ICB_API_BEGIN
   if(n < 0 || !probs || !opts || !rho0 || !hist || nworkers < 1)
-  {
-    set_error("bad batch arguments");
-    return ICB_ERR_BAD_ARG;
-  }
+    throw Error{ICB_ERR_BAD_ARG, "bad batch arguments"};
   std::atomic<int> next{0};
   std::vector<int> st(n, ICB_OK);
   std::vector<std::string> err(n);
@@ -385,8 +401,17 @@ int icb_run_batch(int n, const icb_problem *probs, const int *kinds, const icb_l
     }
   };
   std::vector<std::thread> th;
-  for(int w = 0; w < std::min(nworkers, std::max(n, 1)); w++)
-    th.emplace_back(work);
+  try
+  {
+    for(int w = 0; w < std::min(nworkers, std::max(n, 1)); w++)
+      th.emplace_back(work);
+  }
+  catch(const std::system_error &)
+  {
+    // fewer threads than asked for: the ones that started take every instance
+  }
+  if(th.empty())
+    work();
   for(auto &t : th)
     t.join();
   int first = ICB_OK;
@@ -401,6 +426,7 @@ int icb_run_batch(int n, const icb_problem *probs, const int *kinds, const icb_l
     }
   }
   return first;
+  ICB_API_END
 }
 
 } // extern "C"

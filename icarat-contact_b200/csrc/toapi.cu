@@ -46,25 +46,6 @@ struct icb_gcmma_s
 
 namespace
 {
-#define API_TRY try {
-#define API_CATCH                                                                          \
-  }                                                                                        \
-  catch(const Error &e)                                                                    \
-  {                                                                                        \
-    set_error(e.msg);                                                                      \
-    return e.code;                                                                         \
-  }                                                                                        \
-  catch(const std::bad_alloc &)                                                            \
-  {                                                                                        \
-    set_error("host allocation failed");                                                   \
-    return ICB_ERR_OOM;                                                                    \
-  }                                                                                        \
-  catch(const std::exception &e)                                                           \
-  {                                                                                        \
-    set_error(e.what());                                                                   \
-    return ICB_ERR_STATE;                                                                  \
-  }                                                                                        \
-  return ICB_OK;
 
 void need(bool c, const char *m)
 {
@@ -214,7 +195,7 @@ extern "C" {
 // ----------------------------------------------------------------- cone ----
 int icb_cone_create(icb_problem p, double radius, icb_cone *out)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(out != nullptr, "out is NULL");
   needFinal(p);
   ICB_CUDA(cudaSetDevice(p->ctx->device));
@@ -223,31 +204,31 @@ int icb_cone_create(icb_problem p, double radius, icb_cone *out)
   c->f = std::make_unique<ConeFilter>(p->d, p->hs->h, radius, p->stream());
   ICB_CUDA(cudaStreamSynchronize(p->stream()));
   *out = c.release();
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_cone_destroy(icb_cone c)
 {
-  API_TRY
+  ICB_API_BEGIN
   delete c;
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_cone_filter_device(icb_cone c, const double *in, double *out, int isSens)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(c && in && out, "NULL argument");
   ICB_CUDA(cudaSetDevice(c->p->ctx->device));
   if(isSens)
     c->f->adjoint(in, out, c->p->stream());
   else
     c->f->forward(in, out, 0.0, 0.5, nullptr, nullptr, c->p->stream());
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_cone_filter(icb_cone c, const double *in, double *out, int isSens)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(c && in && out, "NULL argument");
   long long n = c->p->d.nel;
   cudaStream_t s = c->p->stream();
@@ -261,13 +242,13 @@ int icb_cone_filter(icb_cone c, const double *in, double *out, int isSens)
     c->f->forward(c->a.p, c->b.p, 0.0, 0.5, nullptr, nullptr, s);
   ICB_CUDA(cudaMemcpyAsync(out, c->b.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_threshold(icb_ctx ctx, long long n, const double *x, double beta, double T, double *xhat,
                   double *dxhat)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(ctx && x && n >= 0, "bad argument");
   need(beta > 0.0, "beta must be > 0");
   ICB_CUDA(cudaSetDevice(ctx->device));
@@ -280,13 +261,13 @@ int icb_threshold(icb_ctx ctx, long long n, const double *x, double beta, double
   if(dxhat)
     ICB_CUDA(cudaMemcpyAsync(dxhat, c.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 // ------------------------------------------------------------ Helmholtz ----
 int icb_helm_create(icb_problem p, double radius, icb_helm *out)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(out != nullptr, "out is NULL");
   needFinal(p);
   ICB_CUDA(cudaSetDevice(p->ctx->device));
@@ -295,19 +276,19 @@ int icb_helm_create(icb_problem p, double radius, icb_helm *out)
   h->f = std::make_unique<HelmFilter>(p->d, p->hs->h, radius, p->stream());
   ICB_CUDA(cudaStreamSynchronize(p->stream()));
   *out = h.release();
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_helm_destroy(icb_helm h)
 {
-  API_TRY
+  ICB_API_BEGIN
   delete h;
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_helm_filter(icb_helm h, const double *in, double *out, int sensFlag)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(h && in && out, "NULL argument");
   long long n = h->p->d.nel;
   cudaStream_t s = h->p->stream();
@@ -321,7 +302,7 @@ int icb_helm_filter(icb_helm h, const double *in, double *out, int sensFlag)
   ICB_CUDA(cudaStreamSynchronize(s));
   if(st != ICB_OK)
     throw Error{st, "Helmholtz filter solve did not converge"};
-  API_CATCH
+  ICB_API_END
 }
 
 // ------------------------------------------------------------------- OC ----
@@ -329,7 +310,7 @@ int icb_oc_update(icb_problem p, icb_cone cone, double *x, const double *dfdx, d
                   const double *dgdx, const double *xmin, const double *xmax, double movelimit,
                   double beta, double T, int *steps)
 {
-  API_TRY
+  ICB_API_BEGIN
   needFinal(p);
   need(x && dfdx && dgdx && xmin && xmax, "NULL argument");
   ICB_CUDA(cudaSetDevice(p->ctx->device));
@@ -353,13 +334,13 @@ int icb_oc_update(icb_problem p, icb_cone cone, double *x, const double *dfdx, d
   ICB_CUDA(cudaStreamSynchronize(s));
   if(steps)
     *steps = k;
-  API_CATCH
+  ICB_API_END
 }
 
 // ------------------------------------------------------------------ MMA ----
 int icb_mma_create(icb_ctx ctx, long long n, int m, icb_mma *out)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(ctx && out && n > 0, "bad argument");
   need(m == 1, "the device MMA supports one constraint (m = 1)");
   ICB_CUDA(cudaSetDevice(ctx->device));
@@ -369,20 +350,20 @@ int icb_mma_create(icb_ctx ctx, long long n, int m, icb_mma *out)
   for(DevBuf<double> *b : {&h->x, &h->df, &h->dg, &h->lo, &h->hi})
     b->alloc(n);
   *out = h.release();
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_mma_destroy(icb_mma h)
 {
-  API_TRY
+  ICB_API_BEGIN
   delete h;
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_mma_update(icb_mma h, double *x, const double *dfdx, const double *gx,
                    const double *dgdx, const double *xmin, const double *xmax)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(h && x && dfdx && gx && dgdx && xmin && xmax, "NULL argument");
   ICB_CUDA(cudaSetDevice(h->ctx->device));
   cudaStream_t s = h->ctx->stream;
@@ -395,13 +376,13 @@ int icb_mma_update(icb_mma h, double *x, const double *dfdx, const double *gx,
   h->m->update(h->x.p, h->df.p, gx[0], h->dg.p, h->lo.p, h->hi.p, s);
   ICB_CUDA(cudaMemcpyAsync(x, h->x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 // --------------------------------------------------------------- GCMMA ----
 int icb_gcmma_create(icb_ctx ctx, long long n, int m, icb_gcmma *out)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(ctx && out && n > 0, "bad argument");
   need(m == 1, "the device GCMMA supports one constraint (m = 1)");
   ICB_CUDA(cudaSetDevice(ctx->device));
@@ -412,14 +393,14 @@ int icb_gcmma_create(icb_ctx ctx, long long n, int m, icb_gcmma *out)
     b->alloc(n);
   ICB_CUDA(cudaStreamSynchronize(ctx->stream));
   *out = h.release();
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_gcmma_destroy(icb_gcmma h)
 {
-  API_TRY
+  ICB_API_BEGIN
   delete h;
-  API_CATCH
+  ICB_API_END
 }
 
 namespace
@@ -443,7 +424,7 @@ int icb_gcmma_outer(icb_gcmma h, double *xmma, const double *xval, double f0x,
                     const double *df0dx, const double *fx, const double *dfdx, const double *xmin,
                     const double *xmax)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(xmma && fx, "NULL argument");
   gcmmaUpload(h, xval, df0dx, dfdx, xmin, xmax);
   cudaStream_t s = h->ctx->stream;
@@ -451,14 +432,14 @@ int icb_gcmma_outer(icb_gcmma h, double *xmma, const double *xval, double f0x,
   ICB_CUDA(cudaMemcpyAsync(xmma, h->xm.p, sizeof(double) * h->g->core.n, cudaMemcpyDeviceToHost,
                            s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_gcmma_inner(icb_gcmma h, double *xmma, double f0xnew, const double *fxnew,
                     const double *xval, double f0x, const double *df0dx, const double *fx,
                     const double *dfdx, const double *xmin, const double *xmax)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(xmma && fxnew && fx, "NULL argument");
   gcmmaUpload(h, xval, df0dx, dfdx, xmin, xmax);
   cudaStream_t s = h->ctx->stream;
@@ -468,15 +449,15 @@ int icb_gcmma_inner(icb_gcmma h, double *xmma, double f0xnew, const double *fxne
               s);
   ICB_CUDA(cudaMemcpyAsync(xmma, h->xm.p, b, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 int icb_gcmma_concheck(icb_gcmma h, double f0xnew, const double *fxnew, int *conservative)
 {
-  API_TRY
+  ICB_API_BEGIN
   need(h && fxnew && conservative, "NULL argument");
   *conservative = h->g->concheck(f0xnew, fxnew[0]) ? 1 : 0;
-  API_CATCH
+  ICB_API_END
 }
 
 // ---------------------------------------------------------------- loops ----
@@ -485,7 +466,7 @@ int icb_gcmma_concheck(icb_gcmma h, double f0xnew, const double *fxnew, int *con
 int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
                double *xout)
 {
-  API_TRY
+  ICB_API_BEGIN
   needFinal(p);
   need(o && rho0 && hist, "NULL argument");
   need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
@@ -549,7 +530,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 /// The opt-mma-HelmholtzFilter loop (opt_mma_Helmholtz.cpp:81-163) on the
@@ -558,7 +539,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
 int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
                 double *xout)
 {
-  API_TRY
+  ICB_API_BEGIN
   needFinal(p);
   need(o && rho0 && hist, "NULL argument");
   need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
@@ -656,7 +637,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 /// The opt_macro_gcmma loop (opt_macro_gcmma.cpp:83-238) on the device:
@@ -667,7 +648,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
 int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, double *hist,
                   int *inner, double *xout)
 {
-  API_TRY
+  ICB_API_BEGIN
   needFinal(p);
   need(o && rho0 && hist, "NULL argument");
   need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
@@ -747,7 +728,7 @@ int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, dou
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));
-  API_CATCH
+  ICB_API_END
 }
 
 } // extern "C"
