@@ -14,15 +14,21 @@
 // src/analysis/solver/solvers.cpp:64-92); this is the B200 replacement of
 // that solve for large grids.  Design:
 //  * levels by 2:1 coarsening of the element grid (ceil for odd counts: the
-//    last coarse element then sticks out of the domain and only averages the
-//    children that exist), coarse moduli = mean of the children's E, coarse
-//    element matrix = K0 of the 2h element (rediscretisation; equal to the
-//    Galerkin product for constant coefficients);
+//    last coarse element then sticks out of the domain, and its modulus sums
+//    the children that exist over all its child slots), coarse moduli = mean
+//    of the children's E, coarse element matrix = K0 of the 2h element
+//    (rediscretisation; equal to the Galerkin product for constant
+//    coefficients).  An axis that is one element thick is kept while the
+//    others halve (semi-coarsening), so thin and high-aspect grids still
+//    reach a small coarsest system; the coarse elements then change shape
+//    and the smoother's eigenvalue bound covers every level's K0;
 //  * transfer: (bi/tri)linear prolongation P, restriction R = P^T;
 //    constrained DOFs are masked on every level (a coarse DOF is constrained
-//    when the fine DOF at the same point is);
-//  * smoother: damped Jacobi with the fused operator epilogue (one kernel per
-//    sweep), nu sweeps before and after the coarse correction;
+//    when a constrained fine DOF interpolates from it);
+//  * smoother: Chebyshev polynomial in D^-1 K of degree nu on
+//    [lmax/10, lmax], one fused operator kernel per step (three-term form),
+//    before and after the coarse correction; the first pre-smoothing step
+//    starts from zero and needs no operator;
 //  * coarsest level (<= 160 DOFs by default): dense FP64 inverse built on
 //    the device (one CTA, Gauss-Jordan in shared memory), applied as a
 //    dense product.
@@ -62,33 +68,38 @@ __device__ __forceinline__ bool gated(const KState *g)
 }
 
 // ------------------------------------------------------- grid transfer ----
+/// coarse modulus = sum of the children's E over the number of child slots
+/// (2 per halved axis, 1 per kept one; slots outside the fine grid add 0)
 template <typename T>
-__global__ void k_coarsen_E(Dims df, Dims dc, const T *__restrict__ Ef, T *__restrict__ Ec)
+__global__ void k_coarsen_E(Dims df, Dims dc, int3 sh, const T *__restrict__ Ef,
+                            T *__restrict__ Ec)
 {
   long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if(e >= dc.nel)
     return;
   int ci = int(e % dc.nx), cj = int((e / dc.nx) % dc.ny), ck = int(e / ((long long)dc.nx * dc.ny));
   double s = 0.0;
-  int nk = df.dim == 3 ? 2 : 1;
+  const int nk = df.dim == 3 ? 1 << sh.z : 1;
   for(int c = 0; c < nk; c++)
-    for(int b = 0; b < 2; b++)
-      for(int a = 0; a < 2; a++)
+    for(int b = 0; b < (1 << sh.y); b++)
+      for(int a = 0; a < (1 << sh.x); a++)
       {
-        int i = 2 * ci + a, j = 2 * cj + b, k = 2 * ck + c;
+        int i = (ci << sh.x) + a, j = (cj << sh.y) + b, k = (ck << sh.z) + c;
         if(i < df.nx && j < df.ny && (df.dim == 2 || k < df.nz))
           s += double(Ef[i + (long long)j * df.nx + (long long)k * df.nx * df.ny]);
       }
-  Ec[e] = T(s / (df.dim == 3 ? 8.0 : 4.0));
+  Ec[e] = T(s / double((1 << sh.x) * (1 << sh.y) * nk));
 }
 
 /// b_c = R r_f (R = P^T), constrained coarse DOFs zeroed.  One thread per
 /// coarse node (x along threads, y and z along the grid, so no index
-/// division): the 1-D weights of the fine neighbours 2I-1, 2I, 2I+1 are
-/// 1/2, 1, 1/2 (those inside the fine grid), applied row by row.
+/// division): along a halved axis the 1-D weights of the fine neighbours
+/// 2I-1, 2I, 2I+1 are 1/2, 1, 1/2 (those inside the fine grid), along a kept
+/// axis (shift 0) the fine node I alone has weight 1; applied row by row.
 template <typename T>
-__global__ void k_restrict(Dims df, Dims dc, const T *__restrict__ rf, T *__restrict__ bc,
-                           const uint8_t *__restrict__ fixc, const KState *gate)
+__global__ void k_restrict(Dims df, Dims dc, int3 sh, const T *__restrict__ rf,
+                           T *__restrict__ bc, const uint8_t *__restrict__ fixc,
+                           const KState *gate)
 {
   if(gated(gate))
     return;
@@ -96,23 +107,23 @@ __global__ void k_restrict(Dims df, Dims dc, const T *__restrict__ rf, T *__rest
   if(I >= dc.sx)
     return;
   const long long fsxy = (long long)df.sx * df.sy;
-  const int kr = df.dim == 3 ? 1 : 0;
+  const int kr = df.dim == 3 ? sh.z : 0;
   const T h = T(0.5);
   T s[3] = {T(0), T(0), T(0)};
   for(int dk = -kr; dk <= kr; dk++)
   {
-    const int k = 2 * K + dk;
+    const int k = (K << sh.z) + dk;
     if(k < 0 || k >= df.sz)
       continue;
     T sk[3] = {T(0), T(0), T(0)};
-    for(int dj = -1; dj <= 1; dj++)
+    for(int dj = -sh.y; dj <= sh.y; dj++)
     {
-      const int j = 2 * J + dj;
+      const int j = (J << sh.y) + dj;
       if(j < 0 || j >= df.sy)
         continue;
       const long long row = (long long)j * df.sx + (long long)k * fsxy;
-      const int i = 2 * I;
-      const bool lo = i - 1 >= 0, mid = i < df.sx, hi = i + 1 < df.sx;
+      const int i = I << sh.x;
+      const bool lo = sh.x && i - 1 >= 0, mid = i < df.sx, hi = sh.x && i + 1 < df.sx;
 #pragma unroll
       for(int c = 0; c < 3; c++)
         if(c < df.dim)
@@ -128,25 +139,29 @@ __global__ void k_restrict(Dims df, Dims dc, const T *__restrict__ rf, T *__rest
   }
   const long long n = I + (long long)J * dc.sx + (long long)K * dc.sx * dc.sy;
   const unsigned fx = fixc[n];
-  for(int c = 0; c < dc.dim; c++)
-    bc[c * dc.ld + n] = ((fx >> c) & 1u) ? T(0) : s[c];
+#pragma unroll
+  for(int c = 0; c < 3; c++)
+    if(c < dc.dim)
+      bc[c * dc.ld + n] = ((fx >> c) & 1u) ? T(0) : s[c];
 }
 
 /// x_f += P x_c, constrained fine DOFs untouched (they stay 0).  One thread
 /// per fine node (x along threads, y and z along the grid): the trilinear
-/// interpolant as three nested midpoints; an even index takes the same
-/// coarse node twice, which the midpoint returns exactly.
+/// interpolant as three nested midpoints; an even index on a halved axis, and
+/// every index on a kept one, takes the same coarse node twice, which the
+/// midpoint returns exactly.
 template <typename T>
-__global__ void k_prolong_add(Dims df, Dims dc, const T *__restrict__ xc, T *__restrict__ xf,
-                              const uint8_t *__restrict__ fixf, const KState *gate)
+__global__ void k_prolong_add(Dims df, Dims dc, int3 sh, const T *__restrict__ xc,
+                              T *__restrict__ xf, const uint8_t *__restrict__ fixf,
+                              const KState *gate)
 {
   if(gated(gate))
     return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if(i >= df.sx)
     return;
-  const int I0 = i >> 1, I1 = (i + 1) >> 1, J0 = j >> 1, J1 = (j + 1) >> 1;
-  const int K0 = k >> 1, K1 = df.dim == 3 ? (k + 1) >> 1 : K0;
+  const int I0 = i >> sh.x, I1 = (i + sh.x) >> sh.x, J0 = j >> sh.y, J1 = (j + sh.y) >> sh.y;
+  const int K0 = k >> sh.z, K1 = df.dim == 3 ? (k + sh.z) >> sh.z : K0;
   const long long csxy = (long long)dc.sx * dc.sy;
   const long long r00 = (long long)J0 * dc.sx + K0 * csxy, r10 = (long long)J1 * dc.sx + K0 * csxy;
   const long long r01 = (long long)J0 * dc.sx + K1 * csxy, r11 = (long long)J1 * dc.sx + K1 * csxy;
@@ -578,6 +593,9 @@ template <typename T> double element_lmax(int dim, const T *K)
 template <typename T> struct Level
 {
   Dims d;
+  /// coarsening from the next finer level, per axis: 1 halves the element
+  /// count (ceil), 0 keeps an axis that is one element thick
+  int3 sh = make_int3(1, 1, 1);
   double h[3];
   T K[576]; ///< unit element matrix of this level (passed by value)
   DevBuf<T> Eown;
@@ -638,22 +656,7 @@ template <typename TK, typename TP> struct MgPcg
     // before it goes out of scope
     nu = smooth > 0 ? smooth : 2;
     lmax = element_lmax(hs.desc.dim, Kfine);
-    // Chebyshev coefficients of steps 0..nu-1 (Saad, Iterative Methods for
-    // Sparse Linear Systems, 2nd ed., Alg. 12.1) on [lmax/10, lmax]
-    {
-      double a = lmax / 10.0, b = lmax, theta = 0.5 * (b + a), delta = 0.5 * (b - a);
-      double sigma = theta / delta, rho0 = 1.0 / sigma;
-      cc1.assign(nu, 0.0);
-      cc2.assign(nu, 0.0);
-      cc2[0] = 1.0 / theta;
-      for(int k = 1; k < nu; k++)
-      {
-        double rho1 = 1.0 / (2.0 * sigma - rho0);
-        cc1[k] = rho1 * rho0;
-        cc2[k] = 2.0 * rho1 / delta;
-        rho0 = rho1;
-      }
-    }
+    bool shapeChanged = false;
     std::copy(Kkrylov, Kkrylov + 576, Kk);
     Ek = Ekrylov;
     Level<TP> L0;
@@ -677,17 +680,27 @@ template <typename TK, typename TP> struct MgPcg
     {
       const Dims &f = lv.back().d;
       long long dofs = f.nnode * dim;
-      bool can = f.nx >= 2 && f.ny >= 2 && (dim == 2 || f.nz >= 2);
-      if(dofs <= cd || !can)
+      // semi-coarsening: an axis one element thick is kept, the others halve
+      const int3 sh = make_int3(f.nx >= 2, f.ny >= 2, dim == 3 && f.nz >= 2);
+      if(dofs <= cd || !(sh.x || sh.y || sh.z))
         break;
       Level<TP> c;
-      c.d = make_dims(dim, (f.nx + 1) / 2, (f.ny + 1) / 2, dim == 3 ? (f.nz + 1) / 2 : 1);
+      c.sh = sh;
+      c.d = make_dims(dim, sh.x ? (f.nx + 1) / 2 : f.nx, sh.y ? (f.ny + 1) / 2 : f.ny,
+                      dim == 3 ? (sh.z ? (f.nz + 1) / 2 : f.nz) : 1);
+      const int shk[3] = {sh.x, sh.y, sh.z};
       for(int k = 0; k < 3; k++)
-        c.h[k] = 2.0 * lv.back().h[k];
+        c.h[k] = shk[k] ? 2.0 * lv.back().h[k] : lv.back().h[k];
       double Kd[576];
       unit_stiffness(dim, hs.desc.state, hs.desc.poisson, c.h, Kd);
       for(int i = 0; i < 576; i++)
         c.K[i] = TP(Kd[i]);
+      // the elements change shape when some axes halve and others do not;
+      // the smoother's bound must then hold for this level's K0 too
+      if(sh.x != sh.y || (dim == 3 && sh.y != sh.z))
+        shapeChanged = true;
+      if(shapeChanged)
+        lmax = std::max(lmax, element_lmax(dim, c.K));
       // coarse mask: a coarse DOF is constrained when a constrained fine DOF
       // interpolates from it (P(i, I) != 0); for constraints on even grid
       // lines this is the fine DOF at the same point, a constraint at an odd
@@ -699,8 +712,8 @@ template <typename TK, typename TP> struct MgPcg
         if(!fm[nd])
           continue;
         long long i = nd % f.sx, j = (nd / f.sx) % f.sy, k = nd / ((long long)f.sx * f.sy);
-        long long I0 = i / 2, I1 = (i + 1) / 2, J0 = j / 2, J1 = (j + 1) / 2, K0 = k / 2,
-                  K1 = dim == 3 ? (k + 1) / 2 : 0;
+        long long I0 = i >> sh.x, I1 = (i + sh.x) >> sh.x, J0 = j >> sh.y,
+                  J1 = (j + sh.y) >> sh.y, K0 = k >> sh.z, K1 = dim == 3 ? (k + sh.z) >> sh.z : 0;
         for(long long K = K0; K <= K1; K++)
           for(long long J = J0; J <= J1; J++)
             for(long long I = I0; I <= I1; I++)
@@ -714,6 +727,22 @@ template <typename TK, typename TP> struct MgPcg
       c.E = c.Eown.p;
       fm.swap(cm);
       lv.push_back(std::move(c));
+    }
+    // Chebyshev coefficients of steps 0..nu-1 (Saad, Iterative Methods for
+    // Sparse Linear Systems, 2nd ed., Alg. 12.1) on [lmax/10, lmax]
+    {
+      double a = lmax / 10.0, b = lmax, theta = 0.5 * (b + a), delta = 0.5 * (b - a);
+      double sigma = theta / delta, rho0 = 1.0 / sigma;
+      cc1.assign(nu, 0.0);
+      cc2.assign(nu, 0.0);
+      cc2[0] = 1.0 / theta;
+      for(int k = 1; k < nu; k++)
+      {
+        double rho1 = 1.0 / (2.0 * sigma - rho0);
+        cc1[k] = rho1 * rho0;
+        cc2[k] = 2.0 * rho1 / delta;
+        rho0 = rho1;
+      }
     }
     for(size_t l = 0; l < lv.size(); l++)
     {
@@ -784,7 +813,7 @@ template <typename TK, typename TP> struct MgPcg
   {
     for(size_t l = 1; l < lv.size(); l++)
     {
-      k_coarsen_E<TP><<<nblocks(lv[l].d.nel, 256), 256, 0, s>>>(lv[l - 1].d, lv[l].d,
+      k_coarsen_E<TP><<<nblocks(lv[l].d.nel, 256), 256, 0, s>>>(lv[l - 1].d, lv[l].d, lv[l].sh,
                                                                 lv[l - 1].E, lv[l].Eown.p);
       count_launch();
     }
@@ -862,10 +891,10 @@ template <typename TK, typename TP> struct MgPcg
     res.gateConv = 1;
     launch_op<TP>(L.d, L.K, L.E, cur, L.r.p, L.fix, s, res);
     Level<TP> &Cn = lv[l + 1];
-    k_restrict<TP><<<grid3(Cn.d), kTB, 0, s>>>(L.d, Cn.d, L.r.p, Cn.b.p, Cn.fix, gate);
+    k_restrict<TP><<<grid3(Cn.d), kTB, 0, s>>>(L.d, Cn.d, Cn.sh, L.r.p, Cn.b.p, Cn.fix, gate);
     count_launch();
     level(l + 1, Cn.b.p, Cn.x.p, s, gate);
-    k_prolong_add<TP><<<grid3(L.d), kTB, 0, s>>>(L.d, Cn.d, Cn.x.p, cur, L.fix, gate);
+    k_prolong_add<TP><<<grid3(L.d), kTB, 0, s>>>(L.d, Cn.d, Cn.sh, Cn.x.p, cur, L.fix, gate);
     count_launch();
     for(int k = 0; k < nu; k++)
     {

@@ -13,6 +13,9 @@ Workloads (sizes as stated; all inputs synthetic and seeded):
   halfmbb3d     384x128x128 Hex8 half-MBB beam (ux = 0 on x = 0, uz = 0 on
                 the line x = L, z = 0, uy = 0 on y = 0; line load in -z along
                 x = 0, z = H).
+  strip2d       a long Q4 strip clamped along its bottom edge (y = 0), unit
+                downward load at the top-edge middle node, 0.5 along x at the
+                top node at x = L/4 (thin grids that stay well conditioned).
 """
 import numpy as np
 
@@ -56,7 +59,18 @@ def _mask_halfmbb2d(nx, ny):
     return fixed.reshape(-1), f.reshape(-1)
 
 
+def _mask_strip2d(nx, ny):
+    fixed = np.zeros((ny + 1, nx + 1, 2), np.uint8)
+    fixed[0, :, :] = 1
+    f = np.zeros((ny + 1, nx + 1, 2))
+    f[ny, nx // 2, 1] = -1.0
+    f[ny, nx // 4, 0] = 0.5
+    return fixed.reshape(-1), f.reshape(-1)
+
+
 def masks(kind, nx, ny, nz=1):
+    if kind == "strip2d":
+        return _mask_strip2d(nx, ny)
     if kind == "halfmbb2d":
         return _mask_halfmbb2d(nx, ny)
     if kind == "cantilever2d":
