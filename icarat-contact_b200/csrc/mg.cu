@@ -851,9 +851,12 @@ template <typename TK, typename TP> struct MgPcg
     const Level<TP> &C = lv.back();
     long long m = (long long)C.d.dim * C.d.ld;
     k_fill<TP><<<vblocks(m), VB, 0, s>>>(m, TP(0), x);
+    count_launch();
     if(nc)
+    {
       k_dense_apply<TP><<<8, 256, sizeof(double) * nc, s>>>(nc, cA.p, cSoa.p, b, x, gate);
-    count_launch(2);
+      count_launch();
+    }
   }
 
   /// out = V-cycle(b) on level l

@@ -1185,18 +1185,22 @@ void launch_gather_free(const Dims &d, const long long *freeIdx, long long numeq
 {
   (void)d;
   if(numeq)
+  {
     k_gather_free<<<blocks_for(numeq, 256), 256, 0, s>>>(numeq, freeIdx, soa, numeqv);
+    count_launch();
+  }
   ICB_CUDA(cudaGetLastError());
-  count_launch();
 }
 void launch_scatter_free(const Dims &d, const long long *freeIdx, long long numeq,
                          const double *numeqv, double *soa, cudaStream_t s)
 {
   (void)d;
   if(numeq)
+  {
     k_scatter_free<<<blocks_for(numeq, 256), 256, 0, s>>>(numeq, freeIdx, numeqv, soa);
+    count_launch();
+  }
   ICB_CUDA(cudaGetLastError());
-  count_launch();
 }
 void launch_simp(long long n, double y1, double y2, double p, const double *rho, double *E,
                  float *Ef, cudaStream_t s)

@@ -435,9 +435,12 @@ __global__ void k_mma_pass(long long n, MmaVec V, double *__restrict__ x, MmaPar
     if(xi > V.beta[i])
       xi = V.beta[i];
     x[i] = xi;
-    v[0] += V.pij[i] / (upp - xi) + V.qij[i] / (xi - low);
-    double PQ = V.pij[i] / pow(upp - xi, 2.0) - V.qij[i] / pow(xi - low, 2.0);
-    double df2 = -1.0 / (2.0 * pl / pow(upp - xi, 3.0) + 2.0 * ql / pow(xi - low, 3.0));
+    // MMASolver's pow(d, 2.0) and pow(d, 3.0) as products (the square is the
+    // correctly rounded pow; the cube is within an ulp of it)
+    const double du = upp - xi, dl = xi - low, du2 = du * du, dl2 = dl * dl;
+    v[0] += V.pij[i] / du + V.qij[i] / dl;
+    double PQ = V.pij[i] / du2 - V.qij[i] / dl2;
+    double df2 = -1.0 / (2.0 * pl / (du2 * du) + 2.0 * ql / (dl2 * dl));
     if(xp < V.alpha[i] || xp > V.beta[i])
       df2 = 0.0;
     v[1] += PQ * df2 * PQ;

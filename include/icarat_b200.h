@@ -75,7 +75,7 @@ typedef struct
   double tol;     /* relative residual ||r||/||f|| (Solvers tol_, 1e-10)    */
   int maxit;      /* Solvers maxIter_ (10000)                               */
   double inner_tol; /* reserved (0)                                       */
-  int mg_smooth;  /* GMG: Jacobi sweeps before and after (0 = default)      */
+  int mg_smooth;  /* GMG: Chebyshev smoothing steps before and after (0 = 2) */
   int mg_coarse_dofs; /* GMG: coarsen while the grid has more DOFs (0 = 160, at most 1024) */
 } icb_solve_opts;
 

@@ -129,6 +129,30 @@ def test_zero_load_and_errors(ctx):
         icb.Problem(ctx, 4, 2, 2)
 
 
+@pytest.mark.parametrize("dim,n", [(2, (8, 4)), (3, (6, 3, 4))])
+def test_zero_load_and_fully_constrained_with_every_solver(ctx, dim, n):
+    """A problem with no load and one with every DOF constrained (numeq = 0)
+    solve at iteration 0 with every solver and give zero compliance and
+    sensitivities."""
+    box = [0, n[0], 0, n[1], 0, n[2] if dim == 3 else 0]
+    free = icb.Problem(ctx, dim, *n)
+    free.dirichlet_box([1] * dim, [0.0] * dim, [0, 0] + box[2:])
+    free.finalize()
+    fixed = icb.Problem(ctx, dim, *n)
+    fixed.dirichlet_box([1] * dim, [0.0] * dim, box)
+    fixed.finalize()
+    assert fixed.numeq == 0
+    for g in (free, fixed):
+        g.set_density(np.full(g.nel, 0.5))
+        for precision, precond in ((icb.FP64, icb.JACOBI), (icb.FP64, icb.GMG),
+                                   (icb.MIXED, icb.GMG)):
+            info = g.solve(precision=precision, precond=precond)
+            assert info["iters"] == 0, (precision, precond, info)
+            assert g.compliance() == 0.0
+            assert not g.sensitivity().any()
+            assert not g.displacement().any()
+
+
 def test_maxit_status(ctx):
     g = cases.build_gpu(ctx, "cantilever2d", 40, 20)
     g.set_density(cases.uniform_density(g.nel, 3))
