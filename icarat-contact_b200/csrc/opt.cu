@@ -54,7 +54,7 @@ __device__ __forceinline__ double thresh(double x, double beta, double T)
 __device__ __forceinline__ double thresh_d(double x, double beta, double T)
 {
   double t = tanh(beta * (x - T));
-  return (0.5 * (beta * (1.0 - pow(t, 2.0))) / tanh(T * beta));
+  return (0.5 * (beta * (1.0 - t * t)) / tanh(T * beta)); // pow(t, 2.0)
 }
 
 // ---------------------------------------------------------------- cone ----
@@ -128,7 +128,11 @@ __device__ __forceinline__ double oc_candidate(double x, double df, double dg, d
                                                double eta, double move, double xmin,
                                                double xmax)
 {
-  double v = pow(fmax(0.0, -df / (dg * lam)), eta) * x;
+  // OCSolver's pow(B, eta): for the usual eta = 0.5 the square root, which is
+  // that power correctly rounded (the stencil kernel evaluates this for every
+  // neighbour of every element on each bisection step)
+  const double b = fmax(0.0, -df / (dg * lam));
+  double v = (eta == 0.5 ? sqrt(b) : pow(b, eta)) * x;
   double lo = fmax(xmin, (1.0 - move) * x), hi = fmin(xmax, (1.0 + move) * x);
   if(v < lo)
     v = lo;
@@ -314,7 +318,7 @@ __global__ void k_mma_gensub(long long n, MmaVec V, const double *__restrict__ x
     V.alpha[i] = al;
     V.beta[i] = be;
     double inv = 1.0 / fmax(P.xmamieps, range);
-    double u2 = pow(up - xv, 2.0), l2 = pow(xv - lo, 2.0);
+    double u2 = (up - xv) * (up - xv), l2 = (xv - lo) * (xv - lo); // pow(d, 2.0)
     double df = dfdx[i], dg = dgdx[i];
     double pq = 0.001 * fabs(df) + P.raa0 * inv;
     V.p0[i] = u2 * (fmax(0.0, df) + pq);
@@ -526,7 +530,7 @@ __global__ void k_gc_gensub(long long n, MmaVec V, const double *__restrict__ x,
     V.beta[i] = fmin(fmin(xmax[i], up - P.albefa * (up - xv)), xv + P.move * range);
     const double uxinv = 1.0 / (up - xv), xlinv = 1.0 / (xv - lo);
     const double inv = 1.0 / fmax(P.xmamieps, range);
-    const double u2 = pow(up - xv, 2.0), l2 = pow(xv - lo, 2.0);
+    const double u2 = (up - xv) * (up - xv), l2 = (xv - lo) * (xv - lo); // pow(d, 2.0)
     const double df = df0dx[i], dg = dfdx[i];
     const double pq = 0.001 * fabs(df) + raa0 * inv;
     const double p0 = u2 * (fmax(0.0, df) + pq), q0 = l2 * (fmax(0.0, -df) + pq);
