@@ -622,34 +622,36 @@ def workload_serving(args):
     """c5: Poisson job arrivals at each rate lambda into one icb_server (HBM
     budget 150 GB).  Jobs: 70 % 2D Q4 OC (nelx U[64,1024], aspect 2:1), 30 %
     3D Hex8 MMA (nelx U[32,128], nely = nelz = nelx/2), vf U[0.2,0.5],
-    r U[1.5,3]; steps U[50,200] scaled by --iter-scale.  Per rate: jobs/s
-    (completed / makespan), p50/p99 job latency (submit to end) and
-    iteration latency; finally one job re-run alone against its mixed run."""
+    r U[1.5,3]; steps U[50,200] scaled by --iter-scale.  The same seeded job
+    set is submitted at every rate (only the arrival gaps differ), so jobs/s
+    compares one workload across loads.  Per rate: jobs/s (completed /
+    makespan), p50/p99 job latency (submit to end) and iteration latency;
+    finally one job re-run alone against its mixed run."""
     import numpy as np
     import cases
     import icarat_b200 as icb
     rates = args.rates
     out = {}
     probe = None
+    rng = np.random.default_rng(5000)
+    jobs, first, same_all = [], {}, True
+    for _ in range(args.jobs_per_rate):
+        if rng.uniform() < 0.7:
+            inst = cases.random_instance2d(rng, nelx_range=(64, 1024), aspect_fixed=2.0,
+                                           vf_range=(0.2, 0.5), r_range=(1.5, 3.0))
+            kind = icb.JOB_OC
+        else:
+            inst = cases.random_instance3d(rng, nelx_range=(32, 128), vf_range=(0.2, 0.5),
+                                           r_range=(1.5, 3.0))
+            kind = icb.JOB_MMA
+        nsteps = max(1, int(round(rng.integers(50, 201) * args.iter_scale)))
+        nel = inst["nx"] * inst["ny"] * (inst["nz"] if inst["dim"] == 3 else 1)
+        loop = icb.loop_opts(nsteps, inst["r"] if kind == icb.JOB_OC else 2.0 * inst["r"] / 1.5,
+                             move=0.2, precision=icb.MIXED)
+        jobs.append((cases.grid_desc(inst), kind, loop, inst["fixed"], inst["load"],
+                     np.full(nel, inst["vf"])))
     for lam in rates:
-        rng = np.random.default_rng(5000 + int(lam))
-        jobs = []
-        for _ in range(args.jobs_per_rate):
-            if rng.uniform() < 0.7:
-                inst = cases.random_instance2d(rng, nelx_range=(64, 1024), aspect_fixed=2.0,
-                                               vf_range=(0.2, 0.5), r_range=(1.5, 3.0))
-                kind = icb.JOB_OC
-            else:
-                inst = cases.random_instance3d(rng, nelx_range=(32, 128), vf_range=(0.2, 0.5),
-                                               r_range=(1.5, 3.0))
-                kind = icb.JOB_MMA
-            nsteps = max(1, int(round(rng.integers(50, 201) * args.iter_scale)))
-            nel = inst["nx"] * inst["ny"] * (inst["nz"] if inst["dim"] == 3 else 1)
-            loop = icb.loop_opts(nsteps, inst["r"] if kind == icb.JOB_OC else 2.0 * inst["r"] / 1.5,
-                                 move=0.2, precision=icb.MIXED)
-            jobs.append((cases.grid_desc(inst), kind, loop, inst["fixed"], inst["load"],
-                         np.full(nel, inst["vf"])))
-        gaps = rng.exponential(1.0 / lam, len(jobs))
+        gaps = np.random.default_rng(6000 + int(lam)).exponential(1.0 / lam, len(jobs))
         srv = icb.Server(budget_bytes=150 << 30, slots=args.slots)
         t0 = time.perf_counter()
         ids, tnext = [], t0
@@ -664,6 +666,10 @@ def workload_serving(args):
             if rc == 0 and info.status == 0:
                 ok += 1
                 h, x, it = srv.result(jid)
+                if k in first:  # the same job at an earlier rate
+                    same_all = same_all and np.array_equal(h, first[k][0]) and np.array_equal(x, first[k][1])
+                else:
+                    first[k] = (h, x)
                 lat.append(info.end_s - info.submit_s)
                 its.extend(it.tolist())
                 ends.append(info.end_s)
@@ -693,7 +699,8 @@ def workload_serving(args):
                       "config": {"workload": "70% 2D Q4 OC nelx 64-1024 aspect 2:1, 30% 3D Hex8 MMA nelx 32-128",
                                  "jobs_per_rate": args.jobs_per_rate, "iter_scale": args.iter_scale,
                                  "slots": args.slots},
-                      "rates": out, "alone_vs_mixed_bitwise_equal": alone_equal}), flush=True)
+                      "rates": out, "alone_vs_mixed_bitwise_equal": alone_equal,
+                      "same_results_at_every_rate": same_all}), flush=True)
     return 0
 
 
