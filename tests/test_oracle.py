@@ -95,6 +95,59 @@ def test_h8_K0_against_independent_quadrature():
     assert np.abs(K - Ko).max() < 1e-13 * np.abs(K).max()
 
 
+def _heat_Ke_by_quadrature(h, D):
+    """B^T D B integrated by 2-point Gauss per axis (exact for bilinear /
+    trilinear shape functions on a box), corners in meshBox order."""
+    d = len(h)
+    corners = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                        [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])[:2 ** d, :d]
+    s = 2 * corners - 1
+    g = 1 / np.sqrt(3)
+    K = np.zeros((2 ** d, 2 ** d))
+    for r in np.array(np.meshgrid(*[[-g, g]] * d)).reshape(d, -1).T:
+        dN = np.zeros((d, 2 ** d))
+        for a in range(2 ** d):
+            f = (1 + s[a] * r) / 2
+            for i in range(d):
+                dN[i, a] = s[a, i] / 2 * np.prod(np.delete(f, i)) / (h[i] / 2)
+        K += dN.T @ D @ dN * np.prod(h) / 2 ** d
+    return K
+
+
+def test_heat_Ke_against_closed_form_and_quadrature():
+    """The heat element matrices (LinearHeat::makeKeFint) against the
+    bilinear / trilinear Laplacian on a unit square / cube in closed form and
+    an independent quadrature for anisotropic tensors on non-square boxes,
+    with ICARAT's [xx, yy, zz, xy, yz, xz] conductivity order."""
+    # unit square, unit conductivity: 2/3 on the diagonal, -1/6 along an
+    # edge, -1/3 across the diagonal
+    K1, _ = po.Problem(2, 2, 2, state=3).heat_Ke([1, 1, 0, 0, 0, 0], [1, 1, 0, 0, 0, 0])
+    sq = np.array([[4, -1, -2, -1], [-1, 4, -1, -2], [-2, -1, 4, -1], [-1, -2, -1, 4]]) / 6
+    assert np.abs(K1 - sq).max() < 1e-15
+    # unit cube: 1/3, 0 (one coordinate differs), -1/12 (two or three differ)
+    K1, _ = po.Problem(3, 2, 2, 2, state=3).heat_Ke([1, 1, 1, 0, 0, 0], [1, 1, 1, 0, 0, 0])
+    c = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                  [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+    nd = np.abs(c[:, None, :] - c[None, :, :]).sum(2)
+    cube = np.select([nd == 0, nd == 1], [1 / 3, 0.0], -1 / 12)
+    assert np.abs(K1 - cube).max() < 1e-15
+    # anisotropic tensors on boxes with unequal sides, material 2 separately
+    c1, c2 = [3.0, 1.5, 0, 0.4, 0, 0], [0.2, 0.1, 0, -0.05, 0, 0]
+    p = po.Problem(2, 4, 3, lx=4 * 1.3, ly=3 * 0.7, state=3)
+    K1, K2 = p.heat_Ke(c1, c2)
+    for K, cc in ((K1, c1), (K2, c2)):
+        D = np.array([[cc[0], cc[3]], [cc[3], cc[1]]])
+        Kq = _heat_Ke_by_quadrature([1.3, 0.7], D)
+        assert np.abs(K - Kq).max() < 1e-14 * np.abs(Kq).max()
+    c1 = [2.0, 1.0, 0.5, 0.3, -0.2, 0.1]
+    p = po.Problem(3, 2, 3, 2, lx=2 * 1.2, ly=3 * 0.8, lz=2 * 2.0, state=3)
+    K1, _ = p.heat_Ke(c1, c1)
+    D = np.array([[c1[0], c1[3], c1[5]], [c1[3], c1[1], c1[4]], [c1[5], c1[4], c1[2]]])
+    Kq = _heat_Ke_by_quadrature([1.2, 0.8, 2.0], D)
+    assert np.abs(K1 - Kq).max() < 1e-14 * np.abs(Kq).max()
+    assert np.abs(K1.sum(1)).max() < 1e-14 * np.abs(K1).max()  # constants in the null space
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_pcg_matches_direct_factorisation(dim):
     rng = np.random.default_rng(dim)
