@@ -215,6 +215,27 @@ def test_cone_stencil_equals_icarat_neighbour_scan():
         assert tot == _stencil_count(p, ones_w, rfil)
 
 
+def test_filters_preserve_constants_and_sensitivity_maps_are_adjoint():
+    """Properties that follow from the reference's construction of both
+    filters: a constant field comes back unchanged (weights normalised by aa;
+    M 1 = int N and K_grad 1 = 0 with one Gauss point per node), and the
+    sensitivity map is the transpose of the density map (filter.hpp:146
+    divides by the neighbour's aa; the Helmholtz map is symmetric, so its
+    sensitivity mode is the same map)."""
+    rng = np.random.default_rng(7)
+    for dims, r in [((2, 13, 7), 2.5), ((3, 6, 5, 4), 1.8)]:
+        p = po.Problem(*dims, lx=dims[1] * 0.9)
+        x, y = rng.uniform(0, 1, p.nel), rng.uniform(0, 1, p.nel)
+        cone = po.Cone(p, r)
+        assert np.abs(cone.apply(np.ones(p.nel)) - 1.0).max() < 1e-14
+        lhs, rhs = cone.apply(x) @ y, x @ cone.apply(y, sens=True)
+        assert abs(lhs - rhs) < 1e-13 * abs(lhs)
+        assert np.abs(p.helmholtz(r, np.ones(p.nel), tol=1e-13) - 1.0).max() < 1e-11
+        hx, hy = p.helmholtz(r, x, tol=1e-13), p.helmholtz(r, y, sens=True, tol=1e-13)
+        assert abs(hx @ y - x @ hy) < 1e-11 * abs(hx @ y)
+        assert np.abs(p.helmholtz(r, y, tol=1e-13) - hy).max() < 1e-11
+
+
 def _stencil_count(p, cone, r):
     g = p.g
     R = int(np.floor(r)) + 1
