@@ -371,6 +371,7 @@ int icb_solve(icb_problem p, const icb_solve_opts *opts, icb_solve_info *info)
   need(o.tol >= 0.0 && o.maxit > 0, "bad tolerance / iteration limit");
   need(o.precision == ICB_FP64 || o.precision == ICB_MIXED, "unknown precision");
   need(o.precond == ICB_PRECOND_JACOBI || o.precond == ICB_PRECOND_GMG, "unknown preconditioner");
+  NvtxRange range("icb_solve");
   cudaStream_t s = p->stream();
   // fres = fext - fint(u_D) (linear.hpp:74-80)
   const double *bptr = p->f.p;

@@ -233,6 +233,7 @@ void needH(icb_heat h, bool final)
 
 void solveHeat(icb_heat_s &H, const icb_solve_opts *opts, icb_solve_info *info)
 {
+  NvtxRange range("heat solve");
   cudaStream_t s = H.stream();
   const Dims &d = H.d;
   const double tol = opts ? opts->tol : 1e-10;
@@ -550,6 +551,7 @@ int icb_run_heat(icb_heat h, const icb_loop_opts *o, const double *rho0, double 
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
+    NvtxRange stepRange("heat step");
     filt(x.p, xf.p, false);
     const double beta = std::min(std::pow(2.0, (int)(step / 40)), 16.0);
     launch_threshold(n, xf.p, beta, 0.5, xh.p, dxh.p, s);

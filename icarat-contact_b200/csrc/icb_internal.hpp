@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/icarat_b200.h"
+#include <nvtx3/nvToolsExt.h>
 
 namespace icb
 {
@@ -63,6 +64,17 @@ struct Error
     return ICB_ERR_STATE;                                                       \
   }                                                                             \
   return ICB_OK;
+
+/// a named NVTX range over a host scope (the solve, a loop step and its
+/// phases), so Nsight timelines show where the launches of each phase come
+/// from; with no profiler attached the calls return at once
+struct NvtxRange
+{
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ---------------------------------------------------------- device memory --
 template <typename T> struct DevBuf

@@ -494,6 +494,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
+    NvtxRange stepRange("oc step");
     const double beta = o->use_threshold ? std::min(std::pow(2.0, (int)(step / 40)), 16.0) : 0.0;
     cone.forward(x.p, xf.p, beta, 0.5, xh.p, dxh.p, s); // beta 0: xh = xf, dxh = 1
     int rc = icb_set_density_device(p, xh.p);
@@ -520,7 +521,10 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
     cone.adjoint(dc.p, dcf.p, s);
     cone.adjoint(dv.p, dvf.p, s);
     P.beta = beta;
-    oc.update(&cone, x.p, dcf.p, dvf.p, V0, lo.p, hi.p, V.p, P, s);
+    {
+      NvtxRange r("oc update");
+      oc.update(&cone, x.p, dcf.p, dvf.p, V0, lo.p, hi.p, V.p, P, s);
+    }
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -574,6 +578,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
   double V0 = o->volume_ref;
   StepReport report;
   auto filt = [&](const double *in, double *out, bool sens) {
+    NvtxRange r(sens ? "filter (sensitivities)" : "filter");
     if(cone)
     {
       if(sens)
@@ -591,6 +596,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
+    NvtxRange stepRange("mma step");
     filt(x.p, xf.p, false);
     const double beta = std::min(std::pow(2.0, (int)(step / 40)), 16.0);
     launch_threshold(n, xf.p, beta, 0.5, xh.p, dxh.p, s);
@@ -626,7 +632,10 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
       k_zero_masked<<<nb256(n), 256, 0, s>>>(n, nd.p, dcf.p, dvf.p);
       count_launch();
     }
-    mma.update(x.p, dcf.p, g, dvf.p, lo.p, hi.p, s);
+    {
+      NvtxRange r("mma update");
+      mma.update(x.p, dcf.p, g, dvf.p, lo.p, hi.p, s);
+    }
     ICB_CUDA(cudaStreamSynchronize(s));
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
@@ -686,6 +695,7 @@ int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, dou
   for(int step = 1; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
+    NvtxRange stepRange("gcmma step");
     const int btmp = int(std::max((step - 100) / 40.0, 1.0));
     const double beta = std::min(double(btmp), 8.0);
     double f, vs;
@@ -706,13 +716,19 @@ int icb_run_gcmma(icb_problem p, const icb_loop_opts *o, const double *rho0, dou
     count_launch(2);
     cone.adjoint(dc.p, dcf.p, s);
     cone.adjoint(dv.p, dvf.p, s);
-    gc.outer(xnew.p, x.p, f, dcf.p, g, dvf.p, lo.p, hi.p, s);
+    {
+      NvtxRange r("gcmma outer update");
+      gc.outer(xnew.p, x.p, f, dcf.p, g, dvf.p, lo.p, hi.p, s);
+    }
     double fn, vn;
     evaluate(xnew.p, beta, fn, vn);
     int k = 0;
     for(; !gc.concheck(fn, vn - V0) && k < 15; k++)
     {
-      gc.inner(xnew.p, fn, vn - V0, x.p, f, dcf.p, g, dvf.p, lo.p, hi.p, s);
+      {
+        NvtxRange r("gcmma inner update");
+        gc.inner(xnew.p, fn, vn - V0, x.p, f, dcf.p, g, dvf.p, lo.p, hi.p, s);
+      }
       evaluate(xnew.p, beta, fn, vn);
     }
     if(inner)
