@@ -246,18 +246,7 @@ __global__ void k_oc_final(long long n, double *__restrict__ x, const double *__
   x[e] = oc_candidate(x[e], df[e], dg[e], lam, P.eta, P.move, xmin[e], xmax[e]);
 }
 
-
 // ----------------------------------------------------------------- MMA ----
-struct FinSum2
-{
-  double *out;
-  __device__ void operator()(const double *t) const
-  {
-    out[0] = t[0];
-    out[1] = t[1];
-  }
-};
-
 /// GenSub (MMASolver.cpp:400-512) for m = 1: asymptotes, move bounds, p0,
 /// q0, p, q; the constraint constant b = -g + sum(p/(U-x) + q/(x-L)) is
 /// reduced into st->b by the finisher.
