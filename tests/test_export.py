@@ -3,8 +3,6 @@ text layout: checked on a 2 x 1 quad mesh without a GPU."""
 import os
 import subprocess
 
-import pytest
-
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = r'''
 #include <array>

@@ -22,7 +22,6 @@ def _free_port():
 
 def _rank_main(rank, world, port, q):
     import numpy as np
-    import torch
     import torch.distributed as dist
     sys.path.insert(0, REPO)
     sys.path.insert(0, os.path.join(REPO, "icarat-contact_b200", "python"))
