@@ -90,10 +90,14 @@ typedef struct
   int status;         /* ICB_OK, ICB_ERR_MAXITER, ICB_ERR_BREAKDOWN, ...    */
 } icb_solve_info;
 
+/* the message of this thread's last failed call (ICARAT prints it to
+ * std::cerr before exit(1), e.g. solvers.cpp:57-61) */
 const char *icb_last_error(void);
 const char *icb_version(void);
 
 /* ---- context ----------------------------------------------------------- */
+/* No counterpart in ICARAT (one problem per process, no device): a context is
+ * one CUDA device and one stream; problems created on it share the stream. */
 int icb_ctx_create(int device, icb_ctx *out);
 int icb_ctx_destroy(icb_ctx ctx);
 /* cudaStream_t the library launches on (for events / interop) */
@@ -109,7 +113,8 @@ int icb_problem_destroy(icb_problem p);
  * flag[6], val[6], range[6] = {xmin,xmax,ymin,ymax,zmin,zmax}, tol 1e-7. */
 int icb_dirichlet_box(icb_problem p, const int *flag, const double *val,
                       const double *range);
-/* per-DOF Dirichlet flags (neq bytes) and values (neq, or NULL for 0) */
+/* setDirichValue for every node at once (boundary_condition_base.hpp:18-33):
+ * per-DOF Dirichlet flags (neq bytes) and values (neq, or NULL for 0) */
 int icb_dirichlet_mask(icb_problem p, const unsigned char *fixed, const double *val);
 /* BCIcarat::input_neumann / generateLoadMain / SurfaceLoad::generate
  * (boundary_condition_icarat.hpp:253-396, boundary_condition_base.cpp:143-180):
@@ -294,19 +299,26 @@ typedef struct
   double cond1[6], cond2[6];
   double penalty;
 } icb_heat_desc;
+/* MeshIcarat setParameter + generate and Heat::setParameter (heat.cpp:18-51)
+ * for every element of the box */
 int icb_heat_create(icb_ctx ctx, const icb_heat_desc *desc, icb_heat *out);
 int icb_heat_destroy(icb_heat h);
-/* input_dirich with dofnp 1: fixed temperature `val` where flag != 0 in the box */
+/* BCIcarat::input_dirich (boundary_condition_icarat.hpp:68-127) with dofnp 1:
+ * fixed temperature `val` where flag != 0 in the box */
 int icb_heat_dirichlet_box(icb_heat h, int flag, double val, const double *range);
-/* input_neumann with dofnp 1: constant flux q on the element sides of the box */
+/* BCIcarat::input_neumann (boundary_condition_icarat.hpp:253-396) with dofnp
+ * 1: constant flux q on the element sides of the box */
 int icb_heat_flux_box(icb_heat h, double q, const double *range);
+/* nodal heat source (extension, like icb_nodal_load) */
 int icb_heat_nodal_source(icb_heat h, long long node, double q);
+/* makeDOF -> countDOF (boundary_condition_base.hpp:35-88), upload; numeq */
 int icb_heat_finalize(icb_heat h, long long *numeq);
+/* Heat::setDesign for every element (heat.hpp:35), host array of nel */
 int icb_heat_set_density(icb_heat h, const double *rho);
 /* LinearAnalysis<LinearHeat>::solve with Eigen_CG: FP64 Jacobi-PCG (opts NULL:
  * tol 1e-10, 10000 iterations) */
 int icb_heat_solve(icb_heat h, const icb_solve_opts *opts, icb_solve_info *info);
-/* node[].val[0] (nnode) */
+/* node[].val[0] after divideValIntoNode (analysis_utility.hpp:8-31), nnode */
 int icb_heat_get_temperature(icb_heat h, double *nodeval);
 /* the app's objective u^T K u over the free DOFs (opt_heat.cpp:116) */
 int icb_heat_objective(icb_heat h, double *f);
