@@ -9,10 +9,13 @@
 // Parity status: the FEM solve is unpinned by reference-run outputs (ICARAT's
 // solve needs Eigen 3.4 + toml11, absent here, and ICARAT ships no test
 // vectors).  It is pinned instead by (a) published closed-form element
-// stiffness matrices, (b) a direct sparse factorisation of the same assembled
-// matrix, (c) the reference's own finite-difference sensitivity procedure.
-// The OC and MMA updates are pinned bit-for-bit against ICARAT's own
-// OCSolver.hpp / MMASolver.cpp compiled from source into oracle/_ref.
+// stiffness matrices and independent quadratures (elastic and heat), (b) a
+// direct sparse factorisation of the same assembled matrix, (c) the
+// reference's own finite-difference sensitivity procedure, (d) properties the
+// reference's filters have by construction (constants kept, sensitivity map =
+// transpose).  The OC, MMA and GCMMA updates are pinned against ICARAT's own
+// OCSolver.hpp / MMASolver.cpp / GCMMASolver.cpp compiled from source into
+// oracle/_ref.
 //
 // Every function names the ICARAT source (path inside the ICARAT project,
 // file:line) whose behaviour it restates.

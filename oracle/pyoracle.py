@@ -8,8 +8,9 @@ the checker; the product library never does.
 
 Parity status: the FEM solve is unpinned by reference-run outputs (ICARAT's
 solve needs Eigen/toml11, absent here); it is pinned by published closed-form
-element matrices, a direct factorisation and ICARAT's own finite-difference
-procedure.  OC and MMA are pinned against ICARAT's own sources.
+element matrices and independent quadratures (elastic and heat), a direct
+factorisation and ICARAT's own finite-difference procedure.  OC, MMA and GCMMA
+are pinned against ICARAT's own sources.
 """
 import ctypes as C
 import os
