@@ -27,6 +27,7 @@
 #include "reduce.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <unordered_map>
@@ -953,7 +954,7 @@ int matvec_blocks(const Dims &d)
   return bx * ((d.sy + ychunk - 1) / ychunk);
 }
 
-static bool g_hex8_modal = true;
+static std::atomic<bool> g_hex8_modal{true}; // read by every launching thread
 
 /// Kt = H K0 H / 64 on the 11 blocks of the corner-mode form.  False when an
 /// entry outside the blocks is above rounding (|Kt_rc| > tol max |Kt|, tol
@@ -1110,7 +1111,7 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   count_launch();
 }
 
-static bool g_tc_operator = false;
+static std::atomic<bool> g_tc_operator{false};
 bool tc_operator_enabled() { return g_tc_operator; }
 void set_tc_operator(bool on) { g_tc_operator = on; }
 bool hex8_modal_enabled() { return g_hex8_modal; }
