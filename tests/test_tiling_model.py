@@ -1,17 +1,19 @@
-"""The element operators' tilings, restated on the CPU.
+"""The operators' tilings, restated on the CPU.
 
 k_matvec_h8 / k_matvec_h8m (Hex8) and k_matvec_q4 (Q4) give each thread one
 element column (plus a one-element halo on the low side of its tile) and let
-the thread whose column ends at a node write that node.  No atomics: the
-result is only right if every node of the grid is written by exactly one
-thread-layer.  The launchers' grid arithmetic and the kernels' ownership test
-are transcribed here and checked for exact coverage over awkward sizes
-(one-element axes, sizes just past a tile boundary) and every z or y split.
-No GPU.
+the thread whose column ends at a node write that node; k_helm_apply3 (the
+3D Helmholtz operator) gives each thread one node column and stages each plane
+with a one-node halo in shared memory.  No atomics: the result is only right
+if every node of the grid is written by exactly one thread-layer.  The
+launchers' grid arithmetic and the kernels' ownership tests are transcribed
+here and checked for exact coverage over awkward sizes (one-element axes,
+sizes just past a tile boundary) and every z or y split.  No GPU.
 """
 import numpy as np
 
 TX, TY3, TY2 = 32, 8, 4  # operator.cu: threads along x, rows per 3D tile, warps per 2D CTA
+HTX, HTY = 32, 8         # helm.cu: the Helmholtz operator's node tile
 
 
 def _h8_owners(nx, ny, nz, zchunk):
@@ -79,3 +81,42 @@ def test_q4_tiling_writes_every_node_once():
         for target in (1, 3, 148 * 4):
             cnt = _q4_owners(nx, ny, target)
             assert (cnt == 1).all(), (nx, ny, target, cnt.min(), cnt.max())
+
+
+def _helm_owners(sx, sy, sz, zc):
+    """count of writes per node (sz, sy, sx) for one k_helm_apply3 launch, and
+    a check that the staged plane (tile + one-node halo) is filled completely
+    and read inside its bounds"""
+    NX, NY, NT = HTX + 2, HTY + 2, HTX * HTY
+    tx, ty, bz = (sx + HTX - 1) // HTX, (sy + HTY - 1) // HTY, (sz + zc - 1) // zc
+    staged = np.zeros(NX * NY, np.int32)
+    for tid in range(NT):
+        for t in range(2):
+            q = tid + t * NT
+            if q < NX * NY:
+                staged[q] += 1
+    assert (staged == 1).all()  # every halo cell has exactly one loader
+    # reads sP[ly + r][lx + c], r, c in 0..2
+    assert HTY - 1 + 2 < NY and HTX - 1 + 2 < NX
+    cnt = np.zeros((sz, sy, sx), np.int32)
+    lx, ly = np.arange(HTX)[None, :], np.arange(HTY)[:, None]
+    for byi in range(ty):
+        for bxi in range(tx):
+            i = np.broadcast_to(bxi * HTX + lx, (HTY, HTX))
+            j = np.broadcast_to(byi * HTY + ly, (HTY, HTX))
+            own = (i < sx) & (j < sy)
+            for bzi in range(bz):
+                z0 = bzi * zc
+                z1 = min(z0 + zc, sz) - 1
+                for k in range(z0 - 1, z1 + 2):
+                    ko = k - 1
+                    if z0 <= ko <= z1:
+                        cnt[ko, j[own], i[own]] += 1
+    return cnt
+
+
+def test_helmholtz_tiling_writes_every_node_once():
+    for sx, sy, sz in [(2, 2, 2), (33, 9, 2), (32, 8, 5), (65, 17, 13), (7, 40, 3)]:
+        for zc in sorted({1, 2, sz, (sz + 1) // 2}):
+            cnt = _helm_owners(sx, sy, sz, zc)
+            assert (cnt == 1).all(), (sx, sy, sz, zc)
