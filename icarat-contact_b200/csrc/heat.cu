@@ -472,7 +472,9 @@ int icb_heat_get_temperature(icb_heat h, double *nodeval)
 {
   ICB_API_BEGIN
   needH(h, true);
-  if(!nodeval || !h->solved)
+  if(!nodeval)
+    throw Error{ICB_ERR_BAD_ARG, "NULL argument"};
+  if(!h->solved)
     throw Error{ICB_ERR_STATE, "solve first"};
   cudaStream_t s = h->stream();
   std::vector<double> t(h->d.ld);
@@ -487,7 +489,9 @@ int icb_heat_objective(icb_heat h, double *f)
 {
   ICB_API_BEGIN
   needH(h, true);
-  if(!f || !h->solved)
+  if(!f)
+    throw Error{ICB_ERR_BAD_ARG, "NULL argument"};
+  if(!h->solved)
     throw Error{ICB_ERR_STATE, "solve first"};
   *f = heatObjective(*h);
   ICB_API_END
@@ -497,7 +501,9 @@ int icb_heat_sensitivity(icb_heat h, const double *rho, double *dc, double *dv)
 {
   ICB_API_BEGIN
   needH(h, true);
-  if(!rho || !dc || !h->solved)
+  if(!rho || !dc)
+    throw Error{ICB_ERR_BAD_ARG, "NULL argument"};
+  if(!h->solved)
     throw Error{ICB_ERR_STATE, "solve first (and pass the density of the solve)"};
   cudaStream_t s = h->stream();
   const long long n = h->d.nel;
