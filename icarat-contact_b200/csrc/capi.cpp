@@ -479,7 +479,10 @@ int icb_sensitivity(icb_problem p, double *dc, double *dv)
 const double *icb_sensitivity_device(icb_problem p)
 {
   if(!p || !p->solved)
+  {
+    set_error(p ? "solve first" : "NULL problem");
     return nullptr;
+  }
   try
   {
     setDevice(p);
@@ -490,6 +493,11 @@ const double *icb_sensitivity_device(icb_problem p)
   catch(const Error &e)
   {
     set_error(e.msg);
+    return nullptr;
+  }
+  catch(const std::exception &e)
+  {
+    set_error(e.what());
     return nullptr;
   }
   return p->dc.p;

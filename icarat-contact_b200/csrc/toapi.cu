@@ -54,7 +54,9 @@ void need(bool c, const char *m)
 }
 void needFinal(icb_problem p)
 {
-  if(!p || !p->hs->finalized)
+  if(!p)
+    throw Error{ICB_ERR_BAD_ARG, "NULL problem"};
+  if(!p->hs->finalized)
     throw Error{ICB_ERR_STATE, "problem not finalized"};
 }
 

@@ -164,7 +164,9 @@ int icb_compliance(icb_problem p, double *c);
  * opt_mma_Helmholtz.cpp:173-205): dc_e = -(E'/E) u_e^T Ke u_e; dv_e = v_e
  * (dv may be NULL). */
 int icb_sensitivity(icb_problem p, double *dc, double *dv);
-/* device pointers (valid until the problem is destroyed) */
+/* the same dc on the device (nel doubles, valid until the problem is
+ * destroyed or the next sensitivity call); NULL on failure, with the reason in
+ * icb_last_error */
 const double *icb_sensitivity_device(icb_problem p);
 /* Elastic::makeMisesStress (src/problem/elasticity.cpp:165-208) for every
  * element of the last solve: mises[nel] and, when stress is not NULL, the
