@@ -8,6 +8,7 @@ import pytest
 import scipy.sparse as sp
 import scipy.sparse.linalg as spl
 
+import cases
 import pyoracle as po
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -93,6 +94,93 @@ def test_h8_K0_against_independent_quadrature():
                 K += B.T @ D @ B * wts[i] * wts[j] * wts[k] * np.prod(h) / 8
     Ko = po.Problem(3, 2, 2, 2, lx=2 * h[0], ly=2 * h[1], lz=2 * h[2]).K0()
     assert np.abs(K - Ko).max() < 1e-13 * np.abs(K).max()
+
+
+def test_threshold_and_derivative_closed_form():
+    """filter.hpp:153-185: x_hat = (tanh(bT) + tanh(b(x - T))) / (2 tanh(bT)) and its
+    derivative, against numpy and a central difference; threshold(T) = T at T = 1/2."""
+    x = np.linspace(0.0, 1.0, 101)
+    for beta in (1.0, 2.0, 8.0, 16.0):
+        want = 0.5 * (np.tanh(0.5 * beta) + np.tanh(beta * (x - 0.5))) / np.tanh(0.5 * beta)
+        assert np.abs(po.threshold(x, beta) - want).max() < 1e-15
+        h = 1e-6
+        fd = (po.threshold(x + h, beta) - po.threshold(x - h, beta)) / (2 * h)
+        assert np.abs(po.threshold_deriv(x, beta) - fd).max() < 1e-7 * beta
+        assert abs(po.threshold(np.array([0.5]), beta)[0] - 0.5) < 1e-15
+        assert abs(po.threshold(np.array([0.0]), beta)[0]) < 1e-15
+        assert abs(po.threshold(np.array([1.0]), beta)[0] - 1.0) < 1e-15
+
+
+def _affine_nodeval(p, n, h, G):
+    """node values (node-major) of the displacement u(X) = G X on the grid"""
+    d = len(n)
+    coords = np.stack(np.meshgrid(*[np.arange(k + 1) * hk for k, hk in zip(n, h)],
+                                  indexing="ij"), -1)
+    # MeshIcarat numbering: x fastest
+    X = coords.transpose(*reversed(range(d)), d).reshape(-1, d)
+    return (X @ G.T).reshape(-1)
+
+
+def test_stress_recovery_of_affine_fields():
+    """Elastic::makeMisesStress (elasticity.cpp:165-208): for u = G X every element
+    carries the strain of G, so the stress is E(rho) D0 eps exactly and von Mises is
+    sqrt(s^T V s) with ICARAT's V (plane-stress form in 2D for both 2D states)."""
+    rng = np.random.default_rng(3)
+    nu, E1, E2, pen = 0.3, 1e-3, 2.0, 3.0
+    for dim, state in ((2, 0), (2, 1), (3, 2)):
+        n = (3, 2) if dim == 2 else (2, 3, 2)
+        h = (1.3, 0.7) if dim == 2 else (1.3, 0.7, 1.1)
+        p = po.Problem(dim, *n, **{k: v for k, v in zip(("lx", "ly", "lz"),
+                                                     [a * b for a, b in zip(n, h)])},
+                       state=state, young=(E1, E2), nu=nu, penal=pen)
+        G = rng.standard_normal((dim, dim))
+        rho = rng.uniform(0.05, 1.0, p.nel)
+        mises, stress = p.von_mises(rho, _affine_nodeval(p, n, h, G), with_stress=True)
+        E = (1 - rho ** pen) * E1 + rho ** pen * E2
+        if dim == 2:
+            eps = np.array([G[0, 0], G[1, 1], G[0, 1] + G[1, 0]])
+            if state == 0:
+                D0 = np.array([[1, nu, 0], [nu, 1, 0], [0, 0, (1 - nu) / 2]]) / (1 - nu * nu)
+            else:
+                D0 = np.array([[1 - nu, nu, 0], [nu, 1 - nu, 0], [0, 0, (1 - 2 * nu) / 2]]) \
+                    / ((1 + nu) * (1 - 2 * nu))
+            V = np.array([[1, -0.5, 0], [-0.5, 1, 0], [0, 0, 3]])
+        else:
+            eps = np.array([G[0, 0], G[1, 1], G[2, 2], G[0, 1] + G[1, 0], G[1, 2] + G[2, 1],
+                            G[0, 2] + G[2, 0]])
+            lam, mu = nu / ((1 + nu) * (1 - 2 * nu)), 1 / (2 * (1 + nu))
+            D0 = np.zeros((6, 6))
+            D0[:3, :3] = lam
+            D0[np.arange(3), np.arange(3)] += 2 * mu
+            D0[3, 3] = D0[4, 4] = D0[5, 5] = mu
+            V = np.zeros((6, 6))
+            V[:3, :3] = -0.5
+            V[np.arange(3), np.arange(3)] = 1.0
+            V[3, 3] = V[4, 4] = V[5, 5] = 3.0
+        want = E[:, None] * (D0 @ eps)[None, :]
+        assert np.abs(stress - want).max() < 1e-12 * np.abs(want).max(), (dim, state)
+        vm = np.sqrt(np.einsum("ei,ij,ej->e", want, V, want))
+        assert np.abs(mises - vm).max() < 1e-12 * vm.max(), (dim, state)
+
+
+def test_reactions_balance_the_loads():
+    """linear.hpp:89-91 reactions = internal forces sum_e Ke u_e: on free DOFs they
+    equal the applied loads (to the solve tolerance), and over the whole grid each
+    component sums to zero (rigid translations are in every Ke's null space), so the
+    support reactions balance the loads."""
+    for kind, n in (("cantilever2d", (24, 8)), ("cantilever3d", (8, 4, 3))):
+        o = cases.build_oracle(kind, *n)
+        rho = cases.uniform_density(o.nel, 4)
+        ro = o.solve(rho, tol=1e-13)
+        r = o.reactions(rho, ro["nodeval"])
+        free = o.fixed == 0
+        f = o.fext_full
+        assert np.abs(r[free] - f[free]).max() < 1e-9 * np.abs(f).max()
+        d = o.dim
+        tot = r.reshape(-1, d).sum(0)
+        assert np.abs(tot).max() < 1e-9 * np.abs(r).max()
+        support = np.where(free, 0.0, r).reshape(-1, d).sum(0)
+        assert np.allclose(support, -f.reshape(-1, d).sum(0), rtol=1e-8, atol=1e-12)
 
 
 def _heat_Ke_by_quadrature(h, D):
