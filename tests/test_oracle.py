@@ -96,6 +96,19 @@ def test_h8_K0_against_independent_quadrature():
     assert np.abs(K - Ko).max() < 1e-13 * np.abs(K).max()
 
 
+def test_simp_both_branches():
+    """SIMP (elasticity.hpp:15-22): (1 - s^p) y1 + s^p y2 when y2 >= y1, else
+    (1 - s)^p y1 + (1 - (1 - s)^p) y2."""
+    s = np.linspace(0.0, 1.0, 41)
+    for y1, y2, p in ((1e-9, 1.0, 3.0), (1.0, 1e-3, 3.0), (0.2, 0.2, 2.5)):
+        E = po.Problem(2, 41, 1, young=(y1, y2), penal=p).simp(s)
+        if y2 - y1 >= 0.0:
+            want = (1.0 - s ** p) * y1 + s ** p * y2
+        else:
+            want = (1.0 - s) ** p * y1 + (1.0 - (1.0 - s) ** p) * y2
+        assert np.abs(E - want).max() <= 1e-15 * max(y1, y2)
+
+
 def test_threshold_and_derivative_closed_form():
     """filter.hpp:153-185: x_hat = (tanh(bT) + tanh(b(x - T))) / (2 tanh(bT)) and its
     derivative, against numpy and a central difference; threshold(T) = T at T = 1/2."""
