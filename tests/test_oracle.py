@@ -27,6 +27,33 @@ def test_q4_K0_matches_published_closed_form():
     assert np.abs(K - KE).max() < 1e-14
 
 
+def test_q4_K0_plane_stress_and_strain_against_quadrature():
+    """Q4 element matrix (elasticity.cpp:34-98 D, 210-254 Ke) on a rectangle
+    with unequal sides, both 2D states, against 2-point Gauss quadrature of
+    B^T D B in numpy."""
+    nu, h = 0.3, (1.3, 0.7)
+    corners = np.array([[0, 0], [1, 0], [1, 1], [0, 1]])
+    sgn = 2 * corners - 1
+    g = 1 / np.sqrt(3)
+    for state in (0, 1):
+        if state == 0:
+            D = np.array([[1, nu, 0], [nu, 1, 0], [0, 0, (1 - nu) / 2]]) / (1 - nu * nu)
+        else:
+            D = np.array([[1 - nu, nu, 0], [nu, 1 - nu, 0], [0, 0, (1 - 2 * nu) / 2]]) \
+                / ((1 + nu) * (1 - 2 * nu))
+        K = np.zeros((8, 8))
+        for r in ((-g, -g), (g, -g), (g, g), (-g, g)):
+            B = np.zeros((3, 8))
+            for a in range(4):
+                dx = sgn[a, 0] * (1 + sgn[a, 1] * r[1]) / 4 / (h[0] / 2)
+                dy = sgn[a, 1] * (1 + sgn[a, 0] * r[0]) / 4 / (h[1] / 2)
+                B[0, 2 * a], B[1, 2 * a + 1] = dx, dy
+                B[2, 2 * a], B[2, 2 * a + 1] = dy, dx
+            K += B.T @ D @ B * h[0] * h[1] / 4
+        Ko = po.Problem(2, 2, 2, lx=2 * h[0], ly=2 * h[1], state=state).K0()
+        assert np.abs(K - Ko).max() < 1e-14 * np.abs(K).max(), state
+
+
 def _rigid_modes_3d(h):
     X = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
                   [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float) * h
