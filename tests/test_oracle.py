@@ -454,6 +454,36 @@ def test_degenerate_traction_box_loads_nothing():
     assert np.abs(p.fext()).max() == 0.0
 
 
+def test_traction_box_consistent_nodal_forces():
+    """SurfaceLoad::generate (boundary_condition_base.cpp:143-180) for a constant
+    traction on a bilinear side: each element side of measure A gives t A / 2 (edge)
+    or t A / 4 (face) to each of its nodes, so the right-end side of a box receives
+    t h / 2 at its end nodes and t h elsewhere (2D), t A / 4, / 2 and A at corner,
+    edge and interior nodes (3D); the total is t times the side's measure."""
+    # 2D, right edge x = L of a 6 x 4 grid with h = (1.5, 0.5)
+    n, h, t = (6, 4), (1.5, 0.5), np.array([0.3, -2.0])
+    p = po.Problem(2, *n, lx=n[0] * h[0], ly=n[1] * h[1])
+    L = n[0] * h[0]
+    p.traction_box(list(t) + [0.0], [L, L, 0, n[1] * h[1], 0, 0])
+    f = p.fext().reshape(n[1] + 1, n[0] + 1, 2)
+    w = np.full(n[1] + 1, h[1])
+    w[[0, -1]] = h[1] / 2
+    assert np.abs(f[:, -1, :] - w[:, None] * t).max() < 1e-14
+    assert np.abs(f[:, :-1, :]).max() == 0.0
+    # 3D, face x = L of a 3 x 4 x 2 grid with h = (1, 0.5, 2)
+    n, h, t = (3, 4, 2), (1.0, 0.5, 2.0), np.array([0.0, 0.7, -1.1])
+    p = po.Problem(3, *n, lx=n[0] * h[0], ly=n[1] * h[1], lz=n[2] * h[2])
+    L = n[0] * h[0]
+    p.traction_box(list(t), [L, L, 0, n[1] * h[1], 0, n[2] * h[2]])
+    f = p.fext().reshape(n[2] + 1, n[1] + 1, n[0] + 1, 3)
+    wy = np.full(n[1] + 1, h[1]); wy[[0, -1]] = h[1] / 2
+    wz = np.full(n[2] + 1, h[2]); wz[[0, -1]] = h[2] / 2
+    want = (wz[:, None] * wy[None, :])[:, :, None] * t
+    assert np.abs(f[:, :, -1, :] - want).max() < 1e-14
+    assert np.abs(f[:, :, :-1, :]).max() == 0.0
+    assert np.allclose(f.reshape(-1, 3).sum(0), t * n[1] * h[1] * n[2] * h[2], rtol=1e-14)
+
+
 def _gcmma_sequence(gc, G):
     c, v, V, x0 = G["c"], G["v"], float(G["V"]), G["x0"]
     import make_golden as mg
