@@ -484,6 +484,23 @@ def test_traction_box_consistent_nodal_forces():
     assert np.allclose(f.reshape(-1, 3).sum(0), t * n[1] * h[1] * n[2] * h[2], rtol=1e-14)
 
 
+def test_helmholtz_filter_against_the_1d_solution():
+    """FilterHelmholtz (filter_helm.hpp:178-222): on a long strip one element thick
+    the filtered step tends to the solution of phi - r_e^2 phi'' = step,
+    1 - e^(-(x-x0)/r_e) / 2 right of the step and e^((x-x0)/r_e) / 2 left of it,
+    with ICARAT's r_e = R / (2 sqrt 3) (filter_helm.hpp:204); h / r_e = 0.12 here,
+    so the discretisation error is below 1e-3 while R / sqrt 3 or R / 2 would miss
+    by 0.1."""
+    nx, h, R = 400, 0.1, 3.0
+    p = po.Problem(2, nx, 1, lx=nx * h, ly=h)
+    xc = (np.arange(nx) + 0.5) * h
+    x0 = nx * h / 2
+    out = p.helmholtz(R, (xc > x0).astype(float), tol=1e-13)
+    re = R / (2 * np.sqrt(3))
+    phi = np.where(xc > x0, 1 - 0.5 * np.exp(-(xc - x0) / re), 0.5 * np.exp((xc - x0) / re))
+    assert np.abs(out - phi).max() < 1.5e-3
+
+
 def _gcmma_sequence(gc, G):
     c, v, V, x0 = G["c"], G["v"], float(G["V"]), G["x0"]
     import make_golden as mg
