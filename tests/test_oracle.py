@@ -501,6 +501,27 @@ def test_helmholtz_filter_against_the_1d_solution():
     assert np.abs(out - phi).max() < 1.5e-3
 
 
+def test_cone_filter_weights_on_a_delta():
+    """Filter::densityFilter (filter.hpp:102-134): x~_i = sum_j (r - d_ij) x_j / aa_i
+    with aa_i = sum_j (r - d_ij) over the neighbours within r; r = 1.5 on a unit grid
+    gives the weights 1.5 (self), 0.5 (edge neighbours) and 1.5 - sqrt 2 (corners)."""
+    n = 7
+    p = po.Problem(2, n, n)
+    cone = po.Cone(p, 1.5)
+    x = np.zeros(n * n)
+    c = 3 + 3 * n
+    x[c] = 1.0
+    y = cone.apply(x).reshape(n, n)
+    wc = 1.5 - np.sqrt(2.0)
+    aa = 1.5 + 4 * 0.5 + 4 * wc  # every element that sees the delta is interior
+    assert abs(y[3, 3] - 1.5 / aa) < 1e-15
+    for j, i in ((3, 2), (3, 4), (2, 3), (4, 3)):
+        assert abs(y[j, i] - 0.5 / aa) < 1e-15
+    for j, i in ((2, 2), (2, 4), (4, 2), (4, 4)):
+        assert abs(y[j, i] - wc / aa) < 1e-15
+    assert np.count_nonzero(y) == 9
+
+
 def _gcmma_sequence(gc, G):
     c, v, V, x0 = G["c"], G["v"], float(G["V"]), G["x0"]
     import make_golden as mg
