@@ -522,6 +522,23 @@ def test_cone_filter_weights_on_a_delta():
     assert np.count_nonzero(y) == 9
 
 
+def test_count_dof_numbering():
+    """countDOF (boundary_condition_base.hpp:35-88): free DOFs numbered node by
+    node, components interleaved, from 0; then the constrained DOFs, again in
+    node order, from numeq on."""
+    rng = np.random.default_rng(12)
+    for dims in ((2, 5, 3), (3, 3, 2, 2)):
+        p = po.Problem(*dims)
+        p.fixed[:] = rng.random(p.neq) < 0.3
+        dof, numeq = p.dofs()
+        free = p.fixed == 0
+        want = np.empty(p.neq, np.int64)
+        want[free] = np.arange(free.sum())
+        want[~free] = free.sum() + np.arange((~free).sum())
+        assert numeq == free.sum()
+        assert np.array_equal(dof, want)
+
+
 def _gcmma_sequence(gc, G):
     c, v, V, x0 = G["c"], G["v"], float(G["V"]), G["x0"]
     import make_golden as mg
