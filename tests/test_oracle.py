@@ -539,6 +539,42 @@ def test_count_dof_numbering():
         assert np.array_equal(dof, want)
 
 
+def test_heat_solve_energy_identity_and_direct_solve():
+    """The heat solve (LinearAnalysis<LinearHeat>::solve, heat.cpp:53-111) with zero
+    Dirichlet temperatures: the app's objective u^T K u equals f . u, and the
+    temperatures match a direct factorisation of the assembled conductance."""
+    p = po.Problem(2, 12, 9, state=3, penal=3.0)
+    p.dirichlet_box([1], [0.0], [0, 0, 0, 9, 0, 0])
+    rng = np.random.default_rng(5)
+    p.fext_full[:] = rng.uniform(0.0, 1.0, p.neq) * (p.fixed == 0)
+    c1, c2 = [1.0, 1.0, 0, 0, 0, 0], [1e-3, 1e-3, 0, 0, 0, 0]
+    rho = rng.uniform(0.05, 1.0, p.nel)
+    r = p.heat_solve(c1, c2, rho, tol=1e-13)
+    dof, numeq = p.dofs()
+    f = p.fext()
+    T = r["nodeval"]
+    u = np.zeros(numeq)
+    free = dof < numeq
+    u[dof[free]] = T[free]
+    assert abs(r["objective"] - f @ u) < 1e-10 * abs(f @ u)
+    # direct solve of sum_e (rho^p K1 + (1 - rho^p) K2) over the free DOFs
+    K1, K2 = p.heat_Ke(c1, c2)
+    rows, cols, vals = [], [], []
+    nx, ny = 12, 9
+    for e in range(p.nel):
+        i, j = e % nx, e // nx
+        nd = [i + j * (nx + 1), i + 1 + j * (nx + 1), i + 1 + (j + 1) * (nx + 1), i + (j + 1) * (nx + 1)]
+        a = rho[e] ** 3.0
+        Ke = a * K1 + (1 - a) * K2
+        for x in range(4):
+            for y in range(4):
+                if dof[nd[x]] < numeq and dof[nd[y]] < numeq:
+                    rows.append(dof[nd[x]]); cols.append(dof[nd[y]]); vals.append(Ke[x, y])
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(numeq, numeq))
+    ud = spl.spsolve(A.tocsc(), f)
+    assert np.abs(ud - u).max() < 1e-9 * np.abs(ud).max()
+
+
 def _gcmma_sequence(gc, G):
     c, v, V, x0 = G["c"], G["v"], float(G["V"]), G["x0"]
     import make_golden as mg
