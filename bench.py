@@ -4,7 +4,16 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     (N > 1: launched by torch.distributed.run, one rank per GPU)
 
-Workload (one step): the 192x64x64 Hex8 cantilever (2,446,275 DOF, numeq
+Default line (--workload headline): the 384x128x128 Hex8 half-MBB beam
+(19,220,355 DOF), seeded smooth density field; one step = SIMP moduli, the
+mixed-precision GMG-PCG solve to ||r||/||f|| <= 1e-8 (FP32 V-cycle, FP64
+residual), compliance and sensitivities; value = numeq x the Jacobi-PCG
+iterations this system needs to 1e-8 / step time (the reference algorithm's
+DOF*iter, so the ratio to the reference arm is the time-to-solution
+speed-up); the reference arm times the oracle's matrix-free Jacobi-PCG on the
+same system on the host cores.  See headline_ours for the extra keys.
+
+--workload c2 (one step): the 192x64x64 Hex8 cantilever (2,446,275 DOF, numeq
 2,433,600): x = 0 face clamped, unit line load in -z along the bottom edge of
 the x = L face, E0 = 1, Emin = 1e-9, nu = 0.3, p = 3, densities i.i.d.
 U[0.01, 1] from a seed; solve K(rho) u = f to ||r||/||f|| <= 1e-8, then
@@ -327,6 +336,256 @@ def ours_arm(args):
     return 0
 
 
+# ------------------------------------------------------------ headline (c3) --
+C3_GRID = (384, 128, 128)
+C3_METRIC = ("PCG DOF*iter/s at 1e-8, Eigen_CG-equivalent: numeq x the Jacobi-PCG iterations "
+             "this system needs to ||r||/||f|| <= 1e-8, per second of analysis-and-sensitivity "
+             "step (mixed-precision GMG-PCG on ours, Jacobi-PCG on the reference)")
+
+
+def c3_config(grid):
+    nx, ny, nz = grid
+    dof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    return {"workload": f"halfmbb3d {nx}x{ny}x{nz} Hex8 ({dof:,} DOF), seeded smooth density "
+                        f"field on [0.001,1], E0=1, Emin=1e-9, nu=0.3, p=3, tol 1e-8",
+            "tol": TOL,
+            "l2": "inputs larger than L2: one FP64 field vector is 154 MB > 126 MB"}
+
+
+def c3_cpu_sample(grid, nit, seed):
+    """The oracle's matrix-free Jacobi-PCG (the Eigen_CG algorithm; the assembled
+    matrix of this grid needs ~77 GB) on the host cores: seconds per `nit`
+    iterations, numeq, threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cases
+    import pyoracle as po
+    o = cases.build_oracle("halfmbb3d", *grid)
+    rho = smooth_field(*grid, seed=seed)
+    _, numeq = o.dofs()
+    return (lambda: o.ebe_pcg_time(rho, nit)[0]), numeq, po.lib().orc_num_threads()
+
+
+def headline_reference(args):
+    """--impl reference: the CPU restatement of ICARAT's Eigen_CG solve on the
+    same c3 problem, each step a bounded sample of `nit` Jacobi-PCG iterations;
+    rank 0 only."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    grid = tuple(args.size) if args.size else C3_GRID
+    nit = 10
+    run, numeq, threads = c3_cpu_sample(grid, nit, SEED)
+    for _ in range(args.warmup):
+        run()
+    times = [run() for _ in range(args.steps)]
+    tot = sum(times)
+    value = numeq * nit * len(times) / tot
+    sample = (f"{nit} matrix-free Jacobi-PCG iterations per step (Eigen_CG semantics, the "
+              f"oracle's restatement; {tot / len(times) / nit:.3f} s per iteration on {threads} "
+              f"threads)")
+    print(json.dumps({
+        "impl": "reference", "metric": C3_METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded smooth density field)",
+        "config": c3_config(grid),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+        flush=True)
+    return 0
+
+
+def headline_ours(args):
+    """The default bench line: c3, the 384x128x128 Hex8 half-MBB beam.  One step
+    is the analysis-and-sensitivity step on device-resident densities: SIMP
+    moduli, the mixed-precision GMG-PCG solve to ||r||/||f|| <= 1e-8 (FP64
+    residual), compliance and element sensitivities.  The value counts the
+    work of the reference algorithm (numeq x its Jacobi-PCG iteration count
+    to 1e-8, measured on the same system) per second of step, so the ratio to
+    the reference arm is the time-to-solution speed-up; the raw GMG-PCG
+    DOF*iter/s, the FP64 GMG and FP64 Jacobi solves of the same system and the
+    errors of the mixed solve against the FP64 one are reported beside it."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    import cases
+    import icarat_b200 as icb
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    grid = tuple(args.size) if args.size else C3_GRID
+    ctx = icb.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    prob = cases.build_gpu(ctx, "halfmbb3d", *grid)
+    numeq = prob.numeq
+    rho_h = smooth_field(*grid, seed=SEED + rank)
+    rho_d = torch.from_numpy(rho_h).to(dev)
+    torch.cuda.synchronize()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b)
+
+    # the reference algorithm on this system: FP64 Jacobi-PCG (Eigen_CG) to 1e-8
+    prob.set_density_device(rho_d.data_ptr())
+    inf_j, ms_j = timed(lambda: prob.solve(precision=icb.FP64, precond=icb.JACOBI, tol=TOL,
+                                           maxit=200000))
+    n_jacobi = inf_j["iters"]
+    comp_j = prob.compliance()
+    # the plain FP64 GPU path with the same preconditioner: FP64 GMG-PCG
+    prob.solve(precision=icb.FP64, precond=icb.GMG, tol=TOL, maxit=20000)  # builds the hierarchy
+    inf_g, ms_g = timed(lambda: prob.solve(precision=icb.FP64, precond=icb.GMG, tol=TOL,
+                                           maxit=20000))
+    comp_g = prob.compliance()
+    dc_g = prob.sensitivity()
+
+    mixed = dict(precision=icb.MIXED, precond=icb.GMG, tol=TOL, maxit=20000)
+
+    def step():
+        prob.set_density_device(rho_d.data_ptr())
+        info = prob.solve(**mixed)
+        c = prob.compliance()
+        icb.lib().icb_sensitivity_device(prob.h)
+        return info, c
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    clk = clocks_start(local) if rank == 0 else None
+    l0 = icb.launch_count()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    infos = []
+    for k in range(args.steps):
+        info, comp = step()
+        infos.append(info)
+        ev[k + 1].record(stream)
+    barrier()
+    clocks = clocks_stop(clk)
+    launches = icb.launch_count() - l0
+    lat = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps))
+    ms, units = reduce_over_ranks(ev[0].elapsed_time(ev[-1]), float(numeq) * n_jacobi * args.steps,
+                                  dist, dev)
+    _, raw_units = reduce_over_ranks(0.0, float(numeq) * sum(i["iters"] for i in infos), dist, dev)
+    value = units / (ms * 1e-3)
+    comp_m = prob.compliance()
+    dc_m = prob.sensitivity()
+    err = {"compliance_rel_vs_fp64_gmg": abs(comp_m - comp_g) / abs(comp_g),
+           "sens_linf_rel_vs_fp64_gmg": float(np.abs(dc_m - dc_g).max() / np.abs(dc_g).max()),
+           "compliance_rel_vs_fp64_jacobi": abs(comp_m - comp_j) / abs(comp_j)}
+
+    # ---- e2e: the C ABI with pinned host buffers (density in; compliance,
+    # sensitivities and displacement out) inside the timed region
+    rho_pin = torch.from_numpy(rho_h).pin_memory()
+    u_pin = torch.empty(numeq, dtype=torch.float64).pin_memory()
+    dc_pin = torch.empty(prob.nel, dtype=torch.float64).pin_memory()
+    L = icb.lib()
+    dptr = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
+
+    def step_e2e():
+        icb.check(L.icb_set_density(prob.h, dptr(rho_pin)))
+        prob.solve(**mixed)
+        c = C.c_double()
+        icb.check(L.icb_compliance(prob.h, C.byref(c)))
+        icb.check(L.icb_sensitivity(prob.h, dptr(dc_pin), None))
+        icb.check(L.icb_get_displacement(prob.h, dptr(u_pin)))
+
+    step_e2e()
+    barrier()
+    _, ms2 = timed(lambda: [step_e2e() for _ in range(args.steps)])
+    ms2, units2 = reduce_over_ranks(ms2, float(numeq) * n_jacobi * args.steps, dist, dev)
+    e2e = {"value": units2 / (ms2 * 1e-3), "unit": UNIT, "ms_per_step": ms2 / args.steps,
+           "h2d_bytes_per_step": 8 * prob.nel, "d2h_bytes_per_step": 8 * (numeq + prob.nel + 1)}
+
+    # ---- roofline: the FP32 element operator of the V-cycle (the dominant
+    # kernel of the mixed solve) and the FP64 one of the residual, each timed
+    # live with an L2 flush before every launch
+    prob.set_density_device(rho_d.data_ptr())
+    peak, peak_kind = _peaks()
+    rows = {}
+    for name, prec, es, kern in (("fp32", icb.MIXED, 4, "k_matvec_h8m<float>"),
+                                 ("fp64", icb.FP64, 8, "k_matvec_h8m<double>")):
+        t = op_launch_seconds(prob, prec, stream, local)
+        b = es * (2 * prob.neq + prob.nel)
+        rows[name] = {"bound": "hbm", "achieved": b / t / 1e9, "peak": peak, "unit": "GB/s",
+                      "frac": b / t / 1e9 / peak, "kernel": kern, "launch_us": t * 1e6,
+                      "alg_bytes": b, "peak_source": peak_kind,
+                      "traffic": _traffic(f"matvec_h8m_{name}_halfmbb3d_384x128x128")}
+    roofline = dict(rows["fp32"])
+    roofline["fp64_outer_operator"] = rows["fp64"]
+
+    # ---- the topology-optimisation loop on the same beam: 20 MMA steps with
+    # the Helmholtz filter (R = 3, volume fraction 0.3), mixed solves
+    topo = None
+    if args.mma_steps > 0:
+        steps = args.mma_steps
+        o = icb.loop_opts(steps, 3.0, precision=icb.MIXED, volume_ref=0.3 * float(np.prod(grid)))
+        its = np.zeros(steps)
+        o.iter_seconds = its.ctypes.data_as(icb._dp)
+        hist, x = np.zeros(steps), np.zeros(prob.nel)
+        t0 = time.perf_counter()
+        icb.check(L.icb_run_mma(prob.h, C.byref(o), icb._p(rho_h), icb._p(hist), icb._p(x)))
+        dt = time.perf_counter() - t0
+        topo = {"iter_per_s": steps / dt, "steps": steps,
+                "step_ms_p50": 1e3 * float(np.median(its)),
+                "step_ms_p99": 1e3 * float(np.quantile(its, 0.99)),
+                "compliance_first_last": [hist[0], hist[-1]]}
+
+    line = {"metric": C3_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 multigrid / f64 Krylov and residual",
+            "data": "synthetic (seeded smooth density field, one instance per rank)",
+            "config": dict(c3_config(grid), parallelism=f"replicas x{world}"),
+            "solve": {"iters": infos[-1]["iters"], "true_relres": infos[-1]["true_relres"],
+                      "compliance": comp, "jacobi_iters_to_tol": n_jacobi,
+                      "pcg_dof_iter_per_s_raw": raw_units / (ms * 1e-3)},
+            "time_to_solution_ms": {"mixed_gmg_step": ms / args.steps, "fp64_gmg_solve": ms_g,
+                                    "fp64_gmg_iters": inf_g["iters"], "fp64_jacobi_solve": ms_j,
+                                    "fp64_jacobi_iters": n_jacobi},
+            "speedups": {"mixed_step_vs_fp64_gmg_solve": ms_g / (ms / args.steps),
+                         "mixed_step_vs_fp64_jacobi_solve": ms_j / (ms / args.steps)},
+            "mixed_vs_fp64": err,
+            "latency_ms": {"p50": lat[len(lat) // 2],
+                           "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "topopt": topo, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nit = 10
+        run, ne, threads = c3_cpu_sample(grid, nit, SEED)
+        tcpu = min(run() for _ in range(2))
+        line["cpu_baseline"] = {"value": ne * nit / tcpu, "unit": UNIT, "cores": threads,
+                                "kind": "port",
+                                "sample": f"{nit} matrix-free Jacobi-PCG iterations of the oracle "
+                                          f"on the same system ({tcpu / nit:.3f} s per iteration)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    prob.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------- workloads --
 def _clock_wrap(fn):
     clk = clocks_start(int(os.environ.get("LOCAL_RANK", "0")))
@@ -338,27 +597,9 @@ def _clock_wrap(fn):
 
 
 def smooth_field(nx, ny, nz, seed, lo=0.001, hi=1.0, modes=16):
-    """Seeded smooth random density: affine map to [lo, hi] of
-    sum_k a_k cos(2 pi (k . x_c / L) + phi_k), k integer triples in [0,4]^3,
-    a_k ~ N(0,1), phi_k ~ U[0, 2 pi), at element centres."""
-    import numpy as np
-    rng = np.random.default_rng(seed)
-    x = (np.arange(nx) + 0.5) / nx
-    y = (np.arange(ny) + 0.5) / ny
-    z = (np.arange(nz) + 0.5) / nz
-    f = np.zeros((nz, ny, nx))
-    for _ in range(modes):
-        k = rng.integers(0, 5, 3)
-        a, ph = rng.standard_normal(), rng.uniform(0, 2 * np.pi)
-        # separable evaluation of cos(2 pi (kx x + ky y + kz z) + ph)
-        cx, sx = np.cos(2 * np.pi * k[0] * x), np.sin(2 * np.pi * k[0] * x)
-        cy, sy = np.cos(2 * np.pi * k[1] * y), np.sin(2 * np.pi * k[1] * y)
-        cz, sz = np.cos(2 * np.pi * k[2] * z + ph), np.sin(2 * np.pi * k[2] * z + ph)
-        cxy = np.outer(cy, cx) - np.outer(sy, sx)
-        sxy = np.outer(sy, cx) + np.outer(cy, sx)
-        f += a * (cz[:, None, None] * cxy[None] - sz[:, None, None] * sxy[None])
-    f = (f - f.min()) / max(f.max() - f.min(), 1e-300)
-    return (lo + (hi - lo) * f).reshape(-1)
+    """the c3 density field (tests/cases.py holds the definition)"""
+    import cases
+    return cases.smooth_field(nx, ny, nz, seed, lo, hi, modes)
 
 
 def op_launch_seconds(prob, prec, stream, device=0, reps=30):
@@ -402,13 +643,15 @@ def workload_operator(args):
     for n in grids:
         g = cases.build_gpu(ctx, "cantilever3d", *n)
         g.set_density(cases.uniform_density(g.nel, SEED))
-        for name, prec, tc, modal, es in (("fp64_modal", icb.FP64, 0, 1, 8),
-                                          ("fp64_dense", icb.FP64, 0, 0, 8),
-                                          ("fp32_modal", icb.MIXED, 0, 1, 4),
-                                          ("fp32_dense", icb.MIXED, 0, 0, 4),
-                                          ("tf32_tcgen05", icb.TF32, 1, 1, 4)):
+        for name, prec, tc, modal, pair, es in (("fp64_modal", icb.FP64, 0, 1, 1, 8),
+                                                ("fp64_dense", icb.FP64, 0, 0, 1, 8),
+                                                ("fp32_modal_paired", icb.MIXED, 0, 1, 1, 4),
+                                                ("fp32_modal_row", icb.MIXED, 0, 1, 0, 4),
+                                                ("fp32_dense", icb.MIXED, 0, 0, 1, 4),
+                                                ("tf32_tcgen05", icb.TF32, 1, 1, 1, 4)):
             icb.set_option("tc_operator", tc)
             icb.set_option("hex8_modal", modal)
+            icb.set_option("hex8_pair", pair)
             t = op_launch_seconds(g, prec, stream)
             B = es * (2 * g.neq + g.nel)
             rows.append({"grid": "x".join(map(str, n)), "variant": name, "launch_us": t * 1e6,
@@ -416,6 +659,7 @@ def workload_operator(args):
                          "elem_per_s": g.nel / t})
         icb.set_option("tc_operator", 0)
         icb.set_option("hex8_modal", 1)
+        icb.set_option("hex8_pair", 1)
         g.close()
     print(json.dumps({"metric": "Hex8 operator launch time", "unit": "us", "rows": rows,
                       "tc_timeouts": icb.get_option("tc_timeouts"),
@@ -715,19 +959,26 @@ def workload_solve(args):
     import icarat_b200 as icb
     n = tuple(args.size) if args.size else (384, 128, 128)
     prec, pc = {"fp64_jacobi": (icb.FP64, icb.JACOBI), "fp64_gmg": (icb.FP64, icb.GMG),
-                "mixed_gmg": (icb.MIXED, icb.GMG)}[args.solver]
+                "mixed_gmg": (icb.MIXED, icb.GMG),
+                "mixed_refine": (icb.MIXED_REFINE, icb.GMG)}[args.solver]
     ctx = icb.Context(0)
     icb.set_option("tc_operator", args.tc)
     g = cases.build_gpu(ctx, "halfmbb3d", *n)
     g.set_density(smooth_field(*n, seed=SEED))
-    g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000)
-    t0 = time.perf_counter()
-    inf = g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000)
-    dt = time.perf_counter() - t0
-    print(json.dumps({"metric": "solve time", "value": 1e3 * dt, "unit": "ms", "solver": args.solver,
-                      "tc_operator": args.tc, "tc_timeouts": icb.get_option("tc_timeouts"),
+    icb.set_option("hex8_pair", args.pair)
+    g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000, inner_tol=args.inner_tol)
+    times, inf = [], None
+    for _ in range(args.repeat):
+        t0 = time.perf_counter()
+        inf = g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000, inner_tol=args.inner_tol)
+        times.append(time.perf_counter() - t0)
+    print(json.dumps({"metric": "solve time", "value": 1e3 * min(times), "unit": "ms",
+                      "all_ms": [1e3 * t for t in times], "solver": args.solver,
+                      "tc_operator": args.tc, "hex8_pair": args.pair, "inner_tol": args.inner_tol,
+                      "tc_timeouts": icb.get_option("tc_timeouts"),
                       "config": {"workload": f"halfmbb3d {n[0]}x{n[1]}x{n[2]}", "dof": g.neq},
-                      "iters": inf["iters"], "true_relres": inf["true_relres"]}), flush=True)
+                      "iters": inf["iters"], "outer": inf["outer"], "matvecs": inf["matvecs"],
+                      "true_relres": inf["true_relres"]}), flush=True)
     g.close()
     ctx.close()
     return 0
@@ -763,8 +1014,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-operator", action="store_true",
                     help="only launch the operator kernels on the bench problem (for ncu)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "batched", "serving", "operator", "solve"],
-                    help="c2 (default): the bench line; the others print their own line")
+    ap.add_argument("--workload", default="headline",
+                    choices=["headline", "c2", "c1", "c3", "batched", "serving", "operator", "solve"],
+                    help="headline (default): the c3 bench line; c2: the FP64 Jacobi-PCG drop-in on "
+                         "192x64x64 (both arms); the others print their own line")
     ap.add_argument("--size", type=int, nargs="+", default=None, help="c3 / operator grid override")
     ap.add_argument("--mma-steps", type=int, default=20)
     ap.add_argument("--host-loops", action="store_true",
@@ -774,8 +1027,14 @@ def main():
                     help="c3: only the MMA loop (no initial-design solves, no CPU sample)")
     ap.add_argument("--tc", type=int, default=0, choices=[0, 1],
                     help="solve workload: fine-level V-cycle operator on the tensor cores")
-    ap.add_argument("--solver", default="mixed_gmg", choices=["fp64_jacobi", "fp64_gmg", "mixed_gmg"],
+    ap.add_argument("--solver", default="mixed_gmg",
+                    choices=["fp64_jacobi", "fp64_gmg", "mixed_gmg", "mixed_refine"],
                     help="solve workload: which solver")
+    ap.add_argument("--pair", type=int, default=1, choices=[0, 1],
+                    help="solve workload: FP32 Hex8 operator with two element rows per thread")
+    ap.add_argument("--inner-tol", type=float, default=0.0,
+                    help="solve workload, mixed_refine: inner relative tolerance (0: default)")
+    ap.add_argument("--repeat", type=int, default=3, help="solve workload: timed solves")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--loop-steps", type=int, default=10, help="batched: OC steps per instance")
     ap.add_argument("--workers", type=int, nargs="+", default=[1, 8, 16], help="batched: host workers")
@@ -789,6 +1048,8 @@ def main():
         icb.set_option("device_loops", 0)
     if args.profile_operator:
         return profile_operator(args)
+    if args.workload == "headline":
+        return headline_reference(args) if args.impl == "reference" else headline_ours(args)
     if args.workload != "c2" and args.impl == "ours":
         return {"c1": workload_c1, "c3": workload_c3, "batched": workload_batched,
                 "serving": workload_serving, "operator": workload_operator,

@@ -78,6 +78,9 @@ int icb_ctx_create(int device, icb_ctx *out)
   ICB_CUDA(cudaGetDeviceCount(&n));
   need(device >= 0 && device < n, "no such CUDA device");
   ICB_CUDA(cudaSetDevice(device));
+  // the no-alloc solve's static scratch gets its device memory here, when
+  // its module loads, not in the middle of a caller's solve
+  noalloc_prepare_current_device();
   auto *c = new icb_ctx_s;
   c->device = device;
   c->refs = 1;
@@ -369,7 +372,9 @@ int icb_solve(icb_problem p, const icb_solve_opts *opts, icb_solve_info *info)
   if(opts)
     o = *opts;
   need(o.tol >= 0.0 && o.maxit > 0, "bad tolerance / iteration limit");
-  need(o.precision == ICB_FP64 || o.precision == ICB_MIXED, "unknown precision");
+  need(o.precision == ICB_FP64 || o.precision == ICB_MIXED || o.precision == ICB_MIXED_REFINE,
+       "unknown precision");
+  need(o.inner_tol >= 0.0 && o.inner_tol < 1.0, "inner_tol must be in [0, 1)");
   need(o.precond == ICB_PRECOND_JACOBI || o.precond == ICB_PRECOND_GMG, "unknown preconditioner");
   NvtxRange range("icb_solve");
   cudaStream_t s = p->stream();
@@ -409,7 +414,10 @@ int icb_solve(icb_problem p, const icb_solve_opts *opts, icb_solve_info *info)
     *info = inf;
   if(st != ICB_OK)
   {
-    set_error(st == ICB_ERR_MAXITER ? "iteration limit reached" : st == ICB_ERR_BREAKDOWN ? "CG breakdown (p.Kp <= 0)" : "non-finite values in the solve");
+    set_error(st == ICB_ERR_MAXITER     ? "iteration limit reached"
+              : st == ICB_ERR_BREAKDOWN ? "CG breakdown (p.Kp <= 0)"
+              : st == ICB_ERR_TIMEOUT   ? "a tensor-core operator wait timed out inside the V-cycle"
+                                        : "non-finite values in the solve");
     return st;
   }
   ICB_API_END
@@ -591,6 +599,13 @@ int icb_set_option(const char *name, long long value)
     set_hex8_modal(value != 0);
   else if(n == "device_loops")
     set_device_loops(value != 0);
+  else if(n == "hex8_pair")
+    set_hex8_pair(value != 0);
+  else if(n == "tc_spin_limit")
+  {
+    need(value >= 0 && value <= 0x7fffffffLL, "tc_spin_limit must be in [0, 2^31)");
+    set_tc_spin_limit(unsigned(value));
+  }
   else
     need(false, "unknown option");
   ICB_API_END
@@ -607,8 +622,12 @@ long long icb_get_option(const char *name)
     return hex8_modal_enabled() ? 1 : 0;
   if(n == "device_loops")
     return device_loops_enabled() ? 1 : 0;
+  if(n == "hex8_pair")
+    return hex8_pair_enabled() ? 1 : 0;
   if(n == "tc_timeouts")
     return (long long)tc_timeouts();
+  if(n == "tc_spin_limit")
+    return (long long)tc_spin_limit();
   return -1;
 }
 
@@ -623,17 +642,23 @@ int icb_operator_apply_device(icb_problem p, int precision, const void *x, void 
                           p->stream());
   else if(precision == ICB_MIXED)
   {
-    // the FP32 CUDA-core kernel, whatever the tensor-core switch says
-    bool tc = tc_operator_enabled();
-    set_tc_operator(false);
-    launch_matvec<float>(p->d, p->K0f, p->Ef.p, (const float *)x, (float *)y, p->fix.p,
-                         p->stream());
-    set_tc_operator(tc);
+    // the FP32 CUDA-core kernel, whatever the tensor-core switch says (the
+    // process-wide switch is left alone: other threads may be solving)
+    OpExtras<float> ex;
+    ex.cudaCores = 1;
+    launch_op<float>(p->d, p->K0f, p->Ef.p, (const float *)x, (float *)y, p->fix.p,
+                     p->stream(), ex);
   }
   else if(precision == ICB_TF32)
   {
+    // a tensor-core wait that gave up leaves its CTA's tile of y unwritten:
+    // report it as ICB_ERR_TIMEOUT instead of returning a wrong product
+    const unsigned t0 = tc_timeouts();
     OpExtras<float> ex;
     launch_op_tc(p->d, p->K0f, p->Ef.p, (const float *)x, (float *)y, p->fix.p, p->stream(), ex);
+    ICB_CUDA(cudaStreamSynchronize(p->stream()));
+    if(tc_timeouts() != t0)
+      throw Error{ICB_ERR_TIMEOUT, "a tensor-core operator wait timed out; y is incomplete"};
   }
   else
     need(false, "unknown precision");

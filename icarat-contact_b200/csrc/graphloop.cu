@@ -10,6 +10,12 @@ namespace icb
 static std::atomic<bool> g_device_loops{true};
 bool device_loops_enabled() { return g_device_loops.load(); }
 void set_device_loops(bool on) { g_device_loops = on; }
+unsigned long long kernel_switches()
+{
+  return (tc_operator_enabled() ? 1ull : 0ull) | (hex8_modal_enabled() ? 2ull : 0ull) |
+         (device_loops_enabled() ? 4ull : 0ull) | (hex8_pair_enabled() ? 8ull : 0ull) |
+         ((unsigned long long)tc_spin_limit() << 8);
+}
 
 void WhileGraph::reset()
 {

@@ -3,7 +3,11 @@
 // graph launch and one host wait run a Krylov solve or a bisection to its
 // end, with no wasted gated iterations and no host round trip in between.
 #pragma once
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
 #include <functional>
+#include <vector>
 
 #include "icb_internal.hpp"
 
@@ -48,6 +52,46 @@ struct WhileGraph
 /// bisection (icb_set_option "device_loops"; default on)
 bool device_loops_enabled();
 void set_device_loops(bool on);
+
+/// the process-wide kernel switches (tc_operator, hex8_modal, device_loops,
+/// tc_spin_limit) as bits: a captured graph holds the kernels they chose
+unsigned long long kernel_switches();
+
+/// Everything a captured graph bakes in: the device pointers and sizes its
+/// kernels were given, the parameter structs passed by value and the kernel
+/// switches.  A cached graph is relaunched only when every entry is equal.
+/// Keying on the address of a host object is not enough: an object freed and
+/// re-created at the same address owns new device buffers, and the old graph
+/// would read the freed ones.  With every baked value in the key, a graph is
+/// reused only where a fresh capture would record the same launches.
+struct GraphKey
+{
+  std::vector<unsigned long long> v;
+  GraphKey &add(const void *p)
+  {
+    v.push_back((unsigned long long)(uintptr_t)p);
+    return *this;
+  }
+  GraphKey &add(long long x)
+  {
+    v.push_back((unsigned long long)x);
+    return *this;
+  }
+  /// a trivially copyable parameter struct, byte by byte
+  template <typename S> GraphKey &addBytes(const S &s)
+  {
+    const unsigned char *b = reinterpret_cast<const unsigned char *>(&s);
+    for(size_t i = 0; i < sizeof(S); i += 8)
+    {
+      unsigned long long w = 0;
+      std::memcpy(&w, b + i, std::min<size_t>(8, sizeof(S) - i));
+      v.push_back(w);
+    }
+    return *this;
+  }
+  bool operator==(const GraphKey &o) const { return v == o.v; }
+  bool operator!=(const GraphKey &o) const { return v != o.v; }
+};
 
 #ifdef __CUDACC__
 /// one thread, at the end of a Krylov body: count the pass (st->pad, zeroed by

@@ -191,17 +191,30 @@ template <typename T> struct OpExtras
   double *dotOut = nullptr;
   const KState *gate = nullptr; ///< skip when gate->stop (or gate->conv if gateConv)
   int gateConv = 0;
+  int cudaCores = 0; ///< 1: the CUDA-core kernel, whatever the tensor-core switch says
 };
+/// bytes of an app-loop checkpoint (toapi.cu) for nel elements and a job kind
+long long loop_checkpoint_bytes(long long nel, int kind);
+/// look up the no-alloc solve's static scratch on the current device
+/// (noalloc.cu; called by icb_ctx_create)
+void noalloc_prepare_current_device();
 /// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)
 void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u, float *y,
                   const uint8_t *fix, cudaStream_t s, const OpExtras<float> &x);
 unsigned tc_timeouts();
+/// polls of a tensor-core MMA wait before a CTA gives up, counts a timeout
+/// and returns (process-wide; default 2^22)
+unsigned tc_spin_limit();
+void set_tc_spin_limit(unsigned polls);
 /// whether FP32 Hex8 operator launches use the tensor-core kernel
 bool tc_operator_enabled();
 void set_tc_operator(bool on);
 /// whether Hex8 operator launches use the corner-mode kernel when K0 allows it
 bool hex8_modal_enabled();
 void set_hex8_modal(bool on);
+/// whether FP32 corner-mode Hex8 launches run two element rows per thread
+bool hex8_pair_enabled();
+void set_hex8_pair(bool on);
 
 /// K: HOST pointer to the unit element matrix ((d*ne)^2 entries); it is
 /// passed by value, so the kernel's FMAs take it from the constant bank.

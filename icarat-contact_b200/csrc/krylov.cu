@@ -67,8 +67,12 @@ __global__ void k_pcg_init(long long n, const T *__restrict__ b, T *__restrict__
   for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)gridDim.x * blockDim.x)
   {
-    T bi = b[i];
-    T zi = dinv[i] * bi;
+    // b is read on the unknowns only: the inverse diagonal is 0 on
+    // constrained DOFs and on the SoA padding past each component's last
+    // node, and whatever a caller's b holds there never enters r
+    const T di = dinv[i];
+    T bi = di != T(0) ? b[i] : T(0);
+    T zi = di * bi;
     r[i] = bi;
     p[i] = zi;
     x[i] = T(0);
@@ -306,11 +310,10 @@ int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const voi
   // launch, polled from the host (a device-side WHILE loop was measured at
   // the same speed here, 251 against 249 ms for the c2 solve, and profilers
   // cannot follow its kernels)
-  const void *key[6] = {opKey0, opKey1, opKey2, invdiag, x, (const void *)s};
-  bool same = loop.exec != nullptr;
-  for(int i = 0; i < 6 && same; i++)
-    same = key[i] == graphKey[i];
-  if(!same)
+  GraphKey key;
+  key.add(opKey0).add(opKey1).add(opKey2).add(invdiag).add(x).add((const void *)s);
+  key.add((long long)kernel_switches());
+  if(loop.exec == nullptr || key != graphKey)
   {
     KState *stp = st.p;
     const long long before = thread_launch_count();
@@ -322,8 +325,7 @@ int JacobiPcg<T>::solveOp(const std::function<void(cudaStream_t)> &op, const voi
         },
         false, 16);
     count_launch(before - thread_launch_count()); // recorded, not launched
-    for(int i = 0; i < 6; i++)
-      graphKey[i] = key[i];
+    graphKey = key;
   }
   long long launched = 0;
   for(;;)

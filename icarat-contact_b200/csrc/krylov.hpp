@@ -26,7 +26,7 @@ template <typename T> struct JacobiPcg
   RedScratch red;
   KState *hst = nullptr; ///< pinned mirror
   WhileGraph loop; ///< host form: 16 iterations per launch
-  const void *graphKey[6] = {};
+  GraphKey graphKey; ///< what `loop` bakes in besides this object's own buffers
 
   JacobiPcg(const Dims &dims, cudaStream_t s);
   ~JacobiPcg();

@@ -634,7 +634,7 @@ template <typename TK, typename TP> struct MgPcg
   RedScratch red;
   KState *hst = nullptr;
   WhileGraph loop; ///< one FCG iteration, repeated on the device until stop
-  const void *key[4] = {};
+  GraphKey key;    ///< what `loop` bakes in besides this object's own buffers
 
   ~MgPcg()
   {
@@ -936,18 +936,15 @@ template <typename TK, typename TP> struct MgPcg
     k_mg_init2<TK, TP><<<nb, VB, 0, s>>>(n, r.p, z.p, p.p, red, st.p);
     count_launch();
     ICB_CUDA(cudaGetLastError());
-    const void *k[4] = {x, Ek, lv[0].E, (const void *)s};
+    GraphKey k;
+    k.add(x).add(Ek).add(lv[0].E).add((const void *)s).add((long long)kernel_switches());
     const bool dev = device_loops_enabled();
-    bool same_ = loop.exec != nullptr && loop.device == dev;
-    for(int i = 0; i < 4 && same_; i++)
-      same_ = k[i] == key[i];
-    if(!same_)
+    if(loop.exec == nullptr || loop.device != dev || k != key)
     {
       const long long before = thread_launch_count();
       loop.build([&](cudaStream_t cs, const LoopCtl &L) { iteration(x, cs, L); }, dev, 8);
       count_launch(before - thread_launch_count()); // recorded, not launched
-      for(int i = 0; i < 4; i++)
-        key[i] = k[i];
+      key = k;
     }
     if(loop.device)
     {
@@ -983,12 +980,114 @@ template <typename TK, typename TP> struct MgPcg
 };
 
 // ============================================================== Mixed ======
+/// r32 = float(s * r64): the outer residual, scaled to unit norm, as the
+/// right-hand side of the FP32 inner solve
+__global__ void k_dc_to_f32(long long n, const double *__restrict__ r, double sc,
+                            float *__restrict__ r32)
+{
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+    r32[i] = float(sc * r[i]);
+}
+/// x += w * d (the FP32 correction accumulated into the FP64 iterate)
+__global__ void k_dc_update(long long n, double *__restrict__ x, const float *__restrict__ d,
+                            double w)
+{
+  for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+      i += (long long)gridDim.x * blockDim.x)
+    x[i] += w * double(d[i]);
+}
+
 struct Mixed
 {
   int coarseDofs = -1, smooth = -1;
   std::unique_ptr<MgPcg<double, double>> mg64;
   std::unique_ptr<MgPcg<double, float>> mgmx;
+  // defect correction: FP32 GMG-PCG inside an FP64 residual loop
+  std::unique_ptr<MgPcg<float, float>> mg32;
+  DevBuf<double> r64;
+  DevBuf<float> r32, d32;
 };
+
+/// FP64 iterative refinement (defect correction) around an all-FP32
+/// multigrid PCG: r = b - K x in FP64, the correction K d = r solved in FP32
+/// (Krylov vectors, operator, V-cycle; scalars reduced in FP64) to a relative
+/// tolerance, x += d in FP64, until ||r|| <= tol ||b|| measured in FP64.  FP64
+/// work per outer step: one operator application and three vector passes.
+static int solve_refine(icb_problem p, Mixed &M, const icb_solve_opts &o, const double *b,
+                        icb_solve_info &inf)
+{
+  cudaStream_t s = p->stream();
+  const HostSetup &hs = *p->hs;
+  if(!M.mg32)
+  {
+    M.mg32 = std::make_unique<MgPcg<float, float>>();
+    M.mg32->build(hs, p->K0f, p->Ef.p, p->K0f, p->Ef.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth,
+                  s);
+    M.r64.alloc(p->nsoa);
+    M.r32.alloc(p->nsoa);
+    M.d32.alloc(p->nsoa);
+    ICB_CUDA(cudaMemsetAsync(M.r32.p, 0, M.r32.bytes(), s));
+    ICB_CUDA(cudaMemsetAsync(M.d32.p, 0, M.d32.bytes(), s));
+  }
+  M.mg32->refresh(s);
+  const long long n = p->nsoa;
+  const int nb = vblocks(n);
+  double *x = p->x.p, *r = M.r64.p;
+  ICB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+  ICB_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  const double bb = device_dot(n, b, b, p->red, p->scal.p, s);
+  const double thr = std::max(o.tol * o.tol * bb, DBL_MIN);
+  // inner relative tolerance: the requested one (inner_tol), else 1e-4; the
+  // last outer step only solves as far as the outer tolerance needs
+  const double eta = o.inner_tol > 0.0 ? o.inner_tol : 1e-4;
+  double rr = bb;
+  int iters = 0, matvecs = 0, outer = 0, status = ICB_OK;
+  if(!std::isfinite(bb))
+    status = ICB_ERR_NAN;
+  while(status == ICB_OK && bb > 0.0 && rr >= thr)
+  {
+    if(iters >= o.maxit || outer >= 100)
+    {
+      status = ICB_ERR_MAXITER;
+      break;
+    }
+    outer++;
+    const double sc = 1.0 / std::sqrt(rr);
+    k_dc_to_f32<<<nb, VB, 0, s>>>(n, r, sc, M.r32.p);
+    count_launch();
+    const double need = 0.5 * std::sqrt(thr / rr);
+    icb_solve_info ii{};
+    int st = M.mg32->solve(M.r32.p, M.d32.p, std::min(0.5, std::max(eta, need)),
+                           o.maxit - iters, s, &ii);
+    iters += ii.iters;
+    matvecs += ii.matvecs;
+    if(st == ICB_ERR_NAN || (st != ICB_OK && ii.iters == 0))
+    {
+      status = st == ICB_ERR_MAXITER ? ICB_ERR_MAXITER : st;
+      break;
+    }
+    // a breakdown or the iteration cap of the inner solve still leaves a
+    // usable correction; the FP64 residual below judges it
+    k_dc_update<<<nb, VB, 0, s>>>(n, x, M.d32.p, 1.0 / sc);
+    count_launch();
+    OpExtras<double> ex;
+    ex.mode = OP_RESIDUAL;
+    ex.b = b;
+    launch_op<double>(p->d, p->K0, p->E.p, x, r, p->fix.p, s, ex);
+    const double rn = device_dot(n, r, r, p->red, p->scal.p, s);
+    if(!std::isfinite(rn))
+      status = ICB_ERR_NAN;
+    else if(rn >= rr && st != ICB_OK)
+      status = st; // the inner solve failed and the correction did not help
+    rr = rn;
+  }
+  inf.iters = iters;
+  inf.matvecs = matvecs + outer;
+  inf.outer = outer;
+  inf.relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+  return status;
+}
 
 int solve_multigrid(icb_problem p, const icb_solve_opts &o, const double *b, icb_solve_info *info)
 {
@@ -1001,6 +1100,7 @@ int solve_multigrid(icb_problem p, const icb_solve_opts &o, const double *b, icb
   {
     M.mg64.reset();
     M.mgmx.reset();
+    M.mg32.reset();
     M.coarseDofs = o.mg_coarse_dofs;
     M.smooth = o.mg_smooth;
   }
@@ -1008,9 +1108,14 @@ int solve_multigrid(icb_problem p, const icb_solve_opts &o, const double *b, icb
   ICB_CUDA(cudaEventCreate(&e0));
   ICB_CUDA(cudaEventCreate(&e1));
   ICB_CUDA(cudaEventRecord(e0, s));
+  // the FP32 V-cycle may run on the tensor cores: count their timed-out waits
+  const bool tc = o.precision != ICB_FP64 && tc_operator_enabled();
+  const unsigned tc0 = tc ? tc_timeouts() : 0u;
   int status;
   icb_solve_info inf{};
-  if(o.precision == ICB_FP64)
+  if(o.precision == ICB_MIXED_REFINE)
+    status = solve_refine(p, M, o, b, inf);
+  else if(o.precision == ICB_FP64)
   {
     if(!M.mg64)
     {
@@ -1031,7 +1136,15 @@ int solve_multigrid(icb_problem p, const icb_solve_opts &o, const double *b, icb
     M.mgmx->refresh(s);
     status = M.mgmx->solve(b, p->x.p, o.tol, o.maxit, s, &inf);
   }
-  inf.outer = 1;
+  if(o.precision != ICB_MIXED_REFINE)
+    inf.outer = 1;
+  // a CTA whose tensor-core wait gave up left its tile of a V-cycle operator
+  // product unwritten: the solve is not trusted, whatever it converged to
+  if(tc && tc_timeouts() != tc0)
+  {
+    status = ICB_ERR_TIMEOUT;
+    set_error("a tensor-core operator wait timed out inside the V-cycle");
+  }
   ICB_CUDA(cudaEventRecord(e1, s));
   ICB_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;

@@ -554,6 +554,309 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
   }
 }
 
+// ------------------------------------------------- Hex8, paired rows ----
+// The FP32 corner-mode operator with two element rows per thread.  A CTA of
+// 32 x TW threads owns a 31 x (2 TW - 1) tile of output nodes (one element of
+// halo on the low side of each axis) and marches up a chunk of z planes, as
+// k_matvec_h8m does; thread (lx, ly) owns element rows j = Y0 - 1 + 2 ly and
+// j + 1 of element column i = X0 - 1 + lx.  The two elements run in lockstep
+// as the two lanes of packed FP32 pairs (add / sub / mul / fma .f32x2): the
+// x-y butterflies, the z butterfly and the modulus scaling of both elements
+// are one packed instruction each, while the 45 block products stay scalar
+// (their coefficients are constant-bank operands).  The node row between the
+// two elements is summed inside the thread, so only one node row per two
+// element rows goes through shared memory to the warp below.
+template <typename T> struct PairOps;
+template <> struct PairOps<float>
+{
+  using P = float2;
+  static __device__ __forceinline__ P add(P a, P b) { return __fadd2_rn(a, b); }
+  static __device__ __forceinline__ P mul(P a, P b) { return __fmul2_rn(a, b); }
+  static __device__ __forceinline__ P fma(P a, P b, P c) { return __ffma2_rn(a, b, c); }
+  static __device__ __forceinline__ P sub(P a, P b)
+  {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(r)
+        : "l"(*reinterpret_cast<unsigned long long *>(&a)),
+          "l"(*reinterpret_cast<unsigned long long *>(&b)));
+    return *reinterpret_cast<P *>(&r);
+  }
+};
+
+constexpr int kPairWarps = 8;     // warps of k_matvec_h8p (two element rows each)
+constexpr int kPairMinBlocks = 1;
+constexpr int kPairPrefetch = 3;  // planes between the L2 prefetch and the register prefetch
+template <typename T, int TW, bool DOT, int MODE, int MINB>
+__global__ void __launch_bounds__(TX *TW, MINB)
+    k_matvec_h8p(const KModal<T> K, const Dims d, const int zchunk, const T *__restrict__ E,
+                 const T *__restrict__ u, T *__restrict__ y, const uint8_t *__restrict__ fix,
+                 RedScratch red, double *dotOut, const KState *gate, const int gateConv,
+                 const Epi<T> ep)
+{
+  using O = PairOps<T>;
+  using P = typename O::P;
+  if(gate && (gate->stop || (gateConv && gate->conv)))
+    return;
+  __shared__ T sB[2][3][TW][TX];
+  const int lx = threadIdx.x, ly = threadIdx.y;
+  const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (2 * TW - 1);
+  const int ei = X0 - 1 + lx, ej = Y0 - 1 + 2 * ly;
+  const int Z0 = blockIdx.z * zchunk;
+  const int Z1 = min(Z0 + zchunk, d.sz) - 1;
+  const long long sxy = (long long)d.sx * d.sy, exy = (long long)d.nx * d.ny;
+  const long long ld = d.ld;
+  // nodes (ei + a, ej + r), r = 0, 1, 2, a = 0, 1, and the two elements
+  bool nok[3][2];
+#pragma unroll
+  for(int r = 0; r < 3; r++)
+#pragma unroll
+    for(int a = 0; a < 2; a++)
+      nok[r][a] = ei + a >= 0 && ei + a < d.sx && ej + r >= 0 && ej + r < d.sy;
+  const bool ecol = ei >= 0 && ei < d.nx;
+  const bool eok0 = ecol && ej >= 0 && ej < d.ny, eok1 = ecol && ej + 1 >= 0 && ej + 1 < d.ny;
+  // element (ei, ej) of layer 0 and node (ei, ej) of plane 0 (either may lie
+  // outside the grid: every access below is guarded by the flags above)
+  const long long eb = (long long)ei + (long long)ej * d.nx;
+  const long long nb = (long long)ei + (long long)ej * d.sx;
+  auto ldn = [&](int k, int c, int r, int a) -> T {
+    return (nok[r][a] && k >= 0 && k <= d.nz)
+               ? __ldg(u + c * ld + nb + (long long)r * d.sx + a + (long long)k * sxy)
+               : T(0);
+  };
+  // plane k as pairs over the row pairs (j, j + 1) and (j + 1, j + 2)
+  auto load_plane = [&](int k, P (&lo)[3][2], P (&hi)[3][2]) {
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+#pragma unroll
+      for(int a = 0; a < 2; a++)
+      {
+        lo[c][a].x = ldn(k, c, 0, a);
+        lo[c][a].y = ldn(k, c, 1, a);
+        hi[c][a].x = lo[c][a].y;
+        hi[c][a].y = ldn(k, c, 2, a);
+      }
+  };
+  auto load_E = [&](int k) -> P {
+    P e;
+    const bool kok = k >= 0 && k < d.nz;
+    e.x = (eok0 && kok) ? __ldg(E + eb + (long long)k * exy) : T(0);
+    e.y = (eok1 && kok) ? __ldg(E + eb + d.nx + (long long)k * exy) : T(0);
+    return e;
+  };
+  // x-y modes of a plane for both elements: h[c][sx + 2 sy]
+  auto modes = [&](const P (&lo)[3][2], const P (&hi)[3][2], P (&h)[3][4]) {
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      const P sl = O::add(lo[c][0], lo[c][1]), dl = O::sub(lo[c][0], lo[c][1]);
+      const P sh = O::add(hi[c][0], hi[c][1]), dh = O::sub(hi[c][0], hi[c][1]);
+      h[c][0] = O::add(sl, sh);
+      h[c][1] = O::add(dl, dh);
+      h[c][2] = O::sub(sl, sh);
+      h[c][3] = O::sub(dl, dh);
+    }
+  };
+
+  P bh[3][4], carry[3][4], nlo[3][2], nhi[3][2];
+  {
+    load_plane(Z0 - 1, nlo, nhi);
+    modes(nlo, nhi, bh);
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+        carry[c][q] = P{T(0), T(0)};
+  }
+  load_plane(Z0, nlo, nhi);
+  P Enxt = load_E(Z0 - 1);
+  // L2 prefetch, kPairPrefetch planes ahead of the register prefetch: lane
+  // l < 18 takes component l / 6, row l / 2 % 3 and half-row l % 2 of the
+  // warp's three node rows, lanes 18..21 the two element rows' moduli, so one
+  // instruction per warp and layer keeps the plane loads L2 hits
+  long long pfOff = -1;
+  long long pfStep = sxy;
+  bool pfE = false;
+  {
+    const int x0 = min(max(X0 - 1 + 32 * (lx & 1), 0), d.nx);
+    if(lx < 18)
+    {
+      const int c = lx / 6, r = (lx >> 1) % 3;
+      const int row = ej + r;
+      if(row >= 0 && row < d.sy)
+        pfOff = c * ld + x0 + (long long)row * d.sx;
+    }
+    else if(lx < 22)
+    {
+      const int row = ej + ((lx - 18) >> 1);
+      if(row >= 0 && row < d.ny)
+      {
+        pfOff = min(x0, d.nx - 1) + (long long)row * d.nx;
+        pfStep = exy;
+        pfE = true;
+      }
+    }
+  }
+  const int ni = ei + 1;
+  const bool ocol = lx < TX - 1 && ni < d.sx;
+  const bool own1 = ocol && ej + 1 >= 0 && ej + 1 < d.sy;
+  const bool own2 = ocol && ly < TW - 1 && ej + 2 < d.sy;
+  const long long nodeb = (long long)ni + (long long)(ej + 1) * d.sx; // row j + 1, plane 0
+  double dot = 0.0;
+  for(int ek = Z0 - 1; ek <= Z1; ++ek)
+  {
+    P th[3][4];
+    modes(nlo, nhi, th);
+    const P Ee = Enxt;
+    load_plane(ek + 2, nlo, nhi);
+    Enxt = load_E(ek + 1);
+    {
+      const int kp = ek + 2 + kPairPrefetch; // plane (layer for the moduli)
+      if(pfOff >= 0 && kp <= (pfE ? d.nz - 1 : d.nz))
+      {
+        const T *a = (pfE ? E : u) + pfOff + (long long)kp * pfStep;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+      }
+    }
+    const bool out = ek >= Z0;
+    // the epilogue's inputs at the two output nodes of plane ek
+    const long long node1 = nodeb + (long long)ek * sxy, node2 = node1 + d.sx;
+    unsigned f1 = 0, f2 = 0;
+    T us1[3] = {T(0), T(0), T(0)}, us2[3] = {T(0), T(0), T(0)};
+    T b1[3], b2[3], dv1[3], dv2[3], pv1[3], pv2[3];
+    if(out)
+    {
+      if(own1)
+        f1 = __ldg(fix + node1);
+      if(own2)
+        f2 = __ldg(fix + node2);
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const long long i1 = c * ld + node1, i2 = c * ld + node2;
+        if(DOT || MODE >= OP_JACOBI)
+        {
+          us1[c] = own1 ? __ldg(u + i1) : T(0);
+          us2[c] = own2 ? __ldg(u + i2) : T(0);
+        }
+        if(MODE != OP_APPLY)
+        {
+          b1[c] = own1 ? __ldg(ep.b + i1) : T(0);
+          b2[c] = own2 ? __ldg(ep.b + i2) : T(0);
+        }
+        if(MODE >= OP_JACOBI)
+        {
+          dv1[c] = own1 ? __ldg(ep.dinv + i1) : T(0);
+          dv2[c] = own2 ? __ldg(ep.dinv + i2) : T(0);
+        }
+        if(MODE == OP_CHEB)
+        {
+          pv1[c] = (own1 && ep.c1 != T(0)) ? y[i1] : T(0);
+          pv2[c] = (own2 && ep.c1 != T(0)) ? y[i2] : T(0);
+        }
+      }
+    }
+    // element modes (z butterfly) and the 11 blocks, lane by lane
+    T ux[24], uy[24], yx[24], yy[24];
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const P sp = O::add(bh[c][q], th[c][q]), sm = O::sub(bh[c][q], th[c][q]);
+        ux[q * 3 + c] = sp.x;
+        uy[q * 3 + c] = sp.y;
+        ux[(q + 4) * 3 + c] = sm.x;
+        uy[(q + 4) * 3 + c] = sm.y;
+        bh[c][q] = th[c][q];
+      }
+    yx[0] = yx[1] = yx[2] = T(0); // rigid translations
+    yy[0] = yy[1] = yy[2] = T(0);
+    modal_blocks_apply<0, 0>(K, ux, yx);
+    modal_blocks_apply<0, 0>(K, uy, yy);
+    // inverse z butterfly with the moduli: the bottom face completes plane
+    // ek, the top face is carried up
+    T o0[3], o1[3], o2[3]; // x-summed rows j, j + 1, j + 2 of plane ek
+    const int buf = ek & 1;
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      P hb[4];
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+      {
+        const P a = P{yx[q * 3 + c], yy[q * 3 + c]}, b = P{yx[(q + 4) * 3 + c], yy[(q + 4) * 3 + c]};
+        hb[q] = O::fma(Ee, O::add(a, b), carry[c][q]);
+        carry[c][q] = O::mul(Ee, O::sub(a, b));
+      }
+      // inverse x-y butterfly: y stage packed, the shared middle row summed
+      // before its x stage
+      const P pp = O::add(hb[0], hb[2]), mm = O::sub(hb[0], hb[2]);
+      const P rr = O::add(hb[1], hb[3]), nn = O::sub(hb[1], hb[3]);
+      const T pm = mm.x + pp.y, rn = nn.x + rr.y;
+      // corner a = 0 of each row goes to the lane on the left
+      const T l0 = pp.x + rr.x, r0v = pp.x - rr.x;
+      const T l1 = pm + rn, r1v = pm - rn;
+      const T l2 = mm.y + nn.y, r2v = mm.y - nn.y;
+      o0[c] = r0v + __shfl_down_sync(0xffffffffu, l0, 1);
+      o1[c] = r1v + __shfl_down_sync(0xffffffffu, l1, 1);
+      o2[c] = r2v + __shfl_down_sync(0xffffffffu, l2, 1);
+    }
+    if(out)
+    {
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+        sB[buf][c][ly][lx] = o0[c];
+      __syncthreads();
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        T v1 = ((f1 >> c) & 1u) ? T(0) : o1[c];
+        T v2 = o2[c] + (ly < TW - 1 ? sB[buf][c][ly + 1][lx] : T(0));
+        if((f2 >> c) & 1u)
+          v2 = T(0);
+        if(DOT)
+          dot += double(us1[c]) * double(v1) + double(us2[c]) * double(v2);
+        T w1 = v1, w2 = v2;
+        if(MODE != OP_APPLY)
+        {
+          const T q1 = b1[c] - v1, q2 = b2[c] - v2;
+          if(MODE == OP_RESIDUAL)
+          {
+            w1 = q1;
+            w2 = q2;
+          }
+          else if(MODE == OP_JACOBI)
+          {
+            w1 = us1[c] + ep.omega * dv1[c] * q1;
+            w2 = us2[c] + ep.omega * dv2[c] * q2;
+          }
+          else
+          {
+            T d1 = ep.c2 * dv1[c] * q1, d2 = ep.c2 * dv2[c] * q2;
+            if(ep.c1 != T(0))
+            {
+              d1 += ep.c1 * (us1[c] - pv1[c]);
+              d2 += ep.c1 * (us2[c] - pv2[c]);
+            }
+            w1 = us1[c] + d1;
+            w2 = us2[c] + d2;
+          }
+        }
+        if(own1)
+          y[c * ld + node1] = w1;
+        if(own2)
+          y[c * ld + node2] = w2;
+      }
+    }
+  }
+  if(DOT)
+  {
+    double v[1] = {dot};
+    block_reduce<1>(v, red, FinStore{dotOut});
+  }
+}
+
 // ------------------------------------------------------------------- Q4 ----
 template <typename T, bool DOT, int MODE>
 __global__ void __launch_bounds__(TX *TY2)
@@ -936,13 +1239,18 @@ int matvec_blocks(const Dims &d)
 {
   if(d.dim == 3)
   {
-    // the largest CTA count h8_zchunk picks for any occupancy of 1..8 CTAs/SM
-    const long long tiles = (long long)((d.sx + TX - 2) / (TX - 1)) * ((d.sy + TY3 - 2) / (TY3 - 1));
+    // the largest CTA count h8_zchunk picks for any occupancy of 1..8 CTAs/SM,
+    // for the one-row tiles (31 x 7 nodes) and the paired ones (31 x 15)
+    const long long bx = (d.sx + TX - 2) / (TX - 1);
     long long most = 0;
-    for(int k = 1; k <= 8; k++)
+    for(int rows : {TY3 - 1, 2 * kPairWarps - 1})
     {
-      const int zc = h8_zchunk(d, tiles, k * num_sms());
-      most = std::max(most, tiles * ((d.sz + zc - 1) / zc));
+      const long long tiles = bx * ((d.sy + rows - 1) / rows);
+      for(int k = 1; k <= 8; k++)
+      {
+        const int zc = h8_zchunk(d, tiles, k * num_sms());
+        most = std::max(most, tiles * ((d.sz + zc - 1) / zc));
+      }
     }
     return int(most);
   }
@@ -955,6 +1263,7 @@ int matvec_blocks(const Dims &d)
 }
 
 static std::atomic<bool> g_hex8_modal{true}; // read by every launching thread
+static std::atomic<bool> g_hex8_pair{true};  // FP32: two element rows per thread
 
 /// Kt = H K0 H / 64 on the 11 blocks of the corner-mode form.  False when an
 /// entry outside the blocks is above rounding (|Kt_rc| > tol max |Kt|, tol
@@ -1054,6 +1363,28 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
                                                          x.dotOut, x.gate, x.gateConv, ep);
     };
     KModal<T> kmod;
+    if constexpr(std::is_same<T, float>::value)
+    {
+      if(g_hex8_pair && g_hex8_modal && modal_form_cached(K, kmod))
+      {
+        // two element rows per thread (k_matvec_h8p): a 31 x 15 node tile
+        constexpr int TW = kPairWarps;
+        const int bxp = (d.sx + TX - 2) / (TX - 1);
+        const int byp = (d.sy + 2 * TW - 2) / (2 * TW - 1);
+        auto kern = x.dotRed ? k_matvec_h8p<T, TW, true, MODE, kPairMinBlocks>
+                             : k_matvec_h8p<T, TW, false, MODE, kPairMinBlocks>;
+        const int zchunk =
+            h8_zchunk(d, (long long)bxp * byp, resident_ctas((const void *)kern, TX * TW, 0));
+        const int bz = (d.sz + zchunk - 1) / zchunk;
+        if(x.dotRed)
+          ICB_REQUIRE((long long)bxp * byp * bz <= red.maxBlocks, "reduction scratch too small");
+        kern<<<dim3(bxp, byp, bz), dim3(TX, TW), 0, s>>>(kmod, d, zchunk, E, u, y, fix, red,
+                                                          x.dotOut, x.gate, x.gateConv, ep);
+        ICB_CUDA(cudaGetLastError());
+        count_launch();
+        return;
+      }
+    }
     if(g_hex8_modal && modal_form_cached(K, kmod))
     {
       // 2 (FP64) / 3 (FP32) CTAs of 256 threads per SM.  The carry (and for
@@ -1116,6 +1447,8 @@ bool tc_operator_enabled() { return g_tc_operator; }
 void set_tc_operator(bool on) { g_tc_operator = on; }
 bool hex8_modal_enabled() { return g_hex8_modal; }
 void set_hex8_modal(bool on) { g_hex8_modal = on; }
+bool hex8_pair_enabled() { return g_hex8_pair; }
+void set_hex8_pair(bool on) { g_hex8_pair = on; }
 
 template <typename T>
 void launch_op(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,
@@ -1123,7 +1456,7 @@ void launch_op(const Dims &d, const T *K, const T *E, const T *u, T *y, const ui
 {
   if constexpr(sizeof(T) == 4)
   {
-    if(d.dim == 3 && g_tc_operator)
+    if(d.dim == 3 && g_tc_operator && !x.cudaCores)
     {
       launch_op_tc(d, K, E, u, y, fix, s, x);
       return;

@@ -24,6 +24,7 @@
 // the FP32 multigrid V-cycle under the FP64 Krylov iteration (ICB_MIXED),
 // never for a residual the outer iteration relies on.
 #include <algorithm>
+#include <atomic>
 
 #include "icb_internal.hpp"
 #include "reduce.cuh"
@@ -37,7 +38,7 @@ namespace
 constexpr int TX = 32, TY = 4, TY1 = TY + 1;
 constexpr int kTiles = TY / 4;                                 // 128-row MMA tiles per layer
 constexpr int kTmemCols = kTiles * 32 > 32 ? kTiles * 32 : 32; // power of 2, >= 32
-constexpr unsigned kSpinLimit = 1u << 22; // try_wait polls before a CTA gives up
+constexpr unsigned kSpinLimit = 1u << 22; // default try_wait polls before a CTA gives up
 
 __device__ __forceinline__ constexpr int lnodeTc(int a, int b) { return (a ^ b) + 2 * b; }
 
@@ -115,10 +116,10 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
     v[i] = __uint_as_float(r[i]);
 }
 
-/// bounded wait on an mbarrier phase; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity)
+/// bounded wait on an mbarrier phase; false when `limit` polls ran out
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, unsigned limit)
 {
-  for(unsigned spin = 0; spin < kSpinLimit; spin++)
+  for(unsigned spin = 0; spin < limit; spin++)
     if(mbar_try_wait(mbar, parity))
       return true;
   return false;
@@ -160,6 +161,7 @@ struct TcSmem
 struct TcWork
 {
   int bx, by, bz, zchunk, items;
+  unsigned spin; ///< polls of an MMA wait before the CTA gives up (icb option tc_spin_limit)
   __device__ __forceinline__ void item(int it, int &X0, int &Y0, int &Z0, int &Z1, const Dims &d) const
   {
     int tx = it % bx, r = it / bx;
@@ -451,7 +453,11 @@ __global__ void __launch_bounds__(TX *TY, kBlocksPerSm)
       bool ok = true;
       if(tid == 0)
       {
-        ok = mbar_wait_bounded(mbarA, parity);
+        ok = mbar_wait_bounded(mbarA, parity, W.spin);
+        // a CTA that gives up still lets the MMAs it issued finish (again
+        // bounded) before it releases the tensor memory they write
+        if(!ok)
+          mbar_wait_bounded(mbarA, parity, kSpinLimit);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       }
       parity ^= 1u;
@@ -561,6 +567,7 @@ void launch_tc_mode(const Dims &d, const float *K, const float *E, const float *
   w.zchunk = std::max(4, (d.sz + wantBz - 1) / wantBz);
   w.bz = (d.sz + w.zchunk - 1) / w.zchunk;
   w.items = w.bx * w.by * w.bz;
+  w.spin = tc_spin_limit();
   const int grid = std::min(w.items, slots);
   RedScratch red = x.dotRed ? *x.dotRed : RedScratch{};
   Epi<float> ep{x.b, x.dinv, float(x.omega), float(x.c1), float(x.c2)};
@@ -586,6 +593,10 @@ void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u,
   else
     launch_tc_mode<OP_CHEB>(d, K, E, u, y, fix, s, x);
 }
+
+static std::atomic<unsigned> g_tc_spin{kSpinLimit};
+unsigned tc_spin_limit() { return g_tc_spin.load(); }
+void set_tc_spin_limit(unsigned polls) { g_tc_spin = polls; }
 
 unsigned tc_timeouts()
 {

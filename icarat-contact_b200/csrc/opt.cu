@@ -685,14 +685,14 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
   Pp.useFilter = cone != nullptr;
   // graph of the bisection: one step as the body of a conditional WHILE node
   // that the device repeats until done (at most maxiter = 100 steps), rebuilt
-  // when the operands or parameters change
-  const void *k[9] = {cone, x, df, dg, xmin, xmax, vol, (const void *)s, nullptr};
+  // when anything it bakes in changes -- the stencil's device buffers and
+  // size included, never the filter object's host address (a filter rebuilt
+  // for another radius can reuse it while its old buffers are freed)
   const bool dev = device_loops_enabled();
-  bool same = loop.exec != nullptr && loop.device == dev &&
-              std::memcmp(&Pp, &keyP, sizeof(OcParams)) == 0;
-  for(int i = 0; i < 9 && same; i++)
-    same = k[i] == key[i];
-  if(!same)
+  GraphKey k;
+  k.add(off).add(w).add(aa).add((long long)nnb).add(x).add(df).add(dg).add(xmin).add(xmax);
+  k.add(vol).add((const void *)s).addBytes(Pp).add((long long)kernel_switches());
+  if(loop.exec == nullptr || loop.device != dev || k != key)
   {
     // host form: all of ICARAT's 100 steps in one launch, gated after done
     loop.build(
@@ -701,9 +701,7 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
                                        st.p, L);
         },
         dev, 100);
-    for(int i = 0; i < 9; i++)
-      key[i] = k[i];
-    keyP = Pp;
+    key = k;
   }
   loop.launch(s);
   k_oc_final<<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d.nel, x, df, dg, xmin, xmax, Pp, st.p);
@@ -762,12 +760,11 @@ int MmaUpdater::solveDual(double *x, cudaStream_t s)
   const int nb = vblocks(n);
   k_mma_dip_init<<<1, 1, 0, s>>>(st.p, P);
   count_launch();
-  const void *k[3] = {x, (const void *)s, nullptr};
-  bool same = exec != nullptr;
-  for(int i = 0; i < 3 && same; i++)
-    same = k[i] == key[i];
+  // the batch graph bakes in x, the stream and the parameters by value
+  GraphKey k;
+  k.add(x).add((const void *)s).addBytes(P);
   const int batch = 32;
-  if(!same)
+  if(exec == nullptr || k != key)
   {
     if(exec)
       cudaGraphExecDestroy(exec);
@@ -782,8 +779,7 @@ int MmaUpdater::solveDual(double *x, cudaStream_t s)
     ICB_CUDA(cudaGraphInstantiate(&exec, gr, 0));
     cudaGraphDestroy(gr);
     cudaStreamDestroy(cs);
-    for(int i = 0; i < 3; i++)
-      key[i] = k[i];
+    key = k;
   }
   // SolveDIP needs at most 100 x 100 Newton steps; each pass is one step
   for(int launches = 0; launches < 10000 / batch + 1; launches++)

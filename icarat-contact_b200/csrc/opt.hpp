@@ -55,8 +55,7 @@ struct OcUpdater
   RedScratch red;
   OcState *hst = nullptr;
   WhileGraph loop; ///< one bisection step, repeated on the device until done
-  const void *key[9] = {};
-  OcParams keyP;
+  GraphKey key;     ///< what `loop` bakes in
 
   OcUpdater(const Dims &dims, cudaStream_t s);
   ~OcUpdater();
@@ -98,7 +97,7 @@ struct MmaUpdater
   RedScratch red;
   MmaState *hst = nullptr;
   cudaGraphExec_t exec = nullptr;
-  const void *key[3] = {};
+  GraphKey key; ///< what `exec` bakes in
 
   MmaUpdater(long long nvar, cudaStream_t s);
   ~MmaUpdater();

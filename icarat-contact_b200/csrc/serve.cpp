@@ -51,6 +51,7 @@ struct Job
   icb_loop_opts loop{};
   std::vector<unsigned char> fixed, nondesign, volumeSet;
   std::vector<double> load, rho0, hist, x, iters;
+  std::vector<char> resumeBlob; ///< the checkpoint a resumed job starts from
   long long bytes = 0;
   int state = ICB_JOB_QUEUED;
   int status = ICB_OK;
@@ -133,7 +134,8 @@ struct icb_server_s
       {
         icb_loop_opts o = j->loop;
         o.iter_seconds = j->iters.data();
-        st = runOne(p, j->kind, o, j->rho0.data(), j->hist.data(), j->x.data());
+        st = runOne(p, j->kind, o, j->rho0.empty() ? nullptr : j->rho0.data(), j->hist.data(),
+                    j->x.data());
       }
       std::string err = st == ICB_OK ? "" : ctxStatus != ICB_OK ? ctxError : icb_last_error();
       icb_problem_destroy(p);
@@ -221,7 +223,8 @@ int icb_server_create(int device, long long budget_bytes, int slots, icb_server 
 int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
 {
   ICB_API_BEGIN
-  if(!s || !jd || !jd->fixed || !jd->load || !jd->rho0 || jd->loop.nsteps <= 0)
+  if(!s || !jd || !jd->fixed || !jd->load || !(jd->rho0 || jd->loop.resume) ||
+     jd->loop.nsteps <= 0)
     throw Error{ICB_ERR_BAD_ARG, "bad job"};
   if(jd->kind != ICB_JOB_OC && jd->kind != ICB_JOB_MMA)
     throw Error{ICB_ERR_BAD_ARG, "job kind must be ICB_JOB_OC or ICB_JOB_MMA"};
@@ -234,11 +237,13 @@ int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
   j->loop = jd->loop;
   j->loop.iter_seconds = nullptr;
   j->loop.steps_done = nullptr; // the caller's memory is not written later
+  j->loop.checkpoint = nullptr;
   Dims d = make_dims(g.dim, g.nx, g.ny, g.dim == 3 ? g.nz : 1);
   long long neq = d.nnode * g.dim;
   j->fixed.assign(jd->fixed, jd->fixed + neq);
   j->load.assign(jd->load, jd->load + neq);
-  j->rho0.assign(jd->rho0, jd->rho0 + d.nel);
+  if(jd->rho0)
+    j->rho0.assign(jd->rho0, jd->rho0 + d.nel);
   // the element masks are copied like the other arrays; on_step (if set) is
   // called on the worker thread that runs the job
   if(jd->loop.nondesign)
@@ -250,6 +255,13 @@ int icb_server_submit(icb_server s, const icb_job_desc *jd, long long *id)
   {
     j->volumeSet.assign(jd->loop.volume_set, jd->loop.volume_set + d.nel);
     j->loop.volume_set = j->volumeSet.data();
+  }
+  if(jd->loop.resume)
+  {
+    // a resumed job: the checkpoint of an earlier run of this grid and kind
+    const char *b = static_cast<const char *>(jd->loop.resume);
+    j->resumeBlob.assign(b, b + loop_checkpoint_bytes(d.nel, jd->kind));
+    j->loop.resume = j->resumeBlob.data();
   }
   j->hist.assign(jd->loop.nsteps, 0.0);
   j->iters.assign(jd->loop.nsteps, 0.0);

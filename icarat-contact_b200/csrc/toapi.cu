@@ -173,6 +173,40 @@ struct StopRule
   }
 };
 
+/// the state a loop carries from step to step, as written into a checkpoint:
+/// this header, the design x[nel], then for MMA low, upp, xold1, xold2 [nel]
+struct LoopCkpt
+{
+  unsigned long long magic;
+  int kind, step;
+  long long nel;
+  double V0, fold;
+  int mmaIter, pad;
+};
+constexpr unsigned long long kCkptMagic = 0x69636231636b7074ull; // "icb1ckpt"
+long long ckptBytes(long long nel, int kind) { return icb::loop_checkpoint_bytes(nel, kind); }
+/// the header of a resume blob, checked against this run
+const LoopCkpt &ckptRead(const void *blob, int kind, long long nel, int nsteps)
+{
+  const LoopCkpt &h = *static_cast<const LoopCkpt *>(blob);
+  need(h.magic == kCkptMagic && h.kind == kind && h.nel == nel,
+       "resume blob does not belong to this loop kind and grid");
+  need(h.step >= 1 && h.step < nsteps, "resume step outside 1 .. nsteps - 1");
+  return h;
+}
+/// copy n doubles of the blob's payload (after the header) at offset k * nel
+void ckptToDev(const void *blob, long long k, long long nel, double *dst, cudaStream_t s)
+{
+  const double *src =
+      reinterpret_cast<const double *>(static_cast<const char *>(blob) + sizeof(LoopCkpt)) + k * nel;
+  ICB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * nel, cudaMemcpyHostToDevice, s));
+}
+void ckptFromDev(void *blob, long long k, long long nel, const double *src, cudaStream_t s)
+{
+  double *dst = reinterpret_cast<double *>(static_cast<char *>(blob) + sizeof(LoopCkpt)) + k * nel;
+  ICB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * nel, cudaMemcpyDeviceToHost, s));
+}
+
 void toDev(DevBuf<double> &b, const double *h, long long n, cudaStream_t s)
 {
   if((long long)b.n < n)
@@ -183,6 +217,10 @@ void toDev(DevBuf<double> &b, const double *h, long long n, cudaStream_t s)
 
 namespace icb
 {
+long long loop_checkpoint_bytes(long long nel, int kind)
+{
+  return (long long)sizeof(LoopCkpt) + (long long)sizeof(double) * nel * (kind == ICB_JOB_MMA ? 5 : 1);
+}
 /// the problem's loop work space, created on first use
 static LoopCache &loop_cache(icb_problem p)
 {
@@ -470,7 +508,7 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
 {
   ICB_API_BEGIN
   needFinal(p);
-  need(o && rho0 && hist, "NULL argument");
+  need(o && (rho0 || o->resume) && hist, "NULL argument");
   need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
   ICB_CUDA(cudaSetDevice(p->ctx->device));
   cudaStream_t s = p->stream();
@@ -482,18 +520,29 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
   DevBuf<double> &x = LC.buf(0, n), &xf = LC.buf(1, n), &xh = LC.buf(2, n), &dxh = LC.buf(3, n),
                  &dc = LC.buf(4, n), &dv = LC.buf(5, n), &dcf = LC.buf(6, n), &dvf = LC.buf(7, n),
                  &lo = LC.buf(8, n), &hi = LC.buf(9, n), &V = LC.buf(10, n);
-  ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  double V0 = 0.0;
+  StopRule stop;
+  int first = 1;
+  if(o->resume)
+  {
+    const LoopCkpt &h = ckptRead(o->resume, ICB_JOB_OC, n, o->nsteps);
+    ckptToDev(o->resume, 0, n, x.p, s);
+    V0 = h.V0;
+    stop.fold = h.fold;
+    first = h.step + 1;
+  }
+  else
+    ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, vol, V.p);
   count_launch(3);
   icb_solve_opts so = o->solve;
-  double V0 = 0.0;
   StepReport report;
   OcParams P;
   P.move = o->move_limit;
-  StopRule stop;
-  for(int step = 1; step <= o->nsteps; step++)
+  int done = first - 1;
+  for(int step = first; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
     NvtxRange stepRange("oc step");
@@ -530,11 +579,18 @@ int icb_run_oc(icb_problem p, const icb_loop_opts *o, const double *rho0, double
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    done = step;
     if(last)
       break;
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  if(o->checkpoint)
+  {
+    LoopCkpt h{kCkptMagic, ICB_JOB_OC, done, n, V0, stop.fold, 0, 0};
+    std::memcpy(o->checkpoint, &h, sizeof h);
+    ckptFromDev(o->checkpoint, 0, n, x.p, s);
+  }
   ICB_CUDA(cudaStreamSynchronize(s));
   ICB_API_END
 }
@@ -547,7 +603,7 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
 {
   ICB_API_BEGIN
   needFinal(p);
-  need(o && rho0 && hist, "NULL argument");
+  need(o && (rho0 || o->resume) && hist, "NULL argument");
   need(o->nsteps > 0 && o->filter_radius > 0.0, "bad loop options");
   need(o->filter_type == ICB_FILTER_HELMHOLTZ || o->filter_type == ICB_FILTER_CONE,
        "unknown filter_type");
@@ -572,12 +628,28 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     ICB_CUDA(cudaMemcpyAsync(nd.p, o->nondesign, n, cudaMemcpyHostToDevice, s));
   if(o->volume_set)
     ICB_CUDA(cudaMemcpyAsync(vs.p, o->volume_set, n, cudaMemcpyHostToDevice, s));
-  ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  double V0 = o->volume_ref;
+  StopRule stop;
+  int first = 1;
+  if(o->resume)
+  {
+    const LoopCkpt &h = ckptRead(o->resume, ICB_JOB_MMA, n, o->nsteps);
+    ckptToDev(o->resume, 0, n, x.p, s);
+    ckptToDev(o->resume, 1, n, mma.low.p, s);
+    ckptToDev(o->resume, 2, n, mma.upp.p, s);
+    ckptToDev(o->resume, 3, n, mma.xold1.p, s);
+    ckptToDev(o->resume, 4, n, mma.xold2.p, s);
+    mma.iter = h.mmaIter;
+    V0 = h.V0;
+    stop.fold = h.fold;
+    first = h.step + 1;
+  }
+  else
+    ICB_CUDA(cudaMemcpyAsync(x.p, rho0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0e-4, lo.p);
   k_fill_d<<<nb256(n), 256, 0, s>>>(n, 1.0, hi.p);
   count_launch(2);
   icb_solve_opts so = o->solve;
-  double V0 = o->volume_ref;
   StepReport report;
   auto filt = [&](const double *in, double *out, bool sens) {
     NvtxRange r(sens ? "filter (sensitivities)" : "filter");
@@ -594,8 +666,8 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     if(rc)
       throw Error{rc, "Helmholtz filter solve did not converge"};
   };
-  StopRule stop;
-  for(int step = 1; step <= o->nsteps; step++)
+  int done = first - 1;
+  for(int step = first; step <= o->nsteps; step++)
   {
     auto t0 = std::chrono::steady_clock::now();
     NvtxRange stepRange("mma step");
@@ -642,13 +714,31 @@ int icb_run_mma(icb_problem p, const icb_loop_opts *o, const double *rho0, doubl
     if(o->iter_seconds)
       o->iter_seconds[step - 1] =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    done = step;
     if(last)
       break;
   }
   if(xout)
     ICB_CUDA(cudaMemcpyAsync(xout, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  if(o->checkpoint)
+  {
+    LoopCkpt h{kCkptMagic, ICB_JOB_MMA, done, n, V0, stop.fold, mma.iter, 0};
+    std::memcpy(o->checkpoint, &h, sizeof h);
+    ckptFromDev(o->checkpoint, 0, n, x.p, s);
+    ckptFromDev(o->checkpoint, 1, n, mma.low.p, s);
+    ckptFromDev(o->checkpoint, 2, n, mma.upp.p, s);
+    ckptFromDev(o->checkpoint, 3, n, mma.xold1.p, s);
+    ckptFromDev(o->checkpoint, 4, n, mma.xold2.p, s);
+  }
   ICB_CUDA(cudaStreamSynchronize(s));
   ICB_API_END
+}
+
+long long icb_loop_checkpoint_bytes(icb_problem p, int kind)
+{
+  if(!p || !p->hs || (kind != ICB_JOB_OC && kind != ICB_JOB_MMA))
+    return -1;
+  return ckptBytes(p->d.nel, kind);
 }
 
 /// The opt_macro_gcmma loop (opt_macro_gcmma.cpp:83-238) on the device:

@@ -15,7 +15,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(_HERE))  # icarat-contact_b200/
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libicarat_b200.so")
 HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "icarat_b200.h")
 
-FP64, MIXED, TF32 = 0, 1, 2
+FP64, MIXED, TF32, MIXED_REFINE = 0, 1, 2, 3
 JACOBI, GMG = 0, 1
 PLANE_STRESS, PLANE_STRAIN, THREE_D = 0, 1, 2
 JOB_OC, JOB_MMA = 0, 1
@@ -59,7 +59,8 @@ class LoopOpts(C.Structure):
                 ("use_threshold", C.c_int), ("volume_ref", C.c_double), ("solve", SolveOpts),
                 ("iter_seconds", _dp), ("filter_type", C.c_int), ("nondesign", _u8p),
                 ("volume_set", _u8p), ("on_step", STEP_CB), ("step_user", C.c_void_p),
-                ("conv_eps", C.c_double), ("conv_min_steps", C.c_int), ("steps_done", _ip)]
+                ("conv_eps", C.c_double), ("conv_min_steps", C.c_int), ("steps_done", _ip),
+                ("resume", C.c_void_p), ("checkpoint", C.c_void_p)]
 
 
 class JobDesc(C.Structure):
@@ -139,6 +140,7 @@ _SIGS = {
     "icb_solve_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                     C.POINTER(SolveInfo)]),
     "icb_noalloc_max_soa": (C.c_longlong, []),
+    "icb_loop_checkpoint_bytes": (C.c_longlong, [C.c_void_p, C.c_int]),
     "icb_set_option": (C.c_int, [C.c_char_p, C.c_longlong]),
     "icb_run_batch": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), _ip, C.POINTER(LoopOpts),
                                 C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.c_int, _ip]),
@@ -600,13 +602,22 @@ class MMA:
 
 def run_loop(prob, kind, rho0, nsteps, radius, move=0.15, use_threshold=True, volume_ref=0.0,
              precision=FP64, precond=GMG, tol=1e-8, maxit=20000, filter_type=0, nondesign=None,
-             volume_set=None, on_step=None, conv_eps=0.0, conv_min_steps=0, steps_done=None):
+             volume_set=None, on_step=None, conv_eps=0.0, conv_min_steps=0, steps_done=None,
+             resume=None, checkpoint=None):
     """icb_run_oc (kind "oc") or icb_run_mma (kind "mma"): compliance history, design.
     on_step(step, compliance, rho_phys, nodeval, mises) receives numpy copies;
     conv_eps > 0 applies the apps' isConvergence(conv_eps, conv_min_steps)
-    stop rule, steps_done (a one-element int32 array) receives the steps run."""
+    stop rule, steps_done (a one-element int32 array) receives the steps run;
+    resume (bytes-like) continues a run from its checkpoint, checkpoint (a
+    writable uint8 array of checkpoint_bytes(prob, kind)) receives one."""
     o = LoopOpts(nsteps, radius, move, int(use_threshold), volume_ref,
                  SolveOpts(precision, precond, tol, maxit, 0.0, 0, 0), None)
+    if resume is not None:
+        rbuf = np.frombuffer(bytes(resume), np.uint8).copy()
+        o.resume = rbuf.ctypes.data
+    if checkpoint is not None:
+        assert checkpoint.dtype == np.uint8 and checkpoint.size >= checkpoint_bytes(prob, kind)
+        o.checkpoint = checkpoint.ctypes.data
     o.filter_type = filter_type
     o.conv_eps = conv_eps
     o.conv_min_steps = conv_min_steps
@@ -629,10 +640,15 @@ def run_loop(prob, kind, rho0, nsteps, radius, move=0.15, use_threshold=True, vo
         keep.append(o.on_step)
     hist = np.zeros(nsteps)
     x = np.zeros(prob.nel)
-    rho0 = np.ascontiguousarray(rho0, np.float64)
+    rho0 = None if rho0 is None else np.ascontiguousarray(rho0, np.float64)
     f = lib().icb_run_oc if kind == "oc" else lib().icb_run_mma
-    check(f(prob.h, C.byref(o), _p(rho0), _p(hist), _p(x)))
+    check(f(prob.h, C.byref(o), None if rho0 is None else _p(rho0), _p(hist), _p(x)))
     return hist, x
+
+
+def checkpoint_bytes(prob, kind):
+    """icb_loop_checkpoint_bytes for kind "oc" or "mma"."""
+    return lib().icb_loop_checkpoint_bytes(prob.h, 0 if kind == "oc" else 1)
 
 
 # ------------------------------------------------------------ batch/serve --

@@ -42,6 +42,9 @@ extern "C" {
 #define ICB_FP64 0  /* plain FP64 path: the drop-in for Solvers "Eigen_CG"   */
 #define ICB_MIXED 1 /* FP64 Krylov + operator, FP32 multigrid preconditioner */
 #define ICB_TF32 2  /* icb_operator_apply_device only: tensor-core FP32 operator */
+/* FP64 defect correction around an FP32 GMG-PCG: FP32 Krylov vectors, operator
+ * and V-cycle; FP64 residual, iterate and reductions */
+#define ICB_MIXED_REFINE 3
 
 #define ICB_PRECOND_JACOBI 0 /* DiagonalPreconditioner (solvers.cpp:64-92)  */
 #define ICB_PRECOND_GMG 1    /* geometric multigrid V-cycle                 */
@@ -74,7 +77,7 @@ typedef struct
   int precond;    /* ICB_PRECOND_JACOBI | ICB_PRECOND_GMG                   */
   double tol;     /* relative residual ||r||/||f|| (Solvers tol_, 1e-10)    */
   int maxit;      /* Solvers maxIter_ (10000)                               */
-  double inner_tol; /* reserved (0)                                       */
+  double inner_tol; /* ICB_MIXED_REFINE: relative tolerance of each FP32 inner solve (0 = 1e-4) */
   int mg_smooth;  /* GMG: Chebyshev smoothing steps before and after (0 = 2) */
   int mg_coarse_dofs; /* GMG: coarsen while the grid has more DOFs (0 = 160, at most 1024) */
 } icb_solve_opts;
@@ -83,7 +86,7 @@ typedef struct
 {
   int iters;          /* Krylov iterations (Eigen's count: the converging one excluded) */
   int matvecs;        /* fine-level operator applications in the Krylov loop(s) */
-  int outer;          /* Krylov cycles (1)                                  */
+  int outer;          /* Krylov cycles (1; ICB_MIXED_REFINE: refinement steps) */
   double relres;      /* ||r||/||f|| as the solver tracked it               */
   double true_relres; /* ||f - K u|| / ||f|| recomputed in FP64             */
   double seconds;     /* device time of the solve                           */
@@ -268,7 +271,24 @@ typedef struct
   double conv_eps;
   int conv_min_steps;
   int *steps_done;
+  /* checkpoint and resume (icb_run_oc, icb_run_mma; no counterpart in ICARAT,
+   * whose apps only write res<step>.vtk): a run given `checkpoint` (may be
+   * NULL) writes there, after its last step, the state the loop carries from
+   * step to step -- the design, V0, the stop rule's last objective and for MMA
+   * the iteration count, asymptotes and the two previous designs, in
+   * icb_loop_checkpoint_bytes(p, kind) bytes.  A run given `resume` (may be
+   * NULL) takes that state and continues with the step after the recorded
+   * one (rho0 is then ignored; nsteps is still the number of the last step),
+   * so a run stopped and resumed, on this problem or another of the same
+   * grid, repeats the uninterrupted run bitwise.  hist[step - 1] is written
+   * for the steps this call runs.  The job server copies `resume` with the
+   * job and ignores `checkpoint`. */
+  const void *resume;
+  void *checkpoint;
 } icb_loop_opts;
+/* bytes of a checkpoint of icb_run_oc (kind ICB_JOB_OC) or icb_run_mma
+ * (ICB_JOB_MMA) on this problem; < 0 on a bad argument */
+long long icb_loop_checkpoint_bytes(icb_problem p, int kind);
 /* opt-macro-oc/opt_macro_oc.cpp:84-172: cone filter, threshold, solve,
  * compliance, V0 at step 1, sensitivities, adjoint filter, OC; hist[nsteps]
  * receives the compliance of every step, xout (nel, may be NULL) the design. */
@@ -419,15 +439,19 @@ long long icb_get_option(const char *name);
  * that must not stall on the allocator or hit out-of-memory mid-request.
  * The same FP64 Jacobi-PCG as icb_solve with ICB_FP64 / ICB_PRECOND_JACOBI
  * (Eigen_CG semantics), on caller-provided device SoA vectors: b_dev holds
- * the right-hand side (0 on constrained DOFs), x_dev receives the solution;
- * both have icb_soa_length(p) doubles.  Scratch comes from a 32 MiB static
+ * the right-hand side, x_dev receives the solution; both have
+ * icb_soa_length(p) doubles.  b_dev is read on the unknowns only: its
+ * constrained slots and the SoA padding past each component's last node are
+ * ignored, whatever they hold.  Both must be ready on the context's stream
+ * (icb_ctx_stream) when the call is made.  Scratch comes from a 32 MiB static
  * device array that every GPU loading this library holds until exit; problems
  * with icb_soa_length(p) > icb_noalloc_max_soa() are rejected with
- * ICB_ERR_BAD_ARG.  The call itself allocates nothing.  Its first call on a
- * device looks up that array's device address, so make that first call
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race, so serialise them.  info->true_relres is -1 (not
- * recomputed). */
+ * ICB_ERR_BAD_ARG.  The call allocates nothing: icb_ctx_create looks up the
+ * array's device address on its device, which is also when CUDA loads the
+ * module holding it and maps its memory, so create the context before the
+ * host's pool takes the rest of the GPU.  All calls share the array: calls
+ * that overlap on the GPU race, so serialise them.  info->true_relres is -1
+ * (not recomputed). */
 int icb_solve_noalloc(icb_problem p, const double *b_dev, double *x_dev, double tol, int maxit,
                       icb_solve_info *info);
 /* largest icb_soa_length() icb_solve_noalloc accepts */

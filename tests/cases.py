@@ -82,6 +82,29 @@ def masks(kind, nx, ny, nz=1):
     raise ValueError(kind)
 
 
+def smooth_field(nx, ny, nz, seed, lo=0.001, hi=1.0, modes=16):
+    """Seeded smooth random density: affine map to [lo, hi] of
+    sum_k a_k cos(2 pi (k . x_c / L) + phi_k), k integer triples in [0,4]^3,
+    a_k ~ N(0,1), phi_k ~ U[0, 2 pi), at element centres."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+    f = np.zeros((nz, ny, nx))
+    for _ in range(modes):
+        k = rng.integers(0, 5, 3)
+        a, ph = rng.standard_normal(), rng.uniform(0, 2 * np.pi)
+        # separable evaluation of cos(2 pi (kx x + ky y + kz z) + ph)
+        cx, sx = np.cos(2 * np.pi * k[0] * x), np.sin(2 * np.pi * k[0] * x)
+        cy, sy = np.cos(2 * np.pi * k[1] * y), np.sin(2 * np.pi * k[1] * y)
+        cz, sz = np.cos(2 * np.pi * k[2] * z + ph), np.sin(2 * np.pi * k[2] * z + ph)
+        cxy = np.outer(cy, cx) - np.outer(sy, sx)
+        sxy = np.outer(sy, cx) + np.outer(cy, sx)
+        f += a * (cz[:, None, None] * cxy[None] - sz[:, None, None] * sxy[None])
+    f = (f - f.min()) / max(f.max() - f.min(), 1e-300)
+    return (lo + (hi - lo) * f).reshape(-1)
+
+
 def uniform_density(nel, seed, lo=0.01, hi=1.0):
     return np.random.default_rng(seed).uniform(lo, hi, nel)
 

@@ -111,6 +111,38 @@ def test_mma_helmholtz_loop_history(ctx):
     assert np.abs(xg - xo).max() <= 1e-3
 
 
+def test_oc_update_across_filter_rebuilds_matches_oracle(ctx):
+    """OC updates through the C ABI with a cone filter of radius 2, then one of
+    radius 3, then a new one of radius 2 (each created after the previous one
+    was destroyed, so the allocators may hand out the same addresses): every
+    update matches the oracle's OC with the same filtered and thresholded
+    volume callback (OCSolver.hpp:20-68, opt_macro_oc.cpp:153-164)."""
+    nx, ny = 30, 12
+    o = po.Problem(2, nx, ny)
+    g = icb.Problem(ctx, 2, nx, ny)
+    g.finalize()
+    n = o.nel
+    rng = np.random.default_rng(7)
+    x0 = rng.uniform(0.2, 0.8, n)
+    df = -rng.uniform(0.1, 2.0, n)
+    dg = np.ones(n)
+    lo, hi = np.full(n, 1e-4), np.ones(n)
+    beta, target = 2.0, 0.45 * n
+    outs = []
+    for r in (2.0, 3.0, 2.0):
+        cone = icb.Cone(g, r)
+        xg, steps = icb.oc_update(g, cone, x0, df, target, dg, lo, hi, 0.2, beta=beta)
+        cone.close()
+        oc = po.Cone(o, r)
+        xo = po.oc_update(x0, df, target, dg, lo, hi, 0.2,
+                          lambda xk: float(po.threshold(oc.apply(xk), beta).sum()))
+        assert np.abs(xg - xo).max() <= 1e-4, r
+        assert 10 <= steps <= 100
+        outs.append(xg)
+    assert np.array_equal(outs[0], outs[2])
+    assert not np.array_equal(outs[0], outs[1])
+
+
 def test_repeated_loops_on_one_problem_agree(ctx):
     """The app loops keep their filters, updaters and work vectors with the
     problem: a second run (and one with another filter radius in between)
@@ -126,6 +158,25 @@ def test_repeated_loops_on_one_problem_agree(ctx):
     b = icb.run_gcmma(g, rho0, 4, 1.5)
     for u, v in zip(a, b):
         assert np.array_equal(u, v)
+
+
+@pytest.mark.parametrize("kind", ["oc", "mma"])
+def test_loop_checkpoint_resume_repeats_the_run(ctx, kind):
+    """A loop stopped after step 4 with a checkpoint and resumed on another
+    problem of the same grid repeats the uninterrupted 8-step run bitwise:
+    the design, V0, the stop rule's state and (MMA) the iteration count,
+    asymptotes and previous designs are everything carried between steps."""
+    g = cases.build_gpu(ctx, "halfmbb2d", 40, 16)
+    rho0 = np.full(g.nel, 0.4)
+    full_h, full_x = icb.run_loop(g, kind, rho0, 8, 2.0, tol=1e-10)
+    ck = np.zeros(icb.checkpoint_bytes(g, kind), np.uint8)
+    h1, _ = icb.run_loop(g, kind, rho0, 4, 2.0, tol=1e-10, checkpoint=ck)
+    g2 = cases.build_gpu(ctx, "halfmbb2d", 40, 16)
+    h2, x2 = icb.run_loop(g2, kind, None, 8, 2.0, tol=1e-10, resume=ck)
+    assert np.array_equal(h1, full_h[:4])
+    assert np.array_equal(h2[4:], full_h[4:]) and not h2[:4].any()
+    assert np.array_equal(x2, full_x)
+    g2.close()
 
 
 @pytest.mark.parametrize("kind", ["oc", "mma"])

@@ -145,7 +145,7 @@ def test_zero_load_and_fully_constrained_with_every_solver(ctx, dim, n):
     for g in (free, fixed):
         g.set_density(np.full(g.nel, 0.5))
         for precision, precond in ((icb.FP64, icb.JACOBI), (icb.FP64, icb.GMG),
-                                   (icb.MIXED, icb.GMG)):
+                                   (icb.MIXED, icb.GMG), (icb.MIXED_REFINE, icb.GMG)):
             info = g.solve(precision=precision, precond=precond)
             assert info["iters"] == 0, (precision, precond, info)
             assert g.compliance() == 0.0
@@ -181,13 +181,14 @@ def test_full_size_cantilever3d_properties(ctx):
 
 
 # ----------------------------------------------------------- multigrid ----
-@pytest.mark.parametrize("precision", [icb.FP64, icb.MIXED])
+@pytest.mark.parametrize("precision", [icb.FP64, icb.MIXED, icb.MIXED_REFINE])
 @pytest.mark.parametrize("kind,n,seed", [("cantilever2d", (120, 40), 1), ("cantilever2d", (37, 23), 2),
                                          ("halfmbb2d", (61, 20), 6),
                                          ("cantilever3d", (24, 8, 8), 3), ("cantilever3d", (19, 7, 9), 5),
                                          ("halfmbb3d", (16, 8, 8), 4)])
 def test_gmg_solve_parity(ctx, precision, kind, n, seed):
-    """GMG-preconditioned CG, FP64 or with an FP32 V-cycle, reaches the FP64
+    """GMG-preconditioned CG -- FP64, FP64 Krylov with an FP32 V-cycle, or FP64
+    defect correction around an all-FP32 GMG-PCG -- reaches the FP64
     tolerance and matches the oracle; odd element counts exercise the
     ceil-coarsening."""
     o = cases.build_oracle(kind, *n)
@@ -226,10 +227,11 @@ def test_mixed_full_size_cantilever3d(ctx):
     g.set_density(rho)
     i64 = g.solve(precision=icb.FP64, precond=icb.GMG, tol=1e-8, maxit=20000)
     c64, dc64 = g.compliance(), g.sensitivity()
-    imx = g.solve(precision=icb.MIXED, precond=icb.GMG, tol=1e-8, maxit=20000)
-    assert imx["true_relres"] <= 2e-8 and i64["true_relres"] <= 2e-8
-    assert abs(g.compliance() - c64) <= COMPLIANCE_RTOL * c64
-    assert np.abs(g.sensitivity() - dc64).max() <= SENS_RTOL * np.abs(dc64).max()
+    for prec in (icb.MIXED, icb.MIXED_REFINE):
+        imx = g.solve(precision=prec, precond=icb.GMG, tol=1e-8, maxit=20000)
+        assert imx["true_relres"] <= 2e-8 and i64["true_relres"] <= 2e-8
+        assert abs(g.compliance() - c64) <= COMPLIANCE_RTOL * c64
+        assert np.abs(g.sensitivity() - dc64).max() <= SENS_RTOL * np.abs(dc64).max()
 
 
 @pytest.mark.parametrize("kind,n", [("cantilever2d", (61, 20)), ("halfmbb3d", (16, 8, 8))])
@@ -327,7 +329,7 @@ def test_thin_and_high_aspect_grids(ctx, kind, n):
     ro = o.solve(rho, tol=1e-12)
     assert ro["relres"] <= 1e-12
     dco = o.sensitivity(rho, ro["nodeval"])
-    for precision in (icb.FP64, icb.MIXED):
+    for precision in (icb.FP64, icb.MIXED, icb.MIXED_REFINE):
         info = g.solve(precision=precision, precond=icb.GMG, tol=1e-8, maxit=20000)
         assert info["true_relres"] <= 2e-8, info
         assert abs(g.compliance() - ro["compliance"]) <= COMPLIANCE_RTOL * abs(ro["compliance"])

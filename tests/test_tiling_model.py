@@ -2,7 +2,9 @@
 
 k_matvec_h8 / k_matvec_h8m (Hex8) and k_matvec_q4 (Q4) give each thread one
 element column (plus a one-element halo on the low side of its tile) and let
-the thread whose column ends at a node write that node; k_helm_apply3 (the
+the thread whose column ends at a node write that node; k_matvec_h8p (the FP32
+Hex8 default) gives each thread two element rows of a column and writes the
+node row between them and the one above; k_helm_apply3 (the
 3D Helmholtz operator) gives each thread one node column and stages each plane
 with a one-node halo in shared memory.  No atomics: the result is only right
 if every node of the grid is written by exactly one thread-layer.  The
@@ -41,6 +43,51 @@ def _h8_owners(nx, ny, nz, zchunk):
                     if ek >= z0:  # the layer's bottom plane is complete: output it
                         cnt[ek, jj, ii] += 1
     return cnt
+
+
+TW = 8  # operator.cu kPairWarps: warps of the paired-row FP32 Hex8 kernel
+
+
+def _h8p_owners(nx, ny, nz, zchunk):
+    """k_matvec_h8p: two element rows per thread, a 31 x (2 TW - 1) node tile;
+    count of writes per node (sz, sy, sx), and a check that every node a
+    thread loads (unguarded by its validity flags) and every shared-memory
+    exchange slot it reads are inside their ranges"""
+    sx, sy, sz = nx + 1, ny + 1, nz + 1
+    bx, by = (sx + TX - 2) // (TX - 1), (sy + 2 * TW - 2) // (2 * TW - 1)
+    bz = (sz + zchunk - 1) // zchunk
+    cnt = np.zeros((sz, sy, sx), np.int32)
+    lx = np.arange(TX)[None, :]
+    ly = np.arange(TW)[:, None]
+    for byi in range(by):
+        for bxi in range(bx):
+            X0, Y0 = bxi * (TX - 1), byi * (2 * TW - 1)
+            ei = np.broadcast_to(X0 - 1 + lx, (TW, TX))
+            ej = np.broadcast_to(Y0 - 1 + 2 * ly, (TW, TX))
+            lyb = np.broadcast_to(ly, (TW, TX))
+            ni = ei + 1
+            ocol = (np.broadcast_to(lx, (TW, TX)) < TX - 1) & (ni < sx)
+            own1 = ocol & (ej + 1 >= 0) & (ej + 1 < sy)
+            own2 = ocol & (lyb < TW - 1) & (ej + 2 < sy)
+            # the row-(j+2) partner read from shared memory: warp ly + 1, same lane
+            assert (lyb[own2] + 1 < TW).all()
+            for bzi in range(bz):
+                z0 = bzi * zchunk
+                z1 = min(z0 + zchunk, sz) - 1
+                for ek in range(z0 - 1, z1 + 1):
+                    if ek >= z0:
+                        cnt[ek, (ej + 1)[own1], ni[own1]] += 1
+                        cnt[ek, (ej + 2)[own2], ni[own2]] += 1
+    return cnt
+
+
+def test_hex8_paired_tiling_writes_every_node_once():
+    sizes = [(1, 1, 1), (1, 6, 5), (30, 14, 1), (31, 15, 2), (32, 16, 3), (62, 30, 4),
+             (5, 13, 9), (40, 1, 12), (48, 17, 1), (13, 29, 5), (70, 40, 3)]
+    for nx, ny, nz in sizes:
+        for zchunk in sorted({1, 2, 3, nz, nz + 1, (nz + 2) // 2}):
+            cnt = _h8p_owners(nx, ny, nz, zchunk)
+            assert (cnt == 1).all(), (nx, ny, nz, zchunk, cnt.min(), cnt.max())
 
 
 def _q4_owners(nx, ny, target):

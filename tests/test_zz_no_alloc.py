@@ -21,13 +21,15 @@ U_RTOL = 1e-5            # displacement, L-inf relative to max |u| (as the parit
 COMPLIANCE_RTOL = 1e-6
 
 
-def _soa(prob, numeq_vec):
-    """numeq vector -> device SoA vector (component c of node n at c*ld + n)."""
+def _soa(prob, numeq_vec, fill=0.0):
+    """numeq vector -> device SoA vector (component c of node n at c*ld + n);
+    the constrained slots and the padding past each component's last node
+    hold `fill`."""
     import torch
     n = prob.soa_length()
     ld = n // prob.dim
     dof = prob.dof_map()
-    h = np.zeros(n)
+    h = np.full(n, fill)
     nodes = np.arange(prob.nnode)
     for c in range(prob.dim):
         d = dof[nodes * prob.dim + c]
@@ -62,13 +64,17 @@ def test_noalloc_matches_solve_on_consecutive_calls(ctx, kind, n):
     g = cases.build_gpu(ctx, kind, *n)
     assert g.soa_length() <= icb.lib().icb_noalloc_max_soa()
     f = g.load()
-    b = _soa(g, f)
-    for seed in (11, 12):  # two calls in a row on the shared scratch
+    # the second call's b holds NaN in its constrained and padding slots,
+    # which the solve must ignore
+    for seed, fill in ((11, 0.0), (12, np.nan)):  # two calls in a row on the shared scratch
+        b = _soa(g, f, fill)
         rho = cases.uniform_density(g.nel, seed)
         g.set_density(rho)
         ref = g.solve(tol=1e-10, maxit=20000)
         u_ref = g.displacement()
         x = torch.full((g.soa_length(),), 7.0, dtype=torch.float64, device="cuda")
+        # b and x were written on torch's stream; the library solves on its own
+        torch.cuda.synchronize()
         rc, info = _noalloc(g, b, x)
         torch.cuda.synchronize()
         assert rc == 0, icb.lib().icb_last_error().decode()
@@ -86,6 +92,7 @@ def test_noalloc_rejects_problems_beyond_its_limit(ctx):
     g.set_density(np.full(g.nel, 0.5))
     b = torch.zeros(g.soa_length(), dtype=torch.float64, device="cuda")
     x = torch.zeros_like(b)
+    torch.cuda.synchronize()
     rc, _ = _noalloc(g, b, x)
     assert rc == -1  # ICB_ERR_BAD_ARG
     assert "exceeds the static scratch limit" in icb.lib().icb_last_error().decode()
