@@ -796,12 +796,15 @@ def _c3_loop(args, icb, g, n, steps, rho0, out, err, speed, cpu):
 def workload_batched(args):
     """c4: seeded 2D instances (nelx log-uniform 64-1024, aspect U[1,4], vf
     U[0.2,0.6], r U[1.2,4], one clamped edge, 1-4 unit point loads), OC loop
-    with mixed-precision GMG solves, run by icb_run_batch with one stream per
-    instance; instance-iterations/s against the same runs one at a time."""
+    with mixed-precision GMG solves, through icb_run_batch three ways: one
+    run at a time (the sequential baseline), one stream per instance with
+    host workers, and fused (every loop advancing together, the solves of all
+    instances as one batched launch per kernel).  Instance-iterations/s of
+    each, results checked bitwise against the sequential runs."""
     import numpy as np
     import cases
     import icarat_b200 as icb
-    N, steps = args.instances, args.loop_steps
+    N = args.instances
     rng = np.random.default_rng(4)
     insts = [cases.random_instance2d(rng) for _ in range(N)]
     # several GPUs: every rank runs its footprint-balanced share, no exchange
@@ -813,52 +816,59 @@ def workload_batched(args):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         fp = [icb.job_footprint(cases.grid_desc(i), icb.JOB_OC) for i in insts]
         insts = [insts[k] for k in icb.shard_by_footprint(fp, world)[rank]]
     Nloc = len(insts)
     nel_total = sum(i["nx"] * i["ny"] for i in insts)
-    runs, ref = {}, None
-    for W in args.workers:
-        dev = int(os.environ.get("LOCAL_RANK", "0"))
-        ctxs = [icb.Context(dev) for _ in range(Nloc)]
-        probs = [cases.build_instance(c, i) for c, i in zip(ctxs, insts)]
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    ctxs = [icb.Context(dev) for _ in range(Nloc)]
+    probs = [cases.build_instance(c, i) for c, i in zip(ctxs, insts)]
+    rho0 = [np.full(p.nel, i["vf"]) for p, i in zip(probs, insts)]
+
+    def run(steps, fused, workers):
+        icb.set_option("batch_fused", int(fused))
         opts = [icb.loop_opts(steps, i["r"], move=0.2, precision=icb.MIXED) for i in insts]
-        rho0 = [np.full(p.nel, i["vf"]) for p, i in zip(probs, insts)]
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
-        H, X, S = icb.run_batch(probs, [icb.JOB_OC] * Nloc, opts, rho0, nworkers=W)
+        H, X, S = icb.run_batch(probs, [icb.JOB_OC] * Nloc, opts, rho0, nworkers=workers)
         dt = time.perf_counter() - t0
         if dist is not None:
             import torch
             t = torch.tensor([dt], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dt = float(t.item())
-        runs[W] = {"seconds": dt, "inst_iter_s": N * steps / dt, "all_ok": bool((S == 0).all())}
-        if ref is None:
-            ref = (H, X)
-        else:
-            runs[W]["bitwise_equal_to_first"] = all(np.array_equal(a, b) for a, b in zip(ref[0], H)) and \
-                all(np.array_equal(a, b) for a, b in zip(ref[1], X))
-        for p in probs:
-            p.close()
-        for c in ctxs:
-            c.close()
+        icb.set_option("batch_fused", 1)
+        return {"seconds": dt, "inst_iter_s": N * steps / dt, "all_ok": bool((S == 0).all()),
+                "steps": steps}, H, X
+
+    short = args.loop_steps_short
+    run(2, True, 1)  # hierarchies, filters and graphs built once (not timed)
+    seq, Hs, Xs = run(short, False, 1)
+    streams, Hw, Xw = run(short, False, args.workers[-1])
+    fused_short, Hf, Xf = run(short, True, 1)
+    same = all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hf + Xf)) and \
+        all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hw + Xw))
+    fused, _, _ = run(args.loop_steps, True, 1)
+    for p in probs:
+        p.close()
+    for c in ctxs:
+        c.close()
     if dist is not None:
         dist.destroy_process_group()
         if rank != 0:
             return 0
-    seq = runs.get(1, {}).get("inst_iter_s")
-    best_w = max(runs, key=lambda w: runs[w]["inst_iter_s"])
-    print(json.dumps({"metric": "instance-iterations/s (c4 batched 2D OC)", "value": runs[best_w]["inst_iter_s"],
+    print(json.dumps({"metric": "instance-iterations/s (c4 batched 2D OC)", "value": fused["inst_iter_s"],
                       "unit": "instance-iter/s", "n_gpus": world, "higher_is_better": True,
-                      "scaling": "strong (the 256 instances are split over the GPUs by footprint)",
+                      "scaling": "strong (the instances are split over the GPUs by footprint)",
                       "dtype": "f64 Krylov / f32 multigrid", "data": "synthetic (seeded instances)",
                       "config": {"workload": f"{N} 2D Q4 instances, {nel_total} elements on rank 0",
-                                 "oc_steps": steps, "workers": best_w},
-                      "speedup_vs_sequential": (runs[best_w]["inst_iter_s"] / seq) if seq else None,
-                      "runs": {str(k): v for k, v in runs.items()}}), flush=True)
+                                 "oc_steps": args.loop_steps},
+                      "speedup_vs_sequential": fused_short["inst_iter_s"] / seq["inst_iter_s"],
+                      "bitwise_equal_to_sequential": same,
+                      "runs": {"sequential": seq, f"streams_{args.workers[-1]}_workers": streams,
+                               "fused_short": fused_short, "fused": fused}}), flush=True)
     return 0
 
 
@@ -1036,7 +1046,9 @@ def main():
                     help="solve workload, mixed_refine: inner relative tolerance (0: default)")
     ap.add_argument("--repeat", type=int, default=3, help="solve workload: timed solves")
     ap.add_argument("--instances", type=int, default=256)
-    ap.add_argument("--loop-steps", type=int, default=10, help="batched: OC steps per instance")
+    ap.add_argument("--loop-steps", type=int, default=100, help="batched: OC steps per instance")
+    ap.add_argument("--loop-steps-short", type=int, default=10,
+                    help="batched: OC steps of the sequential / streams / fused comparison")
     ap.add_argument("--workers", type=int, nargs="+", default=[1, 8, 16], help="batched: host workers")
     ap.add_argument("--rates", type=float, nargs="+", default=[10, 20, 50, 100, 200, 500])
     ap.add_argument("--jobs-per-rate", type=int, default=24)

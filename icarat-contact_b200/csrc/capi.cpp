@@ -601,6 +601,8 @@ int icb_set_option(const char *name, long long value)
     set_device_loops(value != 0);
   else if(n == "hex8_pair")
     set_hex8_pair(value != 0);
+  else if(n == "batch_fused")
+    set_batch_fused(value != 0);
   else if(n == "tc_spin_limit")
   {
     need(value >= 0 && value <= 0x7fffffffLL, "tc_spin_limit must be in [0, 2^31)");
@@ -624,6 +626,8 @@ long long icb_get_option(const char *name)
     return device_loops_enabled() ? 1 : 0;
   if(n == "hex8_pair")
     return hex8_pair_enabled() ? 1 : 0;
+  if(n == "batch_fused")
+    return batch_fused_enabled() ? 1 : 0;
   if(n == "tc_timeouts")
     return (long long)tc_timeouts();
   if(n == "tc_spin_limit")

@@ -193,11 +193,47 @@ template <typename T> struct OpExtras
   int gateConv = 0;
   int cudaCores = 0; ///< 1: the CUDA-core kernel, whatever the tensor-core switch says
 };
+/// the OC loops of many 2D problems advanced together with batched solves
+/// (mgbatch.cu): whether a batch qualifies, and the run (status / message per
+/// problem)
+bool oc_fused_eligible(int n, icb_problem_s *const *probs, const int *kinds,
+                       const icb_loop_opts *opts);
+void run_oc_fused(int n, icb_problem_s *const *probs, const icb_loop_opts *opts,
+                  const double *const *rho0, double *const *hist, double *const *xout, int *status,
+                  std::vector<std::string> &err);
+/// whether icb_run_batch uses the fused loop when a batch qualifies (option
+/// batch_fused, default on)
+bool batch_fused_enabled();
+void set_batch_fused(bool on);
 /// bytes of an app-loop checkpoint (toapi.cu) for nel elements and a job kind
 long long loop_checkpoint_bytes(long long nel, int kind);
 /// look up the no-alloc solve's static scratch on the current device
 /// (noalloc.cu; called by icb_ctx_create)
 void noalloc_prepare_current_device();
+/// one Q4 operator launch as data, for the batched launch that runs many of
+/// them at once (k_matvec_q4_batch): the element matrix by value, the grid of
+/// its own launch (q4_grid) and every argument of k_matvec_q4
+template <typename T> struct Q4Launch
+{
+  KMat<T, 8> K;
+  Dims d;
+  int ychunk, bx, by, gateConv;
+  const T *E, *u;
+  T *y;
+  const uint8_t *fix;
+  RedScratch red;
+  double *dotOut;
+  const KState *gate;
+  Epi<T> ep;
+};
+/// the launch grid of the Q4 operator on d: (bx, by) blocks, ychunk rows each
+void q4_grid(const Dims &d, int &bx, int &by, int &ychunk);
+/// n Q4 operator launches of one mode as one kernel: D (device, n entries)
+/// and map (device, one (launch, block) pair per block, `blocks` in all)
+template <typename T>
+void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, int blocks, int mode, bool dot,
+                     cudaStream_t s);
+
 /// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)
 void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u, float *y,
                   const uint8_t *fix, cudaStream_t s, const OpExtras<float> &x);

@@ -227,14 +227,19 @@ void launch_add(long long n, const double *a, const double *b, double *out, cuda
   ICB_CUDA(cudaGetLastError());
   count_launch();
 }
-double device_dot(long long n, const double *a, const double *b, RedScratch &red,
-                  double *scratch, cudaStream_t s)
+void launch_dot(long long n, const double *a, const double *b, RedScratch &red, double *out,
+                cudaStream_t s)
 {
   int nb = vec_blocks(n);
   ICB_REQUIRE(nb <= red.maxBlocks, "reduction scratch too small");
-  k_dot<<<nb, VB, 0, s>>>(n, a, b, red, scratch);
+  k_dot<<<nb, VB, 0, s>>>(n, a, b, red, out);
   ICB_CUDA(cudaGetLastError());
   count_launch();
+}
+double device_dot(long long n, const double *a, const double *b, RedScratch &red,
+                  double *scratch, cudaStream_t s)
+{
+  launch_dot(n, a, b, red, scratch, s);
   double h = 0.0;
   ICB_CUDA(cudaMemcpyAsync(&h, scratch, sizeof(double), cudaMemcpyDeviceToHost, s));
   ICB_CUDA(cudaStreamSynchronize(s));

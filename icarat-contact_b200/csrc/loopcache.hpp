@@ -12,6 +12,7 @@
 #include "helm.hpp"
 #include "icb_internal.hpp"
 #include "opt.hpp"
+#include "problem.hpp"
 
 namespace icb
 {
@@ -75,4 +76,11 @@ struct LoopCache
     return *gcmma;
   }
 };
+/// the problem's loop work space, created on first use (toapi.cu)
+LoopCache &loop_cache(icb_problem p);
+/// a[i] = v; a[i] *= sc * m[i]; *out = sum of a (p's reduction scratch), all
+/// asynchronous on the given stream / the problem's stream (toapi.cu)
+void launch_fill(long long n, double v, double *a, cudaStream_t s);
+void launch_scale_mul(long long n, double *a, const double *m, double sc, cudaStream_t s);
+void launch_sum(icb_problem p, const double *a, long long n, double *out);
 } // namespace icb

@@ -1,0 +1,892 @@
+// mgbatch.cu -- the multigrid-preconditioned solves of many independent
+// problems as one sequence of batched launches, and the OC loop of many
+// problems advancing together (the batched form of icb_run_batch).
+//
+// ICARAT solves one problem per process (src/analysis/linear.hpp:15-41).  A
+// batch of small, uneven 2D designs run one at a time leaves the GPU idle:
+// each FCG iteration of a 100k-element problem is ~50 kernels of a few
+// microseconds.  Here every kernel of an iteration (the Krylov operator and
+// vector updates, and per V-cycle level the smoother, residual, transfers
+// and coarse solve) is launched once for all problems: block b of a batched
+// launch looks up (problem, block) in a map and runs that block of that
+// problem's own launch -- same grid, same arithmetic, same reduction order
+// (block_reduce_at) -- so each problem's iterates are bitwise those of its
+// own solve.  A problem that has converged is gated out (its blocks return at
+// once), as in its own solve.  Problems whose hierarchies have fewer levels
+// reach their coarsest solve earlier; a batched launch holds the problems
+// that take that step at that point of the V-cycle.
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <memory>
+
+#include "loopcache.hpp"
+#include "mg_impl.cuh"
+#include "opt.hpp"
+
+namespace icb
+{
+namespace
+{
+/// block b runs block map[b].y of the launch D[map[b].x] (its own grid)
+template <class L>
+__global__ void k_batch(const L *__restrict__ D, const int2 *__restrict__ map)
+{
+  const int2 m = map[blockIdx.x];
+  const L &l = D[m.x];
+  const unsigned b = unsigned(m.y);
+  const Blk B{b % l.g.gx, (b / l.g.gx) % l.g.gy, b / (l.g.gx * l.g.gy), l.g.gx, l.g.gy, l.g.gz};
+  l.run(B);
+}
+
+// the per-problem launches as records: the kernel's arguments and its grid
+template <typename TK, typename TP> struct InitL
+{
+  Blk g;
+  long long n;
+  const TK *b;
+  TK *x, *r;
+  TP *rP;
+  RedScratch red;
+  KState *st;
+  double tol;
+  int maxit;
+  __device__ void run(const Blk &B) const { mg_init_b<TK, TP>(n, b, x, r, rP, red, st, tol, maxit, B); }
+};
+template <typename TK, typename TP> struct Init2L
+{
+  Blk g;
+  long long n;
+  const TK *r;
+  const TP *z;
+  TK *p;
+  RedScratch red;
+  KState *st;
+  __device__ void run(const Blk &B) const { mg_init2_b<TK, TP>(n, r, z, p, red, st, B); }
+};
+template <typename TK, typename TP> struct RL
+{
+  Blk g;
+  long long n;
+  TK *r;
+  TP *rP;
+  const TK *q;
+  const TP *z;
+  const double *pq;
+  RedScratch red;
+  KState *st;
+  __device__ void run(const Blk &B) const { mg_r_b<TK, TP>(n, r, rP, q, z, pq, red, st, B); }
+};
+template <typename TK, typename TP> struct RzL
+{
+  Blk g;
+  long long n;
+  const TK *r;
+  const TP *z;
+  RedScratch red;
+  KState *st;
+  __device__ void run(const Blk &B) const { mg_rz_b<TK, TP>(n, r, z, red, st, B); }
+};
+template <typename TK, typename TP> struct XpL
+{
+  Blk g;
+  long long n;
+  TK *x, *p;
+  const TP *z;
+  RedScratch red;
+  KState *st;
+  __device__ void run(const Blk &B) const { mg_xp_b<TK, TP>(n, x, p, z, red, st, LoopCtl{}, B); }
+};
+template <typename T> struct Jacobi0L
+{
+  Blk g;
+  long long n;
+  T c;
+  const T *dinv, *b;
+  T *x, *x0;
+  const KState *gate;
+  __device__ void run(const Blk &B) const { jacobi0_b<T>(n, c, dinv, b, x, x0, gate, B); }
+};
+template <typename T> struct RestrictL
+{
+  Blk g;
+  Dims df, dc;
+  int3 sh;
+  const T *rf;
+  T *bc;
+  const uint8_t *fixc;
+  const KState *gate;
+  __device__ void run(const Blk &B) const { restrict_b<T>(df, dc, sh, rf, bc, fixc, gate, B); }
+};
+template <typename T> struct ProlongL
+{
+  Blk g;
+  Dims df, dc;
+  int3 sh;
+  const T *xc;
+  T *xf;
+  const uint8_t *fixf;
+  const KState *gate;
+  __device__ void run(const Blk &B) const { prolong_add_b<T>(df, dc, sh, xc, xf, fixf, gate, B); }
+};
+template <typename T> struct FillL
+{
+  Blk g;
+  long long n;
+  T v;
+  T *x;
+  __device__ void run(const Blk &B) const { fill_b<T>(n, v, x, B); }
+};
+template <typename T> struct DenseL
+{
+  Blk g;
+  int n;
+  const double *A;
+  const long long *soa;
+  const T *b;
+  T *x;
+  const KState *gate;
+  __device__ void run(const Blk &B) const { dense_apply_b<T>(n, A, soa, b, x, gate, B); }
+};
+/// y = x over n entries (the V-cycle's result when the smoothing ends in the
+/// scratch vector), grid-stride
+template <typename T> struct CopyL
+{
+  Blk g;
+  long long n;
+  const T *x;
+  T *y;
+  const KState *gate;
+  __device__ void run(const Blk &B) const
+  {
+    if(gated(gate))
+      return;
+    for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
+        i += (long long)B.gx * blockDim.x)
+      y[i] = x[i];
+  }
+};
+
+/// number of problems whose solve has not stopped
+__global__ void k_count_active(int n, KState *const *st, int *out)
+{
+  __shared__ int c;
+  if(threadIdx.x == 0)
+    c = 0;
+  __syncthreads();
+  int mine = 0;
+  for(int i = threadIdx.x; i < n; i += blockDim.x)
+    mine += st[i]->stop ? 0 : 1;
+  atomicAdd(&c, mine);
+  __syncthreads();
+  if(threadIdx.x == 0)
+    *out = c;
+}
+
+using Launch = std::function<void(cudaStream_t)>;
+
+/// records of one batched launch, collected problem by problem
+template <class L> struct Builder
+{
+  std::vector<L> recs;
+  std::vector<int2> map;
+  void add(L l, unsigned gx, unsigned gy = 1, unsigned gz = 1)
+  {
+    l.g = Blk{0, 0, 0, gx, gy, gz};
+    const int id = int(recs.size());
+    recs.push_back(l);
+    const long long nb = (long long)gx * gy * gz;
+    ICB_REQUIRE((long long)map.size() + nb < (1LL << 31), "batched launch too large");
+    for(long long b = 0; b < nb; b++)
+      map.push_back(make_int2(id, int(b)));
+  }
+  /// upload and return the launch (empty when no problem takes this step)
+  Launch finish(int threads, int smem, cudaStream_t s)
+  {
+    if(recs.empty())
+      return {};
+    auto D = std::make_shared<DevBuf<L>>(recs.size());
+    auto M = std::make_shared<DevBuf<int2>>(map.size());
+    ICB_CUDA(cudaMemcpyAsync(D->p, recs.data(), sizeof(L) * recs.size(), cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaMemcpyAsync(M->p, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    const int blocks = int(map.size());
+    return [D, M, blocks, threads, smem](cudaStream_t cs) {
+      k_batch<L><<<blocks, threads, smem, cs>>>(D->p, M->p);
+      ICB_CUDA(cudaGetLastError());
+      count_launch();
+    };
+  }
+};
+
+/// the Q4 operator launches of one step (k_matvec_q4_batch)
+template <typename T> struct Q4Builder
+{
+  std::vector<Q4Launch<T>> recs;
+  std::vector<int2> map;
+  int mode = OP_APPLY;
+  bool dot = false;
+  void add(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,
+           const OpExtras<T> &x)
+  {
+    Q4Launch<T> q{};
+    std::copy(K, K + 64, q.K.k);
+    q.d = d;
+    q4_grid(d, q.bx, q.by, q.ychunk);
+    q.E = E;
+    q.u = u;
+    q.y = y;
+    q.fix = fix;
+    q.red = x.dotRed ? *x.dotRed : RedScratch{};
+    q.dotOut = x.dotOut;
+    q.gate = x.gate;
+    q.gateConv = x.gateConv;
+    q.ep = Epi<T>{x.b, x.dinv, T(x.omega), T(x.c1), T(x.c2)};
+    if(x.dotRed)
+      ICB_REQUIRE((long long)q.bx * q.by <= x.dotRed->maxBlocks, "reduction scratch too small");
+    mode = x.mode;
+    dot = x.dotRed != nullptr;
+    const int id = int(recs.size());
+    recs.push_back(q);
+    for(int b = 0; b < q.bx * q.by; b++)
+      map.push_back(make_int2(id, b));
+  }
+  Launch finish(cudaStream_t s)
+  {
+    if(recs.empty())
+      return {};
+    auto D = std::make_shared<DevBuf<Q4Launch<T>>>(recs.size());
+    auto M = std::make_shared<DevBuf<int2>>(map.size());
+    ICB_CUDA(cudaMemcpyAsync(D->p, recs.data(), sizeof(Q4Launch<T>) * recs.size(),
+                             cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaMemcpyAsync(M->p, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    const int blocks = int(map.size()), md = mode;
+    const bool dt = dot;
+    return [D, M, blocks, md, dt](cudaStream_t cs) { launch_q4_batch<T>(D->p, M->p, blocks, md, dt, cs); };
+  }
+};
+
+} // namespace
+
+/// The FCG iteration with its V-cycle (MgPcg::iteration / level) for many
+/// 2D problems at once, TK = double, V-cycle in TP.
+template <typename TP> struct BatchMg
+{
+  using MG = MgPcg<double, TP>;
+  std::vector<MG *> M;
+  std::vector<Launch> init, iter;
+  DevBuf<KState *> states;
+  DevBuf<int> active;
+  int *hActive = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int batch = 4; ///< iterations per graph launch
+  long long nodes = 0;
+
+  ~BatchMg()
+  {
+    if(exec)
+      cudaGraphExecDestroy(exec);
+    if(hActive)
+      cudaFreeHost(hActive);
+  }
+
+  /// problem i's V-cycle on level l: the state of one problem while the
+  /// sequence of steps is emitted
+  struct Inst
+  {
+    int i;
+    const TP *b;
+    TP *out;
+  };
+
+  /// append the batched steps of level(l, b, out) for the problems `set`
+  void emitLevel(size_t l, const std::vector<Inst> &set, bool gated, std::vector<Launch> &seq,
+                 cudaStream_t s)
+  {
+    std::vector<Inst> coarse, fine;
+    for(const Inst &I : set)
+      (l + 1 == M[I.i]->lv.size() ? coarse : fine).push_back(I);
+    auto gate = [&](int i) -> const KState * { return gated ? M[i]->st.p : nullptr; };
+    auto push = [&](Launch f) {
+      if(f)
+        seq.push_back(std::move(f));
+    };
+    if(!coarse.empty())
+    {
+      // MgPcg::coarseSolve
+      Builder<FillL<TP>> f;
+      Builder<DenseL<TP>> da;
+      int ncmax = 1;
+      for(const Inst &I : coarse)
+      {
+        MG &m = *M[I.i];
+        const Level<TP> &C = m.lv.back();
+        const long long n = (long long)C.d.dim * C.d.ld;
+        f.add(FillL<TP>{{}, n, TP(0), I.out}, unsigned(vblocks(n)));
+        if(m.nc)
+        {
+          da.add(DenseL<TP>{{}, m.nc, m.cA.p, m.cSoa.p, I.b, I.out, gate(I.i)}, 8);
+          ncmax = std::max(ncmax, m.nc);
+        }
+      }
+      push(f.finish(VB, 0, s));
+      push(da.finish(256, int(sizeof(double)) * ncmax, s));
+    }
+    if(fine.empty())
+      return;
+    struct Cur
+    {
+      TP *cur, *oth;
+    };
+    std::vector<Cur> cs(fine.size());
+    const int nu = M[fine[0].i]->nu;
+    for(const Inst &I : fine)
+      ICB_REQUIRE(M[I.i]->nu == nu, "batched problems need the same smoothing degree");
+    {
+      Builder<Jacobi0L<TP>> j0;
+      for(size_t k = 0; k < fine.size(); k++)
+      {
+        const Inst &I = fine[k];
+        MG &m = *M[I.i];
+        Level<TP> &L = m.lv[l];
+        const long long n = (long long)L.d.dim * L.d.ld;
+        cs[k] = Cur{L.t.p, I.out};
+        j0.add(Jacobi0L<TP>{{}, n, TP(m.cc2[0]), L.dinv.p, I.b, cs[k].cur, cs[k].oth, gate(I.i)},
+               unsigned(vblocks(n)));
+      }
+      push(j0.finish(VB, 0, s));
+    }
+    auto cheb = [&](int k) {
+      Q4Builder<TP> op;
+      for(size_t t = 0; t < fine.size(); t++)
+      {
+        const Inst &I = fine[t];
+        MG &m = *M[I.i];
+        Level<TP> &L = m.lv[l];
+        OpExtras<TP> ch;
+        ch.mode = OP_CHEB;
+        ch.b = I.b;
+        ch.dinv = L.dinv.p;
+        ch.gate = gate(I.i);
+        ch.gateConv = 1;
+        ch.c1 = m.cc1[k];
+        ch.c2 = m.cc2[k];
+        op.add(L.d, L.K, L.E, cs[t].cur, cs[t].oth, L.fix, ch);
+        std::swap(cs[t].cur, cs[t].oth);
+      }
+      push(op.finish(s));
+    };
+    for(int k = 1; k < nu; k++)
+      cheb(k);
+    {
+      Q4Builder<TP> op;
+      Builder<RestrictL<TP>> rs;
+      std::vector<Inst> next;
+      for(size_t t = 0; t < fine.size(); t++)
+      {
+        const Inst &I = fine[t];
+        MG &m = *M[I.i];
+        Level<TP> &L = m.lv[l];
+        Level<TP> &Cn = m.lv[l + 1];
+        OpExtras<TP> res;
+        res.mode = OP_RESIDUAL;
+        res.b = I.b;
+        res.gate = gate(I.i);
+        res.gateConv = 1;
+        op.add(L.d, L.K, L.E, cs[t].cur, L.r.p, L.fix, res);
+        const dim3 g3 = grid3(Cn.d);
+        rs.add(RestrictL<TP>{{}, L.d, Cn.d, Cn.sh, L.r.p, Cn.b.p, Cn.fix, gate(I.i)}, g3.x, g3.y,
+               g3.z);
+        next.push_back(Inst{I.i, Cn.b.p, Cn.x.p});
+      }
+      push(op.finish(s));
+      push(rs.finish(kTB, 0, s));
+      emitLevel(l + 1, next, gated, seq, s);
+    }
+    {
+      Builder<ProlongL<TP>> pr;
+      for(size_t t = 0; t < fine.size(); t++)
+      {
+        const Inst &I = fine[t];
+        MG &m = *M[I.i];
+        Level<TP> &L = m.lv[l];
+        Level<TP> &Cn = m.lv[l + 1];
+        const dim3 g3 = grid3(L.d);
+        pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i)}, g3.x, g3.y,
+               g3.z);
+      }
+      push(pr.finish(kTB, 0, s));
+    }
+    for(int k = 0; k < nu; k++)
+      cheb(k);
+    Builder<CopyL<TP>> cp;
+    for(size_t t = 0; t < fine.size(); t++)
+      if(cs[t].cur != fine[t].out)
+      {
+        const Level<TP> &L = M[fine[t].i]->lv[l];
+        const long long n = (long long)L.d.dim * L.d.ld;
+        cp.add(CopyL<TP>{{}, n, cs[t].cur, fine[t].out, gate(fine[t].i)}, unsigned(vblocks(n)));
+      }
+    push(cp.finish(VB, 0, s));
+  }
+
+  /// the step sequences of MgPcg::solve's set-up (init) and of one iteration
+  /// (iter) for problems whose hierarchies are built, solving
+  /// K x[i] = b[i]
+  void build(const std::vector<MG *> &mgs, const std::vector<const double *> &b,
+             const std::vector<double *> &x, const std::vector<double> &tol,
+             const std::vector<int> &maxit, cudaStream_t s)
+  {
+    M = mgs;
+    const int n = int(M.size());
+    init.clear();
+    iter.clear();
+    auto push = [](std::vector<Launch> &seq, Launch f) {
+      if(f)
+        seq.push_back(std::move(f));
+    };
+    std::vector<Inst> all;
+    {
+      Builder<InitL<double, TP>> in;
+      for(int i = 0; i < n; i++)
+      {
+        MG &m = *M[i];
+        in.add(InitL<double, TP>{{}, m.n, b[i], x[i], m.r.p, MG::same() ? nullptr : m.rP.p, m.red,
+                                 m.st.p, tol[i], maxit[i]},
+               unsigned(vblocks(m.n)));
+        all.push_back(Inst{i, m.rin(), m.z.p});
+      }
+      push(init, in.finish(VB, 0, s));
+    }
+    emitLevel(0, all, false, init, s);
+    {
+      Builder<Init2L<double, TP>> in2;
+      for(int i = 0; i < n; i++)
+      {
+        MG &m = *M[i];
+        in2.add(Init2L<double, TP>{{}, m.n, m.r.p, m.z.p, m.p.p, m.red, m.st.p},
+                unsigned(vblocks(m.n)));
+      }
+      push(init, in2.finish(VB, 0, s));
+    }
+    // one iteration (MgPcg::iteration)
+    {
+      Q4Builder<double> op;
+      Builder<RL<double, TP>> rb;
+      for(int i = 0; i < n; i++)
+      {
+        MG &m = *M[i];
+        OpExtras<double> a;
+        a.dotRed = &m.red;
+        a.dotOut = m.dots.p;
+        a.gate = m.st.p;
+        op.add(m.lv[0].d, m.Kk, m.Ek, m.p.p, m.q.p, m.lv[0].fix, a);
+        rb.add(RL<double, TP>{{}, m.n, m.r.p, MG::same() ? nullptr : m.rP.p, m.q.p, m.z.p,
+                              m.dots.p, m.red, m.st.p},
+               unsigned(vblocks(m.n)));
+      }
+      push(iter, op.finish(s));
+      push(iter, rb.finish(VB, 0, s));
+    }
+    emitLevel(0, all, true, iter, s);
+    {
+      Builder<RzL<double, TP>> rz;
+      Builder<XpL<double, TP>> xp;
+      for(int i = 0; i < n; i++)
+      {
+        MG &m = *M[i];
+        rz.add(RzL<double, TP>{{}, m.n, m.r.p, m.z.p, m.red, m.st.p}, unsigned(vblocks(m.n)));
+        xp.add(XpL<double, TP>{{}, m.n, x[i], m.p.p, m.z.p, m.red, m.st.p}, unsigned(vblocks(m.n)));
+      }
+      push(iter, rz.finish(VB, 0, s));
+      push(iter, xp.finish(VB, 0, s));
+    }
+    std::vector<KState *> sp(n);
+    for(int i = 0; i < n; i++)
+      sp[i] = M[i]->st.p;
+    states.alloc(n);
+    active.alloc(1);
+    ICB_CUDA(cudaMemcpyAsync(states.p, sp.data(), sizeof(KState *) * n, cudaMemcpyHostToDevice, s));
+    if(!hActive)
+      ICB_CUDA(cudaMallocHost(&hActive, sizeof(int)));
+    // `batch` iterations and the count of active problems as one graph
+    if(exec)
+      cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    cudaStream_t cs;
+    ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t gr = nullptr;
+    const long long before = thread_launch_count();
+    ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    for(int k = 0; k < batch; k++)
+      for(auto &f : iter)
+        f(cs);
+    k_count_active<<<1, 256, 0, cs>>>(n, states.p, active.p);
+    ICB_CUDA(cudaMemcpyAsync(hActive, active.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
+    ICB_CUDA(cudaStreamEndCapture(cs, &gr));
+    nodes = thread_launch_count() - before;
+    count_launch(-nodes); // recorded, not launched
+    ICB_CUDA(cudaGraphInstantiate(&exec, gr, 0));
+    cudaGraphDestroy(gr);
+    cudaStreamDestroy(cs);
+    ICB_CUDA(cudaStreamSynchronize(s));
+  }
+
+  /// run the set-up and iterations until every problem has stopped (each
+  /// stops at its own tolerance or iteration limit, as its own solve would)
+  void run(int maxit, cudaStream_t s)
+  {
+    for(auto &f : init)
+      f(s);
+    long long launched = 0;
+    for(;;)
+    {
+      ICB_CUDA(cudaGraphLaunch(exec, s));
+      count_launch(nodes + 1);
+      ICB_CUDA(cudaStreamSynchronize(s));
+      launched += batch;
+      if(*hActive == 0 || launched > (long long)maxit + batch)
+        break;
+    }
+  }
+};
+
+/// MgPcg of problem p for solve options o, built (not refreshed)
+template <typename TP> MgPcg<double, TP> *prepare_mg(icb_problem p, const icb_solve_opts &o);
+
+template <> MgPcg<double, double> *prepare_mg<double>(icb_problem p, const icb_solve_opts &o)
+{
+  Mixed &M = mixed_of(p, o);
+  if(!M.mg64)
+  {
+    M.mg64 = std::make_unique<MgPcg<double, double>>();
+    M.mg64->build(*p->hs, p->K0, p->E.p, p->K0, p->E.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth,
+                  p->stream());
+  }
+  return M.mg64.get();
+}
+template <> MgPcg<double, float> *prepare_mg<float>(icb_problem p, const icb_solve_opts &o)
+{
+  Mixed &M = mixed_of(p, o);
+  if(!M.mgmx)
+  {
+    M.mgmx = std::make_unique<MgPcg<double, float>>();
+    M.mgmx->build(*p->hs, p->K0, p->E.p, p->K0f, p->Ef.p, p->fix.p, o.mg_coarse_dofs, o.mg_smooth,
+                  p->stream());
+  }
+  return M.mgmx.get();
+}
+
+template struct BatchMg<double>;
+template struct BatchMg<float>;
+
+namespace
+{
+/// one problem of the fused OC loop: its loop work space and state
+struct OcRun
+{
+  int idx = 0;
+  icb_problem p = nullptr;
+  const icb_loop_opts *o = nullptr;
+  double *hist = nullptr;
+  ConeFilter *cone = nullptr;
+  OcUpdater *oc = nullptr;
+  DevBuf<double> *x, *xf, *xh, *dxh, *dc, *dv, *dcf, *dvf, *lo, *hi, *V;
+  double V0 = 0.0;
+  bool active = true;
+  int status = ICB_OK;
+  std::string err;
+};
+
+/// the opt-macro-oc loop (icb_run_oc, opt_macro_oc.cpp:84-172) of every
+/// problem, advanced together: per step the filters, moduli and multigrid
+/// set-up run on each problem's own stream, the solves of all problems as
+/// one batched sequence (BatchMg), then compliance, sensitivities, adjoint
+/// filters and the OC update again per problem, all queued before one wait.
+/// Each problem's history and design are bitwise those of its own
+/// icb_run_oc.
+template <typename TP>
+void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
+{
+  BatchMg<TP> batch;
+  std::vector<OcRun *> set;
+  auto rebuild = [&]() {
+    set.clear();
+    std::vector<MgPcg<double, TP> *> mgs;
+    std::vector<const double *> b;
+    std::vector<double *> x;
+    std::vector<double> tol;
+    std::vector<int> maxit;
+    for(OcRun &r : R)
+      if(r.active)
+      {
+        set.push_back(&r);
+        mgs.push_back(prepare_mg<TP>(r.p, r.o->solve));
+        b.push_back(r.p->f.p);
+        x.push_back(r.p->x.p);
+        tol.push_back(r.o->solve.tol);
+        maxit.push_back(r.o->solve.maxit);
+      }
+    if(!set.empty())
+      batch.build(mgs, b, x, tol, maxit, sb);
+  };
+  auto fail = [&](OcRun &r, int st, const std::string &msg) {
+    r.active = false;
+    r.status = st;
+    r.err = msg;
+  };
+  int maxSteps = 0;
+  for(OcRun &r : R)
+    maxSteps = std::max(maxSteps, r.o->nsteps);
+  rebuild();
+  double *hc = nullptr, *hv = nullptr;
+  KState *hs = nullptr;
+  const size_t n = R.size();
+  ICB_CUDA(cudaMallocHost(&hc, sizeof(double) * n));
+  ICB_CUDA(cudaMallocHost(&hv, sizeof(double) * n));
+  ICB_CUDA(cudaMallocHost(&hs, sizeof(KState) * n));
+  std::vector<cudaEvent_t> ev(n);
+  for(auto &e : ev)
+    ICB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  try
+  {
+    for(int step = 1; step <= maxSteps && !set.empty(); step++)
+    {
+      auto t0 = std::chrono::steady_clock::now();
+      // filters, moduli and the multigrid set-up, problem by problem
+      for(OcRun *r : set)
+      {
+        cudaStream_t s = r->p->stream();
+        const double beta =
+            r->o->use_threshold ? std::min(std::pow(2.0, (int)(step / 40)), 16.0) : 0.0;
+        r->cone->forward(r->x->p, r->xf->p, beta, 0.5, r->xh->p, r->dxh->p, s);
+        const int rc = icb_set_density_device(r->p, r->xh->p);
+        if(rc)
+        {
+          fail(*r, rc, icb_last_error());
+          continue;
+        }
+        prepare_mg<TP>(r->p, r->o->solve)->refresh(s);
+        ICB_CUDA(cudaEventRecord(ev[r->idx], s));
+      }
+      bool lost = false;
+      for(OcRun *r : set)
+        lost = lost || !r->active;
+      if(lost)
+      {
+        for(OcRun *r : set)
+          if(r->active)
+            ICB_CUDA(cudaStreamSynchronize(r->p->stream()));
+        rebuild();
+        step--;
+        continue; // the remaining problems redo this step's set-up
+      }
+      for(OcRun *r : set)
+        ICB_CUDA(cudaStreamWaitEvent(sb, ev[r->idx], 0));
+      int maxit = 0;
+      for(OcRun *r : set)
+        maxit = std::max(maxit, r->o->solve.maxit);
+      batch.run(maxit, sb);
+      for(size_t k = 0; k < set.size(); k++)
+        ICB_CUDA(cudaMemcpyAsync(&hs[set[k]->idx], batch.M[k]->st.p, sizeof(KState),
+                                 cudaMemcpyDeviceToHost, sb));
+      ICB_CUDA(cudaStreamSynchronize(sb));
+      // compliance, V0 (step 1), sensitivities and adjoint filters
+      for(OcRun *r : set)
+      {
+        const KState &k = hs[r->idx];
+        if(k.status != ICB_OK)
+        {
+          fail(*r, k.status, k.status == ICB_ERR_MAXITER ? "iteration limit reached"
+                                                         : "CG breakdown or non-finite values");
+          continue;
+        }
+        icb_problem p = r->p;
+        cudaStream_t s = p->stream();
+        const long long ne = p->d.nel;
+        ICB_CUDA(cudaMemcpyAsync(p->u.p, p->x.p, sizeof(double) * p->nsoa,
+                                 cudaMemcpyDeviceToDevice, s));
+        p->solved = true;
+        p->last = icb_solve_info{k.iter, k.matvecs, 1, k.bb > 0 ? std::sqrt(k.rr / k.bb) : 0.0,
+                                 -1.0, 0.0, k.status};
+        launch_dot(p->nsoa, p->x.p, p->f.p, p->red, p->scal.p + 2, s);
+        ICB_CUDA(cudaMemcpyAsync(&hc[r->idx], p->scal.p + 2, sizeof(double),
+                                 cudaMemcpyDeviceToHost, s));
+        if(step == 1)
+        {
+          launch_sum(p, r->xh->p, ne, p->scal.p + 8);
+          ICB_CUDA(cudaMemcpyAsync(&hv[r->idx], p->scal.p + 8, sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+        }
+        const icb_grid_desc &g = p->hs->desc;
+        launch_sensitivity(p->d, p->K0, g.young1, g.young2, g.penalty, p->rho.p, p->u.p,
+                           p->dc.p, s);
+        ICB_CUDA(cudaMemcpyAsync(r->dc->p, p->dc.p, sizeof(double) * ne, cudaMemcpyDeviceToDevice,
+                                 s));
+        launch_scale_mul(ne, r->dc->p, r->dxh->p, 1.0, s);
+        ICB_CUDA(cudaMemcpyAsync(r->dv->p, r->V->p, sizeof(double) * ne, cudaMemcpyDeviceToDevice,
+                                 s));
+        launch_scale_mul(ne, r->dv->p, r->dxh->p, 1.0, s);
+        r->cone->adjoint(r->dc->p, r->dcf->p, s);
+        r->cone->adjoint(r->dv->p, r->dvf->p, s);
+      }
+      if(step == 1)
+        for(OcRun *r : set)
+          if(r->active)
+          {
+            ICB_CUDA(cudaStreamSynchronize(r->p->stream()));
+            r->V0 = hv[r->idx] * r->p->hs->volume;
+          }
+      // the OC updates, then one wait for every problem
+      for(OcRun *r : set)
+        if(r->active)
+        {
+          OcParams P;
+          P.move = r->o->move_limit;
+          P.beta = r->o->use_threshold ? std::min(std::pow(2.0, (int)(step / 40)), 16.0) : 0.0;
+          r->oc->launch(r->cone, r->x->p, r->dcf->p, r->dvf->p, r->V0, r->lo->p, r->hi->p,
+                        r->V->p, P, r->p->stream());
+        }
+      bool changed = false;
+      for(OcRun *r : set)
+        if(r->active)
+        {
+          ICB_CUDA(cudaStreamSynchronize(r->p->stream()));
+          r->oc->finish();
+        }
+      const double dt2 =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      for(OcRun *r : set)
+      {
+        if(!r->active)
+        {
+          changed = true;
+          continue;
+        }
+        r->hist[step - 1] = hc[r->idx];
+        if(r->o->iter_seconds)
+          r->o->iter_seconds[step - 1] = dt2;
+        if(step == r->o->nsteps)
+        {
+          r->active = false;
+          changed = true;
+        }
+      }
+      if(changed)
+        rebuild();
+    }
+  }
+  catch(...)
+  {
+    for(auto &e : ev)
+      cudaEventDestroy(e);
+    cudaFreeHost(hc);
+    cudaFreeHost(hv);
+    cudaFreeHost(hs);
+    throw;
+  }
+  for(auto &e : ev)
+    cudaEventDestroy(e);
+  cudaFreeHost(hc);
+  cudaFreeHost(hv);
+  cudaFreeHost(hs);
+}
+} // namespace
+
+static std::atomic<bool> g_batch_fused{true};
+bool batch_fused_enabled() { return g_batch_fused; }
+void set_batch_fused(bool on) { g_batch_fused = on; }
+
+bool oc_fused_eligible(int n, const icb_problem *probs, const int *kinds,
+                       const icb_loop_opts *opts)
+{
+  if(n < 2)
+    return false;
+  for(int i = 0; i < n; i++)
+  {
+    const icb_problem p = probs[i];
+    const icb_loop_opts &o = opts[i];
+    if(!p || !p->hs || !p->hs->finalized || p->d.dim != 2 || p->hasDirichletValues)
+      return false;
+    if(kinds && kinds[i] != ICB_JOB_OC)
+      return false;
+    if(o.solve.precond != ICB_PRECOND_GMG ||
+       (o.solve.precision != ICB_FP64 && o.solve.precision != ICB_MIXED))
+      return false;
+    if(o.solve.precision != opts[0].solve.precision || o.solve.mg_smooth != opts[0].solve.mg_smooth ||
+       p->ctx->device != probs[0]->ctx->device)
+      return false;
+    if(o.on_step || o.resume || o.checkpoint || o.conv_eps > 0.0 || o.nsteps <= 0 ||
+       !(o.filter_radius > 0.0))
+      return false;
+  }
+  return true;
+}
+
+void run_oc_fused(int n, const icb_problem *probs, const icb_loop_opts *opts,
+                  const double *const *rho0, double *const *hist, double *const *xout, int *status,
+                  std::vector<std::string> &err)
+{
+  ICB_CUDA(cudaSetDevice(probs[0]->ctx->device));
+  std::vector<OcRun> R(n);
+  for(int i = 0; i < n; i++)
+  {
+    // icb_run_oc's set-up (toapi.cu): filter, updater, work vectors
+    OcRun &r = R[i];
+    r.idx = i;
+    r.p = probs[i];
+    r.o = &opts[i];
+    r.hist = hist[i];
+    icb_problem p = r.p;
+    cudaStream_t s = p->stream();
+    const long long ne = p->d.nel;
+    LoopCache &LC = loop_cache(p);
+    r.cone = &LC.coneFilter(p->d, p->hs->h, r.o->filter_radius, s);
+    r.oc = &LC.ocUpdater(p->d, s);
+    r.x = &LC.buf(0, ne);
+    r.xf = &LC.buf(1, ne);
+    r.xh = &LC.buf(2, ne);
+    r.dxh = &LC.buf(3, ne);
+    r.dc = &LC.buf(4, ne);
+    r.dv = &LC.buf(5, ne);
+    r.dcf = &LC.buf(6, ne);
+    r.dvf = &LC.buf(7, ne);
+    r.lo = &LC.buf(8, ne);
+    r.hi = &LC.buf(9, ne);
+    r.V = &LC.buf(10, ne);
+    ICB_CUDA(cudaMemcpyAsync(r.x->p, rho0[i], sizeof(double) * ne, cudaMemcpyHostToDevice, s));
+    launch_fill(ne, 1.0e-4, r.lo->p, s);
+    launch_fill(ne, 1.0, r.hi->p, s);
+    launch_fill(ne, p->hs->volume, r.V->p, s);
+  }
+  for(int i = 0; i < n; i++)
+    ICB_CUDA(cudaStreamSynchronize(probs[i]->stream()));
+  cudaStream_t sb;
+  ICB_CUDA(cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking));
+  try
+  {
+    if(opts[0].solve.precision == ICB_FP64)
+      run_oc_fused_tp<double>(R, sb);
+    else
+      run_oc_fused_tp<float>(R, sb);
+  }
+  catch(...)
+  {
+    cudaStreamDestroy(sb);
+    throw;
+  }
+  cudaStreamDestroy(sb);
+  for(int i = 0; i < n; i++)
+  {
+    OcRun &r = R[i];
+    if(xout && xout[i] && r.status == ICB_OK)
+      ICB_CUDA(cudaMemcpyAsync(xout[i], r.x->p, sizeof(double) * r.p->d.nel,
+                               cudaMemcpyDeviceToHost, r.p->stream()));
+    ICB_CUDA(cudaStreamSynchronize(r.p->stream()));
+    status[i] = r.status;
+    err[i] = r.err;
+  }
+}
+
+} // namespace icb

@@ -858,19 +858,22 @@ __global__ void __launch_bounds__(TX *TW, MINB)
 }
 
 // ------------------------------------------------------------------- Q4 ----
+/// the Q4 operator for block (bxi, byi) of a (bx, by) grid: the body of
+/// k_matvec_q4 and of its batched form k_matvec_q4_batch
 template <typename T, bool DOT, int MODE>
-__global__ void __launch_bounds__(TX *TY2)
-    k_matvec_q4(const KMat<T, 8> K, const Dims d, const int ychunk,
-                const T *__restrict__ E, const T *__restrict__ u, T *__restrict__ y,
-                const uint8_t *__restrict__ fix, RedScratch red, double *dotOut,
-                const KState *gate, const int gateConv, const Epi<T> ep)
+__device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, const int ychunk,
+                                        const T *__restrict__ E, const T *__restrict__ u,
+                                        T *__restrict__ y, const uint8_t *__restrict__ fix,
+                                        const RedScratch &red, double *dotOut,
+                                        const KState *gate, const int gateConv, const Epi<T> &ep,
+                                        int bxi, int byi, int nbx, int nby)
 {
   if(gate && (gate->stop || (gateConv && gate->conv)))
     return;
   const int lx = threadIdx.x, w = threadIdx.y;
-  const int X0 = (blockIdx.x * TY2 + w) * (TX - 1);
+  const int X0 = (bxi * TY2 + w) * (TX - 1);
   const int ei = X0 - 1 + lx;
-  const int Y0 = blockIdx.y * ychunk;
+  const int Y0 = byi * ychunk;
   const int Y1 = min(Y0 + ychunk, d.sy) - 1;
   const bool col = ei >= 0 && ei < d.nx;
   const long long ld = d.ld;
@@ -971,8 +974,33 @@ __global__ void __launch_bounds__(TX *TY2)
   if(DOT)
   {
     double v[1] = {dot};
-    block_reduce<1>(v, red, FinStore{dotOut});
+    block_reduce_at<1>(v, red, FinStore{dotOut}, bxi + nbx * byi, nbx * nby);
   }
+}
+
+template <typename T, bool DOT, int MODE>
+__global__ void __launch_bounds__(TX *TY2)
+    k_matvec_q4(const KMat<T, 8> K, const Dims d, const int ychunk,
+                const T *__restrict__ E, const T *__restrict__ u, T *__restrict__ y,
+                const uint8_t *__restrict__ fix, RedScratch red, double *dotOut,
+                const KState *gate, const int gateConv, const Epi<T> ep)
+{
+  q4_body<T, DOT, MODE>(K, d, ychunk, E, u, y, fix, red, dotOut, gate, gateConv, ep, blockIdx.x,
+                        blockIdx.y, gridDim.x, gridDim.y);
+}
+
+/// many Q4 operator launches in one: block b runs block map[b].y of the
+/// launch described by D[map[b].x], with that launch's grid, so each
+/// problem's result (and its fused dot product) is bitwise that of its own
+/// launch
+template <typename T, bool DOT, int MODE>
+__global__ void __launch_bounds__(TX *TY2)
+    k_matvec_q4_batch(const Q4Launch<T> *__restrict__ D, const int2 *__restrict__ map)
+{
+  const int2 m = map[blockIdx.x];
+  const Q4Launch<T> &q = D[m.x];
+  q4_body<T, DOT, MODE>(q.K, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
+                        q.gateConv, q.ep, m.y % q.bx, m.y / q.bx, q.bx, q.by);
 }
 
 // ------------------------------------------------------------ diagonal ----
@@ -1235,6 +1263,16 @@ static int h8_zchunk(const Dims &d, long long tiles, int resident)
   return best;
 }
 
+void q4_grid(const Dims &d, int &bx, int &by, int &ychunk)
+{
+  const int target = num_sms() * 4;
+  const int strips = (d.sx + TX - 2) / (TX - 1);
+  bx = (strips + TY2 - 1) / TY2;
+  by = std::max(1, std::min(d.sy, (target + bx - 1) / bx));
+  ychunk = (d.sy + by - 1) / by;
+  by = (d.sy + ychunk - 1) / ychunk;
+}
+
 int matvec_blocks(const Dims &d)
 {
   if(d.dim == 3)
@@ -1254,12 +1292,9 @@ int matvec_blocks(const Dims &d)
     }
     return int(most);
   }
-  const int target = num_sms() * 4;
-  int strips = (d.sx + TX - 2) / (TX - 1);
-  int bx = (strips + TY2 - 1) / TY2;
-  int by = std::max(1, std::min(d.sy, (target + bx - 1) / bx));
-  int ychunk = (d.sy + by - 1) / by;
-  return bx * ((d.sy + ychunk - 1) / ychunk);
+  int bx, by, ychunk;
+  q4_grid(d, bx, by, ychunk);
+  return bx * by;
 }
 
 static std::atomic<bool> g_hex8_modal{true}; // read by every launching thread
@@ -1422,11 +1457,9 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   {
     KMat<T, 8> km;
     std::copy(K, K + 64, km.k);
-    int strips = (d.sx + TX - 2) / (TX - 1);
-    int bx = (strips + TY2 - 1) / TY2;
-    int by = std::max(1, std::min(d.sy, (target + bx - 1) / bx));
-    int ychunk = (d.sy + by - 1) / by;
-    by = (d.sy + ychunk - 1) / ychunk;
+    int bx, by, ychunk;
+    q4_grid(d, bx, by, ychunk);
+    (void)target;
     dim3 grid(bx, by), block(TX, TY2);
     if(x.dotRed)
     {
@@ -1441,6 +1474,30 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   ICB_CUDA(cudaGetLastError());
   count_launch();
 }
+
+template <typename T>
+void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, int blocks, int mode, bool dot,
+                     cudaStream_t s)
+{
+  if(blocks <= 0)
+    return;
+  const dim3 block(TX, TY2);
+  auto go = [&](auto kern) { kern<<<blocks, block, 0, s>>>(D, map); };
+  if(mode == OP_APPLY)
+    dot ? go(k_matvec_q4_batch<T, true, OP_APPLY>) : go(k_matvec_q4_batch<T, false, OP_APPLY>);
+  else if(mode == OP_RESIDUAL)
+    go(k_matvec_q4_batch<T, false, OP_RESIDUAL>);
+  else if(mode == OP_CHEB)
+    go(k_matvec_q4_batch<T, false, OP_CHEB>);
+  else
+    throw Error{ICB_ERR_BAD_ARG, "batched Q4 operator: unsupported mode"};
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+template void launch_q4_batch<double>(const Q4Launch<double> *, const int2 *, int, int, bool,
+                                      cudaStream_t);
+template void launch_q4_batch<float>(const Q4Launch<float> *, const int2 *, int, int, bool,
+                                     cudaStream_t);
 
 static std::atomic<bool> g_tc_operator{false};
 bool tc_operator_enabled() { return g_tc_operator; }

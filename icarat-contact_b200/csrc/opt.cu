@@ -674,6 +674,21 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
                       double g, const double *xmin, const double *xmax, const double *vol,
                       const OcParams &P, cudaStream_t s)
 {
+  launch(cone, x, df, dg, g, xmin, xmax, vol, P, s);
+  ICB_CUDA(cudaStreamSynchronize(s));
+  return finish();
+}
+
+int OcUpdater::finish()
+{
+  count_launch(1 + (loop.device ? (long long)hst->pad : 1) * loop.graphNodes);
+  return hst->counter;
+}
+
+void OcUpdater::launch(const ConeFilter *cone, double *x, const double *df, const double *dg,
+                       double g, const double *xmin, const double *xmax, const double *vol,
+                       const OcParams &P, cudaStream_t s)
+{
   const int nb = vblocks(d.nel);
   k_oc_init<<<1, 1, 0, s>>>(st.p, g, P);
   count_launch();
@@ -707,9 +722,6 @@ int OcUpdater::update(const ConeFilter *cone, double *x, const double *df, const
   k_oc_final<<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d.nel, x, df, dg, xmin, xmax, Pp, st.p);
   ICB_CUDA(cudaGetLastError());
   ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(OcState), cudaMemcpyDeviceToHost, s));
-  ICB_CUDA(cudaStreamSynchronize(s));
-  count_launch(1 + (loop.device ? (long long)hst->pad : 1) * loop.graphNodes);
-  return hst->counter;
 }
 
 // ================================================================ MMA =====

@@ -63,6 +63,12 @@ struct OcUpdater
   int update(const ConeFilter *cone, double *x, const double *df, const double *dg, double g,
              const double *xmin, const double *xmax, const double *vol, const OcParams &P,
              cudaStream_t s);
+  /// update() in two halves: launch queues the update on s; finish, once s
+  /// has been synchronised, returns the number of bisection steps
+  void launch(const ConeFilter *cone, double *x, const double *df, const double *dg, double g,
+              const double *xmin, const double *xmax, const double *vol, const OcParams &P,
+              cudaStream_t s);
+  int finish();
 };
 
 /// ICARAT's MMASolver parameters (MMASolver.cpp:41-55)

@@ -19,17 +19,18 @@ __device__ __forceinline__ double warp_sum_d(double v)
   return v;
 }
 
+/// the reduction of block `bid` of `nb` blocks: a batched launch that runs
+/// several independent grids passes each block's index and count within its
+/// own grid, so every grid reduces exactly as its own launch would
 template <int NV, class Fin>
-__device__ __forceinline__ void block_reduce(double (&v)[NV], const RedScratch &red,
-                                             Fin fin)
+__device__ __forceinline__ void block_reduce_at(double (&v)[NV], const RedScratch &red, Fin fin,
+                                                int bid, int nb)
 {
   __shared__ double sw[32][NV];
   __shared__ int last;
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nth = blockDim.x * blockDim.y * blockDim.z;
   const int nw = (nth + 31) >> 5;
-  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  const int nb = gridDim.x * gridDim.y * gridDim.z;
 #pragma unroll
   for(int k = 0; k < NV; k++)
     v[k] = warp_sum_d(v[k]);
@@ -86,6 +87,14 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], const RedScratch &
     *red.counter = 0u;
     fin(tot);
   }
+}
+
+template <int NV, class Fin>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], const RedScratch &red,
+                                             Fin fin)
+{
+  block_reduce_at<NV>(v, red, fin, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+                      gridDim.x * gridDim.y * gridDim.z);
 }
 
 struct FinStore

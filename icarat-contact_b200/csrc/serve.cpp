@@ -403,6 +403,12 @@ int icb_run_batch(int n, const icb_problem *probs, const int *kinds, const icb_l
   std::atomic<int> next{0};
   std::vector<int> st(n, ICB_OK);
   std::vector<std::string> err(n);
+  if(batch_fused_enabled() && oc_fused_eligible(n, probs, kinds, opts))
+  {
+    // every loop advances together, the solves as batched launches
+    run_oc_fused(n, probs, opts, rho0, hist, xout, st.data(), err);
+    nworkers = 0;
+  }
   auto work = [&] {
     for(int i; (i = next.fetch_add(1)) < n;)
     {
@@ -422,7 +428,7 @@ int icb_run_batch(int n, const icb_problem *probs, const int *kinds, const icb_l
   {
     // fewer threads than asked for: the ones that started take every instance
   }
-  if(th.empty())
+  if(th.empty() && nworkers > 0)
     work();
   for(auto &t : th)
     t.join();

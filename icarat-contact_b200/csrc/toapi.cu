@@ -44,6 +44,11 @@ struct icb_gcmma_s
   DevBuf<double> xm, xv, df, dg, lo, hi;
 };
 
+namespace icb
+{
+void launch_sum(icb_problem p, const double *a, long long n, double *out);
+}
+
 namespace
 {
 
@@ -105,10 +110,7 @@ __global__ void k_zero_masked(long long n, const uint8_t *__restrict__ m, double
 
 double deviceSum(icb_problem p, const double *a, long long n)
 {
-  int nb = int(std::min<long long>(nb256(n), (long long)p->red.maxBlocks));
-  k_sum<<<nb, 256, 0, p->stream()>>>(n, a, p->red, p->scal.p + 8);
-  ICB_CUDA(cudaGetLastError());
-  count_launch();
+  launch_sum(p, a, n, p->scal.p + 8);
   double h;
   ICB_CUDA(cudaMemcpyAsync(&h, p->scal.p + 8, sizeof(double), cudaMemcpyDeviceToHost, p->stream()));
   ICB_CUDA(cudaStreamSynchronize(p->stream()));
@@ -222,11 +224,30 @@ long long loop_checkpoint_bytes(long long nel, int kind)
   return (long long)sizeof(LoopCkpt) + (long long)sizeof(double) * nel * (kind == ICB_JOB_MMA ? 5 : 1);
 }
 /// the problem's loop work space, created on first use
-static LoopCache &loop_cache(icb_problem p)
+LoopCache &loop_cache(icb_problem p)
 {
   if(!p->loops)
     p->loops = std::make_unique<LoopCache>();
   return *p->loops;
+}
+void launch_fill(long long n, double v, double *a, cudaStream_t s)
+{
+  k_fill_d<<<nb256(n), 256, 0, s>>>(n, v, a);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+void launch_scale_mul(long long n, double *a, const double *m, double sc, cudaStream_t s)
+{
+  k_scale_mul<<<nb256(n), 256, 0, s>>>(n, a, m, sc);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+void launch_sum(icb_problem p, const double *a, long long n, double *out)
+{
+  int nb = int(std::min<long long>(nb256(n), (long long)p->red.maxBlocks));
+  k_sum<<<nb, 256, 0, p->stream()>>>(n, a, p->red, out);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
 }
 } // namespace icb
 

@@ -36,6 +36,41 @@ def test_batch_equals_sequential():
     assert np.array_equal(ha, h1[2]) and np.array_equal(xa, x1[2])
 
 
+@pytest.mark.parametrize("precision", [icb.FP64, icb.MIXED])
+def test_fused_batch_equals_each_problem_alone(precision):
+    """icb_run_batch advances qualifying 2D OC loops together (the solves of
+    every problem as one batched launch per kernel): each problem's history
+    and design are bitwise those of its own icb_run_oc, also when the runs
+    have different step counts (the batch shrinks as runs finish) and
+    hierarchies of different depth."""
+    rng = np.random.default_rng(11)
+    insts = [cases.random_instance2d(rng, nelx_range=(12, 150)) for _ in range(7)]
+    ctxs = [icb.Context(0) for _ in insts]
+    probs = [cases.build_instance(c, i) for c, i in zip(ctxs, insts)]
+    steps = [6, 4, 6, 5, 6, 3, 6]
+    opts = [icb.loop_opts(k, i["r"], move=0.2, precision=precision) for k, i in zip(steps, insts)]
+    rho0 = [np.full(p.nel, i["vf"]) for p, i in zip(probs, insts)]
+    assert icb.get_option("batch_fused") == 1
+    hf, xf, sf = icb.run_batch(probs, [0] * len(probs), opts, rho0, nworkers=1)
+    assert (sf == 0).all()
+    for k, (p, i) in enumerate(zip(probs, insts)):
+        ha, xa = icb.run_loop(p, "oc", rho0[k], steps[k], i["r"], move=0.2, precision=precision)
+        assert np.array_equal(ha, hf[k]), k
+        assert np.array_equal(xa, xf[k]), k
+    icb.set_option("batch_fused", 0)
+    try:
+        hw, xw, sw = icb.run_batch(probs, [0] * len(probs), opts, rho0, nworkers=3)
+    finally:
+        icb.set_option("batch_fused", 1)
+    assert (sw == 0).all()
+    for a, b in zip(hw + xw, hf + xf):
+        assert np.array_equal(a, b)
+    for p in probs:
+        p.close()
+    for c in ctxs:
+        c.close()
+
+
 def _job(inst, kind, nsteps):
     loop = icb.loop_opts(nsteps, inst["r"] if kind == icb.JOB_OC else 2.0 * inst["r"] / 1.5,
                          move=0.2)
