@@ -226,6 +226,18 @@ template <typename T> struct Q4Launch
   const KState *gate;
   Epi<T> ep;
 };
+/// one 2D diagonal launch (k_diag) as data: its own grid is
+/// blocks_for(d.nnode, 256) blocks of 256 threads
+template <typename T> struct Diag2Launch
+{
+  KMat<T, 8> K;
+  Dims d;
+  const T *E;
+  const uint8_t *fix;
+  T *invdiag;
+};
+template <typename T>
+void launch_diag2_batch(const Diag2Launch<T> *D, const int2 *map, int blocks, cudaStream_t s);
 /// the launch grid of the Q4 operator on d: (bx, by) blocks, ychunk rows each
 void q4_grid(const Dims &d, int &bx, int &by, int &ychunk);
 /// n Q4 operator launches of one mode as one kernel: D (device, n entries)

@@ -257,7 +257,7 @@ __global__ void k_dense_assemble(Dims d, KMat<double, 24> K, const T *__restrict
 /// (L2-resident).  Warp w updates rows w, w + 32, ..., its lanes the columns.
 constexpr int kInvSmemMax = 160;
 template <bool SMEM>
-__global__ void __launch_bounds__(1024) k_invert_spd(int n, double *Ag, int *status)
+__device__ __forceinline__ void invert_spd_b(int n, double *Ag, int *status)
 {
   extern __shared__ double sA[];
   __shared__ double rowk[1024];
@@ -311,6 +311,11 @@ __global__ void __launch_bounds__(1024) k_invert_spd(int n, double *Ag, int *sta
   if(SMEM)
     for(int t = tid; t < n * n; t += nth)
       Ag[t] = sA[t];
+}
+template <bool SMEM>
+__global__ void __launch_bounds__(1024) k_invert_spd(int n, double *Ag, int *status)
+{
+  invert_spd_b<SMEM>(n, Ag, status);
 }
 
 /// x_c = A^-1 b_c over the free coarse DOFs (warp per row)

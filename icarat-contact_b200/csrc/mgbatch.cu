@@ -167,6 +167,35 @@ template <typename T> struct CopyL
   }
 };
 
+template <typename T> struct CoarsenL
+{
+  Blk g;
+  Dims df, dc;
+  int3 sh;
+  const T *Ef;
+  T *Ec;
+  __device__ void run(const Blk &B) const { coarsen_E_b<T>(df, dc, sh, Ef, Ec, B); }
+};
+template <typename T> struct AssembleL
+{
+  Blk g;
+  Dims d;
+  KMat<double, 24> K;
+  const T *E;
+  const int *dense;
+  int n;
+  double *A;
+  __device__ void run(const Blk &B) const { dense_assemble_b<T>(d, K, E, dense, n, A, B); }
+};
+template <bool SMEM> struct InvertL
+{
+  Blk g;
+  int n;
+  double *A;
+  int *status;
+  __device__ void run(const Blk &) const { invert_spd_b<SMEM>(n, A, status); }
+};
+
 /// number of problems whose solve has not stopped
 __global__ void k_count_active(int n, KState *const *st, int *out)
 {
@@ -275,7 +304,7 @@ template <typename TP> struct BatchMg
 {
   using MG = MgPcg<double, TP>;
   std::vector<MG *> M;
-  std::vector<Launch> init, iter;
+  std::vector<Launch> refresh, init, iter;
   DevBuf<KState *> states;
   DevBuf<int> active;
   int *hActive = nullptr;
@@ -431,6 +460,97 @@ template <typename TP> struct BatchMg
     push(cp.finish(VB, 0, s));
   }
 
+  /// MgPcg::refresh of every problem (coarse moduli level by level, every
+  /// level's inverse diagonal, the coarsest matrix and its inverse)
+  void buildRefresh(cudaStream_t s)
+  {
+    refresh.clear();
+    auto push = [&](Launch f) {
+      if(f)
+        refresh.push_back(std::move(f));
+    };
+    size_t depth = 0;
+    for(MG *m : M)
+      depth = std::max(depth, m->lv.size());
+    for(size_t l = 1; l < depth; l++)
+    {
+      Builder<CoarsenL<TP>> c;
+      for(MG *m : M)
+        if(l < m->lv.size())
+          c.add(CoarsenL<TP>{{}, m->lv[l - 1].d, m->lv[l].d, m->lv[l].sh, m->lv[l - 1].E,
+                             m->lv[l].Eown.p},
+                nblocks(m->lv[l].d.nel, 256));
+      push(c.finish(256, 0, s));
+    }
+    {
+      std::vector<Diag2Launch<TP>> recs;
+      std::vector<int2> map;
+      for(MG *m : M)
+        for(auto &L : m->lv)
+        {
+          Diag2Launch<TP> q{};
+          std::copy(L.K, L.K + 64, q.K.k);
+          q.d = L.d;
+          q.E = L.E;
+          q.fix = L.fix;
+          q.invdiag = L.dinv.p;
+          const int id = int(recs.size());
+          recs.push_back(q);
+          for(unsigned b = 0; b < nblocks(L.d.nnode, 256); b++)
+            map.push_back(make_int2(id, int(b)));
+        }
+      auto D = std::make_shared<DevBuf<Diag2Launch<TP>>>(recs.size());
+      auto Mp = std::make_shared<DevBuf<int2>>(map.size());
+      ICB_CUDA(cudaMemcpyAsync(D->p, recs.data(), sizeof(Diag2Launch<TP>) * recs.size(),
+                               cudaMemcpyHostToDevice, s));
+      ICB_CUDA(cudaMemcpyAsync(Mp->p, map.data(), sizeof(int2) * map.size(),
+                               cudaMemcpyHostToDevice, s));
+      ICB_CUDA(cudaStreamSynchronize(s));
+      const int blocks = int(map.size());
+      push([D, Mp, blocks](cudaStream_t cs) { launch_diag2_batch<TP>(D->p, Mp->p, blocks, cs); });
+    }
+    Builder<FillL<double>> zA;
+    Builder<FillL<int>> zS;
+    Builder<AssembleL<TP>> as;
+    Builder<InvertL<true>> invS;
+    Builder<InvertL<false>> invG;
+    int smemMax = 0;
+    for(MG *m : M)
+    {
+      if(!m->nc)
+        continue;
+      const Level<TP> &C = m->lv.back();
+      const long long nn = (long long)m->nc * m->nc;
+      zA.add(FillL<double>{{}, nn, 0.0, m->cA.p}, unsigned(vblocks(nn)));
+      zS.add(FillL<int>{{}, 1, 0, m->cStatus.p}, 1);
+      AssembleL<TP> a{};
+      for(int i = 0; i < 576; i++)
+        a.K.k[i] = double(C.K[i]);
+      a.d = C.d;
+      a.E = C.E;
+      a.dense = m->cDense.p;
+      a.n = m->nc;
+      a.A = m->cA.p;
+      as.add(a, nblocks(C.d.nnode * C.d.dim, 128));
+      if(m->nc <= kInvSmemMax)
+      {
+        invS.add(InvertL<true>{{}, m->nc, m->cA.p, m->cStatus.p}, 1);
+        smemMax = std::max(smemMax, int(sizeof(double)) * m->nc * m->nc);
+      }
+      else
+        invG.add(InvertL<false>{{}, m->nc, m->cA.p, m->cStatus.p}, 1);
+    }
+    push(zA.finish(VB, 0, s));
+    push(zS.finish(VB, 0, s));
+    push(as.finish(128, 0, s));
+    if(smemMax > 0)
+      ICB_CUDA(cudaFuncSetAttribute(k_batch<InvertL<true>>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(sizeof(double)) * kInvSmemMax * kInvSmemMax));
+    push(invS.finish(1024, smemMax, s));
+    push(invG.finish(1024, 0, s));
+  }
+
   /// the step sequences of MgPcg::solve's set-up (init) and of one iteration
   /// (iter) for problems whose hierarchies are built, solving
   /// K x[i] = b[i]
@@ -440,6 +560,7 @@ template <typename TP> struct BatchMg
   {
     M = mgs;
     const int n = int(M.size());
+    buildRefresh(s);
     init.clear();
     iter.clear();
     auto push = [](std::vector<Launch> &seq, Launch f) {
@@ -537,6 +658,8 @@ template <typename TP> struct BatchMg
   /// stops at its own tolerance or iteration limit, as its own solve would)
   void run(int maxit, cudaStream_t s)
   {
+    for(auto &f : refresh)
+      f(s);
     for(auto &f : init)
       f(s);
     long long launched = 0;
@@ -667,7 +790,6 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
           fail(*r, rc, icb_last_error());
           continue;
         }
-        prepare_mg<TP>(r->p, r->o->solve)->refresh(s);
         ICB_CUDA(cudaEventRecord(ev[r->idx], s));
       }
       bool lost = false;

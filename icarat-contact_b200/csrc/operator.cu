@@ -1004,12 +1004,14 @@ __global__ void __launch_bounds__(TX *TY2)
 }
 
 // ------------------------------------------------------------ diagonal ----
-template <typename T, int DIM>
-__global__ void k_diag(const KMat<T, 24> K, const Dims d, const T *__restrict__ E,
-                       const uint8_t *__restrict__ fix, T *__restrict__ invdiag,
-                       T *__restrict__ diag)
+/// the diagonal of K(E) and its Eigen-rule inverse for the nodes of block bx
+/// (the body of k_diag and of its batched form); KM holds the element matrix
+template <typename T, int DIM, class KM>
+__device__ __forceinline__ void diag_b(const KM &K, const Dims &d, const T *__restrict__ E,
+                                       const uint8_t *__restrict__ fix, T *__restrict__ invdiag,
+                                       T *__restrict__ diag, unsigned bx)
 {
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long n = bx * (long long)blockDim.x + threadIdx.x;
   if(n >= d.nnode)
     return;
   const int nd = DIM == 2 ? 8 : 24;
@@ -1038,6 +1040,23 @@ __global__ void k_diag(const KMat<T, 24> K, const Dims d, const T *__restrict__ 
     // Eigen's DiagonalPreconditioner: 1 where the diagonal is 0
     invdiag[c * d.ld + n] = fx ? T(0) : (s[c] != 0.0 ? T(1.0 / s[c]) : T(1));
   }
+}
+template <typename T, int DIM>
+__global__ void k_diag(const KMat<T, 24> K, const Dims d, const T *__restrict__ E,
+                       const uint8_t *__restrict__ fix, T *__restrict__ invdiag,
+                       T *__restrict__ diag)
+{
+  diag_b<T, DIM>(K, d, E, fix, invdiag, diag, blockIdx.x);
+}
+
+/// many 2D diagonal launches in one (block b runs block map[b].y of launch
+/// D[map[b].x], 256 threads, its own grid of blocks_for(nnode, 256))
+template <typename T>
+__global__ void k_diag2_batch(const Diag2Launch<T> *__restrict__ D, const int2 *__restrict__ map)
+{
+  const int2 m = map[blockIdx.x];
+  const Diag2Launch<T> &q = D[m.x];
+  diag_b<T, 2>(q.K, q.d, q.E, q.fix, q.invdiag, nullptr, unsigned(m.y));
 }
 
 __global__ void k_gather_free(long long numeq, const long long *__restrict__ idx,
@@ -1494,6 +1513,19 @@ void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, int blocks, int mode
   ICB_CUDA(cudaGetLastError());
   count_launch();
 }
+template <typename T>
+void launch_diag2_batch(const Diag2Launch<T> *D, const int2 *map, int blocks, cudaStream_t s)
+{
+  if(blocks <= 0)
+    return;
+  k_diag2_batch<T><<<blocks, 256, 0, s>>>(D, map);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+}
+template void launch_diag2_batch<double>(const Diag2Launch<double> *, const int2 *, int,
+                                         cudaStream_t);
+template void launch_diag2_batch<float>(const Diag2Launch<float> *, const int2 *, int,
+                                        cudaStream_t);
 template void launch_q4_batch<double>(const Q4Launch<double> *, const int2 *, int, int, bool,
                                       cudaStream_t);
 template void launch_q4_batch<float>(const Q4Launch<float> *, const int2 *, int, int, bool,
