@@ -522,14 +522,15 @@ def headline_ours(args):
     prob.set_density_device(rho_d.data_ptr())
     peak, peak_kind = _peaks()
     rows = {}
-    for name, prec, es, kern in (("fp32", icb.MIXED, 4, "k_matvec_h8m<float>"),
+    k32 = "k_matvec_h8p<float>" if icb.get_option("hex8_pair") == 1 else "k_matvec_h8m<float>"
+    for name, prec, es, kern in (("fp32", icb.MIXED, 4, k32),
                                  ("fp64", icb.FP64, 8, "k_matvec_h8m<double>")):
         t = op_launch_seconds(prob, prec, stream, local)
         b = es * (2 * prob.neq + prob.nel)
         rows[name] = {"bound": "hbm", "achieved": b / t / 1e9, "peak": peak, "unit": "GB/s",
                       "frac": b / t / 1e9 / peak, "kernel": kern, "launch_us": t * 1e6,
                       "alg_bytes": b, "peak_source": peak_kind,
-                      "traffic": _traffic(f"matvec_h8m_{name}_halfmbb3d_384x128x128")}
+                      "traffic": _traffic(f"{kern}_384x128x128")}
     roofline = dict(rows["fp32"])
     roofline["fp64_outer_operator"] = rows["fp64"]
 

@@ -107,6 +107,9 @@ template <typename T> struct Jacobi0L
   const KState *gate;
   __device__ void run(const Blk &B) const { jacobi0_b<T>(n, c, dinv, b, x, x0, gate, B); }
 };
+/// the transfers write each node from its own reads only, so a batched
+/// launch may give a block several node rows: g.gy blocks take the ry rows
+/// of the per-problem grid (same results, far fewer tiny blocks)
 template <typename T> struct RestrictL
 {
   Blk g;
@@ -116,7 +119,13 @@ template <typename T> struct RestrictL
   T *bc;
   const uint8_t *fixc;
   const KState *gate;
-  __device__ void run(const Blk &B) const { restrict_b<T>(df, dc, sh, rf, bc, fixc, gate, B); }
+  unsigned ry;
+  __device__ void run(const Blk &B) const
+  {
+    Blk b = B;
+    for(b.y = B.y; b.y < ry; b.y += B.gy)
+      restrict_b<T>(df, dc, sh, rf, bc, fixc, gate, b);
+  }
 };
 template <typename T> struct ProlongL
 {
@@ -127,8 +136,16 @@ template <typename T> struct ProlongL
   T *xf;
   const uint8_t *fixf;
   const KState *gate;
-  __device__ void run(const Blk &B) const { prolong_add_b<T>(df, dc, sh, xc, xf, fixf, gate, B); }
+  unsigned ry;
+  __device__ void run(const Blk &B) const
+  {
+    Blk b = B;
+    for(b.y = B.y; b.y < ry; b.y += B.gy)
+      prolong_add_b<T>(df, dc, sh, xc, xf, fixf, gate, b);
+  }
 };
+/// node rows per block of a batched transfer
+constexpr unsigned kRowsPerBlock = 8;
 template <typename T> struct FillL
 {
   Blk g;
@@ -248,6 +265,9 @@ template <class L> struct Builder
   }
 };
 
+/// rows per block of a batched Q4 operator launch without a fused dot
+constexpr int kQ4BatchRows = 16;
+
 /// the Q4 operator launches of one step (k_matvec_q4_batch)
 template <typename T> struct Q4Builder
 {
@@ -262,6 +282,14 @@ template <typename T> struct Q4Builder
     std::copy(K, K + 64, q.K.k);
     q.d = d;
     q4_grid(d, q.bx, q.by, q.ychunk);
+    if(!x.dotRed && q.ychunk < kQ4BatchRows)
+    {
+      // without a fused dot the operator's output does not depend on how
+      // its rows are chunked (every node is the same sum computed by its
+      // owner): fewer, taller chunks, each recomputing one halo row
+      q.ychunk = std::min(d.sy, kQ4BatchRows);
+      q.by = (d.sy + q.ychunk - 1) / q.ychunk;
+    }
     q.E = E;
     q.u = u;
     q.y = y;
@@ -425,8 +453,8 @@ template <typename TP> struct BatchMg
         res.gateConv = 1;
         op.add(L.d, L.K, L.E, cs[t].cur, L.r.p, L.fix, res);
         const dim3 g3 = grid3(Cn.d);
-        rs.add(RestrictL<TP>{{}, L.d, Cn.d, Cn.sh, L.r.p, Cn.b.p, Cn.fix, gate(I.i)}, g3.x, g3.y,
-               g3.z);
+        rs.add(RestrictL<TP>{{}, L.d, Cn.d, Cn.sh, L.r.p, Cn.b.p, Cn.fix, gate(I.i), g3.y}, g3.x,
+               (g3.y + kRowsPerBlock - 1) / kRowsPerBlock, g3.z);
         next.push_back(Inst{I.i, Cn.b.p, Cn.x.p});
       }
       push(op.finish(s));
@@ -442,8 +470,8 @@ template <typename TP> struct BatchMg
         Level<TP> &L = m.lv[l];
         Level<TP> &Cn = m.lv[l + 1];
         const dim3 g3 = grid3(L.d);
-        pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i)}, g3.x, g3.y,
-               g3.z);
+        pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i), g3.y}, g3.x,
+               (g3.y + kRowsPerBlock - 1) / kRowsPerBlock, g3.z);
       }
       push(pr.finish(kTB, 0, s));
     }

@@ -584,9 +584,9 @@ template <> struct PairOps<float>
   }
 };
 
-constexpr int kPairWarps = 8;     // warps of k_matvec_h8p (two element rows each)
-constexpr int kPairMinBlocks = 1;
-constexpr int kPairPrefetch = 3;  // planes between the L2 prefetch and the register prefetch
+constexpr int kPairWarps = 4;     // warps of k_matvec_h8p (two element rows each)
+constexpr int kPairMinBlocks = 3;
+constexpr int kPairPrefetch = 4;  // planes the L2 prefetch runs ahead of the loads
 template <typename T, int TW, bool DOT, int MODE, int MINB>
 __global__ void __launch_bounds__(TX *TW, MINB)
     k_matvec_h8p(const KModal<T> K, const Dims d, const int zchunk, const T *__restrict__ E,
@@ -658,19 +658,22 @@ __global__ void __launch_bounds__(TX *TW, MINB)
     }
   };
 
-  P bh[3][4], carry[3][4], nlo[3][2], nhi[3][2];
+  // the carried top-face result lives in shared memory (each thread its own
+  // 12 pairs), the next plane is loaded at the top of its layer from L2 (the
+  // prefetch below runs kPairPrefetch planes ahead): both keep the registers
+  // under the 168 of three 128-thread CTAs per SM
+  __shared__ P sC[12][TW][TX];
+  P bh[3][4];
   {
-    load_plane(Z0 - 1, nlo, nhi);
-    modes(nlo, nhi, bh);
+    P lo[3][2], hi[3][2];
+    load_plane(Z0 - 1, lo, hi);
+    modes(lo, hi, bh);
 #pragma unroll
-    for(int c = 0; c < 3; c++)
-#pragma unroll
-      for(int q = 0; q < 4; q++)
-        carry[c][q] = P{T(0), T(0)};
+    for(int q = 0; q < 12; q++)
+      sC[q][ly][lx] = P{T(0), T(0)};
   }
-  load_plane(Z0, nlo, nhi);
   P Enxt = load_E(Z0 - 1);
-  // L2 prefetch, kPairPrefetch planes ahead of the register prefetch: lane
+  // L2 prefetch, kPairPrefetch planes ahead of the plane loads: lane
   // l < 18 takes component l / 6, row l / 2 % 3 and half-row l % 2 of the
   // warp's three node rows, lanes 18..21 the two element rows' moduli, so one
   // instruction per warp and layer keeps the plane loads L2 hits
@@ -706,12 +709,15 @@ __global__ void __launch_bounds__(TX *TW, MINB)
   for(int ek = Z0 - 1; ek <= Z1; ++ek)
   {
     P th[3][4];
-    modes(nlo, nhi, th);
+    {
+      P lo[3][2], hi[3][2];
+      load_plane(ek + 1, lo, hi);
+      modes(lo, hi, th);
+    }
     const P Ee = Enxt;
-    load_plane(ek + 2, nlo, nhi);
     Enxt = load_E(ek + 1);
     {
-      const int kp = ek + 2 + kPairPrefetch; // plane (layer for the moduli)
+      const int kp = ek + 1 + kPairPrefetch; // plane (layer for the moduli)
       if(pfOff >= 0 && kp <= (pfE ? d.nz - 1 : d.nz))
       {
         const T *a = (pfE ? E : u) + pfOff + (long long)kp * pfStep;
@@ -786,8 +792,8 @@ __global__ void __launch_bounds__(TX *TW, MINB)
       for(int q = 0; q < 4; q++)
       {
         const P a = P{yx[q * 3 + c], yy[q * 3 + c]}, b = P{yx[(q + 4) * 3 + c], yy[(q + 4) * 3 + c]};
-        hb[q] = O::fma(Ee, O::add(a, b), carry[c][q]);
-        carry[c][q] = O::mul(Ee, O::sub(a, b));
+        hb[q] = O::fma(Ee, O::add(a, b), sC[c * 4 + q][ly][lx]);
+        sC[c * 4 + q][ly][lx] = O::mul(Ee, O::sub(a, b));
       }
       // inverse x-y butterfly: y stage packed, the shared middle row summed
       // before its x stage
@@ -999,7 +1005,10 @@ __global__ void __launch_bounds__(TX *TY2)
 {
   const int2 m = map[blockIdx.x];
   const Q4Launch<T> &q = D[m.x];
-  q4_body<T, DOT, MODE>(q.K, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
+  // the element matrix in registers (constant indices once unrolled), as the
+  // single launch has it in the constant bank
+  const KMat<T, 8> K = q.K;
+  q4_body<T, DOT, MODE>(K, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
                         q.gateConv, q.ep, m.y % q.bx, m.y / q.bx, q.bx, q.by);
 }
 

@@ -223,6 +223,7 @@ class Context:
         h = C.c_void_p()
         check(lib().icb_ctx_create(device, C.byref(h)))
         self.h = h
+        self.device = device
 
     def stream(self):
         return lib().icb_ctx_stream(self.h)

@@ -17,6 +17,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("kind,n", [("cantilever3d", (1, 1, 1)), ("cantilever3d", (2, 3, 1)),
+                                    ("cantilever3d", (30, 6, 3)), ("halfmbb3d", (31, 7, 4)),
                                     ("cantilever3d", (5, 4, 3)), ("halfmbb3d", (30, 14, 4)),
                                     ("cantilever3d", (31, 15, 2)), ("cantilever3d", (32, 16, 5)),
                                     ("halfmbb3d", (62, 30, 3)), ("cantilever3d", (70, 40, 10)),

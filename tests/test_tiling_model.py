@@ -45,7 +45,7 @@ def _h8_owners(nx, ny, nz, zchunk):
     return cnt
 
 
-TW = 8  # operator.cu kPairWarps: warps of the paired-row FP32 Hex8 kernel
+TW = 4  # operator.cu kPairWarps: warps of the paired-row FP32 Hex8 kernel
 
 
 def _h8p_owners(nx, ny, nz, zchunk):
