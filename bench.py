@@ -847,11 +847,19 @@ def workload_batched(args):
     short = args.loop_steps_short
     run(2, True, 1)  # hierarchies, filters and graphs built once (not timed)
     seq, Hs, Xs = run(short, False, 1)
-    streams, Hw, Xw = run(short, False, args.workers[-1])
+    runs = {"sequential": seq}
+    same = True
+    if "streams" in args.batch_modes:
+        streams, Hw, Xw = run(short, False, args.workers[-1])
+        runs[f"streams_{args.workers[-1]}_workers"] = streams
+        same = same and all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hw + Xw))
     fused_short, Hf, Xf = run(short, True, 1)
-    same = all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hf + Xf)) and \
-        all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hw + Xw))
+    fused_short["phase_s"] = [icb.get_option(f"fused_phase_us_{k}") * 1e-6 for k in range(5)]
+    same = same and all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hf + Xf))
+    runs["fused_short"] = fused_short
     fused, _, _ = run(args.loop_steps, True, 1)
+    fused["phase_s"] = [icb.get_option(f"fused_phase_us_{k}") * 1e-6 for k in range(5)]
+    runs["fused"] = fused
     for p in probs:
         p.close()
     for c in ctxs:
@@ -868,8 +876,9 @@ def workload_batched(args):
                                  "oc_steps": args.loop_steps},
                       "speedup_vs_sequential": fused_short["inst_iter_s"] / seq["inst_iter_s"],
                       "bitwise_equal_to_sequential": same,
-                      "runs": {"sequential": seq, f"streams_{args.workers[-1]}_workers": streams,
-                               "fused_short": fused_short, "fused": fused}}), flush=True)
+                      "fused_phases": "build, per-instance set-up launches, batched multigrid "
+                                      "set-up and solve, compliance/sensitivity/filters, OC and wait",
+                      "runs": runs}), flush=True)
     return 0
 
 
@@ -1048,6 +1057,8 @@ def main():
     ap.add_argument("--repeat", type=int, default=3, help="solve workload: timed solves")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--loop-steps", type=int, default=100, help="batched: OC steps per instance")
+    ap.add_argument("--batch-modes", nargs="+", default=["streams"],
+                    help="batched: extra comparison modes besides sequential and fused")
     ap.add_argument("--loop-steps-short", type=int, default=10,
                     help="batched: OC steps of the sequential / streams / fused comparison")
     ap.add_argument("--workers", type=int, nargs="+", default=[1, 8, 16], help="batched: host workers")

@@ -628,6 +628,8 @@ long long icb_get_option(const char *name)
     return hex8_pair_enabled() ? 1 : 0;
   if(n == "batch_fused")
     return batch_fused_enabled() ? 1 : 0;
+  if(n.rfind("fused_phase_us_", 0) == 0 && n.size() == 16)
+    return (long long)(1e6 * fused_phase_seconds(n[15] - '0'));
   if(n == "tc_timeouts")
     return (long long)tc_timeouts();
   if(n == "tc_spin_limit")

@@ -201,6 +201,8 @@ bool oc_fused_eligible(int n, icb_problem_s *const *probs, const int *kinds,
 void run_oc_fused(int n, icb_problem_s *const *probs, const icb_loop_opts *opts,
                   const double *const *rho0, double *const *hist, double *const *xout, int *status,
                   std::vector<std::string> &err);
+/// wall seconds of phase k of the last fused run (mgbatch.cu)
+double fused_phase_seconds(int k);
 /// whether icb_run_batch uses the fused loop when a batch qualifies (option
 /// batch_fused, default on)
 bool batch_fused_enabled();

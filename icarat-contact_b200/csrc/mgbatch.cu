@@ -732,8 +732,21 @@ template <> MgPcg<double, float> *prepare_mg<float>(icb_problem p, const icb_sol
 template struct BatchMg<double>;
 template struct BatchMg<float>;
 
+/// wall time of the fused loop's phases over the last run, in seconds:
+/// 0 building the batched launches, 1 per-problem filter and moduli
+/// launches, 2 the batched multigrid set-up and solve, 3 compliance,
+/// sensitivities and adjoint filters, 4 OC updates and the step's wait
+static double g_fused_phase[5];
+double fused_phase_seconds(int k) { return k >= 0 && k < 5 ? g_fused_phase[k] : -1.0; }
+
 namespace
 {
+using PhaseClock = std::chrono::steady_clock;
+double since(PhaseClock::time_point t)
+{
+  return std::chrono::duration<double>(PhaseClock::now() - t).count();
+}
+
 /// one problem of the fused OC loop: its loop work space and state
 struct OcRun
 {
@@ -790,7 +803,13 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
   int maxSteps = 0;
   for(OcRun &r : R)
     maxSteps = std::max(maxSteps, r.o->nsteps);
-  rebuild();
+  for(double &v : g_fused_phase)
+    v = 0.0;
+  {
+    auto tb = PhaseClock::now();
+    rebuild();
+    g_fused_phase[0] += since(tb);
+  }
   double *hc = nullptr, *hv = nullptr;
   KState *hs = nullptr;
   const size_t n = R.size();
@@ -832,6 +851,8 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
         step--;
         continue; // the remaining problems redo this step's set-up
       }
+      auto tp = PhaseClock::now();
+      g_fused_phase[1] += std::chrono::duration<double>(tp - t0).count();
       for(OcRun *r : set)
         ICB_CUDA(cudaStreamWaitEvent(sb, ev[r->idx], 0));
       int maxit = 0;
@@ -842,6 +863,8 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
         ICB_CUDA(cudaMemcpyAsync(&hs[set[k]->idx], batch.M[k]->st.p, sizeof(KState),
                                  cudaMemcpyDeviceToHost, sb));
       ICB_CUDA(cudaStreamSynchronize(sb));
+      g_fused_phase[2] += since(tp);
+      tp = PhaseClock::now();
       // compliance, V0 (step 1), sensitivities and adjoint filters
       for(OcRun *r : set)
       {
@@ -888,6 +911,8 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
             ICB_CUDA(cudaStreamSynchronize(r->p->stream()));
             r->V0 = hv[r->idx] * r->p->hs->volume;
           }
+      g_fused_phase[3] += since(tp);
+      tp = PhaseClock::now();
       // the OC updates, then one wait for every problem
       for(OcRun *r : set)
         if(r->active)
@@ -905,6 +930,7 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
           ICB_CUDA(cudaStreamSynchronize(r->p->stream()));
           r->oc->finish();
         }
+      g_fused_phase[4] += since(tp);
       const double dt2 =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       for(OcRun *r : set)
@@ -924,7 +950,11 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
         }
       }
       if(changed)
+      {
+        auto tb = PhaseClock::now();
         rebuild();
+        g_fused_phase[0] += since(tb);
+      }
     }
   }
   catch(...)

@@ -1326,7 +1326,7 @@ int matvec_blocks(const Dims &d)
 }
 
 static std::atomic<bool> g_hex8_modal{true}; // read by every launching thread
-static std::atomic<bool> g_hex8_pair{true};  // FP32: two element rows per thread
+static std::atomic<bool> g_hex8_pair{false}; // FP32: two element rows per thread
 
 /// Kt = H K0 H / 64 on the 11 blocks of the corner-mode form.  False when an
 /// entry outside the blocks is above rounding (|Kt_rc| > tol max |Kt|, tol

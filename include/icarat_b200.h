@@ -427,8 +427,15 @@ long long icb_launch_count(void);
  * conditional WHILE node, one launch and one host wait each; 0: batches of
  * iterations polled from the host, for profilers that cannot follow
  * conditional graph nodes).  icb_get_option also reports "tc_timeouts"
- * (tensor-core waits that gave up; 0 in a healthy run).  Unknown names:
- * ICB_ERR_BAD_ARG / -1. */
+ * (tensor-core waits that gave up; 0 in a healthy run) and
+ * "fused_phase_us_0" .. "fused_phase_us_4" (wall microseconds of the last
+ * fused icb_run_batch: building its batched launches, per-design filter and
+ * moduli launches, the batched multigrid set-up and solves, compliance /
+ * sensitivities / adjoint filters, OC updates with the step's wait).
+ * Further switches: "hex8_pair" (FP32 Hex8 operator with two element rows per
+ * thread), "tc_spin_limit" (polls of a tensor-core wait before it gives up),
+ * "batch_fused" (icb_run_batch advances qualifying 2D OC batches together).
+ * Unknown names: ICB_ERR_BAD_ARG / -1. */
 int icb_set_option(const char *name, long long value);
 long long icb_get_option(const char *name);
 

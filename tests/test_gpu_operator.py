@@ -1,5 +1,5 @@
-"""The FP32 Hex8 operator with two element rows per thread (k_matvec_h8p, the
-default FP32 corner-mode kernel) against the one-row FP32 kernel and the FP64
+"""The FP32 Hex8 operator with two element rows per thread (k_matvec_h8p,
+switch hex8_pair) against the one-row FP32 kernel (the default) and the FP64
 operator, on grids that end inside, at and just past tile boundaries in every
 axis.
 
@@ -37,14 +37,14 @@ def test_paired_fp32_operator_matches(ctx, kind, n):
     ypair = torch.full_like(x32, 3.0)
     yrow = torch.full_like(x32, 3.0)
     torch.cuda.synchronize()
-    assert icb.get_option("hex8_pair") == 1
     g.operator_apply_device(x64.data_ptr(), y64.data_ptr(), icb.FP64)
-    g.operator_apply_device(x32.data_ptr(), ypair.data_ptr(), icb.MIXED)
-    icb.set_option("hex8_pair", 0)
+    g.operator_apply_device(x32.data_ptr(), yrow.data_ptr(), icb.MIXED)
+    old = icb.get_option("hex8_pair")
+    icb.set_option("hex8_pair", 1)
     try:
-        g.operator_apply_device(x32.data_ptr(), yrow.data_ptr(), icb.MIXED)
+        g.operator_apply_device(x32.data_ptr(), ypair.data_ptr(), icb.MIXED)
     finally:
-        icb.set_option("hex8_pair", 1)
+        icb.set_option("hex8_pair", old)
     g.ctx.synchronize()
     a = y64[live].cpu().numpy()
     p = ypair[live].double().cpu().numpy()
