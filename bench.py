@@ -855,6 +855,8 @@ def workload_batched(args):
         same = same and all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hw + Xw))
     fused_short, Hf, Xf = run(short, True, 1)
     fused_short["phase_s"] = [icb.get_option(f"fused_phase_us_{k}") * 1e-6 for k in range(5)]
+    fused_short["iterations_batch_vs_problems"] = [icb.get_option("fused_batch_iters"),
+                                                   icb.get_option("fused_problem_iters")]
     same = same and all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hf + Xf))
     runs["fused_short"] = fused_short
     fused, _, _ = run(args.loop_steps, True, 1)
@@ -1057,7 +1059,7 @@ def main():
     ap.add_argument("--repeat", type=int, default=3, help="solve workload: timed solves")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--loop-steps", type=int, default=100, help="batched: OC steps per instance")
-    ap.add_argument("--batch-modes", nargs="+", default=["streams"],
+    ap.add_argument("--batch-modes", nargs="+", default=["none"],
                     help="batched: extra comparison modes besides sequential and fused")
     ap.add_argument("--loop-steps-short", type=int, default=10,
                     help="batched: OC steps of the sequential / streams / fused comparison")

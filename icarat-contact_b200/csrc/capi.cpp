@@ -628,6 +628,10 @@ long long icb_get_option(const char *name)
     return hex8_pair_enabled() ? 1 : 0;
   if(n == "batch_fused")
     return batch_fused_enabled() ? 1 : 0;
+  if(n == "fused_batch_iters")
+    return fused_iterations(0);
+  if(n == "fused_problem_iters")
+    return fused_iterations(1);
   if(n.rfind("fused_phase_us_", 0) == 0 && n.size() == 16)
     return (long long)(1e6 * fused_phase_seconds(n[15] - '0'));
   if(n == "tc_timeouts")

@@ -203,6 +203,8 @@ void run_oc_fused(int n, icb_problem_s *const *probs, const icb_loop_opts *opts,
                   std::vector<std::string> &err);
 /// wall seconds of phase k of the last fused run (mgbatch.cu)
 double fused_phase_seconds(int k);
+/// iterations of the last fused run: k = 0 the batch's, 1 the problems' sum
+long long fused_iterations(int k);
 /// whether icb_run_batch uses the fused loop when a batch qualifies (option
 /// batch_fused, default on)
 bool batch_fused_enabled();
@@ -238,15 +240,21 @@ template <typename T> struct Diag2Launch
   const uint8_t *fix;
   T *invdiag;
 };
+struct BatchQueue;
 template <typename T>
-void launch_diag2_batch(const Diag2Launch<T> *D, const int2 *map, int blocks, cudaStream_t s);
+void launch_diag2_batch(const Diag2Launch<T> *D, const int2 *map, const BatchQueue &q,
+                        cudaStream_t s);
 /// the launch grid of the Q4 operator on d: (bx, by) blocks, ychunk rows each
 void q4_grid(const Dims &d, int &bx, int &by, int &ychunk);
-/// n Q4 operator launches of one mode as one kernel: D (device, n entries)
-/// and map (device, one (launch, block) pair per block, `blocks` in all)
+/// n Q4 operator launches of one mode as one persistent kernel: D (device, n
+/// entries), map (device, one (launch, block) item per block of each
+/// launch's own grid) and the work queue over those items (batchq.cuh)
 template <typename T>
-void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, int blocks, int mode, bool dot,
-                     cudaStream_t s);
+void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q, int grid,
+                     int mode, bool dot, cudaStream_t s);
+/// CTAs of that persistent launch (by the kernel's occupancy), found once when
+/// the launch is built, outside any stream capture
+template <typename T> int q4_batch_grid(int mode, bool dot, int items);
 
 /// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)
 void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u, float *y,

@@ -21,6 +21,7 @@
 #include <memory>
 
 #include "loopcache.hpp"
+#include "batchq.cuh"
 #include "mg_impl.cuh"
 #include "opt.hpp"
 
@@ -28,15 +29,20 @@ namespace icb
 {
 namespace
 {
-/// block b runs block map[b].y of the launch D[map[b].x] (its own grid)
+/// persistent CTAs take (record, block) items from the queue; block b of a
+/// record is block b of that problem's own launch (its own grid)
 template <class L>
-__global__ void k_batch(const L *__restrict__ D, const int2 *__restrict__ map)
+__global__ void k_batch(const L *__restrict__ D, const int2 *__restrict__ map, BatchQueue q)
 {
-  const int2 m = map[blockIdx.x];
-  const L &l = D[m.x];
-  const unsigned b = unsigned(m.y);
-  const Blk B{b % l.g.gx, (b / l.g.gx) % l.g.gy, b / (l.g.gx * l.g.gy), l.g.gx, l.g.gy, l.g.gz};
-  l.run(B);
+  batch_queue(
+      D, map, q, [](const L &l) { return int(l.g.gx * l.g.gy * l.g.gz); },
+      [](const L &l) { return l.skip(); },
+      [](const L &l, int bi) {
+        const unsigned b = unsigned(bi);
+        const Blk B{b % l.g.gx, (b / l.g.gx) % l.g.gy, b / (l.g.gx * l.g.gy), l.g.gx, l.g.gy,
+                    l.g.gz};
+        l.run(B);
+      });
 }
 
 // the per-problem launches as records: the kernel's arguments and its grid
@@ -51,6 +57,7 @@ template <typename TK, typename TP> struct InitL
   KState *st;
   double tol;
   int maxit;
+  __device__ bool skip() const { return false; }
   __device__ void run(const Blk &B) const { mg_init_b<TK, TP>(n, b, x, r, rP, red, st, tol, maxit, B); }
 };
 template <typename TK, typename TP> struct Init2L
@@ -62,6 +69,7 @@ template <typename TK, typename TP> struct Init2L
   TK *p;
   RedScratch red;
   KState *st;
+  __device__ bool skip() const { return st->stop != 0; }
   __device__ void run(const Blk &B) const { mg_init2_b<TK, TP>(n, r, z, p, red, st, B); }
 };
 template <typename TK, typename TP> struct RL
@@ -75,6 +83,7 @@ template <typename TK, typename TP> struct RL
   const double *pq;
   RedScratch red;
   KState *st;
+  __device__ bool skip() const { return st->stop != 0; }
   __device__ void run(const Blk &B) const { mg_r_b<TK, TP>(n, r, rP, q, z, pq, red, st, B); }
 };
 template <typename TK, typename TP> struct RzL
@@ -85,6 +94,7 @@ template <typename TK, typename TP> struct RzL
   const TP *z;
   RedScratch red;
   KState *st;
+  __device__ bool skip() const { return st->stop || st->conv; }
   __device__ void run(const Blk &B) const { mg_rz_b<TK, TP>(n, r, z, red, st, B); }
 };
 template <typename TK, typename TP> struct XpL
@@ -95,6 +105,7 @@ template <typename TK, typename TP> struct XpL
   const TP *z;
   RedScratch red;
   KState *st;
+  __device__ bool skip() const { return st->stop != 0; }
   __device__ void run(const Blk &B) const { mg_xp_b<TK, TP>(n, x, p, z, red, st, LoopCtl{}, B); }
 };
 template <typename T> struct Jacobi0L
@@ -105,6 +116,7 @@ template <typename T> struct Jacobi0L
   const T *dinv, *b;
   T *x, *x0;
   const KState *gate;
+  __device__ bool skip() const { return gated(gate); }
   __device__ void run(const Blk &B) const { jacobi0_b<T>(n, c, dinv, b, x, x0, gate, B); }
 };
 /// the transfers write each node from its own reads only, so a batched
@@ -120,6 +132,7 @@ template <typename T> struct RestrictL
   const uint8_t *fixc;
   const KState *gate;
   unsigned ry;
+  __device__ bool skip() const { return gated(gate); }
   __device__ void run(const Blk &B) const
   {
     Blk b = B;
@@ -137,6 +150,7 @@ template <typename T> struct ProlongL
   const uint8_t *fixf;
   const KState *gate;
   unsigned ry;
+  __device__ bool skip() const { return gated(gate); }
   __device__ void run(const Blk &B) const
   {
     Blk b = B;
@@ -152,6 +166,7 @@ template <typename T> struct FillL
   long long n;
   T v;
   T *x;
+  __device__ bool skip() const { return false; }
   __device__ void run(const Blk &B) const { fill_b<T>(n, v, x, B); }
 };
 template <typename T> struct DenseL
@@ -163,6 +178,7 @@ template <typename T> struct DenseL
   const T *b;
   T *x;
   const KState *gate;
+  __device__ bool skip() const { return gated(gate); }
   __device__ void run(const Blk &B) const { dense_apply_b<T>(n, A, soa, b, x, gate, B); }
 };
 /// y = x over n entries (the V-cycle's result when the smoothing ends in the
@@ -174,6 +190,7 @@ template <typename T> struct CopyL
   const T *x;
   T *y;
   const KState *gate;
+  __device__ bool skip() const { return gated(gate); }
   __device__ void run(const Blk &B) const
   {
     if(gated(gate))
@@ -191,6 +208,7 @@ template <typename T> struct CoarsenL
   int3 sh;
   const T *Ef;
   T *Ec;
+  __device__ bool skip() const { return false; }
   __device__ void run(const Blk &B) const { coarsen_E_b<T>(df, dc, sh, Ef, Ec, B); }
 };
 template <typename T> struct AssembleL
@@ -202,6 +220,7 @@ template <typename T> struct AssembleL
   const int *dense;
   int n;
   double *A;
+  __device__ bool skip() const { return false; }
   __device__ void run(const Blk &B) const { dense_assemble_b<T>(d, K, E, dense, n, A, B); }
 };
 template <bool SMEM> struct InvertL
@@ -210,6 +229,7 @@ template <bool SMEM> struct InvertL
   int n;
   double *A;
   int *status;
+  __device__ bool skip() const { return false; }
   __device__ void run(const Blk &) const { invert_spd_b<SMEM>(n, A, status); }
 };
 
@@ -247,7 +267,7 @@ template <class L> struct Builder
       map.push_back(make_int2(id, int(b)));
   }
   /// upload and return the launch (empty when no problem takes this step)
-  Launch finish(int threads, int smem, cudaStream_t s)
+  Launch finish(int threads, int smem, cudaStream_t s, unsigned *counters)
   {
     if(recs.empty())
       return {};
@@ -256,9 +276,10 @@ template <class L> struct Builder
     ICB_CUDA(cudaMemcpyAsync(D->p, recs.data(), sizeof(L) * recs.size(), cudaMemcpyHostToDevice, s));
     ICB_CUDA(cudaMemcpyAsync(M->p, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice, s));
     ICB_CUDA(cudaStreamSynchronize(s));
-    const int blocks = int(map.size());
-    return [D, M, blocks, threads, smem](cudaStream_t cs) {
-      k_batch<L><<<blocks, threads, smem, cs>>>(D->p, M->p);
+    BatchQueue q{counters, counters + 1, int(map.size())};
+    const int grid = queue_grid((const void *)k_batch<L>, threads, smem, q.items);
+    return [D, M, q, grid, threads, smem](cudaStream_t cs) {
+      k_batch<L><<<grid, threads, smem, cs>>>(D->p, M->p, q);
       ICB_CUDA(cudaGetLastError());
       count_launch();
     };
@@ -308,7 +329,7 @@ template <typename T> struct Q4Builder
     for(int b = 0; b < q.bx * q.by; b++)
       map.push_back(make_int2(id, b));
   }
-  Launch finish(cudaStream_t s)
+  Launch finish(cudaStream_t s, unsigned *counters)
   {
     if(recs.empty())
       return {};
@@ -318,9 +339,13 @@ template <typename T> struct Q4Builder
                              cudaMemcpyHostToDevice, s));
     ICB_CUDA(cudaMemcpyAsync(M->p, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice, s));
     ICB_CUDA(cudaStreamSynchronize(s));
-    const int blocks = int(map.size()), md = mode;
+    const int md = mode;
     const bool dt = dot;
-    return [D, M, blocks, md, dt](cudaStream_t cs) { launch_q4_batch<T>(D->p, M->p, blocks, md, dt, cs); };
+    BatchQueue q{counters, counters + 1, int(map.size())};
+    const int grid = q4_batch_grid<T>(md, dt, q.items);
+    return [D, M, q, grid, md, dt](cudaStream_t cs) {
+      launch_q4_batch<T>(D->p, M->p, q, grid, md, dt, cs);
+    };
   }
 };
 
@@ -333,6 +358,7 @@ template <typename TP> struct BatchMg
   using MG = MgPcg<double, TP>;
   std::vector<MG *> M;
   std::vector<Launch> refresh, init, iter;
+  DevBuf<unsigned> qc; ///< the work-queue counters every batched launch uses in turn
   DevBuf<KState *> states;
   DevBuf<int> active;
   int *hActive = nullptr;
@@ -387,8 +413,8 @@ template <typename TP> struct BatchMg
           ncmax = std::max(ncmax, m.nc);
         }
       }
-      push(f.finish(VB, 0, s));
-      push(da.finish(256, int(sizeof(double)) * ncmax, s));
+      push(f.finish(VB, 0, s, qc.p));
+      push(da.finish(256, int(sizeof(double)) * ncmax, s, qc.p));
     }
     if(fine.empty())
       return;
@@ -412,7 +438,7 @@ template <typename TP> struct BatchMg
         j0.add(Jacobi0L<TP>{{}, n, TP(m.cc2[0]), L.dinv.p, I.b, cs[k].cur, cs[k].oth, gate(I.i)},
                unsigned(vblocks(n)));
       }
-      push(j0.finish(VB, 0, s));
+      push(j0.finish(VB, 0, s, qc.p));
     }
     auto cheb = [&](int k) {
       Q4Builder<TP> op;
@@ -432,7 +458,7 @@ template <typename TP> struct BatchMg
         op.add(L.d, L.K, L.E, cs[t].cur, cs[t].oth, L.fix, ch);
         std::swap(cs[t].cur, cs[t].oth);
       }
-      push(op.finish(s));
+      push(op.finish(s, qc.p));
     };
     for(int k = 1; k < nu; k++)
       cheb(k);
@@ -457,8 +483,8 @@ template <typename TP> struct BatchMg
                (g3.y + kRowsPerBlock - 1) / kRowsPerBlock, g3.z);
         next.push_back(Inst{I.i, Cn.b.p, Cn.x.p});
       }
-      push(op.finish(s));
-      push(rs.finish(kTB, 0, s));
+      push(op.finish(s, qc.p));
+      push(rs.finish(kTB, 0, s, qc.p));
       emitLevel(l + 1, next, gated, seq, s);
     }
     {
@@ -473,7 +499,7 @@ template <typename TP> struct BatchMg
         pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i), g3.y}, g3.x,
                (g3.y + kRowsPerBlock - 1) / kRowsPerBlock, g3.z);
       }
-      push(pr.finish(kTB, 0, s));
+      push(pr.finish(kTB, 0, s, qc.p));
     }
     for(int k = 0; k < nu; k++)
       cheb(k);
@@ -485,7 +511,7 @@ template <typename TP> struct BatchMg
         const long long n = (long long)L.d.dim * L.d.ld;
         cp.add(CopyL<TP>{{}, n, cs[t].cur, fine[t].out, gate(fine[t].i)}, unsigned(vblocks(n)));
       }
-    push(cp.finish(VB, 0, s));
+    push(cp.finish(VB, 0, s, qc.p));
   }
 
   /// MgPcg::refresh of every problem (coarse moduli level by level, every
@@ -508,7 +534,7 @@ template <typename TP> struct BatchMg
           c.add(CoarsenL<TP>{{}, m->lv[l - 1].d, m->lv[l].d, m->lv[l].sh, m->lv[l - 1].E,
                              m->lv[l].Eown.p},
                 nblocks(m->lv[l].d.nel, 256));
-      push(c.finish(256, 0, s));
+      push(c.finish(256, 0, s, qc.p));
     }
     {
       std::vector<Diag2Launch<TP>> recs;
@@ -534,8 +560,10 @@ template <typename TP> struct BatchMg
       ICB_CUDA(cudaMemcpyAsync(Mp->p, map.data(), sizeof(int2) * map.size(),
                                cudaMemcpyHostToDevice, s));
       ICB_CUDA(cudaStreamSynchronize(s));
-      const int blocks = int(map.size());
-      push([D, Mp, blocks](cudaStream_t cs) { launch_diag2_batch<TP>(D->p, Mp->p, blocks, cs); });
+      BatchQueue q{qc.p, qc.p + 1, int(map.size())};
+      push([D, Mp, q](cudaStream_t cs) { launch_diag2_batch<TP>(D->p, Mp->p, q, cs); });
+      // (the refresh steps run outside any capture: the diagonal launch sizes
+      // its grid when it runs)
     }
     Builder<FillL<double>> zA;
     Builder<FillL<int>> zS;
@@ -568,15 +596,15 @@ template <typename TP> struct BatchMg
       else
         invG.add(InvertL<false>{{}, m->nc, m->cA.p, m->cStatus.p}, 1);
     }
-    push(zA.finish(VB, 0, s));
-    push(zS.finish(VB, 0, s));
-    push(as.finish(128, 0, s));
+    push(zA.finish(VB, 0, s, qc.p));
+    push(zS.finish(VB, 0, s, qc.p));
+    push(as.finish(128, 0, s, qc.p));
     if(smemMax > 0)
       ICB_CUDA(cudaFuncSetAttribute(k_batch<InvertL<true>>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(sizeof(double)) * kInvSmemMax * kInvSmemMax));
-    push(invS.finish(1024, smemMax, s));
-    push(invG.finish(1024, 0, s));
+    push(invS.finish(1024, smemMax, s, qc.p));
+    push(invG.finish(1024, 0, s, qc.p));
   }
 
   /// the step sequences of MgPcg::solve's set-up (init) and of one iteration
@@ -588,6 +616,11 @@ template <typename TP> struct BatchMg
   {
     M = mgs;
     const int n = int(M.size());
+    if(!qc.p)
+    {
+      qc.alloc(2);
+      ICB_CUDA(cudaMemsetAsync(qc.p, 0, 2 * sizeof(unsigned), s));
+    }
     buildRefresh(s);
     init.clear();
     iter.clear();
@@ -606,7 +639,7 @@ template <typename TP> struct BatchMg
                unsigned(vblocks(m.n)));
         all.push_back(Inst{i, m.rin(), m.z.p});
       }
-      push(init, in.finish(VB, 0, s));
+      push(init, in.finish(VB, 0, s, qc.p));
     }
     emitLevel(0, all, false, init, s);
     {
@@ -617,7 +650,7 @@ template <typename TP> struct BatchMg
         in2.add(Init2L<double, TP>{{}, m.n, m.r.p, m.z.p, m.p.p, m.red, m.st.p},
                 unsigned(vblocks(m.n)));
       }
-      push(init, in2.finish(VB, 0, s));
+      push(init, in2.finish(VB, 0, s, qc.p));
     }
     // one iteration (MgPcg::iteration)
     {
@@ -635,8 +668,8 @@ template <typename TP> struct BatchMg
                               m.dots.p, m.red, m.st.p},
                unsigned(vblocks(m.n)));
       }
-      push(iter, op.finish(s));
-      push(iter, rb.finish(VB, 0, s));
+      push(iter, op.finish(s, qc.p));
+      push(iter, rb.finish(VB, 0, s, qc.p));
     }
     emitLevel(0, all, true, iter, s);
     {
@@ -648,8 +681,8 @@ template <typename TP> struct BatchMg
         rz.add(RzL<double, TP>{{}, m.n, m.r.p, m.z.p, m.red, m.st.p}, unsigned(vblocks(m.n)));
         xp.add(XpL<double, TP>{{}, m.n, x[i], m.p.p, m.z.p, m.red, m.st.p}, unsigned(vblocks(m.n)));
       }
-      push(iter, rz.finish(VB, 0, s));
-      push(iter, xp.finish(VB, 0, s));
+      push(iter, rz.finish(VB, 0, s, qc.p));
+      push(iter, xp.finish(VB, 0, s, qc.p));
     }
     std::vector<KState *> sp(n);
     for(int i = 0; i < n; i++)
@@ -684,6 +717,7 @@ template <typename TP> struct BatchMg
 
   /// run the set-up and iterations until every problem has stopped (each
   /// stops at its own tolerance or iteration limit, as its own solve would)
+  long long iterationsRun = 0; ///< iterations of the last run()
   void run(int maxit, cudaStream_t s)
   {
     for(auto &f : refresh)
@@ -700,6 +734,7 @@ template <typename TP> struct BatchMg
       if(*hActive == 0 || launched > (long long)maxit + batch)
         break;
     }
+    iterationsRun = launched;
   }
 };
 
@@ -738,6 +773,10 @@ template struct BatchMg<float>;
 /// sensitivities and adjoint filters, 4 OC updates and the step's wait
 static double g_fused_phase[5];
 double fused_phase_seconds(int k) { return k >= 0 && k < 5 ? g_fused_phase[k] : -1.0; }
+/// iterations of the last fused run: the batch's (every launch sequence
+/// counted once) and the sum over problems of their own
+static long long g_fused_iters[2];
+long long fused_iterations(int k) { return k >= 0 && k < 2 ? g_fused_iters[k] : -1; }
 
 namespace
 {
@@ -805,6 +844,7 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
     maxSteps = std::max(maxSteps, r.o->nsteps);
   for(double &v : g_fused_phase)
     v = 0.0;
+  g_fused_iters[0] = g_fused_iters[1] = 0;
   {
     auto tb = PhaseClock::now();
     rebuild();
@@ -864,6 +904,9 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
                                  cudaMemcpyDeviceToHost, sb));
       ICB_CUDA(cudaStreamSynchronize(sb));
       g_fused_phase[2] += since(tp);
+      g_fused_iters[0] += batch.iterationsRun;
+      for(size_t k = 0; k < set.size(); k++)
+        g_fused_iters[1] += hs[set[k]->idx].iter;
       tp = PhaseClock::now();
       // compliance, V0 (step 1), sensitivities and adjoint filters
       for(OcRun *r : set)

@@ -24,6 +24,7 @@
 // warp shuffle (x) and one shared-memory exchange (y).  No atomics, no
 // colouring, deterministic results.
 #include "icb_internal.hpp"
+#include "batchq.cuh"
 #include "reduce.cuh"
 
 #include <algorithm>
@@ -1001,15 +1002,21 @@ __global__ void __launch_bounds__(TX *TY2)
 /// launch
 template <typename T, bool DOT, int MODE>
 __global__ void __launch_bounds__(TX *TY2)
-    k_matvec_q4_batch(const Q4Launch<T> *__restrict__ D, const int2 *__restrict__ map)
+    k_matvec_q4_batch(const Q4Launch<T> *__restrict__ D, const int2 *__restrict__ map,
+                      BatchQueue bq)
 {
-  const int2 m = map[blockIdx.x];
-  const Q4Launch<T> &q = D[m.x];
-  // the element matrix in registers (constant indices once unrolled), as the
-  // single launch has it in the constant bank
-  const KMat<T, 8> K = q.K;
-  q4_body<T, DOT, MODE>(K, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
-                        q.gateConv, q.ep, m.y % q.bx, m.y / q.bx, q.bx, q.by);
+  batch_queue(
+      D, map, bq, [](const Q4Launch<T> &q) { return q.bx * q.by; },
+      [](const Q4Launch<T> &q) {
+        return q.gate && (q.gate->stop || (q.gateConv && q.gate->conv));
+      },
+      [](const Q4Launch<T> &q, int b) {
+        // the element matrix in registers (constant indices once unrolled),
+        // as the single launch has it in the constant bank
+        const KMat<T, 8> K = q.K;
+        q4_body<T, DOT, MODE>(K, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
+                              q.gateConv, q.ep, b % q.bx, b / q.bx, q.bx, q.by);
+      });
 }
 
 // ------------------------------------------------------------ diagonal ----
@@ -1061,11 +1068,15 @@ __global__ void k_diag(const KMat<T, 24> K, const Dims d, const T *__restrict__ 
 /// many 2D diagonal launches in one (block b runs block map[b].y of launch
 /// D[map[b].x], 256 threads, its own grid of blocks_for(nnode, 256))
 template <typename T>
-__global__ void k_diag2_batch(const Diag2Launch<T> *__restrict__ D, const int2 *__restrict__ map)
+__global__ void k_diag2_batch(const Diag2Launch<T> *__restrict__ D, const int2 *__restrict__ map,
+                              BatchQueue bq)
 {
-  const int2 m = map[blockIdx.x];
-  const Diag2Launch<T> &q = D[m.x];
-  diag_b<T, 2>(q.K, q.d, q.E, q.fix, q.invdiag, nullptr, unsigned(m.y));
+  batch_queue(
+      D, map, bq, [](const Diag2Launch<T> &q) { return int((q.d.nnode + 255) / 256); },
+      [](const Diag2Launch<T> &) { return false; },
+      [](const Diag2Launch<T> &q, int b) {
+        diag_b<T, 2>(q.K, q.d, q.E, q.fix, q.invdiag, nullptr, unsigned(b));
+      });
 }
 
 __global__ void k_gather_free(long long numeq, const long long *__restrict__ idx,
@@ -1503,14 +1514,32 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   count_launch();
 }
 
-template <typename T>
-void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, int blocks, int mode, bool dot,
-                     cudaStream_t s)
+template <typename T> static const void *q4_batch_kernel(int mode, bool dot)
 {
-  if(blocks <= 0)
+  if(mode == OP_APPLY)
+    return dot ? (const void *)k_matvec_q4_batch<T, true, OP_APPLY>
+               : (const void *)k_matvec_q4_batch<T, false, OP_APPLY>;
+  if(mode == OP_RESIDUAL)
+    return (const void *)k_matvec_q4_batch<T, false, OP_RESIDUAL>;
+  if(mode == OP_CHEB)
+    return (const void *)k_matvec_q4_batch<T, false, OP_CHEB>;
+  throw Error{ICB_ERR_BAD_ARG, "batched Q4 operator: unsupported mode"};
+}
+template <typename T> int q4_batch_grid(int mode, bool dot, int items)
+{
+  return queue_grid(q4_batch_kernel<T>(mode, dot), TX * TY2, 0, items);
+}
+template int q4_batch_grid<double>(int, bool, int);
+template int q4_batch_grid<float>(int, bool, int);
+
+template <typename T>
+void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q, int grid,
+                     int mode, bool dot, cudaStream_t s)
+{
+  if(q.items <= 0)
     return;
   const dim3 block(TX, TY2);
-  auto go = [&](auto kern) { kern<<<blocks, block, 0, s>>>(D, map); };
+  auto go = [&](auto kern) { kern<<<grid, block, 0, s>>>(D, map, q); };
   if(mode == OP_APPLY)
     dot ? go(k_matvec_q4_batch<T, true, OP_APPLY>) : go(k_matvec_q4_batch<T, false, OP_APPLY>);
   else if(mode == OP_RESIDUAL)
@@ -1523,22 +1552,24 @@ void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, int blocks, int mode
   count_launch();
 }
 template <typename T>
-void launch_diag2_batch(const Diag2Launch<T> *D, const int2 *map, int blocks, cudaStream_t s)
+void launch_diag2_batch(const Diag2Launch<T> *D, const int2 *map, const BatchQueue &q,
+                        cudaStream_t s)
 {
-  if(blocks <= 0)
+  if(q.items <= 0)
     return;
-  k_diag2_batch<T><<<blocks, 256, 0, s>>>(D, map);
+  const int grid = queue_grid((const void *)k_diag2_batch<T>, 256, 0, q.items);
+  k_diag2_batch<T><<<grid, 256, 0, s>>>(D, map, q);
   ICB_CUDA(cudaGetLastError());
   count_launch();
 }
-template void launch_diag2_batch<double>(const Diag2Launch<double> *, const int2 *, int,
-                                         cudaStream_t);
-template void launch_diag2_batch<float>(const Diag2Launch<float> *, const int2 *, int,
-                                        cudaStream_t);
-template void launch_q4_batch<double>(const Q4Launch<double> *, const int2 *, int, int, bool,
-                                      cudaStream_t);
-template void launch_q4_batch<float>(const Q4Launch<float> *, const int2 *, int, int, bool,
-                                     cudaStream_t);
+template void launch_diag2_batch<double>(const Diag2Launch<double> *, const int2 *,
+                                         const BatchQueue &, cudaStream_t);
+template void launch_diag2_batch<float>(const Diag2Launch<float> *, const int2 *,
+                                        const BatchQueue &, cudaStream_t);
+template void launch_q4_batch<double>(const Q4Launch<double> *, const int2 *,
+                                      const BatchQueue &, int, int, bool, cudaStream_t);
+template void launch_q4_batch<float>(const Q4Launch<float> *, const int2 *, const BatchQueue &,
+                                     int, int, bool, cudaStream_t);
 
 static std::atomic<bool> g_tc_operator{false};
 bool tc_operator_enabled() { return g_tc_operator; }

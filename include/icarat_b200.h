@@ -431,7 +431,9 @@ long long icb_launch_count(void);
  * "fused_phase_us_0" .. "fused_phase_us_4" (wall microseconds of the last
  * fused icb_run_batch: building its batched launches, per-design filter and
  * moduli launches, the batched multigrid set-up and solves, compliance /
- * sensitivities / adjoint filters, OC updates with the step's wait).
+ * sensitivities / adjoint filters, OC updates with the step's wait),
+ * "fused_batch_iters" and "fused_problem_iters" (its solves' iterations: of
+ * the batch, and summed over the designs).
  * Further switches: "hex8_pair" (FP32 Hex8 operator with two element rows per
  * thread), "tc_spin_limit" (polls of a tensor-core wait before it gives up),
  * "batch_fused" (icb_run_batch advances qualifying 2D OC batches together).
