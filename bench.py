@@ -1068,7 +1068,13 @@ def main():
     ap.add_argument("--jobs-per-rate", type=int, default=24)
     ap.add_argument("--iter-scale", type=float, default=0.2, help="serving: scale on U[50,200] steps")
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--max-connections", type=int, default=32,
+                    help="batched / serving: CUDA_DEVICE_MAX_CONNECTIONS (hardware work queues "
+                         "the many per-instance streams map onto; CUDA's default is 8)")
     args = ap.parse_args()
+    if args.workload in ("batched", "serving") and "CUDA_DEVICE_MAX_CONNECTIONS" not in os.environ:
+        # read by CUDA when the context is created, which has not happened yet
+        os.environ["CUDA_DEVICE_MAX_CONNECTIONS"] = str(args.max_connections)
     if args.host_loops and args.impl == "ours":
         import icarat_b200 as icb
         icb.set_option("device_loops", 0)
