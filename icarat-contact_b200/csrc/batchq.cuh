@@ -3,7 +3,8 @@
 //
 // A batched launch is a table of per-problem launch records and a map of
 // items (record, block of that record's own grid) in record order.  The CTAs
-// take chunks of kQueueChunk items from an atomic counter; an item runs that
+// take chunks of items from an atomic counter (one item each while a launch
+// fits in one wave); an item runs that
 // block of that problem's launch.  A problem whose solve has stopped has
 // nothing to do in any of its blocks, so the CTA that meets one of its items
 // skips the rest of that record's items in its chunk at once: converged
@@ -19,8 +20,15 @@ struct BatchQueue
   unsigned *next = nullptr; ///< items handed out
   unsigned *done = nullptr; ///< CTAs that have left
   int items = 0;
+  int chunk = 1; ///< items a CTA takes at a time (queue_chunk)
 };
-constexpr int kQueueChunk = 4;
+/// items per chunk: 1 while every item gets a CTA of its own in one wave
+/// (small launches stay fully parallel), more for launches many waves long,
+/// so a converged problem's items are skipped several at a time
+inline int queue_chunk(int items, int capacity)
+{
+  return std::max(1, std::min(16, items / std::max(1, 2 * capacity)));
+}
 
 /// nb(rec): blocks of a record's own grid; skip(rec): the record's blocks
 /// have nothing to do (read by one thread, the same for the whole record
@@ -34,13 +42,13 @@ __device__ __forceinline__ void batch_queue(const Rec *__restrict__ D, const int
   for(;;)
   {
     if(lead)
-      base = int(atomicAdd(q.next, unsigned(kQueueChunk)));
+      base = int(atomicAdd(q.next, unsigned(q.chunk)));
     __syncthreads();
     const int b0 = base;
     __syncthreads();
     if(b0 >= q.items)
       break;
-    const int b1 = min(b0 + kQueueChunk, q.items);
+    const int b1 = min(b0 + q.chunk, q.items);
     for(int it = b0; it < b1;)
     {
       const int2 m = map[it];
@@ -72,9 +80,9 @@ __device__ __forceinline__ void batch_queue(const Rec *__restrict__ D, const int
   }
 }
 
-/// CTAs of a persistent batched launch: the kernel's residency on every SM,
-/// no more than the chunks there are
-inline int queue_grid(const void *kern, int threads, int smem, int items)
+/// CTAs of a persistent batched launch (the kernel's residency on every SM,
+/// no more than the chunks there are); sets q.chunk
+inline int queue_grid(const void *kern, int threads, int smem, BatchQueue &q)
 {
   int per = 0;
   if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess ||
@@ -83,7 +91,9 @@ inline int queue_grid(const void *kern, int threads, int smem, int items)
     (void)cudaGetLastError();
     per = 1;
   }
-  const int chunks = (items + kQueueChunk - 1) / kQueueChunk;
-  return std::max(1, std::min(per * num_sms(), chunks));
+  const int cap = per * num_sms();
+  q.chunk = queue_chunk(q.items, cap);
+  const int chunks = (q.items + q.chunk - 1) / q.chunk;
+  return std::max(1, std::min(cap, chunks));
 }
 } // namespace icb

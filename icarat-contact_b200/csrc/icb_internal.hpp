@@ -254,7 +254,7 @@ void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q,
                      int mode, bool dot, cudaStream_t s);
 /// CTAs of that persistent launch (by the kernel's occupancy), found once when
 /// the launch is built, outside any stream capture
-template <typename T> int q4_batch_grid(int mode, bool dot, int items);
+template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q);
 
 /// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)
 void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u, float *y,

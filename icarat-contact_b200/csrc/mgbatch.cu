@@ -158,8 +158,9 @@ template <typename T> struct ProlongL
       prolong_add_b<T>(df, dc, sh, xc, xf, fixf, gate, b);
   }
 };
-/// node rows per block of a batched transfer
-constexpr unsigned kRowsPerBlock = 8;
+/// blocks along y of a batched transfer over ry node rows: one row each on
+/// small grids (parallel), eight rows each on large ones (fewer blocks)
+inline unsigned transfer_rows(unsigned ry) { return ry > 256 ? (ry + 7) / 8 : ry; }
 template <typename T> struct FillL
 {
   Blk g;
@@ -277,7 +278,7 @@ template <class L> struct Builder
     ICB_CUDA(cudaMemcpyAsync(M->p, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice, s));
     ICB_CUDA(cudaStreamSynchronize(s));
     BatchQueue q{counters, counters + 1, int(map.size())};
-    const int grid = queue_grid((const void *)k_batch<L>, threads, smem, q.items);
+    const int grid = queue_grid((const void *)k_batch<L>, threads, smem, q);
     return [D, M, q, grid, threads, smem](cudaStream_t cs) {
       k_batch<L><<<grid, threads, smem, cs>>>(D->p, M->p, q);
       ICB_CUDA(cudaGetLastError());
@@ -303,11 +304,12 @@ template <typename T> struct Q4Builder
     std::copy(K, K + 64, q.K.k);
     q.d = d;
     q4_grid(d, q.bx, q.by, q.ychunk);
-    if(!x.dotRed && q.ychunk < kQ4BatchRows)
+    if(!x.dotRed && q.ychunk < kQ4BatchRows && d.sy > 4 * kQ4BatchRows)
     {
       // without a fused dot the operator's output does not depend on how
       // its rows are chunked (every node is the same sum computed by its
-      // owner): fewer, taller chunks, each recomputing one halo row
+      // owner): on large grids fewer, taller chunks, each recomputing one
+      // halo row; small grids keep their many short ones (parallel)
       q.ychunk = std::min(d.sy, kQ4BatchRows);
       q.by = (d.sy + q.ychunk - 1) / q.ychunk;
     }
@@ -342,7 +344,7 @@ template <typename T> struct Q4Builder
     const int md = mode;
     const bool dt = dot;
     BatchQueue q{counters, counters + 1, int(map.size())};
-    const int grid = q4_batch_grid<T>(md, dt, q.items);
+    const int grid = q4_batch_grid<T>(md, dt, q);
     return [D, M, q, grid, md, dt](cudaStream_t cs) {
       launch_q4_batch<T>(D->p, M->p, q, grid, md, dt, cs);
     };
@@ -480,7 +482,7 @@ template <typename TP> struct BatchMg
         op.add(L.d, L.K, L.E, cs[t].cur, L.r.p, L.fix, res);
         const dim3 g3 = grid3(Cn.d);
         rs.add(RestrictL<TP>{{}, L.d, Cn.d, Cn.sh, L.r.p, Cn.b.p, Cn.fix, gate(I.i), g3.y}, g3.x,
-               (g3.y + kRowsPerBlock - 1) / kRowsPerBlock, g3.z);
+               transfer_rows(g3.y), g3.z);
         next.push_back(Inst{I.i, Cn.b.p, Cn.x.p});
       }
       push(op.finish(s, qc.p));
@@ -497,7 +499,7 @@ template <typename TP> struct BatchMg
         Level<TP> &Cn = m.lv[l + 1];
         const dim3 g3 = grid3(L.d);
         pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i), g3.y}, g3.x,
-               (g3.y + kRowsPerBlock - 1) / kRowsPerBlock, g3.z);
+               transfer_rows(g3.y), g3.z);
       }
       push(pr.finish(kTB, 0, s, qc.p));
     }

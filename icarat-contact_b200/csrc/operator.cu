@@ -1011,10 +1011,15 @@ __global__ void __launch_bounds__(TX *TY2)
         return q.gate && (q.gate->stop || (q.gateConv && q.gate->conv));
       },
       [](const Q4Launch<T> &q, int b) {
-        // the element matrix in registers (constant indices once unrolled),
-        // as the single launch has it in the constant bank
-        const KMat<T, 8> K = q.K;
-        q4_body<T, DOT, MODE>(K, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
+        // the element matrix in shared memory: in registers it would take 64
+        // (FP32) or 128 (FP64) of them and a quarter of the occupancy; the
+        // queue's barrier after each item protects it until every thread is done
+        __shared__ KMat<T, 8> sK;
+        const int t = threadIdx.x + blockDim.x * threadIdx.y;
+        if(t < 64)
+          sK.k[t] = q.K.k[t];
+        __syncthreads();
+        q4_body<T, DOT, MODE>(sK, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
                               q.gateConv, q.ep, b % q.bx, b / q.bx, q.bx, q.by);
       });
 }
@@ -1525,12 +1530,12 @@ template <typename T> static const void *q4_batch_kernel(int mode, bool dot)
     return (const void *)k_matvec_q4_batch<T, false, OP_CHEB>;
   throw Error{ICB_ERR_BAD_ARG, "batched Q4 operator: unsupported mode"};
 }
-template <typename T> int q4_batch_grid(int mode, bool dot, int items)
+template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q)
 {
-  return queue_grid(q4_batch_kernel<T>(mode, dot), TX * TY2, 0, items);
+  return queue_grid(q4_batch_kernel<T>(mode, dot), TX * TY2, 0, q);
 }
-template int q4_batch_grid<double>(int, bool, int);
-template int q4_batch_grid<float>(int, bool, int);
+template int q4_batch_grid<double>(int, bool, BatchQueue &);
+template int q4_batch_grid<float>(int, bool, BatchQueue &);
 
 template <typename T>
 void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q, int grid,
@@ -1557,8 +1562,9 @@ void launch_diag2_batch(const Diag2Launch<T> *D, const int2 *map, const BatchQue
 {
   if(q.items <= 0)
     return;
-  const int grid = queue_grid((const void *)k_diag2_batch<T>, 256, 0, q.items);
-  k_diag2_batch<T><<<grid, 256, 0, s>>>(D, map, q);
+  BatchQueue qq = q;
+  const int grid = queue_grid((const void *)k_diag2_batch<T>, 256, 0, qq);
+  k_diag2_batch<T><<<grid, 256, 0, s>>>(D, map, qq);
   ICB_CUDA(cudaGetLastError());
   count_launch();
 }
