@@ -11,10 +11,23 @@
 // problems cost a counter step, not a block launch each.  The last CTA to
 // leave resets the counters for the next launch on the stream.
 #pragma once
+#include <algorithm>
+
 #include "icb_internal.hpp"
 
 namespace icb
 {
+/// a block's coordinates and its grid's extent: blockIdx / gridDim of a
+/// launch of its own, or the block's place in one grid of a batched launch
+struct Blk
+{
+  unsigned x, y, z, gx, gy, gz;
+};
+__device__ __forceinline__ Blk this_block()
+{
+  return Blk{blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z};
+}
+
 struct BatchQueue
 {
   unsigned *next = nullptr; ///< items handed out

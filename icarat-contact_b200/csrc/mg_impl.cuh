@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "batchq.cuh"
 #include "graphloop.hpp"
 #include "loopcache.hpp"
 #include "mg.hpp"
@@ -28,16 +29,6 @@ inline dim3 grid3(const Dims &d)
 {
   ICB_REQUIRE(d.sy <= 65535 && d.sz <= 65535, "grid too large for the transfer launch");
   return dim3(unsigned((d.sx + kTB - 1) / kTB), unsigned(d.sy), unsigned(d.sz));
-}
-/// a block's coordinates and its grid's extent: blockIdx / gridDim of a
-/// launch of its own, or the block's place in one grid of a batched launch
-struct Blk
-{
-  unsigned x, y, z, gx, gy, gz;
-};
-__device__ __forceinline__ Blk this_block()
-{
-  return Blk{blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z};
 }
 __device__ __forceinline__ bool gated(const KState *g)
 {

@@ -815,9 +815,11 @@ template <typename TP>
 void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
 {
   BatchMg<TP> batch;
+  OcBatch ocb;
   std::vector<OcRun *> set;
   auto rebuild = [&]() {
     set.clear();
+    std::vector<OcBatchItem> ocItems;
     std::vector<MgPcg<double, TP> *> mgs;
     std::vector<const double *> b;
     std::vector<double *> x;
@@ -832,9 +834,14 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
         x.push_back(r.p->x.p);
         tol.push_back(r.o->solve.tol);
         maxit.push_back(r.o->solve.maxit);
+        ocItems.push_back(OcBatchItem{r.cone, r.oc, r.x->p, r.dcf->p, r.dvf->p, r.lo->p, r.hi->p,
+                                      r.V->p});
       }
     if(!set.empty())
+    {
       batch.build(mgs, b, x, tol, maxit, sb);
+      ocb.build(ocItems, sb);
+    }
   };
   auto fail = [&](OcRun &r, int st, const std::string &msg) {
     r.active = false;
@@ -958,23 +965,45 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
           }
       g_fused_phase[3] += since(tp);
       tp = PhaseClock::now();
-      // the OC updates, then one wait for every problem
+      // the OC updates: every problem's bisection as one batched sequence
+      // (OcBatch) when all of the set is still running, else problem by
+      // problem; then one wait
+      auto ocParams = [&](const OcRun *r) {
+        OcParams P;
+        P.move = r->o->move_limit;
+        P.beta = r->o->use_threshold ? std::min(std::pow(2.0, (int)(step / 40)), 16.0) : 0.0;
+        return P;
+      };
+      bool allActive = true;
       for(OcRun *r : set)
-        if(r->active)
+        allActive = allActive && r->active;
+      if(allActive)
+      {
+        std::vector<double> g;
+        std::vector<OcParams> P;
+        for(OcRun *r : set)
         {
-          OcParams P;
-          P.move = r->o->move_limit;
-          P.beta = r->o->use_threshold ? std::min(std::pow(2.0, (int)(step / 40)), 16.0) : 0.0;
-          r->oc->launch(r->cone, r->x->p, r->dcf->p, r->dvf->p, r->V0, r->lo->p, r->hi->p,
-                        r->V->p, P, r->p->stream());
+          ICB_CUDA(cudaEventRecord(ev[r->idx], r->p->stream()));
+          ICB_CUDA(cudaStreamWaitEvent(sb, ev[r->idx], 0));
+          g.push_back(r->V0);
+          P.push_back(ocParams(r));
         }
+        ocb.update(g, P, sb);
+      }
+      else
+      {
+        for(OcRun *r : set)
+          if(r->active)
+            r->oc->launch(r->cone, r->x->p, r->dcf->p, r->dvf->p, r->V0, r->lo->p, r->hi->p,
+                          r->V->p, ocParams(r), r->p->stream());
+        for(OcRun *r : set)
+          if(r->active)
+          {
+            ICB_CUDA(cudaStreamSynchronize(r->p->stream()));
+            r->oc->finish();
+          }
+      }
       bool changed = false;
-      for(OcRun *r : set)
-        if(r->active)
-        {
-          ICB_CUDA(cudaStreamSynchronize(r->p->stream()));
-          r->oc->finish();
-        }
       g_fused_phase[4] += since(tp);
       const double dt2 =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

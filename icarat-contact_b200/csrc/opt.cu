@@ -28,6 +28,7 @@
 
 #include "graphloop.hpp"
 #include "opt.hpp"
+#include "batchq.cuh"
 #include "reduce.cuh"
 
 namespace icb
@@ -171,24 +172,30 @@ struct FinOc
   }
 };
 
-/// one bisection step: volume of threshold(filter(x+(lambda))) at st->lam
-__global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__restrict__ w,
-                          int nnb, const double *__restrict__ aa, const double *__restrict__ x,
-                          const double *__restrict__ df, const double *__restrict__ dg,
-                          const double *__restrict__ xmin, const double *__restrict__ xmax,
-                          const double *__restrict__ vol, OcParams P, RedScratch red,
-                          OcState *st, LoopCtl L)
+/// one bisection step: volume of threshold(filter(x+(lambda))) at st->lam,
+/// block B of its grid (the body of k_oc_step and of the batched step)
+__device__ __forceinline__ void oc_step_b(const Dims &d, const int *__restrict__ off,
+                                          const double *__restrict__ w, int nnb,
+                                          const double *__restrict__ aa,
+                                          const double *__restrict__ x,
+                                          const double *__restrict__ df,
+                                          const double *__restrict__ dg,
+                                          const double *__restrict__ xmin,
+                                          const double *__restrict__ xmax,
+                                          const double *__restrict__ vol, const OcParams &P,
+                                          const RedScratch &red, OcState *st, const LoopCtl &L,
+                                          const Blk &B)
 {
   if(st->done)
   {
-    if(blockIdx.x == 0 && threadIdx.x == 0)
+    if(B.x == 0 && threadIdx.x == 0)
       loop_stop(L);
     return;
   }
   const double lam = st->lam;
   double v[1] = {0.0};
-  for(long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < d.nel;
-      e += (long long)gridDim.x * blockDim.x)
+  for(long long e = B.x * (long long)blockDim.x + threadIdx.x; e < d.nel;
+      e += (long long)B.gx * blockDim.x)
   {
     double xf;
     if(P.useFilter)
@@ -211,10 +218,19 @@ __global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__r
     double xh = P.beta > 0.0 ? thresh(xf, P.beta, P.T) : xf;
     v[0] += xh * vol[e];
   }
-  block_reduce<1>(v, red, FinOc{st, L});
+  block_reduce_at<1>(v, red, FinOc{st, L}, int(B.x), int(B.gx));
+}
+__global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__restrict__ w,
+                          int nnb, const double *__restrict__ aa, const double *__restrict__ x,
+                          const double *__restrict__ df, const double *__restrict__ dg,
+                          const double *__restrict__ xmin, const double *__restrict__ xmax,
+                          const double *__restrict__ vol, OcParams P, RedScratch red,
+                          OcState *st, LoopCtl L)
+{
+  oc_step_b(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, P, red, st, L, this_block());
 }
 
-__global__ void k_oc_init(OcState *st, double g, OcParams P)
+__device__ __forceinline__ void oc_init_b(OcState *st, double g)
 {
   st->l0 = 0.0;
   st->l1 = 1.0e4;
@@ -229,7 +245,11 @@ __global__ void k_oc_init(OcState *st, double g, OcParams P)
   st->lam = 0.5 * (st->l1 + st->l0);
   if(!((st->l1 - st->l0) / (st->l1 + st->l0) > st->lambdaeps && st->maxiter > st->counter))
     st->done = 1;
+}
+__global__ void k_oc_init(OcState *st, double g, OcParams P)
+{
   (void)P;
+  oc_init_b(st, g);
 }
 
 /// x = x+(lambda of the last bisection step): OCSolver.hpp keeps the last
@@ -722,6 +742,196 @@ void OcUpdater::launch(const ConeFilter *cone, double *x, const double *df, cons
   k_oc_final<<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d.nel, x, df, dg, xmin, xmax, Pp, st.p);
   ICB_CUDA(cudaGetLastError());
   ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(OcState), cudaMemcpyDeviceToHost, s));
+}
+
+// ========================================================== OC batch =====
+struct OcBatch::Rec
+{
+  Dims d;
+  unsigned gx; ///< blocks of the problem's own step launch (vblocks(nel))
+  const int *off;
+  const double *w;
+  int nnb;
+  const double *aa;
+  double *x;
+  const double *df, *dg, *xmin, *xmax, *vol;
+  OcParams P;
+  RedScratch red;
+  OcState *st;
+  double g;
+};
+
+namespace
+{
+constexpr int kOcStepsPerLaunch = 8;
+
+__global__ void k_oc_init_batch(const OcBatch::Rec *__restrict__ R, int n)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i < n)
+    oc_init_b(R[i].st, R[i].g);
+}
+__global__ void __launch_bounds__(VB)
+    k_oc_step_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
+{
+  batch_queue(
+      R, map, q, [](const OcBatch::Rec &r) { return int(r.gx); },
+      [](const OcBatch::Rec &r) { return r.st->done != 0; },
+      [](const OcBatch::Rec &r, int b) {
+        oc_step_b(r.d, r.off, r.w, r.nnb, r.aa, r.x, r.df, r.dg, r.xmin, r.xmax, r.vol, r.P, r.red,
+                  r.st, LoopCtl{}, Blk{unsigned(b), 0, 0, r.gx, 1, 1});
+      });
+}
+__global__ void __launch_bounds__(256)
+    k_oc_final_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
+{
+  batch_queue(
+      R, map, q, [](const OcBatch::Rec &r) { return int((r.d.nel + 255) / 256); },
+      [](const OcBatch::Rec &) { return false; },
+      [](const OcBatch::Rec &r, int b) {
+        const long long e = b * 256LL + threadIdx.x;
+        if(e < r.d.nel)
+          r.x[e] = oc_candidate(r.x[e], r.df[e], r.dg[e], r.st->lastLam, r.P.eta, r.P.move,
+                                r.xmin[e], r.xmax[e]);
+      });
+}
+/// every problem's state into one array, and the count of updates not done
+__global__ void k_oc_gather(const OcBatch::Rec *__restrict__ R, int n, OcState *out, int *notDone)
+{
+  __shared__ int c;
+  if(threadIdx.x == 0)
+    c = 0;
+  __syncthreads();
+  int mine = 0;
+  for(int i = threadIdx.x; i < n; i += blockDim.x)
+  {
+    out[i] = *R[i].st;
+    mine += R[i].st->done ? 0 : 1;
+  }
+  atomicAdd(&c, mine);
+  __syncthreads();
+  if(threadIdx.x == 0)
+    *notDone = c;
+}
+} // namespace
+
+OcBatch::~OcBatch()
+{
+  if(exec)
+    cudaGraphExecDestroy(exec);
+  if(hst)
+    cudaFreeHost(hst);
+  if(hNotDone)
+    cudaFreeHost(hNotDone);
+}
+
+void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
+{
+  n = int(items.size());
+  recsHost.assign(sizeof(Rec) * std::max(n, 1), 0);
+  Rec *R = reinterpret_cast<Rec *>(recsHost.data());
+  std::vector<int2> ms, mf;
+  for(int i = 0; i < n; i++)
+  {
+    const OcBatchItem &it = items[i];
+    Rec &r = R[i];
+    r.d = it.oc->d;
+    r.gx = unsigned(vblocks(r.d.nel));
+    r.off = it.cone ? it.cone->offs.p : nullptr;
+    r.w = it.cone ? it.cone->wts.p : nullptr;
+    r.nnb = it.cone ? it.cone->nnb : 0;
+    r.aa = it.cone ? it.cone->aa.p : nullptr;
+    r.x = it.x;
+    r.df = it.df;
+    r.dg = it.dg;
+    r.xmin = it.xmin;
+    r.xmax = it.xmax;
+    r.vol = it.vol;
+    r.red = it.oc->red;
+    r.st = it.oc->st.p;
+    for(unsigned b = 0; b < r.gx; b++)
+      ms.push_back(make_int2(i, int(b)));
+    for(long long b = 0; b < (r.d.nel + 255) / 256; b++)
+      mf.push_back(make_int2(i, int(b)));
+  }
+  recs.alloc(recsHost.size());
+  mapStep.alloc(std::max<size_t>(ms.size(), 1));
+  mapFinal.alloc(std::max<size_t>(mf.size(), 1));
+  if(!ms.empty())
+    ICB_CUDA(cudaMemcpyAsync(mapStep.p, ms.data(), sizeof(int2) * ms.size(), cudaMemcpyHostToDevice, s));
+  if(!mf.empty())
+    ICB_CUDA(cudaMemcpyAsync(mapFinal.p, mf.data(), sizeof(int2) * mf.size(), cudaMemcpyHostToDevice, s));
+  if(!qc.p)
+  {
+    qc.alloc(2);
+    ICB_CUDA(cudaMemsetAsync(qc.p, 0, 2 * sizeof(unsigned), s));
+  }
+  states.alloc(std::max(n, 1));
+  notDone.alloc(1);
+  if(hst)
+    cudaFreeHost(hst);
+  ICB_CUDA(cudaMallocHost(&hst, sizeof(OcState) * std::max(n, 1)));
+  if(!hNotDone)
+    ICB_CUDA(cudaMallocHost(&hNotDone, sizeof(int)));
+  BatchQueue qs{qc.p, qc.p + 1, int(ms.size())}, qf{qc.p, qc.p + 1, int(mf.size())};
+  itemsStep = qs.items;
+  itemsFinal = qf.items;
+  gridStep = queue_grid((const void *)k_oc_step_batch, VB, 0, qs);
+  chunkStep = qs.chunk;
+  gridFinal = queue_grid((const void *)k_oc_final_batch, 256, 0, qf);
+  chunkFinal = qf.chunk;
+  ICB_CUDA(cudaStreamSynchronize(s));
+  // kOcStepsPerLaunch bisection steps of every problem and the done count
+  if(exec)
+    cudaGraphExecDestroy(exec);
+  exec = nullptr;
+  cudaStream_t cs;
+  ICB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t gr = nullptr;
+  ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  const Rec *Rd = reinterpret_cast<const Rec *>(recs.p);
+  for(int k = 0; k < kOcStepsPerLaunch; k++)
+    k_oc_step_batch<<<gridStep, VB, 0, cs>>>(Rd, mapStep.p, qs);
+  k_oc_gather<<<1, 256, 0, cs>>>(Rd, n, states.p, notDone.p);
+  ICB_CUDA(cudaMemcpyAsync(hNotDone, notDone.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
+  ICB_CUDA(cudaStreamEndCapture(cs, &gr));
+  ICB_CUDA(cudaGraphInstantiate(&exec, gr, 0));
+  cudaGraphDestroy(gr);
+  cudaStreamDestroy(cs);
+}
+
+void OcBatch::update(const std::vector<double> &g, const std::vector<OcParams> &P, cudaStream_t s)
+{
+  if(n == 0)
+    return;
+  Rec *R = reinterpret_cast<Rec *>(recsHost.data());
+  for(int i = 0; i < n; i++)
+  {
+    R[i].g = g[i];
+    R[i].P = P[i];
+    R[i].P.useFilter = R[i].off != nullptr;
+  }
+  ICB_CUDA(cudaMemcpyAsync(recs.p, recsHost.data(), recsHost.size(), cudaMemcpyHostToDevice, s));
+  const Rec *Rd = reinterpret_cast<const Rec *>(recs.p);
+  k_oc_init_batch<<<(n + 127) / 128, 128, 0, s>>>(Rd, n);
+  ICB_CUDA(cudaGetLastError());
+  count_launch();
+  // at most ICARAT's 100 bisection steps (the updates stop themselves)
+  for(int steps = 0; steps <= 100; steps += kOcStepsPerLaunch)
+  {
+    ICB_CUDA(cudaGraphLaunch(exec, s));
+    count_launch(kOcStepsPerLaunch + 1);
+    ICB_CUDA(cudaStreamSynchronize(s));
+    if(*hNotDone == 0)
+      break;
+  }
+  BatchQueue qf{qc.p, qc.p + 1, itemsFinal, chunkFinal};
+  k_oc_final_batch<<<gridFinal, 256, 0, s>>>(Rd, mapFinal.p, qf);
+  ICB_CUDA(cudaGetLastError());
+  k_oc_gather<<<1, 256, 0, s>>>(Rd, n, states.p, notDone.p);
+  count_launch(2);
+  ICB_CUDA(cudaMemcpyAsync(hst, states.p, sizeof(OcState) * n, cudaMemcpyDeviceToHost, s));
+  ICB_CUDA(cudaStreamSynchronize(s));
 }
 
 // ================================================================ MMA =====

@@ -71,6 +71,42 @@ struct OcUpdater
   int finish();
 };
 
+/// one problem's OC update in a batch: the operands of OcUpdater::update
+struct OcBatchItem
+{
+  const ConeFilter *cone;
+  OcUpdater *oc;
+  double *x;
+  const double *df, *dg, *xmin, *xmax, *vol;
+};
+/// The OC updates of many problems as batched launches (opt.cu): the init,
+/// every bisection step and the final candidate each launched once for all
+/// problems through the work queue; each problem's blocks run exactly its own
+/// update's blocks, so its design is bitwise that of OcUpdater::update.
+struct OcBatch
+{
+  struct Rec; ///< one problem's step launch (opt.cu)
+  int n = 0;
+  std::vector<unsigned char> recsHost; ///< n records
+  DevBuf<unsigned char> recs;
+  DevBuf<int2> mapStep, mapFinal;
+  DevBuf<unsigned> qc;
+  DevBuf<OcState> states;
+  DevBuf<int> notDone;
+  OcState *hst = nullptr;
+  int *hNotDone = nullptr;
+  int gridStep = 0, gridFinal = 0, chunkStep = 1, chunkFinal = 1, itemsStep = 0, itemsFinal = 0;
+  cudaGraphExec_t exec = nullptr; ///< kStepsPerLaunch steps and the done count
+  OcBatch() = default;
+  OcBatch(const OcBatch &) = delete;
+  OcBatch &operator=(const OcBatch &) = delete;
+  ~OcBatch();
+  void build(const std::vector<OcBatchItem> &items, cudaStream_t s);
+  /// the updates with constraint values g[i] and parameters P[i]; returns
+  /// when every update is done (x updated, states in hst)
+  void update(const std::vector<double> &g, const std::vector<OcParams> &P, cudaStream_t s);
+};
+
 /// ICARAT's MMASolver parameters (MMASolver.cpp:41-55)
 struct MmaParams
 {
