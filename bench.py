@@ -1052,8 +1052,9 @@ def main():
     ap.add_argument("--solver", default="mixed_gmg",
                     choices=["fp64_jacobi", "fp64_gmg", "mixed_gmg", "mixed_refine"],
                     help="solve workload: which solver")
-    ap.add_argument("--pair", type=int, default=1, choices=[0, 1],
-                    help="solve workload: FP32 Hex8 operator with two element rows per thread")
+    ap.add_argument("--pair", type=int, default=0, choices=[0, 1],
+                    help="solve workload: FP32 Hex8 operator with two element rows per thread "
+                         "(the library default is the one-row kernel)")
     ap.add_argument("--inner-tol", type=float, default=0.0,
                     help="solve workload, mixed_refine: inner relative tolerance (0: default)")
     ap.add_argument("--repeat", type=int, default=3, help="solve workload: timed solves")

@@ -12,10 +12,11 @@
 //   fused into the forward filter.
 // * OC: OC::UpdateVariables (src/optimization/opt-solver/OCSolver.hpp:20-68)
 //   with the volume callback of opt_macro_oc.cpp:155-164 (re-filter and
-//   re-threshold the candidate).  One kernel per bisection step evaluates the
-//   candidate on the fly inside the filter stencil and reduces its volume;
-//   the last block runs the bisection logic, so a whole update is one CUDA
-//   graph with early exit.
+//   re-threshold the candidate).  A bisection step is two kernels: every
+//   element's candidate once, then the filter stencil over the stored
+//   candidates with the threshold and the volume reduction, whose last block
+//   runs the bisection logic; a whole update is one CUDA graph with early
+//   exit.  Many problems' updates run as batched launches (OcBatch).
 // * MMA: Svanberg's MMA with ICARAT's MMASolver parameters
 //   (MMASolver.cpp:41-55), m = 1: GenSub as one element pass, the dual
 //   interior-point iteration as one fused pass per Newton step (x(lambda),
@@ -172,8 +173,38 @@ struct FinOc
   }
 };
 
+/// the first half of a filtered bisection step: every element's candidate
+/// x+(lambda) at st->lam, once, into xc (the stencil then sums stored
+/// values instead of re-evaluating the candidate, with its division and
+/// square root, for every neighbour); block B of its grid
+__device__ __forceinline__ void oc_cand_b(long long nel, const double *__restrict__ x,
+                                          const double *__restrict__ df,
+                                          const double *__restrict__ dg,
+                                          const double *__restrict__ xmin,
+                                          const double *__restrict__ xmax, const OcParams &P,
+                                          const OcState *st, double *__restrict__ xc,
+                                          const Blk &B)
+{
+  if(st->done)
+    return;
+  const double lam = st->lam;
+  for(long long e = B.x * (long long)blockDim.x + threadIdx.x; e < nel;
+      e += (long long)B.gx * blockDim.x)
+    xc[e] = oc_candidate(x[e], df[e], dg[e], lam, P.eta, P.move, xmin[e], xmax[e]);
+}
+__global__ void k_oc_cand(long long nel, const double *__restrict__ x,
+                          const double *__restrict__ df, const double *__restrict__ dg,
+                          const double *__restrict__ xmin, const double *__restrict__ xmax,
+                          OcParams P, const OcState *st, double *__restrict__ xc)
+{
+  oc_cand_b(nel, x, df, dg, xmin, xmax, P, st, xc, this_block());
+}
+
 /// one bisection step: volume of threshold(filter(x+(lambda))) at st->lam,
-/// block B of its grid (the body of k_oc_step and of the batched step)
+/// block B of its grid (the body of k_oc_step and of the batched step).
+/// With the filter the candidates come from xc (oc_cand_b of this step);
+/// the sum over the stencil takes the same values in the same order as
+/// evaluating each neighbour's candidate in place.
 __device__ __forceinline__ void oc_step_b(const Dims &d, const int *__restrict__ off,
                                           const double *__restrict__ w, int nnb,
                                           const double *__restrict__ aa,
@@ -182,7 +213,8 @@ __device__ __forceinline__ void oc_step_b(const Dims &d, const int *__restrict__
                                           const double *__restrict__ dg,
                                           const double *__restrict__ xmin,
                                           const double *__restrict__ xmax,
-                                          const double *__restrict__ vol, const OcParams &P,
+                                          const double *__restrict__ vol,
+                                          const double *__restrict__ xc, const OcParams &P,
                                           const RedScratch &red, OcState *st, const LoopCtl &L,
                                           const Blk &B)
 {
@@ -209,7 +241,7 @@ __device__ __forceinline__ void oc_step_b(const Dims &d, const int *__restrict__
         if(ii < 0 || jj < 0 || kk < 0 || ii >= d.nx || jj >= d.ny || kk >= d.nz)
           continue;
         long long f = ii + (long long)jj * d.nx + (long long)kk * d.nx * d.ny;
-        s += w[t] * oc_candidate(x[f], df[f], dg[f], lam, P.eta, P.move, xmin[f], xmax[f]);
+        s += w[t] * xc[f];
       }
       xf = s / aa[e];
     }
@@ -224,10 +256,10 @@ __global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__r
                           int nnb, const double *__restrict__ aa, const double *__restrict__ x,
                           const double *__restrict__ df, const double *__restrict__ dg,
                           const double *__restrict__ xmin, const double *__restrict__ xmax,
-                          const double *__restrict__ vol, OcParams P, RedScratch red,
-                          OcState *st, LoopCtl L)
+                          const double *__restrict__ vol, const double *__restrict__ xc,
+                          OcParams P, RedScratch red, OcState *st, LoopCtl L)
 {
-  oc_step_b(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, P, red, st, L, this_block());
+  oc_step_b(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, xc, P, red, st, L, this_block());
 }
 
 __device__ __forceinline__ void oc_init_b(OcState *st, double g)
@@ -682,6 +714,7 @@ OcUpdater::OcUpdater(const Dims &dims, cudaStream_t s) : d(dims)
   counter.alloc(1);
   ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
   red = RedScratch{partials.p, counter.p, nb};
+  cand.alloc(std::max<long long>(d.nel, 1));
   ICB_CUDA(cudaMallocHost(&hst, sizeof(OcState)));
 }
 OcUpdater::~OcUpdater()
@@ -726,14 +759,16 @@ void OcUpdater::launch(const ConeFilter *cone, double *x, const double *df, cons
   const bool dev = device_loops_enabled();
   GraphKey k;
   k.add(off).add(w).add(aa).add((long long)nnb).add(x).add(df).add(dg).add(xmin).add(xmax);
-  k.add(vol).add((const void *)s).addBytes(Pp).add((long long)kernel_switches());
+  k.add(vol).add(cand.p).add((const void *)s).addBytes(Pp).add((long long)kernel_switches());
   if(loop.exec == nullptr || loop.device != dev || k != key)
   {
     // host form: all of ICARAT's 100 steps in one launch, gated after done
     loop.build(
         [&](cudaStream_t cs, const LoopCtl &L) {
-          k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, Pp, red,
-                                       st.p, L);
+          if(Pp.useFilter)
+            k_oc_cand<<<nb, VB, 0, cs>>>(d.nel, x, df, dg, xmin, xmax, Pp, st.p, cand.p);
+          k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, cand.p, Pp,
+                                       red, st.p, L);
         },
         dev, 100);
     key = k;
@@ -755,6 +790,7 @@ struct OcBatch::Rec
   const double *aa;
   double *x;
   const double *df, *dg, *xmin, *xmax, *vol;
+  double *xc; ///< the candidates of the step (the problem's OcUpdater::cand)
   OcParams P;
   RedScratch red;
   OcState *st;
@@ -772,14 +808,25 @@ __global__ void k_oc_init_batch(const OcBatch::Rec *__restrict__ R, int n)
     oc_init_b(R[i].st, R[i].g);
 }
 __global__ void __launch_bounds__(VB)
+    k_oc_cand_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
+{
+  batch_queue(
+      R, map, q, [](const OcBatch::Rec &r) { return int(r.gx); },
+      [](const OcBatch::Rec &r) { return r.st->done != 0 || !r.P.useFilter; },
+      [](const OcBatch::Rec &r, int b) {
+        oc_cand_b(r.d.nel, r.x, r.df, r.dg, r.xmin, r.xmax, r.P, r.st, r.xc,
+                  Blk{unsigned(b), 0, 0, r.gx, 1, 1});
+      });
+}
+__global__ void __launch_bounds__(VB)
     k_oc_step_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
 {
   batch_queue(
       R, map, q, [](const OcBatch::Rec &r) { return int(r.gx); },
       [](const OcBatch::Rec &r) { return r.st->done != 0; },
       [](const OcBatch::Rec &r, int b) {
-        oc_step_b(r.d, r.off, r.w, r.nnb, r.aa, r.x, r.df, r.dg, r.xmin, r.xmax, r.vol, r.P, r.red,
-                  r.st, LoopCtl{}, Blk{unsigned(b), 0, 0, r.gx, 1, 1});
+        oc_step_b(r.d, r.off, r.w, r.nnb, r.aa, r.x, r.df, r.dg, r.xmin, r.xmax, r.vol, r.xc, r.P,
+                  r.red, r.st, LoopCtl{}, Blk{unsigned(b), 0, 0, r.gx, 1, 1});
       });
 }
 __global__ void __launch_bounds__(256)
@@ -847,6 +894,7 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
     r.xmin = it.xmin;
     r.xmax = it.xmax;
     r.vol = it.vol;
+    r.xc = it.oc->cand.p;
     r.red = it.oc->red;
     r.st = it.oc->st.p;
     for(unsigned b = 0; b < r.gx; b++)
@@ -876,6 +924,9 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
   BatchQueue qs{qc.p, qc.p + 1, int(ms.size())}, qf{qc.p, qc.p + 1, int(mf.size())};
   itemsStep = qs.items;
   itemsFinal = qf.items;
+  BatchQueue qa = qs;
+  gridCand = queue_grid((const void *)k_oc_cand_batch, VB, 0, qa);
+  chunkCand = qa.chunk;
   gridStep = queue_grid((const void *)k_oc_step_batch, VB, 0, qs);
   chunkStep = qs.chunk;
   gridFinal = queue_grid((const void *)k_oc_final_batch, 256, 0, qf);
@@ -891,7 +942,10 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
   ICB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
   const Rec *Rd = reinterpret_cast<const Rec *>(recs.p);
   for(int k = 0; k < kOcStepsPerLaunch; k++)
+  {
+    k_oc_cand_batch<<<gridCand, VB, 0, cs>>>(Rd, mapStep.p, qa);
     k_oc_step_batch<<<gridStep, VB, 0, cs>>>(Rd, mapStep.p, qs);
+  }
   k_oc_gather<<<1, 256, 0, cs>>>(Rd, n, states.p, notDone.p);
   ICB_CUDA(cudaMemcpyAsync(hNotDone, notDone.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
   ICB_CUDA(cudaStreamEndCapture(cs, &gr));
@@ -920,7 +974,7 @@ void OcBatch::update(const std::vector<double> &g, const std::vector<OcParams> &
   for(int steps = 0; steps <= 100; steps += kOcStepsPerLaunch)
   {
     ICB_CUDA(cudaGraphLaunch(exec, s));
-    count_launch(kOcStepsPerLaunch + 1);
+    count_launch(2 * kOcStepsPerLaunch + 1);
     ICB_CUDA(cudaStreamSynchronize(s));
     if(*hNotDone == 0)
       break;

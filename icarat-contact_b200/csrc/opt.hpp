@@ -53,6 +53,7 @@ struct OcUpdater
   DevBuf<double> partials;
   DevBuf<unsigned> counter;
   RedScratch red;
+  DevBuf<double> cand; ///< the candidates x+(lambda) of the current step
   OcState *hst = nullptr;
   WhileGraph loop; ///< one bisection step, repeated on the device until done
   GraphKey key;     ///< what `loop` bakes in
@@ -95,7 +96,8 @@ struct OcBatch
   DevBuf<int> notDone;
   OcState *hst = nullptr;
   int *hNotDone = nullptr;
-  int gridStep = 0, gridFinal = 0, chunkStep = 1, chunkFinal = 1, itemsStep = 0, itemsFinal = 0;
+  int gridCand = 0, gridStep = 0, gridFinal = 0, chunkCand = 1, chunkStep = 1, chunkFinal = 1,
+      itemsStep = 0, itemsFinal = 0;
   cudaGraphExec_t exec = nullptr; ///< kStepsPerLaunch steps and the done count
   OcBatch() = default;
   OcBatch(const OcBatch &) = delete;
