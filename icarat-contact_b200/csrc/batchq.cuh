@@ -7,8 +7,9 @@
 // fits in one wave); an item runs that
 // block of that problem's launch.  A problem whose solve has stopped has
 // nothing to do in any of its blocks, so the CTA that meets one of its items
-// skips the rest of that record's items in its chunk at once: converged
-// problems cost a counter step, not a block launch each.  The last CTA to
+// skips the rest of that record's items in its chunk at once and moves the
+// counter past the record's last item: a converged problem costs a few
+// counter steps, not a block launch (or a chunk) each.  The last CTA to
 // leave resets the counters for the next launch on the stream.
 #pragma once
 #include <algorithm>
@@ -67,7 +68,14 @@ __device__ __forceinline__ void batch_queue(const Rec *__restrict__ D, const int
       const int2 m = map[it];
       const Rec &r = D[m.x];
       if(lead)
+      {
         jump = skip(r) ? nb(r) - m.y : 0;
+        // the record's items are contiguous in the map: move the queue past
+        // its last one, so no CTA takes another chunk of it (chunks already
+        // taken skip it here)
+        if(jump > 0)
+          atomicMax(q.next, unsigned(it + jump));
+      }
       __syncthreads();
       const int j = jump;
       __syncthreads();

@@ -42,16 +42,41 @@ inline int vblocks(long long n)
   return int(std::max<long long>(1, std::min<long long>((n + VB - 1) / VB, num_sms() * 8LL)));
 }
 
+/// element e's grid coordinates (the cone filter's grids hold fewer than
+/// 2^31 elements: 32-bit division)
 __device__ __forceinline__ void elemIJK(const Dims &d, long long e, int &i, int &j, int &k)
 {
-  i = int(e % d.nx);
-  j = int((e / d.nx) % d.ny);
-  k = int(e / ((long long)d.nx * d.ny));
+  const unsigned ue = unsigned(e), t = ue / unsigned(d.nx);
+  i = int(ue - t * unsigned(d.nx));
+  j = int(t % unsigned(d.ny));
+  k = int(t / unsigned(d.ny));
+}
+
+/// f(w_t, f_t) for the stencil's neighbours of element (i, j, k) = e that lie
+/// in the grid, in the stencil's order; nb[t] = (di, dj, dk, linear offset)
+template <class F>
+__device__ __forceinline__ void cone_each(const Dims &d, int i, int j, int k, long long e,
+                                          const int4 *__restrict__ nb,
+                                          const double *__restrict__ w, int nnb, F f)
+{
+  for(int t = 0; t < nnb; t++)
+  {
+    const int4 o = __ldg(nb + t);
+    if(unsigned(i + o.x) >= unsigned(d.nx) || unsigned(j + o.y) >= unsigned(d.ny) ||
+       unsigned(k + o.z) >= unsigned(d.nz))
+      continue;
+    f(__ldg(w + t), e + o.w);
+  }
 }
 
 __device__ __forceinline__ double thresh(double x, double beta, double T)
 {
   return 0.5 * (tanh(T * beta) + tanh(beta * (x - T))) / tanh(T * beta);
+}
+/// thresh with tanh(T beta) given (the same value thresh computes)
+__device__ __forceinline__ double thresh_tb(double x, double beta, double T, double tb)
+{
+  return 0.5 * (tb + tanh(beta * (x - T))) / tb;
 }
 __device__ __forceinline__ double thresh_d(double x, double beta, double T)
 {
@@ -60,7 +85,7 @@ __device__ __forceinline__ double thresh_d(double x, double beta, double T)
 }
 
 // ---------------------------------------------------------------- cone ----
-__global__ void k_cone_aa(Dims d, const int *__restrict__ off, const double *__restrict__ w,
+__global__ void k_cone_aa(Dims d, const int4 *__restrict__ nb, const double *__restrict__ w,
                           int nnb, double *__restrict__ aa)
 {
   long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -69,20 +94,14 @@ __global__ void k_cone_aa(Dims d, const int *__restrict__ off, const double *__r
   int i, j, k;
   elemIJK(d, e, i, j, k);
   double s = 0.0;
-  for(int t = 0; t < nnb; t++)
-  {
-    int ii = i + off[3 * t], jj = j + off[3 * t + 1], kk = k + off[3 * t + 2];
-    if(ii < 0 || jj < 0 || kk < 0 || ii >= d.nx || jj >= d.ny || kk >= d.nz)
-      continue;
-    s += w[t];
-  }
+  cone_each(d, i, j, k, e, nb, w, nnb, [&](double wt, long long) { s += wt; });
   aa[e] = s;
 }
 
 /// forward: out = sum w x / aa (+ threshold and its derivative when beta > 0)
 /// adjoint: out = sum w g / aa_j
 template <bool SENS>
-__global__ void k_cone(Dims d, const int *__restrict__ off, const double *__restrict__ w,
+__global__ void k_cone(Dims d, const int4 *__restrict__ nb, const double *__restrict__ w,
                        int nnb, const double *__restrict__ aa, const double *__restrict__ in,
                        double *__restrict__ out, double beta, double T,
                        double *__restrict__ xhat, double *__restrict__ dxhat)
@@ -93,17 +112,12 @@ __global__ void k_cone(Dims d, const int *__restrict__ off, const double *__rest
   int i, j, k;
   elemIJK(d, e, i, j, k);
   double s = 0.0;
-  for(int t = 0; t < nnb; t++)
-  {
-    int ii = i + off[3 * t], jj = j + off[3 * t + 1], kk = k + off[3 * t + 2];
-    if(ii < 0 || jj < 0 || kk < 0 || ii >= d.nx || jj >= d.ny || kk >= d.nz)
-      continue;
-    long long f = ii + (long long)jj * d.nx + (long long)kk * d.nx * d.ny;
+  cone_each(d, i, j, k, e, nb, w, nnb, [&](double wt, long long f) {
     if(SENS)
-      s += w[t] * in[f] / aa[f];
+      s += wt * in[f] / aa[f];
     else
-      s += w[t] * in[f];
-  }
+      s += wt * in[f];
+  });
   double v = SENS ? s : s / aa[e];
   out[e] = v;
   if(!SENS && xhat)
@@ -205,7 +219,7 @@ __global__ void k_oc_cand(long long nel, const double *__restrict__ x,
 /// With the filter the candidates come from xc (oc_cand_b of this step);
 /// the sum over the stencil takes the same values in the same order as
 /// evaluating each neighbour's candidate in place.
-__device__ __forceinline__ void oc_step_b(const Dims &d, const int *__restrict__ off,
+__device__ __forceinline__ void oc_step_b(const Dims &d, const int4 *__restrict__ nb,
                                           const double *__restrict__ w, int nnb,
                                           const double *__restrict__ aa,
                                           const double *__restrict__ x,
@@ -224,7 +238,7 @@ __device__ __forceinline__ void oc_step_b(const Dims &d, const int *__restrict__
       loop_stop(L);
     return;
   }
-  const double lam = st->lam;
+  const double lam = st->lam, tb = st->tanhTb;
   double v[1] = {0.0};
   for(long long e = B.x * (long long)blockDim.x + threadIdx.x; e < d.nel;
       e += (long long)B.gx * blockDim.x)
@@ -235,35 +249,30 @@ __device__ __forceinline__ void oc_step_b(const Dims &d, const int *__restrict__
       int i, j, k;
       elemIJK(d, e, i, j, k);
       double s = 0.0;
-      for(int t = 0; t < nnb; t++)
-      {
-        int ii = i + off[3 * t], jj = j + off[3 * t + 1], kk = k + off[3 * t + 2];
-        if(ii < 0 || jj < 0 || kk < 0 || ii >= d.nx || jj >= d.ny || kk >= d.nz)
-          continue;
-        long long f = ii + (long long)jj * d.nx + (long long)kk * d.nx * d.ny;
-        s += w[t] * xc[f];
-      }
+      cone_each(d, i, j, k, e, nb, w, nnb, [&](double wt, long long f) { s += wt * xc[f]; });
       xf = s / aa[e];
     }
     else
       xf = oc_candidate(x[e], df[e], dg[e], lam, P.eta, P.move, xmin[e], xmax[e]);
-    double xh = P.beta > 0.0 ? thresh(xf, P.beta, P.T) : xf;
+    double xh = P.beta > 0.0 ? thresh_tb(xf, P.beta, P.T, tb) : xf;
     v[0] += xh * vol[e];
   }
   block_reduce_at<1>(v, red, FinOc{st, L}, int(B.x), int(B.gx));
 }
-__global__ void k_oc_step(Dims d, const int *__restrict__ off, const double *__restrict__ w,
+__global__ void k_oc_step(Dims d, const int4 *__restrict__ nb, const double *__restrict__ w,
                           int nnb, const double *__restrict__ aa, const double *__restrict__ x,
                           const double *__restrict__ df, const double *__restrict__ dg,
                           const double *__restrict__ xmin, const double *__restrict__ xmax,
                           const double *__restrict__ vol, const double *__restrict__ xc,
                           OcParams P, RedScratch red, OcState *st, LoopCtl L)
 {
-  oc_step_b(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, xc, P, red, st, L, this_block());
+  oc_step_b(d, nb, w, nnb, aa, x, df, dg, xmin, xmax, vol, xc, P, red, st, L, this_block());
 }
 
-__device__ __forceinline__ void oc_init_b(OcState *st, double g)
+__device__ __forceinline__ void oc_init_b(OcState *st, double g, const OcParams &P)
 {
+  // the threshold's constant tanh(T beta), once per update
+  st->tanhTb = P.beta > 0.0 ? tanh(P.T * P.beta) : 0.0;
   st->l0 = 0.0;
   st->l1 = 1.0e4;
   st->lambdaeps = 1.0e-5;
@@ -278,11 +287,7 @@ __device__ __forceinline__ void oc_init_b(OcState *st, double g)
   if(!((st->l1 - st->l0) / (st->l1 + st->l0) > st->lambdaeps && st->maxiter > st->counter))
     st->done = 1;
 }
-__global__ void k_oc_init(OcState *st, double g, OcParams P)
-{
-  (void)P;
-  oc_init_b(st, g);
-}
+__global__ void k_oc_init(OcState *st, double g, OcParams P) { oc_init_b(st, g, P); }
 
 /// x = x+(lambda of the last bisection step): OCSolver.hpp keeps the last
 /// evaluated candidate, not the midpoint of the final bracket
@@ -669,9 +674,20 @@ ConeFilter::ConeFilter(const Dims &dims, const double *h, double radius, cudaStr
         }
       }
   nnb = int(w.size());
-  offs.alloc(off.size());
+  // (di, dj, dk, linear offset) per neighbour; the kernels index elements in
+  // 32 bits
+  ICB_REQUIRE(d.nel < (1LL << 31), "grid too large for the cone filter");
+  std::vector<int4> nb4(nnb);
+  for(int t = 0; t < nnb; t++)
+  {
+    const long long lo = off[3 * t] + (long long)off[3 * t + 1] * d.nx +
+                         (long long)off[3 * t + 2] * d.nx * d.ny;
+    ICB_REQUIRE(lo > -(1LL << 31) && lo < (1LL << 31), "filter stencil too large");
+    nb4[t] = make_int4(off[3 * t], off[3 * t + 1], off[3 * t + 2], int(lo));
+  }
+  offs.alloc(std::max(nnb, 1));
   wts.alloc(w.size());
-  ICB_CUDA(cudaMemcpyAsync(offs.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s));
+  ICB_CUDA(cudaMemcpyAsync(offs.p, nb4.data(), sizeof(int4) * nnb, cudaMemcpyHostToDevice, s));
   ICB_CUDA(cudaMemcpyAsync(wts.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, s));
   aa.alloc(d.nel);
   k_cone_aa<<<unsigned((d.nel + 255) / 256), 256, 0, s>>>(d, offs.p, wts.p, nnb, aa.p);
@@ -745,7 +761,7 @@ void OcUpdater::launch(const ConeFilter *cone, double *x, const double *df, cons
   const int nb = vblocks(d.nel);
   k_oc_init<<<1, 1, 0, s>>>(st.p, g, P);
   count_launch();
-  const int *off = cone ? cone->offs.p : nullptr;
+  const int4 *off = cone ? cone->offs.p : nullptr;
   const double *w = cone ? cone->wts.p : nullptr;
   const double *aa = cone ? cone->aa.p : nullptr;
   int nnb = cone ? cone->nnb : 0;
@@ -784,7 +800,7 @@ struct OcBatch::Rec
 {
   Dims d;
   unsigned gx; ///< blocks of the problem's own step launch (vblocks(nel))
-  const int *off;
+  const int4 *off;
   const double *w;
   int nnb;
   const double *aa;
@@ -805,9 +821,9 @@ __global__ void k_oc_init_batch(const OcBatch::Rec *__restrict__ R, int n)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if(i < n)
-    oc_init_b(R[i].st, R[i].g);
+    oc_init_b(R[i].st, R[i].g, R[i].P);
 }
-__global__ void __launch_bounds__(VB)
+__global__ void __launch_bounds__(VB, 4)
     k_oc_cand_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
 {
   batch_queue(
@@ -818,7 +834,7 @@ __global__ void __launch_bounds__(VB)
                   Blk{unsigned(b), 0, 0, r.gx, 1, 1});
       });
 }
-__global__ void __launch_bounds__(VB)
+__global__ void __launch_bounds__(VB, 4)
     k_oc_step_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
 {
   batch_queue(

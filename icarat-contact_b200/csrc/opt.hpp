@@ -14,7 +14,7 @@ struct ConeFilter
   Dims d;
   double r;
   int nnb = 0;           ///< neighbours in the stencil
-  DevBuf<int> offs;      ///< (di,dj,dk) per neighbour, element-index order
+  DevBuf<int4> offs;     ///< (di,dj,dk, linear offset) per neighbour, element-index order
   DevBuf<double> wts;    ///< r - distance
   DevBuf<double> aa;     ///< sum of weights per element (dfilters_ds)
 
@@ -42,6 +42,7 @@ struct OcParams
 struct OcState
 {
   double l0, l1, lam, lastLam, lambdaeps, g, vol;
+  double tanhTb; ///< tanh(T beta) of the update's threshold
   int counter, maxiter, done, pad;
 };
 
