@@ -63,26 +63,32 @@ __device__ __forceinline__ void batch_queue(const Rec *__restrict__ D, const int
     if(b0 >= q.items)
       break;
     const int b1 = min(b0 + q.chunk, q.items);
+    int running = -1; // the record of the last item run: not skipped
     for(int it = b0; it < b1;)
     {
       const int2 m = map[it];
       const Rec &r = D[m.x];
-      if(lead)
+      // a record found running stays so while any of its items is pending
+      if(m.x != running)
       {
-        jump = skip(r) ? nb(r) - m.y : 0;
-        // the record's items are contiguous in the map: move the queue past
-        // its last one, so no CTA takes another chunk of it (chunks already
-        // taken skip it here)
-        if(jump > 0)
-          atomicMax(q.next, unsigned(it + jump));
-      }
-      __syncthreads();
-      const int j = jump;
-      __syncthreads();
-      if(j > 0)
-      {
-        it += j;
-        continue;
+        if(lead)
+        {
+          jump = skip(r) ? nb(r) - m.y : 0;
+          // the record's items are contiguous in the map: move the queue
+          // past its last one, so no CTA takes another chunk of it (chunks
+          // already taken skip it here)
+          if(jump > 0)
+            atomicMax(q.next, unsigned(it + jump));
+        }
+        __syncthreads();
+        const int j = jump;
+        __syncthreads();
+        if(j > 0)
+        {
+          it += j;
+          continue;
+        }
+        running = m.x;
       }
       run(r, m.y);
       __syncthreads(); // the bodies' shared memory is reused by the next item

@@ -18,9 +18,15 @@ namespace icb
 namespace
 {
 constexpr int VB = 256;
+/// blocks of a vector kernel over n entries: at least four entries per
+/// thread, at most eight blocks per SM (a batched launch runs each block as
+/// one work item, so small problems do not split into many tiny ones)
+constexpr int kVecPerThread = 4;
 inline int vblocks(long long n)
 {
-  return int(std::max<long long>(1, std::min<long long>((n + VB - 1) / VB, num_sms() * 8LL)));
+  return int(std::max<long long>(
+      1, std::min<long long>((n + VB * kVecPerThread - 1) / (VB * kVecPerThread),
+                             num_sms() * 8LL)));
 }
 inline unsigned nblocks(long long n, int bs) { return unsigned((n + bs - 1) / bs); }
 /// transfer kernels: kTB threads along x, one grid row per (y, z) node line

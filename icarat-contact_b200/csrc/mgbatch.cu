@@ -159,8 +159,9 @@ template <typename T> struct ProlongL
   }
 };
 /// blocks along y of a batched transfer over ry node rows: one row each on
-/// small grids (parallel), eight rows each on large ones (fewer blocks)
-inline unsigned transfer_rows(unsigned ry) { return ry > 256 ? (ry + 7) / 8 : ry; }
+/// grids of up to 16 rows, eight rows each on taller ones (fewer, larger
+/// work items)
+inline unsigned transfer_rows(unsigned ry) { return ry > 16 ? (ry + 7) / 8 : ry; }
 template <typename T> struct FillL
 {
   Blk g;
@@ -288,7 +289,7 @@ template <class L> struct Builder
 };
 
 /// rows per block of a batched Q4 operator launch without a fused dot
-constexpr int kQ4BatchRows = 16;
+constexpr int kQ4BatchRows = 32;
 
 /// the Q4 operator launches of one step (k_matvec_q4_batch)
 template <typename T> struct Q4Builder
@@ -304,7 +305,7 @@ template <typename T> struct Q4Builder
     std::copy(K, K + 64, q.K.k);
     q.d = d;
     q4_grid(d, q.bx, q.by, q.ychunk);
-    if(!x.dotRed && q.ychunk < kQ4BatchRows && d.sy > 4 * kQ4BatchRows)
+    if(!x.dotRed && q.ychunk < kQ4BatchRows && d.sy > 2 * kQ4BatchRows)
     {
       // without a fused dot the operator's output does not depend on how
       // its rows are chunked (every node is the same sum computed by its

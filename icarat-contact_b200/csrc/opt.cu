@@ -269,6 +269,98 @@ __global__ void k_oc_step(Dims d, const int4 *__restrict__ nb, const double *__r
   oc_step_b(d, nb, w, nnb, aa, x, df, dg, xmin, xmax, vol, xc, P, red, st, L, this_block());
 }
 
+/// The filtered bisection step on a 2D grid, one kOcTW x kOcTH tile of
+/// elements per block (256 threads, four rows each): the tile's candidates
+/// with a halo of (hx, hy) elements are staged in shared memory (zero outside
+/// the grid, which adds exactly nothing) with the stencil as shared-memory
+/// offsets, so each neighbour costs a shared load and an FMA instead of
+/// bounds checks and a dependent global load.  Each element sums its
+/// neighbours in the stencil's order, as oc_step_b does; the tile of block
+/// B.x is (B.x mod ntx, B.x div ntx).
+constexpr int kOcTW = 32, kOcTH = 32, kOcHalo = 8;
+__host__ __device__ constexpr int oc_tile_smem(int hx, int hy, int nnb)
+{
+  return 8 * ((kOcTW + 2 * hx) * (kOcTH + 2 * hy) + nnb) + 4 * nnb;
+}
+__device__ __forceinline__ void oc_step_tile_b(const Dims &d, int hx, int hy, unsigned ntx,
+                                               const int4 *__restrict__ nb,
+                                               const double *__restrict__ w, int nnb,
+                                               const double *__restrict__ aa,
+                                               const double *__restrict__ vol,
+                                               const double *__restrict__ xc, const OcParams &P,
+                                               const RedScratch &red, OcState *st,
+                                               const LoopCtl &L, const Blk &B,
+                                               unsigned char *smem)
+{
+  if(st->done)
+  {
+    if(B.x == 0 && threadIdx.x == 0)
+      loop_stop(L);
+    return;
+  }
+  const double tb = st->tanhTb;
+  const int TWP = kOcTW + 2 * hx, THP = kOcTH + 2 * hy;
+  double *tile = reinterpret_cast<double *>(smem);
+  double *sw = tile + TWP * THP;
+  int *so = reinterpret_cast<int *>(sw + nnb);
+  const int x0 = int(B.x % ntx) * kOcTW, y0 = int(B.x / ntx) * kOcTH;
+  for(int q = threadIdx.x; q < TWP * THP; q += blockDim.x)
+  {
+    const int ty = q / TWP, tx = q - ty * TWP;
+    const int i = x0 - hx + tx, j = y0 - hy + ty;
+    tile[q] = unsigned(i) < unsigned(d.nx) && unsigned(j) < unsigned(d.ny)
+                  ? __ldg(xc + i + (long long)j * d.nx)
+                  : 0.0;
+  }
+  for(int t = threadIdx.x; t < nnb; t += blockDim.x)
+  {
+    const int4 o = __ldg(nb + t);
+    so[t] = o.y * TWP + o.x;
+    sw[t] = __ldg(w + t);
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  constexpr int kRows = kOcTH / 8;
+  const double *c0 = tile + (ty + hy) * TWP + tx + hx;
+  const int rs = 8 * TWP;
+  double acc[kRows];
+#pragma unroll
+  for(int k = 0; k < kRows; k++)
+    acc[k] = 0.0;
+  for(int t = 0; t < nnb; t++)
+  {
+    const double wt = sw[t];
+    const double *c = c0 + so[t];
+#pragma unroll
+    for(int k = 0; k < kRows; k++)
+      acc[k] += wt * c[k * rs];
+  }
+  double v[1] = {0.0};
+#pragma unroll
+  for(int k = 0; k < kRows; k++)
+  {
+    const int i = x0 + tx, j = y0 + ty + 8 * k;
+    if(i < d.nx && j < d.ny)
+    {
+      const long long e = i + (long long)j * d.nx;
+      const double xf = acc[k] / aa[e];
+      const double xh = P.beta > 0.0 ? thresh_tb(xf, P.beta, P.T, tb) : xf;
+      v[0] += xh * vol[e];
+    }
+  }
+  block_reduce_at<1>(v, red, FinOc{st, L}, int(B.x), int(B.gx));
+}
+__global__ void __launch_bounds__(VB)
+    k_oc_step_tile(Dims d, int hx, int hy, unsigned ntx, const int4 *__restrict__ nb,
+                   const double *__restrict__ w, int nnb, const double *__restrict__ aa,
+                   const double *__restrict__ vol, const double *__restrict__ xc, OcParams P,
+                   RedScratch red, OcState *st, LoopCtl L)
+{
+  extern __shared__ __align__(16) unsigned char oc_tile_dyn[];
+  oc_step_tile_b(d, hx, hy, ntx, nb, w, nnb, aa, vol, xc, P, red, st, L, this_block(),
+                 oc_tile_dyn);
+}
+
 __device__ __forceinline__ void oc_init_b(OcState *st, double g, const OcParams &P)
 {
   // the threshold's constant tanh(T beta), once per update
@@ -684,6 +776,8 @@ ConeFilter::ConeFilter(const Dims &dims, const double *h, double radius, cudaStr
                          (long long)off[3 * t + 2] * d.nx * d.ny;
     ICB_REQUIRE(lo > -(1LL << 31) && lo < (1LL << 31), "filter stencil too large");
     nb4[t] = make_int4(off[3 * t], off[3 * t + 1], off[3 * t + 2], int(lo));
+    hx = std::max(hx, std::abs(off[3 * t]));
+    hy = std::max(hy, std::abs(off[3 * t + 1]));
   }
   offs.alloc(std::max(nnb, 1));
   wts.alloc(w.size());
@@ -722,10 +816,41 @@ void launch_threshold(long long n, const double *x, double beta, double T, doubl
 }
 
 // ================================================================= OC =====
+namespace
+{
+/// the form of a problem's bisection step: 2D grids with a cone filter whose
+/// halo fits kOcHalo take the tiled kernel (one block per tile), the rest the
+/// element-strided one (vblocks)
+struct OcTiling
+{
+  bool tiled = false;
+  int hx = 0, hy = 0, smem = 0, blocks = 0;
+  unsigned ntx = 0;
+};
+OcTiling oc_tiling(const Dims &d, const ConeFilter *cone)
+{
+  OcTiling t;
+  if(!cone || d.dim != 2 || cone->hx > kOcHalo || cone->hy > kOcHalo)
+    return t;
+  t.tiled = true;
+  t.hx = cone->hx;
+  t.hy = cone->hy;
+  t.smem = oc_tile_smem(t.hx, t.hy, cone->nnb);
+  t.ntx = unsigned((d.nx + kOcTW - 1) / kOcTW);
+  t.blocks = int(t.ntx) * ((d.ny + kOcTH - 1) / kOcTH);
+  return t;
+}
+} // namespace
+
 OcUpdater::OcUpdater(const Dims &dims, cudaStream_t s) : d(dims)
 {
   st.alloc(1);
-  int nb = vblocks(d.nel);
+  // enough partials for either form of the step: the element-strided grid
+  // and the 2D tiles
+  const long long tiles =
+      d.dim == 2 ? ((d.nx + kOcTW - 1) / kOcTW) * (long long)((d.ny + kOcTH - 1) / kOcTH) : 0;
+  ICB_REQUIRE(tiles < (1LL << 31), "grid too large for the OC update");
+  const int nb = std::max(vblocks(d.nel), int(tiles));
   partials.alloc(nb);
   counter.alloc(1);
   ICB_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), s));
@@ -767,6 +892,8 @@ void OcUpdater::launch(const ConeFilter *cone, double *x, const double *df, cons
   int nnb = cone ? cone->nnb : 0;
   OcParams Pp = P;
   Pp.useFilter = cone != nullptr;
+  const OcTiling tl = oc_tiling(d, cone);
+  const int sb = tl.tiled ? tl.blocks : nb;
   // graph of the bisection: one step as the body of a conditional WHILE node
   // that the device repeats until done (at most maxiter = 100 steps), rebuilt
   // when anything it bakes in changes -- the stencil's device buffers and
@@ -783,8 +910,12 @@ void OcUpdater::launch(const ConeFilter *cone, double *x, const double *df, cons
         [&](cudaStream_t cs, const LoopCtl &L) {
           if(Pp.useFilter)
             k_oc_cand<<<nb, VB, 0, cs>>>(d.nel, x, df, dg, xmin, xmax, Pp, st.p, cand.p);
-          k_oc_step<<<nb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, cand.p, Pp,
-                                       red, st.p, L);
+          if(tl.tiled)
+            k_oc_step_tile<<<sb, VB, tl.smem, cs>>>(d, tl.hx, tl.hy, tl.ntx, off, w, nnb, aa, vol,
+                                                    cand.p, Pp, red, st.p, L);
+          else
+            k_oc_step<<<sb, VB, 0, cs>>>(d, off, w, nnb, aa, x, df, dg, xmin, xmax, vol, cand.p,
+                                         Pp, red, st.p, L);
         },
         dev, 100);
     key = k;
@@ -799,7 +930,10 @@ void OcUpdater::launch(const ConeFilter *cone, double *x, const double *df, cons
 struct OcBatch::Rec
 {
   Dims d;
-  unsigned gx; ///< blocks of the problem's own step launch (vblocks(nel))
+  unsigned gx;  ///< blocks of the problem's own step launch (tiles or vblocks(nel))
+  unsigned gxc; ///< blocks of its candidate launch (vblocks(nel))
+  int tiled, hx, hy;
+  unsigned ntx;
   const int4 *off;
   const double *w;
   int nnb;
@@ -827,22 +961,28 @@ __global__ void __launch_bounds__(VB, 4)
     k_oc_cand_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
 {
   batch_queue(
-      R, map, q, [](const OcBatch::Rec &r) { return int(r.gx); },
+      R, map, q, [](const OcBatch::Rec &r) { return int(r.gxc); },
       [](const OcBatch::Rec &r) { return r.st->done != 0 || !r.P.useFilter; },
       [](const OcBatch::Rec &r, int b) {
         oc_cand_b(r.d.nel, r.x, r.df, r.dg, r.xmin, r.xmax, r.P, r.st, r.xc,
-                  Blk{unsigned(b), 0, 0, r.gx, 1, 1});
+                  Blk{unsigned(b), 0, 0, r.gxc, 1, 1});
       });
 }
 __global__ void __launch_bounds__(VB, 4)
     k_oc_step_batch(const OcBatch::Rec *__restrict__ R, const int2 *__restrict__ map, BatchQueue q)
 {
+  extern __shared__ __align__(16) unsigned char oc_batch_dyn[];
   batch_queue(
       R, map, q, [](const OcBatch::Rec &r) { return int(r.gx); },
       [](const OcBatch::Rec &r) { return r.st->done != 0; },
       [](const OcBatch::Rec &r, int b) {
-        oc_step_b(r.d, r.off, r.w, r.nnb, r.aa, r.x, r.df, r.dg, r.xmin, r.xmax, r.vol, r.xc, r.P,
-                  r.red, r.st, LoopCtl{}, Blk{unsigned(b), 0, 0, r.gx, 1, 1});
+        const Blk B{unsigned(b), 0, 0, r.gx, 1, 1};
+        if(r.tiled)
+          oc_step_tile_b(r.d, r.hx, r.hy, r.ntx, r.off, r.w, r.nnb, r.aa, r.vol, r.xc, r.P, r.red,
+                         r.st, LoopCtl{}, B, oc_batch_dyn);
+        else
+          oc_step_b(r.d, r.off, r.w, r.nnb, r.aa, r.x, r.df, r.dg, r.xmin, r.xmax, r.vol, r.xc,
+                    r.P, r.red, r.st, LoopCtl{}, B);
       });
 }
 __global__ void __launch_bounds__(256)
@@ -893,13 +1033,21 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
   n = int(items.size());
   recsHost.assign(sizeof(Rec) * std::max(n, 1), 0);
   Rec *R = reinterpret_cast<Rec *>(recsHost.data());
-  std::vector<int2> ms, mf;
+  std::vector<int2> ms, mc, mf;
+  smemStep = 0;
   for(int i = 0; i < n; i++)
   {
     const OcBatchItem &it = items[i];
     Rec &r = R[i];
     r.d = it.oc->d;
-    r.gx = unsigned(vblocks(r.d.nel));
+    const OcTiling tl = oc_tiling(r.d, it.cone);
+    r.gxc = unsigned(vblocks(r.d.nel));
+    r.gx = tl.tiled ? unsigned(tl.blocks) : r.gxc;
+    r.tiled = tl.tiled;
+    r.hx = tl.hx;
+    r.hy = tl.hy;
+    r.ntx = tl.ntx;
+    smemStep = std::max(smemStep, tl.smem);
     r.off = it.cone ? it.cone->offs.p : nullptr;
     r.w = it.cone ? it.cone->wts.p : nullptr;
     r.nnb = it.cone ? it.cone->nnb : 0;
@@ -915,11 +1063,16 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
     r.st = it.oc->st.p;
     for(unsigned b = 0; b < r.gx; b++)
       ms.push_back(make_int2(i, int(b)));
+    for(unsigned b = 0; b < r.gxc; b++)
+      mc.push_back(make_int2(i, int(b)));
     for(long long b = 0; b < (r.d.nel + 255) / 256; b++)
       mf.push_back(make_int2(i, int(b)));
   }
   recs.alloc(recsHost.size());
   mapStep.alloc(std::max<size_t>(ms.size(), 1));
+  mapCand.alloc(std::max<size_t>(mc.size(), 1));
+  if(!mc.empty())
+    ICB_CUDA(cudaMemcpyAsync(mapCand.p, mc.data(), sizeof(int2) * mc.size(), cudaMemcpyHostToDevice, s));
   mapFinal.alloc(std::max<size_t>(mf.size(), 1));
   if(!ms.empty())
     ICB_CUDA(cudaMemcpyAsync(mapStep.p, ms.data(), sizeof(int2) * ms.size(), cudaMemcpyHostToDevice, s));
@@ -938,12 +1091,12 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
   if(!hNotDone)
     ICB_CUDA(cudaMallocHost(&hNotDone, sizeof(int)));
   BatchQueue qs{qc.p, qc.p + 1, int(ms.size())}, qf{qc.p, qc.p + 1, int(mf.size())};
+  BatchQueue qa{qc.p, qc.p + 1, int(mc.size())};
   itemsStep = qs.items;
   itemsFinal = qf.items;
-  BatchQueue qa = qs;
   gridCand = queue_grid((const void *)k_oc_cand_batch, VB, 0, qa);
   chunkCand = qa.chunk;
-  gridStep = queue_grid((const void *)k_oc_step_batch, VB, 0, qs);
+  gridStep = queue_grid((const void *)k_oc_step_batch, VB, smemStep, qs);
   chunkStep = qs.chunk;
   gridFinal = queue_grid((const void *)k_oc_final_batch, 256, 0, qf);
   chunkFinal = qf.chunk;
@@ -959,8 +1112,8 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
   const Rec *Rd = reinterpret_cast<const Rec *>(recs.p);
   for(int k = 0; k < kOcStepsPerLaunch; k++)
   {
-    k_oc_cand_batch<<<gridCand, VB, 0, cs>>>(Rd, mapStep.p, qa);
-    k_oc_step_batch<<<gridStep, VB, 0, cs>>>(Rd, mapStep.p, qs);
+    k_oc_cand_batch<<<gridCand, VB, 0, cs>>>(Rd, mapCand.p, qa);
+    k_oc_step_batch<<<gridStep, VB, smemStep, cs>>>(Rd, mapStep.p, qs);
   }
   k_oc_gather<<<1, 256, 0, cs>>>(Rd, n, states.p, notDone.p);
   ICB_CUDA(cudaMemcpyAsync(hNotDone, notDone.p, sizeof(int), cudaMemcpyDeviceToHost, cs));

@@ -14,6 +14,7 @@ struct ConeFilter
   Dims d;
   double r;
   int nnb = 0;           ///< neighbours in the stencil
+  int hx = 0, hy = 0;    ///< the stencil's largest |di|, |dj|
   DevBuf<int4> offs;     ///< (di,dj,dk, linear offset) per neighbour, element-index order
   DevBuf<double> wts;    ///< r - distance
   DevBuf<double> aa;     ///< sum of weights per element (dfilters_ds)
@@ -91,7 +92,8 @@ struct OcBatch
   int n = 0;
   std::vector<unsigned char> recsHost; ///< n records
   DevBuf<unsigned char> recs;
-  DevBuf<int2> mapStep, mapFinal;
+  DevBuf<int2> mapStep, mapCand, mapFinal;
+  int smemStep = 0; ///< dynamic shared memory of the step launch (tiled problems)
   DevBuf<unsigned> qc;
   DevBuf<OcState> states;
   DevBuf<int> notDone;
