@@ -46,7 +46,9 @@ inline int queue_chunk(int items, int capacity)
 
 /// nb(rec): blocks of a record's own grid; skip(rec): the record's blocks
 /// have nothing to do (read by one thread, the same for the whole record
-/// while any of its blocks is pending); run(rec, b): block b of the record
+/// while any of its blocks is pending); run(rec, b, fresh): block b of the
+/// record, fresh when the CTA's previous item was of another record (what
+/// a body stages per record in shared memory survives until then)
 template <class Rec, class Nb, class Skip, class Run>
 __device__ __forceinline__ void batch_queue(const Rec *__restrict__ D, const int2 *__restrict__ map,
                                             const BatchQueue &q, Nb nb, Skip skip, Run run)
@@ -69,7 +71,8 @@ __device__ __forceinline__ void batch_queue(const Rec *__restrict__ D, const int
       const int2 m = map[it];
       const Rec &r = D[m.x];
       // a record found running stays so while any of its items is pending
-      if(m.x != running)
+      const bool fresh = m.x != running;
+      if(fresh)
       {
         if(lead)
         {
@@ -90,7 +93,7 @@ __device__ __forceinline__ void batch_queue(const Rec *__restrict__ D, const int
         }
         running = m.x;
       }
-      run(r, m.y);
+      run(r, m.y, fresh);
       __syncthreads(); // the bodies' shared memory is reused by the next item
       ++it;
     }

@@ -255,6 +255,10 @@ void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q,
 /// CTAs of that persistent launch (by the kernel's occupancy), found once when
 /// the launch is built, outside any stream capture
 template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q);
+/// warps of one block of the Q4 operator, and the resident warps of its
+/// batched launch on the whole GPU
+int q4_block_warps();
+template <typename T> long long q4_batch_capacity_warps(int mode, bool dot);
 
 /// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)
 void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u, float *y,

@@ -37,7 +37,7 @@ __global__ void k_batch(const L *__restrict__ D, const int2 *__restrict__ map, B
   batch_queue(
       D, map, q, [](const L &l) { return int(l.g.gx * l.g.gy * l.g.gz); },
       [](const L &l) { return l.skip(); },
-      [](const L &l, int bi) {
+      [](const L &l, int bi, bool) {
         const unsigned b = unsigned(bi);
         const Blk B{b % l.g.gx, (b / l.g.gx) % l.g.gy, b / (l.g.gx * l.g.gy), l.g.gx, l.g.gy,
                     l.g.gz};
@@ -158,10 +158,21 @@ template <typename T> struct ProlongL
       prolong_add_b<T>(df, dc, sh, xc, xf, fixf, gate, b);
   }
 };
-/// blocks along y of a batched transfer over ry node rows: one row each on
-/// grids of up to 16 rows, eight rows each on taller ones (fewer, larger
-/// work items)
-inline unsigned transfer_rows(unsigned ry) { return ry > 16 ? (ry + 7) / 8 : ry; }
+/// Rows per work item of a batched launch whose rows are independent: one
+/// while the launch's rows (`rows`, over every problem) fill the GPU's
+/// resident warps twice (`capacity`), more as they exceed it, at most `most`.
+/// A work item walks its rows in sequence, so on small (coarse) launches one
+/// row each keeps them short and parallel, and on large ones several rows
+/// each keep the per-item overhead small.
+inline unsigned rows_per_item(long long rows, long long capacity, unsigned most)
+{
+  const long long r = rows / std::max(1LL, 2 * capacity);
+  return unsigned(std::max(1LL, std::min<long long>(most, r)));
+}
+/// blocks along y of a batched transfer over ry node rows, k rows each
+inline unsigned transfer_rows(unsigned ry, unsigned k) { return (ry + k - 1) / k; }
+/// resident CTAs of a transfer launch (kTB threads) on the whole GPU
+inline long long transfer_capacity() { return num_sms() * 16LL; }
 template <typename T> struct FillL
 {
   Blk g;
@@ -288,14 +299,13 @@ template <class L> struct Builder
   }
 };
 
-/// rows per block of a batched Q4 operator launch without a fused dot
-constexpr int kQ4BatchRows = 32;
+/// most rows per work item of a batched Q4 operator launch without a fused dot
+constexpr unsigned kQ4BatchRows = 16;
 
 /// the Q4 operator launches of one step (k_matvec_q4_batch)
 template <typename T> struct Q4Builder
 {
   std::vector<Q4Launch<T>> recs;
-  std::vector<int2> map;
   int mode = OP_APPLY;
   bool dot = false;
   void add(const Dims &d, const T *K, const T *E, const T *u, T *y, const uint8_t *fix,
@@ -305,15 +315,6 @@ template <typename T> struct Q4Builder
     std::copy(K, K + 64, q.K.k);
     q.d = d;
     q4_grid(d, q.bx, q.by, q.ychunk);
-    if(!x.dotRed && q.ychunk < kQ4BatchRows && d.sy > 2 * kQ4BatchRows)
-    {
-      // without a fused dot the operator's output does not depend on how
-      // its rows are chunked (every node is the same sum computed by its
-      // owner): on large grids fewer, taller chunks, each recomputing one
-      // halo row; small grids keep their many short ones (parallel)
-      q.ychunk = std::min(d.sy, kQ4BatchRows);
-      q.by = (d.sy + q.ychunk - 1) / q.ychunk;
-    }
     q.E = E;
     q.u = u;
     q.y = y;
@@ -327,15 +328,35 @@ template <typename T> struct Q4Builder
       ICB_REQUIRE((long long)q.bx * q.by <= x.dotRed->maxBlocks, "reduction scratch too small");
     mode = x.mode;
     dot = x.dotRed != nullptr;
-    const int id = int(recs.size());
     recs.push_back(q);
-    for(int b = 0; b < q.bx * q.by; b++)
-      map.push_back(make_int2(id, b));
   }
   Launch finish(cudaStream_t s, unsigned *counters)
   {
     if(recs.empty())
       return {};
+    if(!dot)
+    {
+      // without a fused dot the operator's output does not depend on how its
+      // rows are chunked (every node is the same sum, computed by its owner):
+      // rows per block from the size of the whole launch -- one on small
+      // (coarse) launches, so their blocks stay short and parallel, up to
+      // kQ4BatchRows on large ones, so the per-item overhead stays small
+      long long rows = 0;
+      for(const Q4Launch<T> &q : recs)
+        rows += (long long)q.bx * q4_block_warps() * q.d.sy;
+      const unsigned k =
+          rows_per_item(rows, q4_batch_capacity_warps<T>(mode, false), kQ4BatchRows);
+      for(Q4Launch<T> &q : recs)
+      {
+        q.ychunk = std::min<int>(q.d.sy, int(k));
+        q.by = (q.d.sy + q.ychunk - 1) / q.ychunk;
+      }
+    }
+    std::vector<int2> map;
+    for(size_t id = 0; id < recs.size(); id++)
+      for(int b = 0; b < recs[id].bx * recs[id].by; b++)
+        map.push_back(make_int2(int(id), b));
+    ICB_REQUIRE(map.size() < (1ULL << 31), "batched launch too large");
     auto D = std::make_shared<DevBuf<Q4Launch<T>>>(recs.size());
     auto M = std::make_shared<DevBuf<int2>>(map.size());
     ICB_CUDA(cudaMemcpyAsync(D->p, recs.data(), sizeof(Q4Launch<T>) * recs.size(),
@@ -469,6 +490,13 @@ template <typename TP> struct BatchMg
       Q4Builder<TP> op;
       Builder<RestrictL<TP>> rs;
       std::vector<Inst> next;
+      long long rowsR = 0;
+      for(const Inst &I : fine)
+      {
+        const dim3 g3 = grid3(M[I.i]->lv[l + 1].d);
+        rowsR += (long long)g3.x * g3.y * g3.z;
+      }
+      const unsigned kR = rows_per_item(rowsR, transfer_capacity(), 8);
       for(size_t t = 0; t < fine.size(); t++)
       {
         const Inst &I = fine[t];
@@ -483,7 +511,7 @@ template <typename TP> struct BatchMg
         op.add(L.d, L.K, L.E, cs[t].cur, L.r.p, L.fix, res);
         const dim3 g3 = grid3(Cn.d);
         rs.add(RestrictL<TP>{{}, L.d, Cn.d, Cn.sh, L.r.p, Cn.b.p, Cn.fix, gate(I.i), g3.y}, g3.x,
-               transfer_rows(g3.y), g3.z);
+               transfer_rows(g3.y, kR), g3.z);
         next.push_back(Inst{I.i, Cn.b.p, Cn.x.p});
       }
       push(op.finish(s, qc.p));
@@ -492,6 +520,13 @@ template <typename TP> struct BatchMg
     }
     {
       Builder<ProlongL<TP>> pr;
+      long long rowsP = 0;
+      for(const Inst &I : fine)
+      {
+        const dim3 g3 = grid3(M[I.i]->lv[l].d);
+        rowsP += (long long)g3.x * g3.y * g3.z;
+      }
+      const unsigned kP = rows_per_item(rowsP, transfer_capacity(), 8);
       for(size_t t = 0; t < fine.size(); t++)
       {
         const Inst &I = fine[t];
@@ -500,7 +535,7 @@ template <typename TP> struct BatchMg
         Level<TP> &Cn = m.lv[l + 1];
         const dim3 g3 = grid3(L.d);
         pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i), g3.y}, g3.x,
-               transfer_rows(g3.y), g3.z);
+               transfer_rows(g3.y, kP), g3.z);
       }
       push(pr.finish(kTB, 0, s, qc.p));
     }

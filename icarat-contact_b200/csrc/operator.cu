@@ -867,6 +867,11 @@ __global__ void __launch_bounds__(TX *TW, MINB)
 // ------------------------------------------------------------------- Q4 ----
 /// the Q4 operator for block (bxi, byi) of a (bx, by) grid: the body of
 /// k_matvec_q4 and of its batched form k_matvec_q4_batch
+/// The Q4 operator over one block's columns and element rows.  Each row's
+/// loads (the next node row, the element modulus, and the inputs of this
+/// row's fused update) are issued one row ahead of, or before, the element
+/// work that consumes them, so their latency overlaps arithmetic; the
+/// arithmetic is the same, in the same order.
 template <typename T, bool DOT, int MODE>
 __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, const int ychunk,
                                         const T *__restrict__ E, const T *__restrict__ u,
@@ -884,7 +889,7 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
   const int Y1 = min(Y0 + ychunk, d.sy) - 1;
   const bool col = ei >= 0 && ei < d.nx;
   const long long ld = d.ld;
-  T ub[2][2], ut[2][2], carry[2][2];
+  T ub[2][2], ut[2][2], un[2][2], carry[2][2];
 #pragma unroll
   for(int c = 0; c < 2; c++)
 #pragma unroll
@@ -902,17 +907,54 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
       for(int a = 0; a < 2; a++)
         ub[c][a] = __ldg(u + c * ld + base + a);
   }
-  double dot = 0.0;
-  for(int ej = Y0 - 1; ej <= Y1; ++ej)
-  {
-    const bool lay = col && ej >= 0 && ej < d.ny;
+  // the top node row and the modulus of element row ej
+  auto load_row = [&](int ej, T(&v)[2][2], T &Ev) {
     const bool topok = col && ej + 1 >= 0 && ej + 1 <= d.ny;
 #pragma unroll
     for(int c = 0; c < 2; c++)
 #pragma unroll
       for(int a = 0; a < 2; a++)
-        ut[c][a] = topok ? __ldg(u + c * ld + ei + (long long)(ej + 1) * d.sx + a) : T(0);
-    const T Ee = lay ? __ldg(E + (long long)ei + (long long)ej * d.nx) : T(0);
+        v[c][a] = topok ? __ldg(u + c * ld + ei + (long long)(ej + 1) * d.sx + a) : T(0);
+    const bool lay = col && ej >= 0 && ej < d.ny;
+    Ev = lay ? __ldg(E + (long long)ei + (long long)ej * d.nx) : T(0);
+  };
+  T En;
+  load_row(Y0 - 1, un, En);
+  const int ni = ei + 1;
+  const bool ownCol = lx < TX - 1 && ni < d.sx && X0 < d.sx;
+  double dot = 0.0;
+  for(int ej = Y0 - 1; ej <= Y1; ++ej)
+  {
+#pragma unroll
+    for(int c = 0; c < 2; c++)
+#pragma unroll
+      for(int a = 0; a < 2; a++)
+        ut[c][a] = un[c][a];
+    const T Ee = En;
+    if(ej < Y1)
+      load_row(ej + 1, un, En);
+    // this row's output node and the inputs of its update
+    const bool own = ej >= Y0 && ownCol;
+    const long long node = (long long)ni + (long long)ej * d.sx;
+    unsigned f = 0;
+    T us[2] = {T(0), T(0)}, bv[2] = {T(0), T(0)}, dv[2] = {T(0), T(0)}, yp[2] = {T(0), T(0)};
+    if(own)
+    {
+      f = __ldg(fix + node);
+#pragma unroll
+      for(int c = 0; c < 2; c++)
+      {
+        const long long i = c * ld + node;
+        if(DOT || MODE >= OP_JACOBI)
+          us[c] = __ldg(u + i); // node i = 0 belongs to a halo column
+        if(MODE != OP_APPLY)
+          bv[c] = __ldg(ep.b + i);
+        if(MODE >= OP_JACOBI)
+          dv[c] = __ldg(ep.dinv + i);
+        if(MODE == OP_CHEB && ep.c1 != T(0))
+          yp[c] = y[i]; // the previous iterate, read before this thread overwrites it
+      }
+    }
     // element vector in local order: n0=(0,0) n1=(1,0) n2=(1,1) n3=(0,1)
     T ue[8];
 #pragma unroll
@@ -938,25 +980,38 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
       }
     if(ej >= Y0)
     {
-      const int ni = ei + 1;
       T o[2];
 #pragma unroll
       for(int c = 0; c < 2; c++)
         o[c] = acc[c][1] + __shfl_down_sync(0xffffffffu, acc[c][0], 1);
-      if(lx < TX - 1 && ni < d.sx && X0 < d.sx)
+      if(own)
       {
-        const long long node = (long long)ni + (long long)ej * d.sx;
-        const unsigned f = __ldg(fix + node);
 #pragma unroll
         for(int c = 0; c < 2; c++)
         {
           T v = ((f >> c) & 1u) ? T(0) : o[c];
-          T us = T(0);
-          if(DOT || MODE >= OP_JACOBI)
-            us = __ldg(u + c * ld + node); // node i = 0 belongs to a halo column
           if(DOT)
-            dot += double(us) * double(v);
-          y[c * ld + node] = epilogue<T, MODE>(v, us, c * ld + node, ep, y);
+            dot += double(us[c]) * double(v);
+          // the fused update (epilogue's arithmetic, inputs loaded above)
+          T out;
+          if(MODE == OP_APPLY)
+            out = v;
+          else
+          {
+            T r = bv[c] - v;
+            if(MODE == OP_RESIDUAL)
+              out = r;
+            else if(MODE == OP_JACOBI)
+              out = us[c] + ep.omega * dv[c] * r;
+            else
+            {
+              T dn = ep.c2 * dv[c] * r;
+              if(ep.c1 != T(0))
+                dn += ep.c1 * (us[c] - yp[c]);
+              out = us[c] + dn;
+            }
+          }
+          y[c * ld + node] = out;
         }
       }
     }
@@ -1001,7 +1056,7 @@ __global__ void __launch_bounds__(TX *TY2)
 /// problem's result (and its fused dot product) is bitwise that of its own
 /// launch
 template <typename T, bool DOT, int MODE>
-__global__ void __launch_bounds__(TX *TY2)
+__global__ void __launch_bounds__(TX *TY2, sizeof(T) == 4 ? 8 : 4)
     k_matvec_q4_batch(const Q4Launch<T> *__restrict__ D, const int2 *__restrict__ map,
                       BatchQueue bq)
 {
@@ -1010,15 +1065,19 @@ __global__ void __launch_bounds__(TX *TY2)
       [](const Q4Launch<T> &q) {
         return q.gate && (q.gate->stop || (q.gateConv && q.gate->conv));
       },
-      [](const Q4Launch<T> &q, int b) {
+      [](const Q4Launch<T> &q, int b, bool fresh) {
         // the element matrix in shared memory: in registers it would take 64
-        // (FP32) or 128 (FP64) of them and a quarter of the occupancy; the
-        // queue's barrier after each item protects it until every thread is done
+        // (FP32) or 128 (FP64) of them and a quarter of the occupancy; staged
+        // once per run of items of one record (the queue's barrier after each
+        // item protects it until every thread is done)
         __shared__ KMat<T, 8> sK;
-        const int t = threadIdx.x + blockDim.x * threadIdx.y;
-        if(t < 64)
-          sK.k[t] = q.K.k[t];
-        __syncthreads();
+        if(fresh)
+        {
+          const int t = threadIdx.x + blockDim.x * threadIdx.y;
+          if(t < 64)
+            sK.k[t] = q.K.k[t];
+          __syncthreads();
+        }
         q4_body<T, DOT, MODE>(sK, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
                               q.gateConv, q.ep, b % q.bx, b / q.bx, q.bx, q.by);
       });
@@ -1079,7 +1138,7 @@ __global__ void k_diag2_batch(const Diag2Launch<T> *__restrict__ D, const int2 *
   batch_queue(
       D, map, bq, [](const Diag2Launch<T> &q) { return int((q.d.nnode + 255) / 256); },
       [](const Diag2Launch<T> &) { return false; },
-      [](const Diag2Launch<T> &q, int b) {
+      [](const Diag2Launch<T> &q, int b, bool) {
         diag_b<T, 2>(q.K, q.d, q.E, q.fix, q.invdiag, nullptr, unsigned(b));
       });
 }
@@ -1536,6 +1595,14 @@ template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q)
 }
 template int q4_batch_grid<double>(int, bool, BatchQueue &);
 template int q4_batch_grid<float>(int, bool, BatchQueue &);
+int q4_block_warps() { return TY2; }
+template <typename T> long long q4_batch_capacity_warps(int mode, bool dot)
+{
+  BatchQueue q{nullptr, nullptr, 1 << 30};
+  return (long long)q4_batch_grid<T>(mode, dot, q) * TY2;
+}
+template long long q4_batch_capacity_warps<double>(int, bool);
+template long long q4_batch_capacity_warps<float>(int, bool);
 
 template <typename T>
 void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q, int grid,

@@ -963,7 +963,7 @@ __global__ void __launch_bounds__(VB, 4)
   batch_queue(
       R, map, q, [](const OcBatch::Rec &r) { return int(r.gxc); },
       [](const OcBatch::Rec &r) { return r.st->done != 0 || !r.P.useFilter; },
-      [](const OcBatch::Rec &r, int b) {
+      [](const OcBatch::Rec &r, int b, bool) {
         oc_cand_b(r.d.nel, r.x, r.df, r.dg, r.xmin, r.xmax, r.P, r.st, r.xc,
                   Blk{unsigned(b), 0, 0, r.gxc, 1, 1});
       });
@@ -975,7 +975,7 @@ __global__ void __launch_bounds__(VB, 4)
   batch_queue(
       R, map, q, [](const OcBatch::Rec &r) { return int(r.gx); },
       [](const OcBatch::Rec &r) { return r.st->done != 0; },
-      [](const OcBatch::Rec &r, int b) {
+      [](const OcBatch::Rec &r, int b, bool) {
         const Blk B{unsigned(b), 0, 0, r.gx, 1, 1};
         if(r.tiled)
           oc_step_tile_b(r.d, r.hx, r.hy, r.ntx, r.off, r.w, r.nnb, r.aa, r.vol, r.xc, r.P, r.red,
@@ -991,7 +991,7 @@ __global__ void __launch_bounds__(256)
   batch_queue(
       R, map, q, [](const OcBatch::Rec &r) { return int((r.d.nel + 255) / 256); },
       [](const OcBatch::Rec &) { return false; },
-      [](const OcBatch::Rec &r, int b) {
+      [](const OcBatch::Rec &r, int b, bool) {
         const long long e = b * 256LL + threadIdx.x;
         if(e < r.d.nel)
           r.x[e] = oc_candidate(r.x[e], r.df[e], r.dg[e], r.st->lastLam, r.P.eta, r.P.move,

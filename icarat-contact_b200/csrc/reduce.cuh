@@ -11,6 +11,20 @@
 namespace icb
 {
 
+/// the ticket of the last-block pattern: an atomic add with acquire-release
+/// semantics at GPU scope, which orders this thread's partial stores before
+/// the ticket (release) and, for the last block, the other blocks' partials
+/// before its reads (acquire) -- without a full sequentially consistent fence
+__device__ __forceinline__ unsigned ticket_acq_rel(unsigned *counter)
+{
+  unsigned t;
+  asm volatile("atom.acq_rel.gpu.add.u32 %0, [%1], 1;"
+               : "=r"(t)
+               : "l"(counter)
+               : "memory");
+  return t;
+}
+
 __device__ __forceinline__ double warp_sum_d(double v)
 {
 #pragma unroll
@@ -49,8 +63,7 @@ __device__ __forceinline__ void block_reduce_at(double (&v)[NV], const RedScratc
         s += sw[w][k];
       red.partials[(long long)bid * NV + k] = s;
     }
-    __threadfence();
-    unsigned t = atomicAdd(red.counter, 1u);
+    const unsigned t = ticket_acq_rel(red.counter);
     last = (t == unsigned(nb - 1));
   }
   __syncthreads();
