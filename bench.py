@@ -516,22 +516,31 @@ def headline_ours(args):
     e2e = {"value": units2 / (ms2 * 1e-3), "unit": UNIT, "ms_per_step": ms2 / args.steps,
            "h2d_bytes_per_step": 8 * prob.nel, "d2h_bytes_per_step": 8 * (numeq + prob.nel + 1)}
 
-    # ---- roofline: the FP32 element operator of the V-cycle (the dominant
-    # kernel of the mixed solve) and the FP64 one of the residual, each timed
-    # live with an L2 flush before every launch
+    # ---- roofline: the dominant kernel of the step is the V-cycle's FP32
+    # Chebyshev smoother on the fine level (the element operator with its fused
+    # update: 37 % of the solve's device time in the launch list); beside it the
+    # same FP32 operator without the update and the FP64 operator of the outer
+    # iteration.  Each timed live with an L2 flush before every launch.
     prob.set_density_device(rho_d.data_ptr())
     peak, peak_kind = _peaks()
     rows = {}
     k32 = "k_matvec_h8p<float>" if icb.get_option("hex8_pair") == 1 else "k_matvec_h8m<float>"
-    for name, prec, es, kern in (("fp32", icb.MIXED, 4, k32),
-                                 ("fp64", icb.FP64, 8, "k_matvec_h8m<double>")):
-        t = op_launch_seconds(prob, prec, stream, local)
-        b = es * (2 * prob.neq + prob.nel)
+    vec = 3 * prob.nnode  # entries of one field vector the kernels touch
+    for name, prec, es, kern, cheb in (
+            ("fp32_cheb", icb.MIXED, 4, k32 + " OP_CHEB", True),
+            ("fp32_apply", icb.MIXED, 4, k32, False),
+            ("fp64", icb.FP64, 8, "k_matvec_h8m<double>", False)):
+        t = op_launch_seconds(prob, prec, stream, local, cheb=cheb)
+        # u, b, D^-1 and the previous iterate read, y written, the moduli and
+        # the constraint flags; the plain operator reads u and writes y
+        b = es * ((5 if cheb else 2) * vec + prob.nel) + (prob.nnode if cheb else 0)
+        tkey = (k32 + ("_cheb" if cheb else "")) if prec == icb.MIXED else kern
         rows[name] = {"bound": "hbm", "achieved": b / t / 1e9, "peak": peak, "unit": "GB/s",
                       "frac": b / t / 1e9 / peak, "kernel": kern, "launch_us": t * 1e6,
                       "alg_bytes": b, "peak_source": peak_kind,
-                      "traffic": _traffic(f"{kern}_384x128x128")}
-    roofline = dict(rows["fp32"])
+                      "traffic": _traffic(f"{tkey}_384x128x128")}
+    roofline = dict(rows["fp32_cheb"])
+    roofline["fp32_operator_alone"] = rows["fp32_apply"]
     roofline["fp64_outer_operator"] = rows["fp64"]
 
     # ---- the topology-optimisation loop on the same beam: 20 MMA steps with
@@ -603,29 +612,41 @@ def smooth_field(nx, ny, nz, seed, lo=0.001, hi=1.0, modes=16):
     return cases.smooth_field(nx, ny, nz, seed, lo, hi, modes)
 
 
-def op_launch_seconds(prob, prec, stream, device=0, reps=30):
-    """Mean device time of one icb_operator_apply_device launch, each launch
-    bracketed by CUDA events on the problem's stream and preceded by a write
-    of 256 MiB (> L2) on that stream."""
+def op_launch_seconds(prob, prec, stream, device=0, reps=30, cheb=False):
+    """Mean device time of one operator launch, each launch bracketed by CUDA
+    events on the problem's stream and preceded by a write of 256 MiB (> L2)
+    on that stream: icb_operator_apply_device (y = K x), or with cheb the
+    V-cycle's fused Chebyshev step icb_smoother_apply_device (c1 != 0, so it
+    reads u, b, D^-1 and the previous iterate and writes y)."""
     import torch
     import icarat_b200 as icb
     dt = torch.float64 if prec == icb.FP64 else torch.float32
     nsoa = prob.soa_length()
-    x = torch.randn(nsoa, dtype=dt, device=f"cuda:{device}")
-    y = torch.empty_like(x)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    dev = f"cuda:{device}"
+    x = torch.randn(nsoa, dtype=dt, device=dev)
+    y = torch.zeros_like(x)
+    b = torch.randn(nsoa, dtype=dt, device=dev)
+    dinv = torch.rand(nsoa, dtype=dt, device=dev) * 0.1
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def launch():
+        if cheb:
+            prob.smoother_apply_device(x.data_ptr(), y.data_ptr(), b.data_ptr(), dinv.data_ptr(),
+                                       0.3, 0.7, precision=prec)
+        else:
+            prob.operator_apply_device(x.data_ptr(), y.data_ptr(), prec)
     torch.cuda.synchronize()
     for _ in range(3):
-        prob.operator_apply_device(x.data_ptr(), y.data_ptr(), prec)
+        launch()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
     with torch.cuda.stream(stream):
-        for a, b in ev:
+        for a, e in ev:
             flush.fill_(1)
             a.record(stream)
-            prob.operator_apply_device(x.data_ptr(), y.data_ptr(), prec)
-            b.record(stream)
+            launch()
+            e.record(stream)
     torch.cuda.synchronize()
-    return sum(a.elapsed_time(b) for a, b in ev) / reps * 1e-3
+    return sum(a.elapsed_time(e) for a, e in ev) / reps * 1e-3
 
 
 def workload_operator(args):

@@ -675,4 +675,41 @@ int icb_operator_apply_device(icb_problem p, int precision, const void *x, void 
   ICB_API_END
 }
 
+int icb_smoother_apply_device(icb_problem p, int precision, const void *u, void *y,
+                              const void *b, const void *dinv, double c1, double c2)
+{
+  ICB_API_BEGIN
+  need(p && u && y && b && dinv, "NULL argument");
+  needState(p->hasDensity, "set the density first");
+  need(u != y, "u and y must be different vectors");
+  setDevice(p);
+  if(precision == ICB_FP64)
+  {
+    OpExtras<double> ex;
+    ex.mode = OP_CHEB;
+    ex.b = (const double *)b;
+    ex.dinv = (const double *)dinv;
+    ex.c1 = c1;
+    ex.c2 = c2;
+    ex.cudaCores = 1;
+    launch_op<double>(p->d, p->K0, p->E.p, (const double *)u, (double *)y, p->fix.p,
+                      p->stream(), ex);
+  }
+  else if(precision == ICB_MIXED)
+  {
+    OpExtras<float> ex;
+    ex.mode = OP_CHEB;
+    ex.b = (const float *)b;
+    ex.dinv = (const float *)dinv;
+    ex.c1 = c1;
+    ex.c2 = c2;
+    ex.cudaCores = 1;
+    launch_op<float>(p->d, p->K0f, p->Ef.p, (const float *)u, (float *)y, p->fix.p,
+                     p->stream(), ex);
+  }
+  else
+    need(false, "unknown precision");
+  ICB_API_END
+}
+
 } // extern "C"

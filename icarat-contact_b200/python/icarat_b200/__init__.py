@@ -136,6 +136,8 @@ _SIGS = {
     "icb_diagonal": (C.c_int, [C.c_void_p, _dp]),
     "icb_soa_length": (C.c_longlong, [C.c_void_p]),
     "icb_operator_apply_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "icb_smoother_apply_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_double, C.c_double]),
     "icb_launch_count": (C.c_longlong, []),
     "icb_solve_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                     C.POINTER(SolveInfo)]),
@@ -382,6 +384,13 @@ class Problem:
 
     def operator_apply_device(self, x_ptr, y_ptr, precision=FP64):
         check(lib().icb_operator_apply_device(self.h, precision, C.c_void_p(x_ptr), C.c_void_p(y_ptr)))
+
+    def smoother_apply_device(self, u_ptr, y_ptr, b_ptr, dinv_ptr, c1, c2, precision=FP64):
+        """one fused Chebyshev step y <- u + c2 D^-1 (b - K u) + c1 (u - y) on
+        device SoA vectors (icb_smoother_apply_device)"""
+        check(lib().icb_smoother_apply_device(self.h, precision, C.c_void_p(u_ptr),
+                                              C.c_void_p(y_ptr), C.c_void_p(b_ptr),
+                                              C.c_void_p(dinv_ptr), float(c1), float(c2)))
 
     def diagonal(self):
         d = np.zeros(self.numeq)

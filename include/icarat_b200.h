@@ -415,6 +415,15 @@ long long icb_soa_length(icb_problem p);
  * tensor cores, Hex8 only); one operator launch on the context's stream, no
  * synchronisation.  Constrained rows of y are 0. */
 int icb_operator_apply_device(icb_problem p, int precision, const void *x, void *y);
+/* One Chebyshev smoothing step of the multigrid V-cycle as the library runs it:
+ * the operator with its fused update, y <- u + c2 D^-1 (b - K u) + c1 (u - y)
+ * (y holds the previous iterate on entry; with c1 = 0 it is not read).  Device
+ * SoA vectors of icb_soa_length() entries, double* for ICB_FP64, float* for
+ * ICB_MIXED (the FP32 CUDA-core kernel); dinv is the inverse diagonal (0 on
+ * constrained DOFs).  One launch on the context's stream, no
+ * synchronisation; u and y must differ. */
+int icb_smoother_apply_device(icb_problem p, int precision, const void *u, void *y,
+                              const void *b, const void *dinv, double c1, double c2);
 /* number of kernels this library has launched in the process (graph nodes
  * counted one by one) */
 long long icb_launch_count(void);
