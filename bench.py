@@ -878,6 +878,11 @@ def workload_batched(args):
     fused_short["phase_s"] = [icb.get_option(f"fused_phase_us_{k}") * 1e-6 for k in range(5)]
     fused_short["iterations_batch_vs_problems"] = [icb.get_option("fused_batch_iters"),
                                                    icb.get_option("fused_problem_iters")]
+    # the batched solves' graph launches by the share of designs still
+    # iterating: > 1/2, > 1/8, <= 1/8 (seconds, launches)
+    fused_short["solve_by_active_share"] = {
+        "s": [icb.get_option(f"fused_active_us_{k}") * 1e-6 for k in range(3)],
+        "launches": [icb.get_option(f"fused_active_launches_{k}") for k in range(3)]}
     same = same and all(np.array_equal(a, b) for a, b in zip(Hs + Xs, Hf + Xf))
     runs["fused_short"] = fused_short
     fused, _, _ = run(args.loop_steps, True, 1)

@@ -634,6 +634,10 @@ long long icb_get_option(const char *name)
     return fused_iterations(1);
   if(n.rfind("fused_phase_us_", 0) == 0 && n.size() == 16)
     return (long long)(1e6 * fused_phase_seconds(n[15] - '0'));
+  if(n.rfind("fused_active_us_", 0) == 0 && n.size() == 17)
+    return (long long)(1e6 * fused_active_seconds(n[16] - '0'));
+  if(n.rfind("fused_active_launches_", 0) == 0 && n.size() == 23)
+    return fused_active_launches(n[22] - '0');
   if(n == "tc_timeouts")
     return (long long)tc_timeouts();
   if(n == "tc_spin_limit")

@@ -205,6 +205,12 @@ void run_oc_fused(int n, icb_problem_s *const *probs, const icb_loop_opts *opts,
 double fused_phase_seconds(int k);
 /// iterations of the last fused run: k = 0 the batch's, 1 the problems' sum
 long long fused_iterations(int k);
+/// the batched solves' graph launches of the last fused run, binned by the
+/// share of the batch still iterating (k = 0: > 1/2, 1: > 1/8, 2: <= 1/8):
+/// wall seconds and launches
+void fused_active_record(int active, int n, double seconds);
+double fused_active_seconds(int k);
+long long fused_active_launches(int k);
 /// whether icb_run_batch uses the fused loop when a batch qualifies (option
 /// batch_fused, default on)
 bool batch_fused_enabled();

@@ -763,11 +763,17 @@ template <typename TP> struct BatchMg
     for(auto &f : init)
       f(s);
     long long launched = 0;
+    const int n = int(M.size());
     for(;;)
     {
+      // the share of the batch still iterating when this launch starts
+      const int act = launched == 0 ? n : *hActive;
+      const auto t0 = std::chrono::steady_clock::now();
       ICB_CUDA(cudaGraphLaunch(exec, s));
       count_launch(nodes + 1);
       ICB_CUDA(cudaStreamSynchronize(s));
+      fused_active_record(act, n, std::chrono::duration<double>(
+                                      std::chrono::steady_clock::now() - t0).count());
       launched += batch;
       if(*hActive == 0 || launched > (long long)maxit + batch)
         break;
@@ -804,6 +810,20 @@ template <> MgPcg<double, float> *prepare_mg<float>(icb_problem p, const icb_sol
 
 template struct BatchMg<double>;
 template struct BatchMg<float>;
+
+/// the batched solves' graph launches of the last fused run by the share of
+/// the batch still iterating when each started: more than half, more than an
+/// eighth, at most an eighth (seconds and launches)
+static double g_active_s[3];
+static long long g_active_n[3];
+void fused_active_record(int active, int n, double seconds)
+{
+  const int k = 2 * active > n ? 0 : (8 * active > n ? 1 : 2);
+  g_active_s[k] += seconds;
+  g_active_n[k]++;
+}
+double fused_active_seconds(int k) { return k >= 0 && k < 3 ? g_active_s[k] : -1.0; }
+long long fused_active_launches(int k) { return k >= 0 && k < 3 ? g_active_n[k] : -1; }
 
 /// wall time of the fused loop's phases over the last run, in seconds:
 /// 0 building the batched launches, 1 per-problem filter and moduli
@@ -889,6 +909,11 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
     maxSteps = std::max(maxSteps, r.o->nsteps);
   for(double &v : g_fused_phase)
     v = 0.0;
+  for(int k = 0; k < 3; k++)
+  {
+    g_active_s[k] = 0.0;
+    g_active_n[k] = 0;
+  }
   g_fused_iters[0] = g_fused_iters[1] = 0;
   {
     auto tb = PhaseClock::now();

@@ -442,7 +442,10 @@ long long icb_launch_count(void);
  * moduli launches, the batched multigrid set-up and solves, compliance /
  * sensitivities / adjoint filters, OC updates with the step's wait),
  * "fused_batch_iters" and "fused_problem_iters" (its solves' iterations: of
- * the batch, and summed over the designs).
+ * the batch, and summed over the designs), "fused_active_us_0" .. "_2" and
+ * "fused_active_launches_0" .. "_2" (its solves' graph launches, wall
+ * microseconds and count, by the share of the batch still iterating when
+ * each started: more than a half, more than an eighth, at most an eighth).
  * Further switches: "hex8_pair" (FP32 Hex8 operator with two element rows per
  * thread), "tc_spin_limit" (polls of a tensor-core wait before it gives up),
  * "batch_fused" (icb_run_batch advances qualifying 2D OC batches together).
