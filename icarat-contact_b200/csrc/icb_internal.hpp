@@ -264,6 +264,8 @@ template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q);
 /// warps of one block of the Q4 operator, and the resident warps of its
 /// batched launch on the whole GPU
 int q4_block_warps();
+/// reduction slots of the Q4 operator's fused dot (a node row per warp strip)
+int q4_dot_slots(const Dims &d);
 template <typename T> long long q4_batch_capacity_warps(int mode, bool dot);
 
 /// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)

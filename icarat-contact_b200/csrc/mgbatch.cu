@@ -325,7 +325,7 @@ template <typename T> struct Q4Builder
     q.gateConv = x.gateConv;
     q.ep = Epi<T>{x.b, x.dinv, T(x.omega), T(x.c1), T(x.c2)};
     if(x.dotRed)
-      ICB_REQUIRE((long long)q.bx * q.by <= x.dotRed->maxBlocks, "reduction scratch too small");
+      ICB_REQUIRE(q4_dot_slots(d) <= x.dotRed->maxBlocks, "reduction scratch too small");
     mode = x.mode;
     dot = x.dotRed != nullptr;
     recs.push_back(q);
@@ -334,18 +334,18 @@ template <typename T> struct Q4Builder
   {
     if(recs.empty())
       return {};
-    if(!dot)
     {
-      // without a fused dot the operator's output does not depend on how its
-      // rows are chunked (every node is the same sum, computed by its owner):
-      // rows per block from the size of the whole launch -- one on small
-      // (coarse) launches, so their blocks stay short and parallel, up to
-      // kQ4BatchRows on large ones, so the per-item overhead stays small
+      // the operator's output does not depend on how its rows are cut into
+      // blocks (every node is the same sum, computed by its owner), nor does
+      // its fused dot (one slot per node row and warp strip, summed in slot
+      // order): rows per block from the size of the whole launch -- one on
+      // small (coarse) launches, so their blocks stay short and parallel, up
+      // to kQ4BatchRows on large ones, so the per-item overhead stays small
       long long rows = 0;
       for(const Q4Launch<T> &q : recs)
         rows += (long long)q.bx * q4_block_warps() * q.d.sy;
       const unsigned k =
-          rows_per_item(rows, q4_batch_capacity_warps<T>(mode, false), kQ4BatchRows);
+          rows_per_item(rows, q4_batch_capacity_warps<T>(mode, dot), kQ4BatchRows);
       for(Q4Launch<T> &q : recs)
       {
         q.ychunk = std::min<int>(q.d.sy, int(k));

@@ -38,7 +38,7 @@
 namespace
 {
 constexpr size_t kNoAllocBytes = size_t(32) << 20;
-constexpr int kNoAllocMaxBlocks = 8192;
+constexpr int kNoAllocMaxBlocks = 32768;
 constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 // layout: [KState][counter][pq][partials: 2*kNoAllocMaxBlocks][r][p][q]
 constexpr size_t kOffState = 0;

@@ -922,7 +922,10 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
   load_row(Y0 - 1, un, En);
   const int ni = ei + 1;
   const bool ownCol = lx < TX - 1 && ni < d.sx && X0 < d.sx;
-  double dot = 0.0;
+  // the fused dot: one slot per (node row, warp strip), the warp's sum over
+  // its strip of that row, so the total does not depend on how the rows are
+  // cut into blocks
+  const int strips = nbx * TY2, strip = bxi * TY2 + w;
   for(int ej = Y0 - 1; ej <= Y1; ++ej)
   {
 #pragma unroll
@@ -984,6 +987,7 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
 #pragma unroll
       for(int c = 0; c < 2; c++)
         o[c] = acc[c][1] + __shfl_down_sync(0xffffffffu, acc[c][0], 1);
+      double dot = 0.0;
       if(own)
       {
 #pragma unroll
@@ -1014,6 +1018,12 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
           y[c * ld + node] = out;
         }
       }
+      if(DOT)
+      {
+        dot = warp_sum_d(dot);
+        if(lx == 0)
+          red.partials[(long long)ej * strips + strip] = dot;
+      }
     }
 #pragma unroll
     for(int a = 0; a < 2; a++)
@@ -1034,10 +1044,8 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
         ub[c][a] = ut[c][a];
   }
   if(DOT)
-  {
-    double v[1] = {dot};
-    block_reduce_at<1>(v, red, FinStore{dotOut}, bxi + nbx * byi, nbx * nby);
-  }
+    slots_reduce_finish(red, (long long)d.sy * strips, nbx * nby, lx == 0 && Y0 <= Y1,
+                        FinStore{dotOut});
 }
 
 template <typename T, bool DOT, int MODE>
@@ -1397,7 +1405,8 @@ int matvec_blocks(const Dims &d)
   }
   int bx, by, ychunk;
   q4_grid(d, bx, by, ychunk);
-  return bx * by;
+  // the fused dot's slots (a node row per warp strip) and the blocks
+  return std::max(bx * by, q4_dot_slots(d));
 }
 
 static std::atomic<bool> g_hex8_modal{true}; // read by every launching thread
@@ -1566,7 +1575,7 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
     dim3 grid(bx, by), block(TX, TY2);
     if(x.dotRed)
     {
-      ICB_REQUIRE(bx * by <= red.maxBlocks, "reduction scratch too small");
+      ICB_REQUIRE(q4_dot_slots(d) <= red.maxBlocks, "reduction scratch too small");
       k_matvec_q4<T, true, MODE><<<grid, block, 0, s>>>(km, d, ychunk, E, u, y, fix, red,
                                                         x.dotOut, x.gate, x.gateConv, ep);
     }
@@ -1596,6 +1605,14 @@ template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q)
 template int q4_batch_grid<double>(int, bool, BatchQueue &);
 template int q4_batch_grid<float>(int, bool, BatchQueue &);
 int q4_block_warps() { return TY2; }
+int q4_dot_slots(const Dims &d)
+{
+  int bx, by, ychunk;
+  q4_grid(d, bx, by, ychunk);
+  const long long n = (long long)bx * TY2 * d.sy;
+  ICB_REQUIRE(n < (1LL << 31), "grid too large for the Q4 operator's dot");
+  return int(n);
+}
 template <typename T> long long q4_batch_capacity_warps(int mode, bool dot)
 {
   BatchQueue q{nullptr, nullptr, 1 << 30};

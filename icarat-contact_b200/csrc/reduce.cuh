@@ -102,6 +102,47 @@ __device__ __forceinline__ void block_reduce_at(double (&v)[NV], const RedScratc
   }
 }
 
+/// The finish of a sum whose partials sit at slots fixed by the work, not by
+/// the block that computed them (so the launch may be cut into any number of
+/// blocks): each block calls it once, after its threads stored their slots;
+/// the last of the nb blocks to arrive sums slots [0, nslots) in a fixed order
+/// (thread t takes t, t + blockDim, ...; then the warps in order) and hands
+/// the total to fin.  `wrote`: this thread stored slots (it fences them).
+template <class Fin>
+__device__ __forceinline__ void slots_reduce_finish(const RedScratch &red, long long nslots,
+                                                    int nb, bool wrote, Fin fin)
+{
+  __shared__ double sw[32];
+  __shared__ int last;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nth = blockDim.x * blockDim.y * blockDim.z;
+  const int nw = (nth + 31) >> 5;
+  if(wrote)
+    __threadfence();
+  __syncthreads();
+  if(tid == 0)
+    last = ticket_acq_rel(red.counter) == unsigned(nb - 1);
+  __syncthreads();
+  if(!last)
+    return;
+  __threadfence();
+  double s = 0.0;
+  for(long long k = tid; k < nslots; k += nth)
+    s += __ldcg(red.partials + k);
+  s = warp_sum_d(s);
+  if((tid & 31) == 0)
+    sw[tid >> 5] = s;
+  __syncthreads();
+  if(tid == 0)
+  {
+    double tot = 0.0;
+    for(int w = 0; w < nw; w++)
+      tot += sw[w];
+    *red.counter = 0u;
+    fin(&tot);
+  }
+}
+
 template <int NV, class Fin>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], const RedScratch &red,
                                              Fin fin)
