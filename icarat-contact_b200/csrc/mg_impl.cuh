@@ -133,44 +133,72 @@ __global__ void k_restrict(Dims df, Dims dc, int3 sh, const T *__restrict__ rf,
 }
 
 /// x_f += P x_c, constrained fine DOFs untouched (they stay 0).  One thread
-/// per fine node (x along threads, y and z along the grid): the trilinear
-/// interpolant as three nested midpoints; an even index on a halved axis, and
-/// every index on a kept one, takes the same coarse node twice, which the
-/// midpoint returns exactly.
+/// per fine node of kProlongRows node rows (x along threads, a group of rows
+/// and z along the grid): the trilinear interpolant as three nested
+/// midpoints; an even index on a halved axis, and every index on a kept one,
+/// takes the same coarse node twice, which the midpoint returns exactly.  The
+/// thread loads its rows' fine values and flags first and then the coarse
+/// values, so the loads of all its rows are in flight together.
+constexpr int kProlongRows = 4;
 template <typename T>
-__device__ __forceinline__ void prolong_add_b(Dims df, Dims dc, int3 sh, const T *__restrict__ xc,
-                              T *__restrict__ xf, const uint8_t *__restrict__ fixf,
-                              const KState *gate, const Blk &B)
+__device__ __forceinline__ void prolong_rows_b(const Dims &df, const Dims &dc, const int3 &sh,
+                                               const T *__restrict__ xc, T *__restrict__ xf,
+                                               const uint8_t *__restrict__ fixf, int i, int j0,
+                                               int k)
 {
-  if(gated(gate))
-    return;
-  const int i = B.x * blockDim.x + threadIdx.x, j = B.y, k = B.z;
   if(i >= df.sx)
     return;
-  const int I0 = i >> sh.x, I1 = (i + sh.x) >> sh.x, J0 = j >> sh.y, J1 = (j + sh.y) >> sh.y;
+  constexpr int R = kProlongRows;
+  const long long fsxy = (long long)df.sx * df.sy;
+  T old[R][3];
+  unsigned fx[R];
+#pragma unroll
+  for(int r = 0; r < R; r++)
+  {
+    const int j = j0 + r;
+    const long long n = i + (long long)j * df.sx + (long long)k * fsxy;
+    fx[r] = j < df.sy ? unsigned(fixf[n]) : 7u; // a row past the grid: nothing to do
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+      old[r][c] = c < df.dim && !((fx[r] >> c) & 1u) ? xf[c * df.ld + n] : T(0);
+  }
+  const int I0 = i >> sh.x, I1 = (i + sh.x) >> sh.x;
   const int K0 = k >> sh.z, K1 = df.dim == 3 ? (k + sh.z) >> sh.z : K0;
   const long long csxy = (long long)dc.sx * dc.sy;
-  const long long r00 = (long long)J0 * dc.sx + K0 * csxy, r10 = (long long)J1 * dc.sx + K0 * csxy;
-  const long long r01 = (long long)J0 * dc.sx + K1 * csxy, r11 = (long long)J1 * dc.sx + K1 * csxy;
-  const long long n = i + (long long)j * df.sx + (long long)k * df.sx * df.sy;
-  const unsigned fx = fixf[n];
   const T h = T(0.5);
 #pragma unroll
-  for(int c = 0; c < 3; c++)
-    if(c < df.dim && !((fx >> c) & 1u))
-    {
-      const T *x = xc + c * dc.ld;
-      const T a = h * (x[r00 + I0] + x[r00 + I1]), b = h * (x[r10 + I0] + x[r10 + I1]);
-      const T a2 = h * (x[r01 + I0] + x[r01 + I1]), b2 = h * (x[r11 + I0] + x[r11 + I1]);
-      xf[c * df.ld + n] += h * (h * (a + b) + h * (a2 + b2));
-    }
+  for(int r = 0; r < R; r++)
+  {
+    const int j = j0 + r;
+    const int J0 = j >> sh.y, J1 = (j + sh.y) >> sh.y;
+    const long long r00 = (long long)J0 * dc.sx + K0 * csxy, r10 = (long long)J1 * dc.sx + K0 * csxy;
+    const long long r01 = (long long)J0 * dc.sx + K1 * csxy, r11 = (long long)J1 * dc.sx + K1 * csxy;
+    const long long n = i + (long long)j * df.sx + (long long)k * fsxy;
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+      if(c < df.dim && !((fx[r] >> c) & 1u))
+      {
+        const T *x = xc + c * dc.ld;
+        const T a = h * (x[r00 + I0] + x[r00 + I1]), b = h * (x[r10 + I0] + x[r10 + I1]);
+        const T a2 = h * (x[r01 + I0] + x[r01 + I1]), b2 = h * (x[r11 + I0] + x[r11 + I1]);
+        xf[c * df.ld + n] = old[r][c] + h * (h * (a + b) + h * (a2 + b2));
+      }
+  }
+}
+/// rows of a prolongation launch block: kProlongRows node rows each
+inline unsigned prolong_row_blocks(const Dims &d)
+{
+  return unsigned((d.sy + kProlongRows - 1) / kProlongRows);
 }
 template <typename T>
 __global__ void k_prolong_add(Dims df, Dims dc, int3 sh, const T *__restrict__ xc,
                               T *__restrict__ xf, const uint8_t *__restrict__ fixf,
                               const KState *gate)
 {
-  prolong_add_b<T>(df, dc, sh, xc, xf, fixf, gate, this_block());
+  if(gated(gate))
+    return;
+  prolong_rows_b<T>(df, dc, sh, xc, xf, fixf, blockIdx.x * blockDim.x + threadIdx.x,
+                    blockIdx.y * kProlongRows, blockIdx.z);
 }
 
 /// first smoothing step from a zero guess: x = c D^-1 b, x0 = 0
@@ -181,6 +209,7 @@ __device__ __forceinline__ void jacobi0_b(long long n, T c, const T *__restrict_
 {
   if(gated(gate))
     return;
+#pragma unroll 4
   for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)B.gx * blockDim.x)
   {
@@ -350,6 +379,7 @@ __global__ void k_dense_apply(int n, const double *__restrict__ Ainv,
 template <typename T>
 __device__ __forceinline__ void fill_b(long long n, T v, T *__restrict__ x, const Blk &B)
 {
+#pragma unroll 4
   for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)B.gx * blockDim.x)
     x[i] = v;
@@ -401,6 +431,7 @@ __device__ __forceinline__ void mg_init_b(long long n, const TK *__restrict__ b,
                           double tol, int maxit, const Blk &B)
 {
   double v[1] = {0.0};
+#pragma unroll 4
   for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)B.gx * blockDim.x)
   {
@@ -443,6 +474,7 @@ __device__ __forceinline__ void mg_init2_b(long long n, const TK *__restrict__ r
   if(st->stop)
     return;
   double v[1] = {0.0};
+#pragma unroll 4
   for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)B.gx * blockDim.x)
   {
@@ -503,6 +535,7 @@ __device__ __forceinline__ void mg_r_b(long long n, TK *__restrict__ r, TP *__re
   if(!bad)
   {
     const TK a = TK(alpha);
+#pragma unroll 4
     for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
         i += (long long)B.gx * blockDim.x)
     {
@@ -549,6 +582,7 @@ __device__ __forceinline__ void mg_rz_b(long long n, const TK *__restrict__ r, c
   if(st->stop || st->conv)
     return;
   double v[1] = {0.0};
+#pragma unroll 4
   for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)B.gx * blockDim.x)
     v[0] += double(r[i]) * double(z[i]);
@@ -596,6 +630,7 @@ __device__ __forceinline__ void mg_xp_b(long long n, TK *__restrict__ x, TK *__r
   }
   const TK a = TK(st->alpha), bt = TK(st->beta);
   const bool conv = st->conv;
+#pragma unroll 4
   for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)B.gx * blockDim.x)
   {
@@ -953,7 +988,9 @@ template <typename TK, typename TP> struct MgPcg
     k_restrict<TP><<<grid3(Cn.d), kTB, 0, s>>>(L.d, Cn.d, Cn.sh, L.r.p, Cn.b.p, Cn.fix, gate);
     count_launch();
     level(l + 1, Cn.b.p, Cn.x.p, s, gate);
-    k_prolong_add<TP><<<grid3(L.d), kTB, 0, s>>>(L.d, Cn.d, Cn.sh, Cn.x.p, cur, L.fix, gate);
+    dim3 gp = grid3(L.d);
+    gp.y = prolong_row_blocks(L.d);
+    k_prolong_add<TP><<<gp, kTB, 0, s>>>(L.d, Cn.d, Cn.sh, Cn.x.p, cur, L.fix, gate);
     count_launch();
     for(int k = 0; k < nu; k++)
     {

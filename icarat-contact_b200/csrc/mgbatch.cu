@@ -136,10 +136,13 @@ template <typename T> struct RestrictL
   __device__ void run(const Blk &B) const
   {
     Blk b = B;
+#pragma unroll 2
     for(b.y = B.y; b.y < ry; b.y += B.gy)
       restrict_b<T>(df, dc, sh, rf, bc, fixc, gate, b);
   }
 };
+/// g.gy blocks along y, each ry node rows from its first, kProlongRows at a
+/// time
 template <typename T> struct ProlongL
 {
   Blk g;
@@ -153,9 +156,12 @@ template <typename T> struct ProlongL
   __device__ bool skip() const { return gated(gate); }
   __device__ void run(const Blk &B) const
   {
-    Blk b = B;
-    for(b.y = B.y; b.y < ry; b.y += B.gy)
-      prolong_add_b<T>(df, dc, sh, xc, xf, fixf, gate, b);
+    if(gated(gate))
+      return;
+    const int i = B.x * blockDim.x + threadIdx.x;
+    const int j1 = min(df.sy, int((B.y + 1) * ry));
+    for(int j = int(B.y * ry); j < j1; j += kProlongRows)
+      prolong_rows_b<T>(df, dc, sh, xc, xf, fixf, i, j, B.z);
   }
 };
 /// Rows per work item of a batched launch whose rows are independent: one
@@ -523,10 +529,12 @@ template <typename TP> struct BatchMg
       long long rowsP = 0;
       for(const Inst &I : fine)
       {
-        const dim3 g3 = grid3(M[I.i]->lv[l].d);
-        rowsP += (long long)g3.x * g3.y * g3.z;
+        const Dims &d = M[I.i]->lv[l].d;
+        const dim3 g3 = grid3(d);
+        rowsP += (long long)g3.x * prolong_row_blocks(d) * g3.z;
       }
-      const unsigned kP = rows_per_item(rowsP, transfer_capacity(), 8);
+      // row groups of kProlongRows per work item
+      const unsigned kP = rows_per_item(rowsP, transfer_capacity(), 4);
       for(size_t t = 0; t < fine.size(); t++)
       {
         const Inst &I = fine[t];
@@ -534,8 +542,9 @@ template <typename TP> struct BatchMg
         Level<TP> &L = m.lv[l];
         Level<TP> &Cn = m.lv[l + 1];
         const dim3 g3 = grid3(L.d);
-        pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i), g3.y}, g3.x,
-               transfer_rows(g3.y, kP), g3.z);
+        const unsigned rows = kP * kProlongRows; // node rows per work item
+        pr.add(ProlongL<TP>{{}, L.d, Cn.d, Cn.sh, Cn.x.p, cs[t].cur, L.fix, gate(I.i), rows}, g3.x,
+               transfer_rows(g3.y, rows), g3.z);
       }
       push(pr.finish(kTB, 0, s, qc.p));
     }
