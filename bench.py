@@ -872,7 +872,9 @@ def workload_batched(args):
                 "steps": steps}, H, X
 
     short = args.loop_steps_short
-    run(2, True, 1)  # hierarchies, filters and graphs built once (not timed)
+    # hierarchies, filters and graphs built once for both paths (not timed)
+    run(2, True, 1)
+    run(2, False, 1)
     seq, Hs, Xs = run(short, False, 1)
     runs = {"sequential": seq}
     same = True

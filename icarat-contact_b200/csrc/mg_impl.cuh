@@ -40,6 +40,12 @@ __device__ __forceinline__ bool gated(const KState *g)
 {
   return g && (g->stop || g->conv);
 }
+/// The vector kernels walk their grid-stride loop (i, i + s, i + 2s, ...) in
+/// groups of kGroup iterations: the operands of a group are loaded before any
+/// of its iterations is processed, so a thread has kGroup loads in flight per
+/// operand instead of one; the iterations (and the order of every sum) are
+/// those of the plain loop.
+constexpr int kGroup = 4;
 
 // ------------------------------------------------------- grid transfer ----
 /// coarse modulus = sum of the children's E over the number of child slots
@@ -209,12 +215,27 @@ __device__ __forceinline__ void jacobi0_b(long long n, T c, const T *__restrict_
 {
   if(gated(gate))
     return;
-#pragma unroll 4
-  for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
-      i += (long long)B.gx * blockDim.x)
+  const long long st = (long long)B.gx * blockDim.x;
+  for(long long i0 = B.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += kGroup * st)
   {
-    x[i] = c * dinv[i] * b[i];
-    x0[i] = T(0); // the iterate before x, for the next three-term step
+    T dv[kGroup], bv[kGroup];
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * st;
+      dv[g] = i < n ? dinv[i] : T(0);
+      bv[g] = i < n ? b[i] : T(0);
+    }
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * st;
+      if(i < n)
+      {
+        x[i] = c * dv[g] * bv[g];
+        x0[i] = T(0); // the iterate before x, for the next three-term step
+      }
+    }
   }
 }
 template <typename T>
@@ -379,7 +400,6 @@ __global__ void k_dense_apply(int n, const double *__restrict__ Ainv,
 template <typename T>
 __device__ __forceinline__ void fill_b(long long n, T v, T *__restrict__ x, const Blk &B)
 {
-#pragma unroll 4
   for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
       i += (long long)B.gx * blockDim.x)
     x[i] = v;
@@ -431,16 +451,27 @@ __device__ __forceinline__ void mg_init_b(long long n, const TK *__restrict__ b,
                           double tol, int maxit, const Blk &B)
 {
   double v[1] = {0.0};
-#pragma unroll 4
-  for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
-      i += (long long)B.gx * blockDim.x)
+  const long long sd = (long long)B.gx * blockDim.x;
+  for(long long i0 = B.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += kGroup * sd)
   {
-    TK bi = b[i];
-    r[i] = bi;
-    if(rP)
-      rP[i] = TP(bi);
-    x[i] = TK(0);
-    v[0] += double(bi) * double(bi);
+    TK bv[kGroup];
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+      bv[g] = i0 + g * sd < n ? b[i0 + g * sd] : TK(0);
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * sd;
+      if(i < n)
+      {
+        const TK bi = bv[g];
+        r[i] = bi;
+        if(rP)
+          rP[i] = TP(bi);
+        x[i] = TK(0);
+        v[0] += double(bi) * double(bi);
+      }
+    }
   }
   block_reduce_at<1>(v, red, FinInitMg{st, tol, maxit}, int(B.x), int(B.gx));
 }
@@ -474,13 +505,29 @@ __device__ __forceinline__ void mg_init2_b(long long n, const TK *__restrict__ r
   if(st->stop)
     return;
   double v[1] = {0.0};
-#pragma unroll 4
-  for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
-      i += (long long)B.gx * blockDim.x)
+  const long long sd = (long long)B.gx * blockDim.x;
+  for(long long i0 = B.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += kGroup * sd)
   {
-    TK zi = TK(z[i]);
-    p[i] = zi;
-    v[0] += double(r[i]) * double(zi);
+    TP zv[kGroup];
+    TK rv[kGroup];
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * sd;
+      zv[g] = i < n ? z[i] : TP(0);
+      rv[g] = i < n ? r[i] : TK(0);
+    }
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * sd;
+      if(i < n)
+      {
+        TK zi = TK(zv[g]);
+        p[i] = zi;
+        v[0] += double(rv[g]) * double(zi);
+      }
+    }
   }
   block_reduce_at<1>(v, red, FinRz0{st}, int(B.x), int(B.gx));
 }
@@ -535,16 +582,33 @@ __device__ __forceinline__ void mg_r_b(long long n, TK *__restrict__ r, TP *__re
   if(!bad)
   {
     const TK a = TK(alpha);
-#pragma unroll 4
-    for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
-        i += (long long)B.gx * blockDim.x)
+    const long long sd = (long long)B.gx * blockDim.x;
+    for(long long i0 = B.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += kGroup * sd)
     {
-      TK ri = r[i] - a * q[i];
-      r[i] = ri;
-      if(rP)
-        rP[i] = TP(ri);
-      v[0] += double(ri) * double(ri);
-      v[1] += double(ri) * double(zold[i]);
+      TK rv[kGroup], qv[kGroup];
+      TP zv[kGroup];
+#pragma unroll
+      for(int g = 0; g < kGroup; g++)
+      {
+        const long long i = i0 + g * sd;
+        rv[g] = i < n ? r[i] : TK(0);
+        qv[g] = i < n ? q[i] : TK(0);
+        zv[g] = i < n ? zold[i] : TP(0);
+      }
+#pragma unroll
+      for(int g = 0; g < kGroup; g++)
+      {
+        const long long i = i0 + g * sd;
+        if(i < n)
+        {
+          TK ri = rv[g] - a * qv[g];
+          r[i] = ri;
+          if(rP)
+            rP[i] = TP(ri);
+          v[0] += double(ri) * double(ri);
+          v[1] += double(ri) * double(zv[g]);
+        }
+      }
     }
   }
   block_reduce_at<2>(v, red, FinRmg{st, pqv, alpha, bad}, int(B.x), int(B.gx));
@@ -582,10 +646,23 @@ __device__ __forceinline__ void mg_rz_b(long long n, const TK *__restrict__ r, c
   if(st->stop || st->conv)
     return;
   double v[1] = {0.0};
-#pragma unroll 4
-  for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
-      i += (long long)B.gx * blockDim.x)
-    v[0] += double(r[i]) * double(z[i]);
+  const long long sd = (long long)B.gx * blockDim.x;
+  for(long long i0 = B.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += kGroup * sd)
+  {
+    TK rv[kGroup];
+    TP zv[kGroup];
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * sd;
+      rv[g] = i < n ? r[i] : TK(0);
+      zv[g] = i < n ? z[i] : TP(0);
+    }
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+      if(i0 + g * sd < n)
+        v[0] += double(rv[g]) * double(zv[g]);
+  }
   block_reduce_at<1>(v, red, FinRz{st}, int(B.x), int(B.gx));
 }
 template <typename TK, typename TP>
@@ -630,14 +707,31 @@ __device__ __forceinline__ void mg_xp_b(long long n, TK *__restrict__ x, TK *__r
   }
   const TK a = TK(st->alpha), bt = TK(st->beta);
   const bool conv = st->conv;
-#pragma unroll 4
-  for(long long i = B.x * (long long)blockDim.x + threadIdx.x; i < n;
-      i += (long long)B.gx * blockDim.x)
+  const long long sd = (long long)B.gx * blockDim.x;
+  for(long long i0 = B.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += kGroup * sd)
   {
-    TK pi = p[i];
-    x[i] += a * pi;
-    if(!conv)
-      p[i] = TK(z[i]) + bt * pi;
+    TK pv[kGroup], xv[kGroup];
+    TP zv[kGroup];
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * sd;
+      pv[g] = i < n ? p[i] : TK(0);
+      xv[g] = i < n ? x[i] : TK(0);
+      zv[g] = i < n && !conv ? z[i] : TP(0);
+    }
+#pragma unroll
+    for(int g = 0; g < kGroup; g++)
+    {
+      const long long i = i0 + g * sd;
+      if(i < n)
+      {
+        const TK pi = pv[g];
+        x[i] = xv[g] + a * pi;
+        if(!conv)
+          p[i] = TK(zv[g]) + bt * pi;
+      }
+    }
   }
   double v[1] = {0.0};
   block_reduce_at<1>(v, red, FinXPmg{st, L}, int(B.x), int(B.gx));
