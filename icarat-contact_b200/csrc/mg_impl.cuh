@@ -1123,6 +1123,13 @@ template <typename TK, typename TP> struct MgPcg
     k_mg_init2<TK, TP><<<nb, VB, 0, s>>>(n, r.p, z.p, p.p, red, st.p);
     count_launch();
     ICB_CUDA(cudaGetLastError());
+    return iterate(x, maxit, s, info);
+  }
+
+  /// the iteration graph for iterates x on stream s (built when anything it
+  /// bakes in changed)
+  void prepareLoop(TK *x, cudaStream_t s)
+  {
     GraphKey k;
     k.add(x).add(Ek).add(lv[0].E).add((const void *)s).add((long long)kernel_switches());
     const bool dev = device_loops_enabled();
@@ -1133,11 +1140,25 @@ template <typename TK, typename TP> struct MgPcg
       count_launch(before - thread_launch_count()); // recorded, not launched
       key = k;
     }
+  }
+  /// device form: the iterations until the solve stops as one launch on s,
+  /// and the final state copied to hst (valid once s is synchronised)
+  void launchLoop(cudaStream_t s)
+  {
+    loop.launch(s);
+    ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+  }
+
+  /// the FCG iterations from the current state until the solve stops: the
+  /// rest of a solve that solve() or a batched solve of many problems began
+  /// (the same kernels per iteration, so the same iterates)
+  int iterate(TK *x, int maxit, cudaStream_t s, icb_solve_info *info)
+  {
+    prepareLoop(x, s);
     if(loop.device)
     {
       // the whole solve: one launch, one wait
-      loop.launch(s);
-      ICB_CUDA(cudaMemcpyAsync(hst, st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+      launchLoop(s);
       ICB_CUDA(cudaStreamSynchronize(s));
       count_launch((long long)hst->pad * loop.graphNodes);
     }

@@ -763,9 +763,15 @@ template <typename TP> struct BatchMg
   }
 
   /// run the set-up and iterations until every problem has stopped (each
-  /// stops at its own tolerance or iteration limit, as its own solve would)
-  long long iterationsRun = 0; ///< iterations of the last run()
-  void run(int maxit, cudaStream_t s)
+  /// stops at its own tolerance or iteration limit, as its own solve would).
+  /// When at most handOff() problems are left, each finishes in its own
+  /// solve loop on its own stream (own[i], solving into x[i]): the same
+  /// iterations, without the batch's launches over every problem.
+  long long iterationsRun = 0; ///< batched iterations of the last run()
+  int handedOff = 0;           ///< problems of the last run() finished on their own
+  int handOff() const { return std::min(32, std::max(1, int(M.size()) / 8)); }
+  void run(int maxit, cudaStream_t s, const std::vector<cudaStream_t> &own,
+           const std::vector<double *> &x)
   {
     for(auto &f : refresh)
       f(s);
@@ -773,6 +779,7 @@ template <typename TP> struct BatchMg
       f(s);
     long long launched = 0;
     const int n = int(M.size());
+    handedOff = 0;
     for(;;)
     {
       // the share of the batch still iterating when this launch starts
@@ -786,8 +793,51 @@ template <typename TP> struct BatchMg
       launched += batch;
       if(*hActive == 0 || launched > (long long)maxit + batch)
         break;
+      if(*hActive <= handOff() && n > handOff())
+      {
+        const int left = *hActive;
+        const auto t1 = std::chrono::steady_clock::now();
+        finishAlone(maxit, s, own, x);
+        fused_active_record(left, n, std::chrono::duration<double>(
+                                         std::chrono::steady_clock::now() - t1).count());
+        break;
+      }
     }
     iterationsRun = launched;
+  }
+
+  /// every problem still iterating continues in its own loop on its own
+  /// stream (after the batch's work on s), then s waits for them all
+  void finishAlone(int maxit, cudaStream_t s, const std::vector<cudaStream_t> &own,
+                   const std::vector<double *> &x)
+  {
+    const int n = int(M.size());
+    std::vector<KState> hs(n);
+    for(int i = 0; i < n; i++)
+      ICB_CUDA(cudaMemcpyAsync(&hs[i], M[i]->st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> left;
+    for(int i = 0; i < n; i++)
+      if(!hs[i].stop)
+        left.push_back(i);
+    // s is idle (synchronised above): the problems' streams may start, and
+    // in the device form their loops run side by side
+    for(int i : left)
+    {
+      MG &m = *M[i];
+      m.prepareLoop(x[i], own[i]);
+      if(m.loop.device)
+        m.launchLoop(own[i]);
+      else
+        m.iterate(x[i], maxit, own[i], nullptr);
+    }
+    handedOff = int(left.size());
+    for(int i : left)
+    {
+      ICB_CUDA(cudaStreamSynchronize(own[i]));
+      if(M[i]->loop.device)
+        count_launch((long long)M[i]->hst->pad * M[i]->loop.graphNodes);
+    }
   }
 };
 
@@ -977,7 +1027,16 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
       int maxit = 0;
       for(OcRun *r : set)
         maxit = std::max(maxit, r->o->solve.maxit);
-      batch.run(maxit, sb);
+      {
+        std::vector<cudaStream_t> own;
+        std::vector<double *> xs;
+        for(OcRun *r : set)
+        {
+          own.push_back(r->p->stream());
+          xs.push_back(r->p->x.p);
+        }
+        batch.run(maxit, sb, own, xs);
+      }
       for(size_t k = 0; k < set.size(); k++)
         ICB_CUDA(cudaMemcpyAsync(&hs[set[k]->idx], batch.M[k]->st.p, sizeof(KState),
                                  cudaMemcpyDeviceToHost, sb));

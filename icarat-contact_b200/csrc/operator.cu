@@ -926,23 +926,17 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
   // its strip of that row, so the total does not depend on how the rows are
   // cut into blocks
   const int strips = nbx * TY2, strip = bxi * TY2 + w;
-  for(int ej = Y0 - 1; ej <= Y1; ++ej)
-  {
+  // the inputs of the update of row ej's output node (FP32: loaded a row
+  // ahead, with the next node row; the previous iterate in y is read before
+  // this thread, its only writer, overwrites it)
+  auto load_inp = [&](int ej, unsigned &f, T(&us)[2], T(&bv)[2], T(&dv)[2], T(&yp)[2]) {
+    f = 0;
 #pragma unroll
     for(int c = 0; c < 2; c++)
-#pragma unroll
-      for(int a = 0; a < 2; a++)
-        ut[c][a] = un[c][a];
-    const T Ee = En;
-    if(ej < Y1)
-      load_row(ej + 1, un, En);
-    // this row's output node and the inputs of its update
-    const bool own = ej >= Y0 && ownCol;
-    const long long node = (long long)ni + (long long)ej * d.sx;
-    unsigned f = 0;
-    T us[2] = {T(0), T(0)}, bv[2] = {T(0), T(0)}, dv[2] = {T(0), T(0)}, yp[2] = {T(0), T(0)};
-    if(own)
+      us[c] = bv[c] = dv[c] = yp[c] = T(0);
+    if(ej >= Y0 && ej <= Y1 && ownCol)
     {
+      const long long node = (long long)ni + (long long)ej * d.sx;
       f = __ldg(fix + node);
 #pragma unroll
       for(int c = 0; c < 2; c++)
@@ -955,9 +949,48 @@ __device__ __forceinline__ void q4_body(const KMat<T, 8> &K, const Dims &d, cons
         if(MODE >= OP_JACOBI)
           dv[c] = __ldg(ep.dinv + i);
         if(MODE == OP_CHEB && ep.c1 != T(0))
-          yp[c] = y[i]; // the previous iterate, read before this thread overwrites it
+          yp[c] = y[i];
       }
     }
+  };
+  constexpr bool kAhead = sizeof(T) == 4;
+  unsigned nf = 0;
+  T nus[2], nbv[2], ndv[2], nyp[2];
+  if(kAhead)
+    load_inp(Y0 - 1, nf, nus, nbv, ndv, nyp);
+  for(int ej = Y0 - 1; ej <= Y1; ++ej)
+  {
+#pragma unroll
+    for(int c = 0; c < 2; c++)
+#pragma unroll
+      for(int a = 0; a < 2; a++)
+        ut[c][a] = un[c][a];
+    const T Ee = En;
+    // this row's output node and the inputs of its update
+    const bool own = ej >= Y0 && ownCol;
+    const long long node = (long long)ni + (long long)ej * d.sx;
+    unsigned f;
+    T us[2], bv[2], dv[2], yp[2];
+    if(kAhead)
+    {
+      f = nf;
+#pragma unroll
+      for(int c = 0; c < 2; c++)
+      {
+        us[c] = nus[c];
+        bv[c] = nbv[c];
+        dv[c] = ndv[c];
+        yp[c] = nyp[c];
+      }
+    }
+    if(ej < Y1)
+    {
+      load_row(ej + 1, un, En);
+      if(kAhead)
+        load_inp(ej + 1, nf, nus, nbv, ndv, nyp);
+    }
+    if(!kAhead)
+      load_inp(ej, f, us, bv, dv, yp);
     // element vector in local order: n0=(0,0) n1=(1,0) n2=(1,1) n3=(0,1)
     T ue[8];
 #pragma unroll
