@@ -206,6 +206,45 @@ __device__ __forceinline__ void oc_cand_b(long long nel, const double *__restric
       e += (long long)B.gx * blockDim.x)
     xc[e] = oc_candidate(x[e], df[e], dg[e], lam, P.eta, P.move, xmin[e], xmax[e]);
 }
+/// the candidates of elements [base, base + VB * kCandPerThread) (the
+/// batched launch's work item: no reduction, so any cut of the elements
+/// gives the same values); each thread's loads in groups of four
+constexpr int kCandPerThread = 8;
+__device__ __forceinline__ void oc_cand_chunk(long long nel, const double *__restrict__ x,
+                                              const double *__restrict__ df,
+                                              const double *__restrict__ dg,
+                                              const double *__restrict__ xmin,
+                                              const double *__restrict__ xmax, const OcParams &P,
+                                              const OcState *st, double *__restrict__ xc,
+                                              long long base)
+{
+  if(st->done)
+    return;
+  const double lam = st->lam;
+  constexpr int G = 4;
+  for(int k0 = 0; k0 < kCandPerThread; k0 += G)
+  {
+    double xv[G], fv[G], gv[G], lo[G], hi[G];
+#pragma unroll
+    for(int g = 0; g < G; g++)
+    {
+      const long long e = base + threadIdx.x + (long long)(k0 + g) * VB;
+      const bool in = e < nel;
+      xv[g] = in ? x[e] : 0.0;
+      fv[g] = in ? df[e] : 0.0;
+      gv[g] = in ? dg[e] : 1.0;
+      lo[g] = in ? xmin[e] : 0.0;
+      hi[g] = in ? xmax[e] : 0.0;
+    }
+#pragma unroll
+    for(int g = 0; g < G; g++)
+    {
+      const long long e = base + threadIdx.x + (long long)(k0 + g) * VB;
+      if(e < nel)
+        xc[e] = oc_candidate(xv[g], fv[g], gv[g], lam, P.eta, P.move, lo[g], hi[g]);
+    }
+  }
+}
 __global__ void k_oc_cand(long long nel, const double *__restrict__ x,
                           const double *__restrict__ df, const double *__restrict__ dg,
                           const double *__restrict__ xmin, const double *__restrict__ xmax,
@@ -304,13 +343,25 @@ __device__ __forceinline__ void oc_step_tile_b(const Dims &d, int hx, int hy, un
   double *sw = tile + TWP * THP;
   int *so = reinterpret_cast<int *>(sw + nnb);
   const int x0 = int(B.x % ntx) * kOcTW, y0 = int(B.x / ntx) * kOcTH;
-  for(int q = threadIdx.x; q < TWP * THP; q += blockDim.x)
+  // every load of the tile in flight before the first shared store
+  constexpr int kPer = ((kOcTW + 2 * kOcHalo) * (kOcTH + 2 * kOcHalo) + VB - 1) / VB;
+  double tv[kPer];
+#pragma unroll
+  for(int k = 0; k < kPer; k++)
   {
+    const int q = threadIdx.x + k * VB;
     const int ty = q / TWP, tx = q - ty * TWP;
     const int i = x0 - hx + tx, j = y0 - hy + ty;
-    tile[q] = unsigned(i) < unsigned(d.nx) && unsigned(j) < unsigned(d.ny)
-                  ? __ldg(xc + i + (long long)j * d.nx)
-                  : 0.0;
+    tv[k] = q < TWP * THP && unsigned(i) < unsigned(d.nx) && unsigned(j) < unsigned(d.ny)
+                ? __ldg(xc + i + (long long)j * d.nx)
+                : 0.0;
+  }
+#pragma unroll
+  for(int k = 0; k < kPer; k++)
+  {
+    const int q = threadIdx.x + k * VB;
+    if(q < TWP * THP)
+      tile[q] = tv[k];
   }
   for(int t = threadIdx.x; t < nnb; t += blockDim.x)
   {
@@ -931,7 +982,7 @@ struct OcBatch::Rec
 {
   Dims d;
   unsigned gx;  ///< blocks of the problem's own step launch (tiles or vblocks(nel))
-  unsigned gxc; ///< blocks of its candidate launch (vblocks(nel))
+  unsigned gxc; ///< work items of its candidates (VB * kCandPerThread elements each)
   int tiled, hx, hy;
   unsigned ntx;
   const int4 *off;
@@ -964,8 +1015,8 @@ __global__ void __launch_bounds__(VB, 4)
       R, map, q, [](const OcBatch::Rec &r) { return int(r.gxc); },
       [](const OcBatch::Rec &r) { return r.st->done != 0 || !r.P.useFilter; },
       [](const OcBatch::Rec &r, int b, bool) {
-        oc_cand_b(r.d.nel, r.x, r.df, r.dg, r.xmin, r.xmax, r.P, r.st, r.xc,
-                  Blk{unsigned(b), 0, 0, r.gxc, 1, 1});
+        oc_cand_chunk(r.d.nel, r.x, r.df, r.dg, r.xmin, r.xmax, r.P, r.st, r.xc,
+                      (long long)b * VB * kCandPerThread);
       });
 }
 __global__ void __launch_bounds__(VB, 4)
@@ -1041,7 +1092,7 @@ void OcBatch::build(const std::vector<OcBatchItem> &items, cudaStream_t s)
     Rec &r = R[i];
     r.d = it.oc->d;
     const OcTiling tl = oc_tiling(r.d, it.cone);
-    r.gxc = unsigned(vblocks(r.d.nel));
+    r.gxc = unsigned((r.d.nel + VB * kCandPerThread - 1) / (VB * kCandPerThread));
     r.gx = tl.tiled ? unsigned(tl.blocks) : r.gxc;
     r.tiled = tl.tiled;
     r.hx = tl.hx;
