@@ -414,20 +414,12 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
   load_plane(Z0, nxt);
   T Enxt = load_E(Z0 - 1);
   double dot = 0.0;
-  // FP32: the output node's own value is corner (1,1) of the plane loaded a
-  // layer earlier; kept from there instead of loaded again (columns outside
-  // the grid load zeros and load their node instead)
-  constexpr bool kKeepOwn = sizeof(T) == 4;
-  T ownU[3] = {T(0), T(0), T(0)};
   for(int ek = Z0 - 1; ek <= Z1; ++ek)
   {
-    T th[3][4], nextOwn[3];
+    T th[3][4];
 #pragma unroll
     for(int c = 0; c < 3; c++)
-    {
-      nextOwn[c] = nxt[c][2];
       plane_modes(nxt[c], th[c]);
-    }
     const T Ee = Enxt;
     // next layer's inputs: FP32 at the top of the layer, FP64 after the
     // element product (its registers are the limit)
@@ -451,7 +443,7 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
         for(int c = 0; c < 3; c++)
         {
           if(DOT || MODE >= OP_JACOBI)
-            in.us[c] = kKeepOwn && col ? ownU[c] : __ldg(u + c * ld + node);
+            in.us[c] = __ldg(u + c * ld + node);
           if(MODE != OP_APPLY)
             in.b[c] = __ldg(ep.b + c * ld + node);
           if(MODE >= OP_JACOBI)
@@ -555,10 +547,6 @@ __global__ void __launch_bounds__(TX *TYK, MINB)
         }
       }
     }
-    if(kKeepOwn)
-#pragma unroll
-      for(int c = 0; c < 3; c++)
-        ownU[c] = nextOwn[c];
   }
   if(DOT)
   {
