@@ -833,6 +833,7 @@ def workload_batched(args):
     import cases
     import icarat_b200 as icb
     N = args.instances
+    icb.set_option("batch_handoff", args.handoff)
     rng = np.random.default_rng(4)
     insts = [cases.random_instance2d(rng) for _ in range(N)]
     # several GPUs: every rank runs its footprint-balanced share, no exchange
@@ -909,7 +910,9 @@ def workload_batched(args):
                       "scaling": "strong (the instances are split over the GPUs by footprint)",
                       "dtype": "f64 Krylov / f32 multigrid", "data": "synthetic (seeded instances)",
                       "config": {"workload": f"{N} 2D Q4 instances, {nel_total} elements on rank 0",
-                                 "oc_steps": args.loop_steps},
+                                 "oc_steps": args.loop_steps,
+                                 "oc_steps_vs_sequential": args.loop_steps_short,
+                                 "handoff": icb.get_option("batch_handoff")},
                       "speedup_vs_sequential": fused_short["inst_iter_s"] / seq["inst_iter_s"],
                       "bitwise_equal_to_sequential": same,
                       "fused_phases": "build, per-instance set-up launches, batched multigrid "
@@ -1103,6 +1106,9 @@ def main():
     ap.add_argument("--jobs-per-rate", type=int, default=24)
     ap.add_argument("--iter-scale", type=float, default=0.2, help="serving: scale on U[50,200] steps")
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--handoff", type=int, default=0,
+                    help="batched: designs left when the fused solves hand them to their own "
+                         "loops (0: the library default)")
     ap.add_argument("--max-connections", type=int, default=32,
                     help="batched / serving: CUDA_DEVICE_MAX_CONNECTIONS (hardware work queues "
                          "the many per-instance streams map onto; CUDA's default is 8)")

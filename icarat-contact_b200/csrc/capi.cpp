@@ -603,6 +603,11 @@ int icb_set_option(const char *name, long long value)
     set_hex8_pair(value != 0);
   else if(n == "batch_fused")
     set_batch_fused(value != 0);
+  else if(n == "batch_handoff")
+  {
+    need(value >= 0 && value <= 1000000, "batch_handoff must be in [0, 1e6]");
+    set_batch_handoff(int(value));
+  }
   else if(n == "tc_spin_limit")
   {
     need(value >= 0 && value <= 0x7fffffffLL, "tc_spin_limit must be in [0, 2^31)");
@@ -628,6 +633,8 @@ long long icb_get_option(const char *name)
     return hex8_pair_enabled() ? 1 : 0;
   if(n == "batch_fused")
     return batch_fused_enabled() ? 1 : 0;
+  if(n == "batch_handoff")
+    return batch_handoff();
   if(n == "fused_batch_iters")
     return fused_iterations(0);
   if(n == "fused_problem_iters")

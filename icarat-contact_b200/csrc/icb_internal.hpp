@@ -209,6 +209,10 @@ long long fused_iterations(int k);
 /// share of the batch still iterating (k = 0: > 1/2, 1: > 1/8, 2: <= 1/8):
 /// wall seconds and launches
 void fused_active_record(int active, int n, double seconds);
+/// designs left when a fused batch hands them to their own solve loops
+/// (option batch_handoff; 0: an eighth of the batch, at most 32)
+int batch_handoff();
+void set_batch_handoff(int k);
 double fused_active_seconds(int k);
 long long fused_active_launches(int k);
 /// whether icb_run_batch uses the fused loop when a batch qualifies (option

@@ -769,7 +769,11 @@ template <typename TP> struct BatchMg
   /// iterations, without the batch's launches over every problem.
   long long iterationsRun = 0; ///< batched iterations of the last run()
   int handedOff = 0;           ///< problems of the last run() finished on their own
-  int handOff() const { return std::min(32, std::max(1, int(M.size()) / 8)); }
+  int handOff() const
+  {
+    const int k = batch_handoff();
+    return k > 0 ? k : std::min(32, std::max(1, int(M.size()) / 8));
+  }
   void run(int maxit, cudaStream_t s, const std::vector<cudaStream_t> &own,
            const std::vector<double *> &x)
   {
@@ -1176,6 +1180,10 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
   cudaFreeHost(hs);
 }
 } // namespace
+
+static std::atomic<int> g_batch_handoff{0};
+int batch_handoff() { return g_batch_handoff; }
+void set_batch_handoff(int k) { g_batch_handoff = k; }
 
 static std::atomic<bool> g_batch_fused{true};
 bool batch_fused_enabled() { return g_batch_fused; }

@@ -448,7 +448,10 @@ long long icb_launch_count(void);
  * each started: more than a half, more than an eighth, at most an eighth).
  * Further switches: "hex8_pair" (FP32 Hex8 operator with two element rows per
  * thread), "tc_spin_limit" (polls of a tensor-core wait before it gives up),
- * "batch_fused" (icb_run_batch advances qualifying 2D OC batches together).
+ * "batch_fused" (icb_run_batch advances qualifying 2D OC batches together),
+ * "batch_handoff" (a fused batch's solves hand the designs still iterating to
+ * their own solve loops once at most this many are left; 0, the default: an
+ * eighth of the batch, at most 32).
  * Unknown names: ICB_ERR_BAD_ARG / -1. */
 int icb_set_option(const char *name, long long value);
 long long icb_get_option(const char *name);
