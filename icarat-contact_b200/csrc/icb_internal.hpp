@@ -261,16 +261,16 @@ void q4_grid(const Dims &d, int &bx, int &by, int &ychunk);
 /// launch's own grid) and the work queue over those items (batchq.cuh)
 template <typename T>
 void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q, int grid,
-                     int mode, bool dot, cudaStream_t s);
+                     int mode, bool dot, const KMat<T, 8> *uniformK, cudaStream_t s);
 /// CTAs of that persistent launch (by the kernel's occupancy), found once when
 /// the launch is built, outside any stream capture
-template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q);
+template <typename T> int q4_batch_grid(int mode, bool dot, bool uniformK, BatchQueue &q);
 /// warps of one block of the Q4 operator, and the resident warps of its
 /// batched launch on the whole GPU
 int q4_block_warps();
 /// reduction slots of the Q4 operator's fused dot (a node row per warp strip)
 int q4_dot_slots(const Dims &d);
-template <typename T> long long q4_batch_capacity_warps(int mode, bool dot);
+template <typename T> long long q4_batch_capacity_warps(int mode, bool dot, bool uniformK);
 
 /// tensor-core (tcgen05, TF32) Hex8 operator (operator_tc.cu)
 void launch_op_tc(const Dims &d, const float *K, const float *E, const float *u, float *y,

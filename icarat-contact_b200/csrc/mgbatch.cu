@@ -340,6 +340,11 @@ template <typename T> struct Q4Builder
   {
     if(recs.empty())
       return {};
+    // one element matrix for every launch (the same material and element
+    // shape): it goes to the kernel as a parameter
+    bool uniform = true;
+    for(const Q4Launch<T> &q : recs)
+      uniform = uniform && std::memcmp(q.K.k, recs[0].K.k, sizeof(q.K.k)) == 0;
     {
       // the operator's output does not depend on how its rows are cut into
       // blocks (every node is the same sum, computed by its owner), nor does
@@ -351,7 +356,7 @@ template <typename T> struct Q4Builder
       for(const Q4Launch<T> &q : recs)
         rows += (long long)q.bx * q4_block_warps() * q.d.sy;
       const unsigned k =
-          rows_per_item(rows, q4_batch_capacity_warps<T>(mode, dot), kQ4BatchRows);
+          rows_per_item(rows, q4_batch_capacity_warps<T>(mode, dot, uniform), kQ4BatchRows);
       for(Q4Launch<T> &q : recs)
       {
         q.ychunk = std::min<int>(q.d.sy, int(k));
@@ -372,9 +377,11 @@ template <typename T> struct Q4Builder
     const int md = mode;
     const bool dt = dot;
     BatchQueue q{counters, counters + 1, int(map.size())};
-    const int grid = q4_batch_grid<T>(md, dt, q);
-    return [D, M, q, grid, md, dt](cudaStream_t cs) {
-      launch_q4_batch<T>(D->p, M->p, q, grid, md, dt, cs);
+    const int grid = q4_batch_grid<T>(md, dt, uniform, q);
+    const bool uk = uniform;
+    const KMat<T, 8> K = recs[0].K;
+    return [D, M, q, grid, md, dt, uk, K](cudaStream_t cs) {
+      launch_q4_batch<T>(D->p, M->p, q, grid, md, dt, uk ? &K : nullptr, cs);
     };
   }
 };

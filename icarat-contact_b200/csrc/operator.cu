@@ -1095,32 +1095,43 @@ __global__ void __launch_bounds__(TX *TY2)
 /// many Q4 operator launches in one: block b runs block map[b].y of the
 /// launch described by D[map[b].x], with that launch's grid, so each
 /// problem's result (and its fused dot product) is bitwise that of its own
-/// launch
-template <typename T, bool DOT, int MODE>
+/// launch.  UK: every launch has the same element matrix, passed as the
+/// kernel parameter Ku (constant-bank FMA operands, as in the per-problem
+/// kernel); otherwise each record's matrix is staged in shared memory.
+template <typename T, bool DOT, int MODE, bool UK>
 __global__ void __launch_bounds__(TX *TY2, sizeof(T) == 4 ? 8 : 4)
     k_matvec_q4_batch(const Q4Launch<T> *__restrict__ D, const int2 *__restrict__ map,
-                      BatchQueue bq)
+                      BatchQueue bq, const KMat<T, 8> Ku)
 {
   batch_queue(
       D, map, bq, [](const Q4Launch<T> &q) { return q.bx * q.by; },
       [](const Q4Launch<T> &q) {
         return q.gate && (q.gate->stop || (q.gateConv && q.gate->conv));
       },
-      [](const Q4Launch<T> &q, int b, bool fresh) {
-        // the element matrix in shared memory: in registers it would take 64
-        // (FP32) or 128 (FP64) of them and a quarter of the occupancy; staged
-        // once per run of items of one record (the queue's barrier after each
-        // item protects it until every thread is done)
-        __shared__ KMat<T, 8> sK;
-        if(fresh)
+      [&](const Q4Launch<T> &q, int b, bool fresh) {
+        if constexpr(UK)
         {
-          const int t = threadIdx.x + blockDim.x * threadIdx.y;
-          if(t < 64)
-            sK.k[t] = q.K.k[t];
-          __syncthreads();
+          (void)fresh;
+          q4_body<T, DOT, MODE>(Ku, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
+                                q.gateConv, q.ep, b % q.bx, b / q.bx, q.bx, q.by);
         }
-        q4_body<T, DOT, MODE>(sK, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut, q.gate,
-                              q.gateConv, q.ep, b % q.bx, b / q.bx, q.bx, q.by);
+        else
+        {
+          // the element matrix in shared memory: in registers it would take
+          // 64 (FP32) or 128 (FP64) of them and a quarter of the occupancy;
+          // staged once per run of items of one record (the queue's barrier
+          // after each item protects it until every thread is done)
+          __shared__ KMat<T, 8> sK;
+          if(fresh)
+          {
+            const int t = threadIdx.x + blockDim.x * threadIdx.y;
+            if(t < 64)
+              sK.k[t] = q.K.k[t];
+            __syncthreads();
+          }
+          q4_body<T, DOT, MODE>(sK, q.d, q.ychunk, q.E, q.u, q.y, q.fix, q.red, q.dotOut,
+                                q.gate, q.gateConv, q.ep, b % q.bx, b / q.bx, q.bx, q.by);
+        }
       });
 }
 
@@ -1620,23 +1631,27 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
   count_launch();
 }
 
-template <typename T> static const void *q4_batch_kernel(int mode, bool dot)
+template <typename T, bool UK> static const void *q4_batch_kernel_uk(int mode, bool dot)
 {
   if(mode == OP_APPLY)
-    return dot ? (const void *)k_matvec_q4_batch<T, true, OP_APPLY>
-               : (const void *)k_matvec_q4_batch<T, false, OP_APPLY>;
+    return dot ? (const void *)k_matvec_q4_batch<T, true, OP_APPLY, UK>
+               : (const void *)k_matvec_q4_batch<T, false, OP_APPLY, UK>;
   if(mode == OP_RESIDUAL)
-    return (const void *)k_matvec_q4_batch<T, false, OP_RESIDUAL>;
+    return (const void *)k_matvec_q4_batch<T, false, OP_RESIDUAL, UK>;
   if(mode == OP_CHEB)
-    return (const void *)k_matvec_q4_batch<T, false, OP_CHEB>;
+    return (const void *)k_matvec_q4_batch<T, false, OP_CHEB, UK>;
   throw Error{ICB_ERR_BAD_ARG, "batched Q4 operator: unsupported mode"};
 }
-template <typename T> int q4_batch_grid(int mode, bool dot, BatchQueue &q)
+template <typename T> static const void *q4_batch_kernel(int mode, bool dot, bool uk)
 {
-  return queue_grid(q4_batch_kernel<T>(mode, dot), TX * TY2, 0, q);
+  return uk ? q4_batch_kernel_uk<T, true>(mode, dot) : q4_batch_kernel_uk<T, false>(mode, dot);
 }
-template int q4_batch_grid<double>(int, bool, BatchQueue &);
-template int q4_batch_grid<float>(int, bool, BatchQueue &);
+template <typename T> int q4_batch_grid(int mode, bool dot, bool uk, BatchQueue &q)
+{
+  return queue_grid(q4_batch_kernel<T>(mode, dot, uk), TX * TY2, 0, q);
+}
+template int q4_batch_grid<double>(int, bool, bool, BatchQueue &);
+template int q4_batch_grid<float>(int, bool, bool, BatchQueue &);
 int q4_block_warps() { return TY2; }
 int q4_dot_slots(const Dims &d)
 {
@@ -1646,30 +1661,41 @@ int q4_dot_slots(const Dims &d)
   ICB_REQUIRE(n < (1LL << 31), "grid too large for the Q4 operator's dot");
   return int(n);
 }
-template <typename T> long long q4_batch_capacity_warps(int mode, bool dot)
+template <typename T> long long q4_batch_capacity_warps(int mode, bool dot, bool uk)
 {
   BatchQueue q{nullptr, nullptr, 1 << 30};
-  return (long long)q4_batch_grid<T>(mode, dot, q) * TY2;
+  return (long long)q4_batch_grid<T>(mode, dot, uk, q) * TY2;
 }
-template long long q4_batch_capacity_warps<double>(int, bool);
-template long long q4_batch_capacity_warps<float>(int, bool);
+template long long q4_batch_capacity_warps<double>(int, bool, bool);
+template long long q4_batch_capacity_warps<float>(int, bool, bool);
 
 template <typename T>
 void launch_q4_batch(const Q4Launch<T> *D, const int2 *map, const BatchQueue &q, int grid,
-                     int mode, bool dot, cudaStream_t s)
+                     int mode, bool dot, const KMat<T, 8> *uniformK, cudaStream_t s)
 {
   if(q.items <= 0)
     return;
   const dim3 block(TX, TY2);
-  auto go = [&](auto kern) { kern<<<grid, block, 0, s>>>(D, map, q); };
-  if(mode == OP_APPLY)
-    dot ? go(k_matvec_q4_batch<T, true, OP_APPLY>) : go(k_matvec_q4_batch<T, false, OP_APPLY>);
-  else if(mode == OP_RESIDUAL)
-    go(k_matvec_q4_batch<T, false, OP_RESIDUAL>);
-  else if(mode == OP_CHEB)
-    go(k_matvec_q4_batch<T, false, OP_CHEB>);
+  KMat<T, 8> K{};
+  if(uniformK)
+    K = *uniformK;
+  auto go = [&](auto kern) { kern<<<grid, block, 0, s>>>(D, map, q, K); };
+  auto pick = [&](auto uk) {
+    constexpr bool U = decltype(uk)::value;
+    if(mode == OP_APPLY)
+      dot ? go(k_matvec_q4_batch<T, true, OP_APPLY, U>)
+          : go(k_matvec_q4_batch<T, false, OP_APPLY, U>);
+    else if(mode == OP_RESIDUAL)
+      go(k_matvec_q4_batch<T, false, OP_RESIDUAL, U>);
+    else if(mode == OP_CHEB)
+      go(k_matvec_q4_batch<T, false, OP_CHEB, U>);
+    else
+      throw Error{ICB_ERR_BAD_ARG, "batched Q4 operator: unsupported mode"};
+  };
+  if(uniformK)
+    pick(std::true_type{});
   else
-    throw Error{ICB_ERR_BAD_ARG, "batched Q4 operator: unsupported mode"};
+    pick(std::false_type{});
   ICB_CUDA(cudaGetLastError());
   count_launch();
 }
@@ -1690,9 +1716,10 @@ template void launch_diag2_batch<double>(const Diag2Launch<double> *, const int2
 template void launch_diag2_batch<float>(const Diag2Launch<float> *, const int2 *,
                                         const BatchQueue &, cudaStream_t);
 template void launch_q4_batch<double>(const Q4Launch<double> *, const int2 *,
-                                      const BatchQueue &, int, int, bool, cudaStream_t);
+                                      const BatchQueue &, int, int, bool,
+                                      const KMat<double, 8> *, cudaStream_t);
 template void launch_q4_batch<float>(const Q4Launch<float> *, const int2 *, const BatchQueue &,
-                                     int, int, bool, cudaStream_t);
+                                     int, int, bool, const KMat<float, 8> *, cudaStream_t);
 
 static std::atomic<bool> g_tc_operator{false};
 bool tc_operator_enabled() { return g_tc_operator; }
