@@ -6,7 +6,6 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
-#include <type_traits>
 
 #include "batchq.cuh"
 #include "graphloop.hpp"
@@ -173,53 +172,24 @@ __device__ __forceinline__ void prolong_rows_b(const Dims &df, const Dims &dc, c
   const int K0 = k >> sh.z, K1 = df.dim == 3 ? (k + sh.z) >> sh.z : K0;
   const long long csxy = (long long)dc.sx * dc.sy;
   const T h = T(0.5);
-  // the x-midpoints h (x[I0] + x[I1]) of the coarse rows the group's fine
-  // rows interpolate from, each formed once: coarse rows Jb .. Jb + R (at
-  // most R + 1 of them) in the planes K0 and K1
-  const int Jb = j0 >> sh.y;
-  const int nJ = min(R + 1, dc.sy - Jb);
-  const bool oneK = K1 == K0, oneI = I1 == I0;
-  T mid[3][R + 1][2];
 #pragma unroll
-  for(int c = 0; c < 3; c++)
+  for(int r = 0; r < R; r++)
+  {
+    const int j = j0 + r;
+    const int J0 = j >> sh.y, J1 = (j + sh.y) >> sh.y;
+    const long long r00 = (long long)J0 * dc.sx + K0 * csxy, r10 = (long long)J1 * dc.sx + K0 * csxy;
+    const long long r01 = (long long)J0 * dc.sx + K1 * csxy, r11 = (long long)J1 * dc.sx + K1 * csxy;
+    const long long n = i + (long long)j * df.sx + (long long)k * fsxy;
 #pragma unroll
-    for(int q = 0; q <= R; q++)
-#pragma unroll
-      for(int kk = 0; kk < 2; kk++)
+    for(int c = 0; c < 3; c++)
+      if(c < df.dim && !((fx[r] >> c) & 1u))
       {
-        mid[c][q][kk] = T(0);
-        if(c < df.dim && q < nJ && (kk == 0 || !oneK))
-        {
-          const T *x = xc + c * dc.ld + (long long)(Jb + q) * dc.sx + (kk ? K1 : K0) * csxy;
-          const T x0 = x[I0];
-          mid[c][q][kk] = h * (x0 + (oneI ? x0 : x[I1]));
-        }
+        const T *x = xc + c * dc.ld;
+        const T a = h * (x[r00 + I0] + x[r00 + I1]), b = h * (x[r10 + I0] + x[r10 + I1]);
+        const T a2 = h * (x[r01 + I0] + x[r01 + I1]), b2 = h * (x[r11 + I0] + x[r11 + I1]);
+        xf[c * df.ld + n] = old[r][c] + h * (h * (a + b) + h * (a2 + b2));
       }
-  // fine row j0 + r takes coarse rows J0 = (j0 + r) >> sy and J1 = (j0 + r + sy) >> sy;
-  // j0 is a multiple of R, so their places in mid are r >> sy and (r + sy) >> sy:
-  // compile-time indices in each of the two branches
-  auto rows = [&](auto syc) {
-    constexpr int sy = decltype(syc)::value;
-#pragma unroll
-    for(int r = 0; r < R; r++)
-    {
-      const int j = j0 + r;
-      const long long n = i + (long long)j * df.sx + (long long)k * fsxy;
-      const int q0 = r >> sy, q1 = (r + sy) >> sy;
-#pragma unroll
-      for(int c = 0; c < 3; c++)
-        if(c < df.dim && !((fx[r] >> c) & 1u))
-        {
-          const T a = mid[c][q0][0], b = mid[c][q1][0];
-          const T a2 = oneK ? a : mid[c][q0][1], b2 = oneK ? b : mid[c][q1][1];
-          xf[c * df.ld + n] = old[r][c] + h * (h * (a + b) + h * (a2 + b2));
-        }
-    }
-  };
-  if(sh.y)
-    rows(std::integral_constant<int, 1>{});
-  else
-    rows(std::integral_constant<int, 0>{});
+  }
 }
 /// rows of a prolongation launch block: kProlongRows node rows each
 inline unsigned prolong_row_blocks(const Dims &d)
