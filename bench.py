@@ -1025,15 +1025,18 @@ def workload_solve(args):
     g = cases.build_gpu(ctx, "halfmbb3d", *n)
     g.set_density(smooth_field(*n, seed=SEED))
     icb.set_option("hex8_pair", args.pair)
-    g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000, inner_tol=args.inner_tol)
+    mg = {"mg_smooth": args.smooth, "mg_coarse_dofs": args.coarse_dofs}
+    g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000, inner_tol=args.inner_tol, **mg)
     times, inf = [], None
     for _ in range(args.repeat):
         t0 = time.perf_counter()
-        inf = g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000, inner_tol=args.inner_tol)
+        inf = g.solve(precision=prec, precond=pc, tol=TOL, maxit=200000, inner_tol=args.inner_tol,
+                      **mg)
         times.append(time.perf_counter() - t0)
     print(json.dumps({"metric": "solve time", "value": 1e3 * min(times), "unit": "ms",
                       "all_ms": [1e3 * t for t in times], "solver": args.solver,
                       "tc_operator": args.tc, "hex8_pair": args.pair, "inner_tol": args.inner_tol,
+                      "mg_smooth": args.smooth, "mg_coarse_dofs": args.coarse_dofs,
                       "tc_timeouts": icb.get_option("tc_timeouts"),
                       "config": {"workload": f"halfmbb3d {n[0]}x{n[1]}x{n[2]}", "dof": g.neq},
                       "iters": inf["iters"], "outer": inf["outer"], "matvecs": inf["matvecs"],
@@ -1095,6 +1098,10 @@ def main():
     ap.add_argument("--inner-tol", type=float, default=0.0,
                     help="solve workload, mixed_refine: inner relative tolerance (0: default)")
     ap.add_argument("--repeat", type=int, default=3, help="solve workload: timed solves")
+    ap.add_argument("--smooth", type=int, default=0,
+                    help="solve workload: Chebyshev steps before and after (0: the default, 2)")
+    ap.add_argument("--coarse-dofs", type=int, default=0,
+                    help="solve workload: coarsest-level DOF bound (0: the default, 160)")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--loop-steps", type=int, default=100, help="batched: OC steps per instance")
     ap.add_argument("--batch-modes", nargs="+", default=["none"],
