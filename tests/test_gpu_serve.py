@@ -71,6 +71,37 @@ def test_fused_batch_equals_each_problem_alone(precision):
         c.close()
 
 
+@pytest.mark.parametrize("handoff", [0, 5, 1000])
+def test_fused_batch_handoff_keeps_results(handoff):
+    """The fused batch hands the designs still iterating to their own solve
+    loops once few are left (option batch_handoff): never (0 here means the
+    default rule, which hands off the last one of these seven), with five
+    left, or at once (1000): each design's history and design stay bitwise
+    those of its own icb_run_oc."""
+    rng = np.random.default_rng(12)
+    insts = [cases.random_instance2d(rng, nelx_range=(12, 120)) for _ in range(7)]
+    ctxs = [icb.Context(0) for _ in insts]
+    probs = [cases.build_instance(c, i) for c, i in zip(ctxs, insts)]
+    steps = [4, 3, 4, 4, 2, 4, 4]
+    opts = [icb.loop_opts(k, i["r"], move=0.2, precision=icb.MIXED) for k, i in zip(steps, insts)]
+    rho0 = [np.full(p.nel, i["vf"]) for p, i in zip(probs, insts)]
+    icb.set_option("batch_handoff", handoff)
+    try:
+        assert icb.get_option("batch_handoff") == handoff
+        hf, xf, sf = icb.run_batch(probs, [0] * len(probs), opts, rho0, nworkers=1)
+    finally:
+        icb.set_option("batch_handoff", 0)
+    assert (sf == 0).all()
+    for k, (p, i) in enumerate(zip(probs, insts)):
+        ha, xa = icb.run_loop(p, "oc", rho0[k], steps[k], i["r"], move=0.2, precision=icb.MIXED)
+        assert np.array_equal(ha, hf[k]), k
+        assert np.array_equal(xa, xf[k]), k
+    for p in probs:
+        p.close()
+    for c in ctxs:
+        c.close()
+
+
 def _job(inst, kind, nsteps):
     loop = icb.loop_opts(nsteps, inst["r"] if kind == icb.JOB_OC else 2.0 * inst["r"] / 1.5,
                          move=0.2)
