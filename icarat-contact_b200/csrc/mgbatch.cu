@@ -804,7 +804,7 @@ template <typename TP> struct BatchMg
       launched += batch;
       if(*hActive == 0 || launched > (long long)maxit + batch)
         break;
-      if(*hActive <= handOff() && n > handOff())
+      if(*hActive <= handOff())
       {
         const int left = *hActive;
         const auto t1 = std::chrono::steady_clock::now();
