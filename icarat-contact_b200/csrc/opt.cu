@@ -356,6 +356,30 @@ __device__ __forceinline__ void oc_step_tile_b(const Dims &d, int hx, int hy, un
                 ? __ldg(xc + i + (long long)j * d.nx)
                 : 0.0;
   }
+  // the stencil table (at most (2 kOcHalo + 1)^2 entries, two per thread) and
+  // this thread's four elements' weight sums and volumes, in the same round
+  constexpr int kTab = ((2 * kOcHalo + 1) * (2 * kOcHalo + 1) + VB - 1) / VB;
+  int4 tn[kTab];
+  double twv[kTab];
+#pragma unroll
+  for(int k = 0; k < kTab; k++)
+  {
+    const int t = threadIdx.x + k * VB;
+    tn[k] = t < nnb ? __ldg(nb + t) : make_int4(0, 0, 0, 0);
+    twv[k] = t < nnb ? __ldg(w + t) : 0.0;
+  }
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  constexpr int kRows = kOcTH / 8;
+  double aav[kRows], volv[kRows];
+#pragma unroll
+  for(int k = 0; k < kRows; k++)
+  {
+    const int i = x0 + tx, j = y0 + ty + 8 * k;
+    const bool in = i < d.nx && j < d.ny;
+    const long long e = i + (long long)j * d.nx;
+    aav[k] = in ? aa[e] : 1.0;
+    volv[k] = in ? vol[e] : 0.0;
+  }
 #pragma unroll
   for(int k = 0; k < kPer; k++)
   {
@@ -363,15 +387,17 @@ __device__ __forceinline__ void oc_step_tile_b(const Dims &d, int hx, int hy, un
     if(q < TWP * THP)
       tile[q] = tv[k];
   }
-  for(int t = threadIdx.x; t < nnb; t += blockDim.x)
+#pragma unroll
+  for(int k = 0; k < kTab; k++)
   {
-    const int4 o = __ldg(nb + t);
-    so[t] = o.y * TWP + o.x;
-    sw[t] = __ldg(w + t);
+    const int t = threadIdx.x + k * VB;
+    if(t < nnb)
+    {
+      so[t] = tn[k].y * TWP + tn[k].x;
+      sw[t] = twv[k];
+    }
   }
   __syncthreads();
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  constexpr int kRows = kOcTH / 8;
   const double *c0 = tile + (ty + hy) * TWP + tx + hx;
   const int rs = 8 * TWP;
   double acc[kRows];
@@ -393,10 +419,9 @@ __device__ __forceinline__ void oc_step_tile_b(const Dims &d, int hx, int hy, un
     const int i = x0 + tx, j = y0 + ty + 8 * k;
     if(i < d.nx && j < d.ny)
     {
-      const long long e = i + (long long)j * d.nx;
-      const double xf = acc[k] / aa[e];
+      const double xf = acc[k] / aav[k];
       const double xh = P.beta > 0.0 ? thresh_tb(xf, P.beta, P.T, tb) : xf;
-      v[0] += xh * vol[e];
+      v[0] += xh * volv[k];
     }
   }
   block_reduce_at<1>(v, red, FinOc{st, L}, int(B.x), int(B.gx));
