@@ -924,6 +924,8 @@ struct OcRun
   ConeFilter *cone = nullptr;
   OcUpdater *oc = nullptr;
   DevBuf<double> *x, *xf, *xh, *dxh, *dc, *dv, *dcf, *dvf, *lo, *hi, *V;
+  cudaGraphExec_t g3 = nullptr; ///< the step's work after the solve (built in the loop)
+  long long g3nodes = 0;
   double V0 = 0.0;
   bool active = true;
   int status = ICB_OK;
@@ -1070,31 +1072,48 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
         icb_problem p = r->p;
         cudaStream_t s = p->stream();
         const long long ne = p->d.nel;
-        ICB_CUDA(cudaMemcpyAsync(p->u.p, p->x.p, sizeof(double) * p->nsoa,
-                                 cudaMemcpyDeviceToDevice, s));
         p->solved = true;
         p->last = icb_solve_info{k.iter, k.matvecs, 1, k.bb > 0 ? std::sqrt(k.rr / k.bb) : 0.0,
                                  -1.0, 0.0, k.status};
-        launch_dot(p->nsoa, p->x.p, p->f.p, p->red, p->scal.p + 2, s);
-        ICB_CUDA(cudaMemcpyAsync(&hc[r->idx], p->scal.p + 2, sizeof(double),
-                                 cudaMemcpyDeviceToHost, s));
+        // the step's per-design work after the solve, the same every step: a
+        // graph captured at the first step and relaunched (one host call per
+        // design instead of ten)
+        if(!r->g3)
+        {
+          const long long before = thread_launch_count();
+          ICB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+          ICB_CUDA(cudaMemcpyAsync(p->u.p, p->x.p, sizeof(double) * p->nsoa,
+                                   cudaMemcpyDeviceToDevice, s));
+          launch_dot(p->nsoa, p->x.p, p->f.p, p->red, p->scal.p + 2, s);
+          ICB_CUDA(cudaMemcpyAsync(&hc[r->idx], p->scal.p + 2, sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+          const icb_grid_desc &g = p->hs->desc;
+          launch_sensitivity(p->d, p->K0, g.young1, g.young2, g.penalty, p->rho.p, p->u.p,
+                             p->dc.p, s);
+          ICB_CUDA(cudaMemcpyAsync(r->dc->p, p->dc.p, sizeof(double) * ne,
+                                   cudaMemcpyDeviceToDevice, s));
+          launch_scale_mul(ne, r->dc->p, r->dxh->p, 1.0, s);
+          ICB_CUDA(cudaMemcpyAsync(r->dv->p, r->V->p, sizeof(double) * ne,
+                                   cudaMemcpyDeviceToDevice, s));
+          launch_scale_mul(ne, r->dv->p, r->dxh->p, 1.0, s);
+          r->cone->adjoint(r->dc->p, r->dcf->p, s);
+          r->cone->adjoint(r->dv->p, r->dvf->p, s);
+          cudaGraph_t gr = nullptr;
+          ICB_CUDA(cudaStreamEndCapture(s, &gr));
+          r->g3nodes = thread_launch_count() - before;
+          count_launch(-r->g3nodes); // recorded, not launched
+          const cudaError_t e = cudaGraphInstantiate(&r->g3, gr, 0);
+          cudaGraphDestroy(gr);
+          ICB_CUDA(e);
+        }
+        ICB_CUDA(cudaGraphLaunch(r->g3, s));
+        count_launch(r->g3nodes);
         if(step == 1)
         {
           launch_sum(p, r->xh->p, ne, p->scal.p + 8);
           ICB_CUDA(cudaMemcpyAsync(&hv[r->idx], p->scal.p + 8, sizeof(double),
                                    cudaMemcpyDeviceToHost, s));
         }
-        const icb_grid_desc &g = p->hs->desc;
-        launch_sensitivity(p->d, p->K0, g.young1, g.young2, g.penalty, p->rho.p, p->u.p,
-                           p->dc.p, s);
-        ICB_CUDA(cudaMemcpyAsync(r->dc->p, p->dc.p, sizeof(double) * ne, cudaMemcpyDeviceToDevice,
-                                 s));
-        launch_scale_mul(ne, r->dc->p, r->dxh->p, 1.0, s);
-        ICB_CUDA(cudaMemcpyAsync(r->dv->p, r->V->p, sizeof(double) * ne, cudaMemcpyDeviceToDevice,
-                                 s));
-        launch_scale_mul(ne, r->dv->p, r->dxh->p, 1.0, s);
-        r->cone->adjoint(r->dc->p, r->dcf->p, s);
-        r->cone->adjoint(r->dv->p, r->dvf->p, s);
       }
       if(step == 1)
         for(OcRun *r : set)
@@ -1173,6 +1192,14 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
   }
   catch(...)
   {
+    // the step graphs copy into hc: released before it
+    for(OcRun &r : R)
+      if(r.g3)
+      {
+        cudaStreamSynchronize(r.p->stream());
+        cudaGraphExecDestroy(r.g3);
+        r.g3 = nullptr;
+      }
     for(auto &e : ev)
       cudaEventDestroy(e);
     cudaFreeHost(hc);
@@ -1180,6 +1207,13 @@ void run_oc_fused_tp(std::vector<OcRun> &R, cudaStream_t sb)
     cudaFreeHost(hs);
     throw;
   }
+  for(OcRun &r : R)
+    if(r.g3)
+    {
+      ICB_CUDA(cudaStreamSynchronize(r.p->stream()));
+      cudaGraphExecDestroy(r.g3);
+      r.g3 = nullptr;
+    }
   for(auto &e : ev)
     cudaEventDestroy(e);
   cudaFreeHost(hc);
