@@ -1578,15 +1578,18 @@ static void launch_op_mode(const Dims &d, const T *K, const T *E, const T *u, T 
     }
     if(g_hex8_modal && modal_form_cached(K, kmod))
     {
-      // 2 (FP64) / 3 (FP32) CTAs of 256 threads per SM.  The carry (and for
-      // FP64 the bottom plane's modes) live in shared memory: FP64 with both
-      // in registers spills, and the dot-fused FP64 Jacobi-PCG on
-      // halfmbb3d 192x64x64 took 208 ms against 172 ms for 2374 iterations
-      constexpr int MB = sizeof(T) == 8 ? 2 : 3;
+      // 3 (FP32) CTAs of 256 threads per SM; FP64 2 with the fused dot and 1
+      // without (no register cap short of the kernel's own: the FP64 V-cycle
+      // took 58.3 against 59.4 ms at 384x128x128, the dot-fused form was
+      // unchanged).  The carry (and for FP64 the bottom plane's modes) live
+      // in shared memory: FP64 with both in registers spills, and the
+      // dot-fused FP64 Jacobi-PCG on halfmbb3d 192x64x64 took 208 ms against
+      // 172 ms for 2374 iterations
+      constexpr int MB = sizeof(T) == 8 ? 2 : 3, MBnodot = sizeof(T) == 8 ? 1 : 3;
       if(x.dotRed)
         run(k_matvec_h8m<T, TYK, true, MODE, MB>, kmod, h8m_smem_bytes<T, TYK>());
       else
-        run(k_matvec_h8m<T, TYK, false, MODE, MB>, kmod, h8m_smem_bytes<T, TYK>());
+        run(k_matvec_h8m<T, TYK, false, MODE, MBnodot>, kmod, h8m_smem_bytes<T, TYK>());
     }
     else if constexpr(std::is_same<T, double>::value)
     {
