@@ -388,8 +388,8 @@ class _Level:
 
 
 class SlabMg:
-    """The library's V-cycle (MgPcg::level in mg_impl.cuh, FP64 levels) on an
-    x-slab partition.  Levels 0 .. g-1 are split over the ranks: level l
+    """The library's V-cycle (MgPcg::level in mg_impl.cuh) on an x-slab
+    partition.  Levels 0 .. g-1 are split over the ranks: level l
     keeps the fine slabs' boundaries divided by 2^(x halvings so far), which
     slab_ranges(..., align=2^m) keeps integral, so every rank coarsens its
     own moduli and restricts and prolongates its own node planes; a
@@ -406,13 +406,23 @@ class SlabMg:
     kmat(h): the unit element matrix (24, 24) of an element with edges h
     (the library's K0 of a one-element problem); h: the fine element's
     edges.  gather_level: g (default: the coarsest level the slab
-    boundaries allow, at most the coarsest level)."""
+    boundaries allow, at most the coarsest level).
+
+    dtype: the V-cycle's precision.  float32 is the library's mixed form
+    (MgPcg<double, float>): the levels' vectors, moduli, diagonals and
+    element sums in FP32, the coarsest system assembled and solved in FP64,
+    the flexible CG (operator `op`, residual, reductions) in FP64.  vop: the
+    V-cycle's fine-level operator in dtype (on a GPU rank the library's FP32
+    operator on the slab problem); by default `op` for float64 and a torch
+    element sum otherwise."""
 
     def __init__(self, ex, op, diag, free, E, kmat, h=(1.0, 1.0, 1.0), smooth=2,
-                 coarse_dofs=COARSE_DOFS, gather_level=None):
+                 coarse_dofs=COARSE_DOFS, gather_level=None, dtype=torch.float64, vop=None):
         L0 = ex.L
         W, rank = L0.world, L0.rank
-        dev, dt = E.device, E.dtype
+        dev, dt = E.device, dtype
+        self.op, self.dtype = op, dtype
+        E = E.to(torch.float64)
         self.rank, self.ex, self.nu = rank, ex, int(smooth) if smooth > 0 else 2
         self.dims = dims = mg_levels(L0.nx, L0.ny, L0.nz, coarse_dofs)
         nl = self.nl = len(dims)
@@ -431,20 +441,24 @@ class SlabMg:
             raise ValueError("gather level %d not in %s for these slab boundaries" % (g, allowed))
         self.g = g
         # element edges, matrices and the Chebyshev bound of every level
-        hs, Ks = [tuple(h)], [None]
-        lmax, changed = element_lmax(kmat(tuple(h))), False
+        hs = [tuple(h)]
+        K64 = [torch.as_tensor(kmat(hs[0]), dtype=torch.float64)]
+        lmax, changed = element_lmax(K64[0].numpy()), False
         for l in range(1, nl):
             sh = dims[l][3]
             hs.append(tuple(2.0 * hs[-1][k] if sh[k] else hs[-1][k] for k in range(3)))
-            Ks.append(torch.as_tensor(kmat(hs[-1]), dtype=dt, device=dev))
+            K64.append(torch.as_tensor(kmat(hs[-1]), dtype=torch.float64))
             changed = changed or sh[0] != sh[1] or sh[1] != sh[2]
             if changed:
-                lmax = max(lmax, element_lmax(Ks[-1].cpu().numpy()))
+                lmax = max(lmax, element_lmax(K64[-1].numpy()))
+        Ks = [k.to(device=dev, dtype=dt) for k in K64]
         self.lmax = lmax
         self.c1, self.c2 = chebyshev_coefficients(lmax, self.nu)
 
-        d0 = ex.add_shared_planes(diag.clone())
-        self.lv = [_Level(L0, ex, (1, 1, 1), None, E, free, op, _inv_diag(d0, free))]
+        d0 = ex.add_shared_planes(diag.to(torch.float64).clone()).to(dt)
+        if vop is None:
+            vop = op if dt == torch.float64 else element_sum(L0, Ks[0], E.to(dt), ~free)[0]
+        self.lv = [_Level(L0, ex, (1, 1, 1), Ks[0], E, free, vop, _inv_diag(d0, free))]
 
         def fixed_float(lv):
             m = torch.zeros(3 * lv.L.ld, dtype=dt, device=dev)
@@ -454,7 +468,7 @@ class SlabMg:
         def make(L, lex, l, E_l, mask):
             free = torch.zeros(3 * L.ld, dtype=torch.bool, device=dev)
             L.grid(free).copy_(L.grid(mask) == 0)
-            o, dg = element_sum(L, Ks[l], E_l, ~free)
+            o, dg = element_sum(L, Ks[l], E_l.to(dt), ~free)
             return _Level(L, lex, dims[l][3], Ks[l], E_l, free, o,
                           _inv_diag(lex.add_shared_planes(dg()), free))
 
@@ -491,24 +505,26 @@ class SlabMg:
                                     restrict_slab(f.L, L, sh, fixed_float(f))))
             self._factor(self.lv[-1])
 
-    # coarsest level: dense Cholesky of the free DOFs (rank 0)
+    # coarsest level: dense Cholesky of the free DOFs in FP64 (rank 0)
     def _factor(self, C):
         idx = torch.nonzero(C.free).reshape(-1)
         self.cidx, self.chol = idx, None
         n = idx.numel()
         if n == 0:
             return
+        op64, _ = element_sum(C.L, C.K.to(torch.float64), C.E, C.fixed)
         A = C.E.new_zeros((n, n))
         for j in range(n):
             e = C.E.new_zeros(3 * C.L.ld)
             e[idx[j]] = 1.0
-            A[:, j] = C.op(e)[idx]
+            A[:, j] = op64(e)[idx]
         self.chol = torch.linalg.cholesky(0.5 * (A + A.T))
 
     def _coarse(self, b):
         x = torch.zeros_like(b)
         if self.chol is not None:
-            x[self.cidx] = torch.cholesky_solve(b[self.cidx].unsqueeze(1), self.chol).squeeze(1)
+            bd = b[self.cidx].to(torch.float64).unsqueeze(1)
+            x[self.cidx] = torch.cholesky_solve(bd, self.chol).squeeze(1).to(b.dtype)
         return x
 
     def _to_full(self, part):
@@ -553,13 +569,15 @@ class SlabMg:
         return cur
 
     def vcycle(self, r):
-        """z = V-cycle(r) on the fine slabs (every rank calls it together)"""
-        return self._level(0, r)
+        """z = V-cycle(r) on the fine slabs in the V-cycle's precision, returned
+        in r's (every rank calls it together)"""
+        return self._level(0, r.to(self.dtype)).to(r.dtype)
 
 
 def slab_gmg_pcg(mg, b, tol, maxit):
-    """The library's multigrid-preconditioned flexible CG (MgPcg::solve,
-    FP64) on the partitioned system: x0 = 0, stop when
+    """The library's multigrid-preconditioned flexible CG (MgPcg::solve: FP64
+    iterate, operator and reductions, the V-cycle in mg.dtype) on the
+    partitioned system: x0 = 0, stop when
     ||r||^2 < max(tol^2 ||b||^2, DBL_MIN), Polak-Ribiere beta
     (r.z_new - r.z_old) / r.z_old, the converging iteration not counted.
     Per iteration one operator application with its plane exchange, one
@@ -589,7 +607,7 @@ def slab_gmg_pcg(mg, b, tol, maxit):
     p = z.clone()
     it, mv, rr, status = 0, 0, bb, -4
     while it < maxit:
-        q = lv.apply(p)
+        q = ex.add_shared_planes(mg.op(p))
         mv += 1
         (pq,) = ex.allreduce([owned_dot(L, p, q)])
         alpha = rz / pq if pq > 0.0 else math.nan
@@ -653,15 +671,23 @@ def gpu_slab(ctx, L, fixed4, load4, rho_slab, young=(1e-9, 1.0), nu=0.3, penal=3
             free.to(dev))
 
 
-def device_operator(prob, stream=None):
-    """op(u) for a GPU rank: the library's FP64 matrix-free operator on the
-    slab's icb_problem (density already set), on SoA tensors of the device"""
-    from . import FP64
+def device_operator(prob, stream=None, precision=None):
+    """op(u) for a GPU rank: the library's matrix-free operator on the slab's
+    icb_problem (density already set), on SoA tensors of the device: FP64
+    (float64 tensors) by default, the FP32 CUDA-core operator (float32
+    tensors) with precision=MIXED"""
+    from . import FP64, MIXED
+    precision = FP64 if precision is None else precision
+    dt = torch.float64 if precision == FP64 else torch.float32
+    if precision not in (FP64, MIXED):
+        raise ValueError("precision must be FP64 or MIXED")
 
     def op(u):
+        if u.dtype != dt or not u.is_contiguous():
+            raise ValueError("operator input must be a contiguous %s tensor" % dt)
         y = torch.empty_like(u)
         torch.cuda.current_stream().synchronize()
-        prob.operator_apply_device(u.data_ptr(), y.data_ptr(), FP64)
+        prob.operator_apply_device(u.data_ptr(), y.data_ptr(), precision)
         prob.ctx.synchronize()
         return y
 

@@ -156,10 +156,10 @@ def test_slab_partition_reproduces_one_rank_solve():
 MG_GRID = (23, 6, 5)
 
 
-def _mg_solve(rank, world, dist, align, gather, grid=MG_GRID):
-    """the multigrid-preconditioned slab solve of `grid` on this rank; the
-    coarse levels' element matrices from the oracle's K0 of a one-element
-    problem with the level's edges"""
+def _mg_solve(rank, world, dist, align, gather, grid=MG_GRID, mixed=False):
+    """the multigrid-preconditioned slab solve of `grid` on this rank (FP64, or
+    the FP32 V-cycle under FP64 CG); the coarse levels' element matrices from
+    the oracle's K0 of a one-element problem with the level's edges"""
     import torch
     sys.path.insert(0, os.path.join(REPO, "icarat-contact_b200", "python"))
     sys.path.insert(0, os.path.join(REPO, "oracle"))
@@ -185,28 +185,30 @@ def _mg_solve(rank, world, dist, align, gather, grid=MG_GRID):
     b = torch.where(free, L.to_slab(to4(f)), torch.zeros(3 * L.ld, dtype=torch.float64))
     op, diag = slab.element_sum(L, torch.from_numpy(kmat((1.0, 1.0, 1.0))), E, ~free)
     ex = slab.Exchange(L, dist)
-    mg = slab.SlabMg(ex, op, diag(), free, E, kmat, gather_level=gather)
+    mg = slab.SlabMg(ex, op, diag(), free, E, kmat, gather_level=gather,
+                     dtype=torch.float32 if mixed else torch.float64)
     x, info = slab.slab_gmg_pcg(mg, b, 1e-8, 1000)
     counts = dict(ex.counts)
     (c,) = ex.allreduce([slab.owned_dot(L, x, b)])
     return info, c, counts
 
 
-def _mg_rank_main(rank, world, port, q, align, gather, grid):
+def _mg_rank_main(rank, world, port, q, align, gather, grid, mixed):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    out = _mg_solve(rank, world, dist, align, gather, grid)
+    out = _mg_solve(rank, world, dist, align, gather, grid, mixed)
     dist.destroy_process_group()
     q.put((rank,) + out)
 
 
-def _mg_run(world, align, gather, grid=MG_GRID):
+def _mg_run(world, align, gather, grid=MG_GRID, mixed=False):
     port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_mg_rank_main, args=(r, world, port, q, align, gather, grid))
+    procs = [ctx.Process(target=_mg_rank_main,
+                         args=(r, world, port, q, align, gather, grid, mixed))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -273,3 +275,22 @@ def test_slab_multigrid_thin_grid_and_bad_partitions():
         _mg_solve(0, 1, None, 1, 0)
     with pytest.raises(ValueError, match="gather level"):
         _mg_solve(0, 2, None, 4, 3)  # 12 keeps two coarsenings, not three
+
+
+@pytest.mark.timeout(300)
+def test_slab_multigrid_fp32_vcycle_partitions_like_one_rank():
+    """the library's mixed form (FP32 levels, FP64 coarsest solve and CG) on
+    the slabs: the iteration count of the FP64 V-cycle, and worlds 2 and 3
+    reproduce the one-rank compliance (the FP32 V-cycles of the partitions
+    round differently, so to 1e-10 rather than 1e-12)"""
+    info64, c64, _ = _mg_solve(0, 1, None, 1, None)
+    info1, c1, _ = _mg_solve(0, 1, None, 1, None, mixed=True)
+    assert info1["status"] == 0 and info1["relres"] <= 1e-8
+    assert abs(info1["iters"] - info64["iters"]) <= 1 and abs(c1 - c64) <= 1e-10 * abs(c64)
+    for world, align, gather in ((2, 4, None), (3, 2, 1)):
+        res = _mg_run(world, align, gather, mixed=True)
+        for rank, info, c, counts in res:
+            assert info["status"] == 0 and abs(info["iters"] - info1["iters"]) <= 1
+            assert abs(c - c1) <= 1e-10 * abs(c1), (world, rank, c, c1)
+            assert counts["allreduce"] == 2 + 2 * info["matvecs"]
+        assert len({r[2] for r in res}) == 1
