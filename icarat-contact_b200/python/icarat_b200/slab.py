@@ -405,8 +405,9 @@ class SlabMg:
     diagonal, the unknowns' mask); E: the slab's moduli (nz, ny, nxl);
     kmat(h): the unit element matrix (24, 24) of an element with edges h
     (the library's K0 of a one-element problem); h: the fine element's
-    edges.  gather_level: g (default: the coarsest level the slab
-    boundaries allow, at most the coarsest level).
+    edges.  gather_level: g; by default the first level of at most
+    gather_dofs DOFs (constrained ones counted), or the coarsest level the
+    slab boundaries allow if that comes first or gather_dofs is None.
 
     dtype: the V-cycle's precision.  float32 is the library's mixed form
     (MgPcg<double, float>): the levels' vectors, moduli, diagonals and
@@ -417,7 +418,8 @@ class SlabMg:
     element sum otherwise."""
 
     def __init__(self, ex, op, diag, free, E, kmat, h=(1.0, 1.0, 1.0), smooth=2,
-                 coarse_dofs=COARSE_DOFS, gather_level=None, dtype=torch.float64, vop=None):
+                 coarse_dofs=COARSE_DOFS, gather_level=None, gather_dofs=None,
+                 dtype=torch.float64, vop=None):
         L0 = ex.L
         W, rank = L0.world, L0.rank
         dev, dt = E.device, dtype
@@ -436,7 +438,12 @@ class SlabMg:
         if not allowed:
             raise ValueError("slab boundaries must be even for a multigrid partition "
                              "(slab_ranges(..., align=2**m))")
-        g = max(allowed) if gather_level is None else int(gather_level)
+        if gather_level is not None:
+            g = int(gather_level)
+        else:
+            small = [l for l in allowed if gather_dofs is not None and
+                     3 * (dims[l][0] + 1) * (dims[l][1] + 1) * (dims[l][2] + 1) <= gather_dofs]
+            g = min(small) if small else max(allowed)
         if g not in allowed:
             raise ValueError("gather level %d not in %s for these slab boundaries" % (g, allowed))
         self.g = g

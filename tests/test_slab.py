@@ -269,6 +269,21 @@ def test_slab_multigrid_thin_grid_and_bad_partitions():
     assert abs(c1 - ro["compliance"]) <= 1e-10 * abs(ro["compliance"])
     for rank, info, c, counts in _mg_run(2, 4, None, grid):
         assert abs(info["iters"] - info1["iters"]) <= 1 and abs(c - c1) <= 1e-10 * abs(c1)
+    # the gather level by size: the first level of at most gather_dofs DOFs
+    # (23 x 6 x 5 -> 12 x 3 x 3: 624 DOFs -> 6 x 2 x 2: 189 -> 3 x 1 x 1: 48),
+    # else the deepest the boundaries allow (one rank: the coarsest)
+    import torch
+    from icarat_b200 import slab
+    L = slab.SlabLayout(23, 6, 5, 0, 1)
+    E = torch.ones(5, 6, L.nxl, dtype=torch.float64)
+    free = torch.zeros(3 * L.ld, dtype=torch.bool)
+    L.grid(free).fill_(True)
+    K = torch.eye(24, dtype=torch.float64)
+    op, diag = slab.element_sum(L, K, E, ~free)
+    for gd, g in ((100000, 1), (624, 1), (623, 2), (189, 2), (188, 3), (10, 3), (None, 3)):
+        mg = slab.SlabMg(slab.Exchange(L, None), op, diag(), free, E, lambda h: K.numpy(),
+                         gather_dofs=gd)
+        assert mg.g == g, (gd, mg.g)
     with pytest.raises(ValueError, match="even"):
         _mg_solve(1, 3, None, 1, None)  # boundaries 7 and 15
     with pytest.raises(ValueError, match="gather level"):
